@@ -1,0 +1,433 @@
+// oracle_capi.cpp -- TEST INFRASTRUCTURE ONLY (the oracle's C entry points for ctypes).
+//
+// Render drivers for the oracle: interior term (path_integrator.cc:355-372), primary
+// boundary (:188-272) and direct boundary (:274-353), in float, double or Dual<K>.
+// PARITY UNPINNED (see psdr_oracle.hpp). Built by oracle/build.py into
+// oracle/_build/liborc.so; loaded only by tests, smoke() and the bench CPU baseline.
+#include <omp.h>
+
+#include <cstdio>
+
+#include "psdr_oracle.hpp"
+
+namespace orc {
+
+template <class S, bool AD> struct Ctx {
+  using R = typename Traits<S>::R;
+  const Scene<S>& sc;    // scene in S (Dual when differentiating)
+  const Scene<R>& scv;   // value scene for the non-AD evaluations
+  Camera<R> cam;
+  V3<S> cam_pos;
+  OrcConfig cfg;
+};
+
+// camera.h:235-258 PerspectiveCamera::gen_camera_ray_ for sample i.
+template <class S, bool AD>
+inline V3<S> interior_sample(const Ctx<S, AD>& c, uint64_t i, int& pix, bool& valid) {
+  using R = typename Traits<S>::R;
+  const int W = c.cam.W;
+  const int spp = c.cfg.spp_interior;
+  Pcg32 rng = make_sampler(i);
+  R jx = rng.next_float(), jy = rng.next_float();
+  pix = spp > 1 ? int(i / (uint64_t)spp) : int(i);
+  int x = pix % W, y = pix / W;
+  V3<R> fp(jx + R(x), jy + R(y), R(1));
+  V3<R> pc = Camera<R>::xpos(c.cam.r2c, fp);
+  V3<R> d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
+  V3<S> ds(S(d.x), S(d.y), S(d.z));
+  Its<S> its = scene_hit<S, AD>(c.sc, c.cam_pos, ds, true);
+  valid = its.valid;
+  V3<S> L = trace2light<S, AD>(c.sc, rng, its, its.valid, c.cfg.mis_light_samples, c.cfg.mis_bsdf_samples,
+                               c.cfg.max_bounce, c.cfg.enable_light_visable != 0);
+  return L * its.jac;
+}
+
+template <class S, class R>
+inline void project(const Camera<R>& cam, const V3<S>& pt, bool& valid, int& rx, int& ry) {
+  V3<S> pc = Camera<R>::xpos(cam.w2c, pt);
+  V3<S> p = Camera<R>::xpos(cam.c2r, pc);
+  double px = val(p.x), py = val(p.y);
+  valid = valid && val(pc.z) < 0 && px > 0 && px < cam.W && py > 0 && py < cam.H;
+  rx = (int)std::floor(px);
+  ry = (int)std::floor(py);
+}
+
+// path_integrator.cc:203-251 eval_primary_boundary.
+template <class S, bool AD>
+inline V3<S> eval_primary(const Ctx<S, AD>& c, Pcg32& rng, typename Traits<S>::R s1, int& rx, int& ry, bool& valid) {
+  using R = typename Traits<S>::R;
+  const Scene<S>& sc = c.sc;
+  R s = s1, pe;
+  int ei = sc.edge_cdf.sample_reuse(s, pe);
+  const Edge<S>& E = sc.edges[ei];
+  V3<S> xe = E.p0 + (E.p1 - E.p0) * S(s);
+  S pdf_e = S(pe) / E.len;
+  valid = true;
+  project(c.cam, xe, valid, rx, ry);
+  V3<S> rd = normalize(xe - c.cam_pos);
+  V3<R> n = valv(cross(rd, normalize(detach(E.p1 - E.p0))));
+  V3<R> o = valv(c.cam_pos), d = valv(rd);
+  const R eps = R(1e-5);
+  V3<R> da = d - n * eps, db = d + n * eps;
+  Its<R> ia = scene_hit<R, false>(c.scv, o, da, valid);
+  Its<R> ib = scene_hit<R, false>(c.scv, o, db, valid);
+  V3<R> xev = valv(xe);
+  valid = valid && ia.valid && ib.valid &&
+          (double(norm(ia.p - xev)) < 1e-4 || double(norm(ib.p - xev)) < 1e-4);
+  V3<R> La = trace2light<R, false>(c.scv, rng, ia, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
+  V3<R> Lb = trace2light<R, false>(c.scv, rng, ib, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
+  V3<R> dL = La - Lb;
+  V3<S> value;
+  if (AD) {
+    V3<S> ns(S(n.x), S(n.y), S(n.z));
+    V3<S> nflip(S(n.x), S(n.y), S(-n.z));
+    S xdn = dot(xe - detach(xe), ns) + dot(c.cam_pos - detach(c.cam_pos), nflip);
+    V3<S> dLs(S(dL.x), S(dL.y), S(dL.z));
+    value = dLs * (xdn / detach(pdf_e));
+  } else {
+    value = V3<S>(S(dL.x), S(dL.y), S(dL.z)) / pdf_e;
+  }
+  valid = valid && finite3(value);
+  return value;
+}
+
+// path_integrator.cc:11-24 hit_triangle
+template <class S>
+inline V3<S> hit_triangle(const V3<S>& o, const V3<S>& d, const V3<S>& p0, const V3<S>& e1, const V3<S>& e2) {
+  V3<S> T = o - p0;
+  V3<S> P = cross(d, e2), Q = cross(T, e1);
+  S inv = S(1) / clamp_(dot(P, e1), 1e-5, 1 - 1e-5);
+  S u = dot(P, T) * inv, v = dot(Q, d) * inv;
+  return p0 + e1 * u + e2 * v;
+}
+
+// path_integrator.cc:31-78 boundary_term
+template <class S, bool AD>
+inline V3<S> boundary_term(const V3<S>& xs, const V3<S>& xd, const V3<S>& xb, const V3<S>& ns, const V3<S>& nd,
+                           const Edge<S>& E) {
+  V3<S> xs_ = detach(xs), xd_ = detach(xd), xb_ = detach(xb), ns_ = detach(ns), nd_ = detach(nd);
+  V3<S> dir = normalize(xb - xs_);
+  V3<S> dir_ = detach(dir);
+  V3<S> ev = normalize(detach(E.p1) - detach(E.p0));
+  if (val(dot(cross(dir_, ev), detach(E.out))) < 0) ev = -ev;
+  V3<S> n_plane = cross(dir_, ev);
+  V3<S> eproj = cross(nd_, n_plane);
+  S cos_s = abs_(dot(ns_, dir_));
+  S cos_b = dot(ev, dir_), cos_d = dot(eproj, dir_);
+  S sin_b = safe_sqrt(S(1) - cos_b * cos_b), sin_d = safe_sqrt(S(1) - cos_d * cos_d);
+  S len_sb = norm(xb_ - xs_), len_sd = norm(xd_ - xs_);
+  S Jb = len_sd * len_sb * sin_b / (sin_d * cos_s);
+  S dG = cos_s * dot(nd_, -dir_) / (len_sd * len_sd);
+  V3<S> fb;
+  if (AD) {
+    V3<S> nep = cross(nd_, eproj);
+    V3<S> xh = hit_triangle(xs_, dir, xd_, eproj, nep);
+    xh = xh - detach(xh);
+    fb = mul(xh, nep * dG);
+  } else {
+    fb = V3<S>(dG, dG, dG);
+  }
+  return fb * Jb;
+}
+
+// path_integrator.cc:288-329 eval_direct_boundary
+template <class S, bool AD>
+inline V3<S> eval_direct(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], int& rx, int& ry, bool& valid) {
+  using R = typename Traits<S>::R;
+  const Scene<S>& sc = c.sc;
+  R s = s3[0], pe;
+  int ei = sc.edge_cdf.sample_reuse(s, pe);
+  const Edge<S>& E = sc.edges[ei];
+  V3<S> xb = E.p0 + (E.p1 - E.p0) * S(s);
+  S pdf_e = S(pe) / E.len;
+  R sy = s3[1], sz = s3[2], pch = R(1);
+  int l = sc.light_cdf.sample_reuse(sy, pch);
+  R pl;
+  V3<S> yl = light_sample_point(sc, l, sy, sz, pl);
+  R pdf_l = pl * pch;
+  V3<S> dir = normalize(xb - yl);
+  valid = val(dot(E.nl, dir)) * val(dot(E.nr, dir)) < 0 && val(norm(E.nl - E.nr)) > 1e-5;
+  rx = ry = 0;
+  Its<S> is0 = scene_hit<S, AD>(sc, xb, -dir, valid);
+  valid = valid && is0.valid && is0.is_light && val(sqnorm(is0.p - yl)) < double(R(1e-5));
+  Its<S> id0 = scene_hit<S, AD>(sc, xb, dir, valid);
+  valid = valid && id0.valid && !id0.is_light;
+  project(c.cam, id0.p, valid, rx, ry);
+  V3<S> cd = normalize(id0.p - c.cam_pos);
+  Its<S> i2 = scene_hit<S, AD>(sc, c.cam_pos, cd, valid);
+  valid = valid && i2.valid && !i2.is_light && val(sqnorm(i2.p - id0.p)) < double(R(1e-5));
+  V3<S> value;
+  if (!valid) return value;
+  S pdf_xw = is0.sqd * pdf_e * S(pdf_l) / dot(is0.n, dir);
+  V3<S> Tb = boundary_term<S, AD>(is0.p, id0.p, xb, is0.n, id0.n, E) / pdf_xw;
+  V3<S> Ts = detach(sc.emit[is0.light]);
+  V3<S> Td = detach(tex_at(sc, id0.obj, id0.u, id0.v) * inv_pi<S>());
+  value = mul(mul(Tb, Ts), Td);
+  valid = valid && finite3(value);
+  return value;
+}
+
+// sampler.h:201-247 HyperCubeSampler: cells in row-major order of the resolution.
+template <class R> struct HyperCube {
+  int N = 1;
+  int res[3] = {1, 1, 1};
+  int cells = 1;
+  R unit[3];
+  Discrete<R> d;
+  void init(int n, const int* r) {
+    N = n;
+    cells = 1;
+    for (int i = 0; i < n; ++i) { res[i] = r[i]; cells *= r[i]; unit[i] = R(1) / R(r[i]); }
+  }
+  void cell_coords(int c, int* out) const {
+    int cnt = cells, rem = c;
+    for (int i = 0; i < N; ++i) { cnt /= res[i]; out[i] = rem / cnt; rem -= out[i] * cnt; }
+  }
+  R sample_reuse(R* s) const {
+    R pdf;
+    int idx = d.sample_reuse(s[N - 1], pdf);
+    int cc[3];
+    cell_coords(idx, cc);
+    for (int i = 0; i < N; ++i) s[i] = (s[i] + R(cc[i])) * unit[i];
+    return pdf;
+  }
+};
+
+// path_integrator.cc:253-272 preprocess_primary_boundary (value mode)
+template <class R>
+inline HyperCube<R> preprocess_primary(const Ctx<R, false>& c) {
+  HyperCube<R> hc;
+  int r = c.cfg.pe_res;
+  hc.init(1, &r);
+  std::vector<double> rst(hc.cells, 0.0);
+  std::vector<Pcg32> rngs(hc.cells);
+  for (int i = 0; i < hc.cells; ++i) rngs[i] = make_sampler(i);
+  for (int round = 0; round < c.cfg.pe_rounds; ++round) {
+    std::vector<double> add(hc.cells, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < hc.cells; ++i) {
+      R s1 = (R(i) + rngs[i].next_float()) * hc.unit[0];
+      int rx, ry;
+      bool valid;
+      V3<R> v = eval_primary<R, false>(c, rngs[i], s1, rx, ry, valid);
+      if (valid) add[i] = double(R(norm(v)));
+    }
+    for (int i = 0; i < hc.cells; ++i) rst[i] = double(R(R(rst[i]) + R(add[i])));
+  }
+  hc.d.build(rst);
+  return hc;
+}
+
+// path_integrator.cc:331-353 preprocess_direct_boundary (value mode)
+template <class R>
+inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
+  HyperCube<R> hc;
+  hc.init(3, c.cfg.se_res);
+  std::vector<double> rst(hc.cells, 0.0);
+  std::vector<Pcg32> rngs(hc.cells);
+  for (int i = 0; i < hc.cells; ++i) rngs[i] = make_sampler(i);
+  for (int round = 0; round < c.cfg.se_rounds; ++round) {
+    std::vector<double> add(hc.cells, 0.0);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int i = 0; i < hc.cells; ++i) {
+      int cc[3];
+      hc.cell_coords(i, cc);
+      R s3[3];
+      for (int k = 0; k < 3; ++k) s3[k] = rngs[i].next_float();
+      for (int k = 0; k < 3; ++k) s3[k] = (R(cc[k]) + s3[k]) * hc.unit[k];
+      int rx, ry;
+      bool valid;
+      V3<R> v = eval_direct<R, false>(c, s3, rx, ry, valid);
+      for (int k = 0; k < 3; ++k) if (v[k] < R(1e-5)) v[k] = R(1e-5);
+      if (valid) add[i] = double(R(norm(v)));
+    }
+    for (int i = 0; i < hc.cells; ++i) rst[i] = double(R(R(rst[i]) + R(add[i])));
+  }
+  hc.d.build(rst);
+  return hc;
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+// Film::add (camera.h:75-87): per pixel sum of the samples, divided by spp.
+template <class S, bool AD>
+static void render_camera(const Ctx<S, AD>& c, int which, double* img, const double* dLdI, double* dphi,
+                          double* per_sample, const Ctx<typename Traits<S>::R, false>* cv) {
+  using R = typename Traits<S>::R;
+  const int H = c.cam.H, W = c.cam.W;
+  const size_t npix = (size_t)H * W;
+  constexpr int KD = std::is_same<S, R>::value ? 0 : sizeof(S) / sizeof(double) - 1;
+  // ---- interior
+  if (which & 1) {
+    const int spp = c.cfg.spp_interior;
+    const uint64_t N = (uint64_t)npix * spp;
+    std::vector<R> samp(N * 3, R(0));
+    std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)N; ++i) {
+      int pix;
+      bool valid;
+      V3<S> L = interior_sample<S, AD>(c, (uint64_t)i, pix, valid);
+      if (!valid) L = V3<S>();
+      for (int k = 0; k < 3; ++k) samp[3 * i + k] = R(val(L[k]));
+      if constexpr (KD > 0) {
+        for (int k = 0; k < 3; ++k)
+          for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += dLdI[3 * pix + k] * L[k].d[j] / spp;
+      }
+      if (per_sample) for (int k = 0; k < 3; ++k) per_sample[3 * i + k] = double(val(L[k]));
+    }
+    for (size_t p = 0; p < npix; ++p)
+      for (int k = 0; k < 3; ++k) {
+        R acc = R(0);
+        for (int s = 0; s < spp; ++s) acc += samp[3 * (p * spp + s) + k];
+        img[3 * p + k] += double(acc / R(spp));
+      }
+    if constexpr (KD > 0) for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+  }
+  // ---- primary boundary (renderD only; zero-valued, gradient only)
+  if (which & 2) {
+    HyperCube<R> hc = preprocess_primary<R>(*cv);
+    const int spp = c.cfg.spp_primary_edge;
+    const uint64_t N = (uint64_t)npix * spp;
+    std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)N; ++i) {
+      Pcg32 rng = make_sampler((uint64_t)i);
+      R s1 = rng.next_float();
+      R hp = hc.sample_reuse(&s1);
+      int rx, ry;
+      bool valid;
+      V3<S> v = eval_primary<S, AD>(c, rng, s1, rx, ry, valid);
+      if (!valid) continue;
+      if constexpr (KD > 0) {
+        size_t pix = (size_t)ry * W + rx;
+        for (int k = 0; k < 3; ++k)
+          for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += dLdI[3 * pix + k] * v[k].d[j] / double(hp) / spp;
+      }
+    }
+    if constexpr (KD > 0) for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+  }
+  // ---- direct boundary
+  if (which & 4) {
+    HyperCube<R> hc = preprocess_direct<R>(*cv);
+    const int spp = c.cfg.spp_secondary_edge;
+    const uint64_t N = (uint64_t)npix * spp;
+    std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)N; ++i) {
+      Pcg32 rng = make_sampler((uint64_t)i);
+      R s3[3];
+      for (int k = 0; k < 3; ++k) s3[k] = rng.next_float();
+      R hp = hc.sample_reuse(s3);
+      int rx, ry;
+      bool valid;
+      V3<S> v = eval_direct<S, AD>(c, s3, rx, ry, valid);
+      if (!valid) continue;
+      if constexpr (KD > 0) {
+        size_t pix = (size_t)ry * W + rx;
+        for (int k = 0; k < 3; ++k)
+          for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += dLdI[3 * pix + k] * v[k].d[j] / double(hp) / spp;
+      }
+    }
+    if constexpr (KD > 0) for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+  }
+}
+
+template <class S>
+static Scene<S> mk_scene(const OrcMesh* m, int nm, const OrcLight* l, int nl, const Seeds<S>& seeds) {
+  return build_scene<S>(m, nm, l, nl, seeds);
+}
+
+template <class S, bool AD>
+static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
+                       const OrcConfig* cfg, int which, double* images, const double* dLdI, double* dphi,
+                       double* per_sample, const Seeds<S>& seeds) {
+  using R = typename Traits<S>::R;
+  Scene<S> sc = mk_scene<S>(m, nm, l, nl, seeds);
+  Seeds<R> none;
+  Scene<R> scv_own;
+  const Scene<R>* scv;
+  if constexpr (std::is_same<S, R>::value) scv = &sc;
+  else { scv_own = mk_scene<R>(m, nm, l, nl, none); scv = &scv_own; }
+  size_t off = 0;
+  for (int ci = 0; ci < nc; ++ci) {
+    Ctx<S, AD> c{sc, *scv, {}, {}, *cfg};
+    c.cam.setup(cams[ci]);
+    Ctx<R, false> cv{*scv, *scv, {}, {}, *cfg};
+    cv.cam = c.cam;
+    for (int k = 0; k < 3; ++k) {
+      c.cam_pos[k] = Seeder<S>::make(cams[ci].look_from[k], seeds.campos, 3 * ci + k);
+      cv.cam_pos[k] = R(cams[ci].look_from[k]);
+    }
+    size_t npix = (size_t)c.cam.H * c.cam.W;
+    std::vector<double> img(3 * npix, 0.0);
+    for (int pass = 0; pass < std::max(1, cfg->n_pass); ++pass)
+      render_camera<S, AD>(c, which, img.data(), dLdI ? dLdI + off : nullptr, dphi, per_sample, &cv);
+    if (images) for (size_t i = 0; i < 3 * npix; ++i) images[off + i] = img[i] / std::max(1, cfg->n_pass);
+    off += 3 * npix;
+    if (per_sample) per_sample += 3 * npix * cfg->spp_interior;
+  }
+  return 0;
+}
+
+extern "C" {
+
+int orc_num_threads() { return omp_get_max_threads(); }
+void orc_set_threads(int n) { omp_set_num_threads(n); }
+
+// Image render (interior term). precision 0 = float, 1 = double.
+int orc_render(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
+               const OrcConfig* cfg, int precision, double* images, double* per_sample) {
+  if (precision == 0) return render_impl<float, false>(m, nm, l, nl, cams, nc, cfg, 1, images, nullptr, nullptr, per_sample, Seeds<float>{});
+  return render_impl<double, false>(m, nm, l, nl, cams, nc, cfg, 1, images, nullptr, nullptr, per_sample, Seeds<double>{});
+}
+
+// Directional derivatives dPhi/dtheta . seed_k (k < 8) of Phi = sum dLdI * image, with the
+// reference's renderD semantics. which: bit0 interior, bit1 primary edges, bit2 direct edges.
+int orc_grad_dir(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
+                 const OrcConfig* cfg, int which, const double* dLdI, const double* seed_verts,
+                 const double* seed_tex, const double* seed_emit, const double* seed_cam, double* dphi_out) {
+  using D = Dual<8>;
+  Seeds<D> s;
+  s.verts = seed_verts; s.tex = seed_tex; s.emit = seed_emit; s.campos = seed_cam;
+  double dphi[8] = {0};
+  int rc = render_impl<D, true>(m, nm, l, nl, cams, nc, cfg, which, nullptr, dLdI, dphi, nullptr, s);
+  for (int k = 0; k < 8; ++k) dphi_out[k] = dphi[k];
+  return rc;
+}
+
+// Closest-hit queries in float (bit-exact KAT reference). rays: n x 6 (o, d).
+int orc_intersect(const OrcMesh* m, int nm, const OrcLight* l, int nl, const float* rays, int n, int use_bvh,
+                  int* tri, float* bary, float* tout) {
+  Seeds<float> none;
+  Scene<float> sc = build_scene<float>(m, nm, l, nl, none);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    Hit<float> h = intersect(sc, rays + 6 * i, rays + 6 * i + 3, use_bvh != 0);
+    tri[i] = h.tri;
+    bary[2 * i] = h.tri >= 0 ? h.b1 : -1.f;
+    bary[2 * i + 1] = h.tri >= 0 ? h.b2 : -1.f;
+    if (tout) tout[i] = h.tri >= 0 ? h.t : -1.f;
+  }
+  return 0;
+}
+
+// Edge list (float instance): v0, v1 global vertex ids; geo: 16 floats per edge
+// (p0, p1, out, n_left, n_right, length).
+int orc_edges(const OrcMesh* m, int nm, const OrcLight* l, int nl, int cap, int* v01, float* geo) {
+  Seeds<float> none;
+  Scene<float> sc = build_scene<float>(m, nm, l, nl, none);
+  int ne = (int)sc.edges.size();
+  for (int i = 0; i < ne && i < cap; ++i) {
+    const auto& e = sc.edges[i];
+    v01[2 * i] = e.v0; v01[2 * i + 1] = e.v1;
+    const V3<float>* vs[5] = {&e.p0, &e.p1, &e.out, &e.nl, &e.nr};
+    for (int q = 0; q < 5; ++q) for (int k = 0; k < 3; ++k) geo[16 * i + 3 * q + k] = (*vs[q])[k];
+    geo[16 * i + 15] = e.len;
+  }
+  return ne;
+}
+
+}  // extern "C"
