@@ -1,0 +1,188 @@
+/* psdr.h -- C ABI of the B200 differentiable path tracer (libpsdr_b200.so).
+ *
+ * Drop-in replacement for the native layer under torch_psdr's Python API
+ * (src/python/torch_psdr.py). All buffers are DEVICE pointers owned by the caller
+ * (torch tensors in the Python binding) unless stated otherwise; the library owns
+ * only its acceleration structures and scratch memory. Every call takes an explicit
+ * CUDA stream (cudaStream_t passed as void*) and never synchronises the device,
+ * except the few query calls documented as synchronous.
+ *
+ * Errors: every entry point returns a psdr_status; psdr_last_error() returns a
+ * thread-local message for the last failure (replaces the C++ exceptions of
+ * src/optix_def.h:9-81 and the Python asserts of torch_psdr.py).
+ */
+#ifndef PSDR_H_
+#define PSDR_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PSDR_API __attribute__((visibility("default")))
+#else
+#define PSDR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct psdr_scene psdr_scene;
+typedef struct psdr_workspace psdr_workspace;
+typedef struct psdr_batch psdr_batch;
+
+typedef enum {
+  PSDR_OK = 0,
+  PSDR_ERR_INVALID_ARG = 1,
+  PSDR_ERR_OOM = 2,
+  PSDR_ERR_CUDA = 3,
+  PSDR_ERR_TIMEOUT = 4,
+  PSDR_ERR_NUMERIC = 5,
+  PSDR_ERR_UNSUPPORTED = 6
+} psdr_status;
+
+enum { PSDR_TEX_NONE = -1, PSDR_TEX_CONSTANT = 0, PSDR_TEX_UV = 1 };
+enum { PSDR_MAT_DIFFUSE = 0, PSDR_MAT_DIFFUSE_BSDF = 1 };
+enum { PSDR_CAM_PERSPECTIVE = 0, PSDR_CAM_ORTHOGRAPHIC = 1 };
+enum { PSDR_EST_REFERENCE = 0, PSDR_EST_UNBIASED = 1 };
+
+/* A texture (texture.h:16-111; torch_psdr.py:209-269 Texture).
+ * UV maps are (height, width, channels) row-major with row 0 at the TOP of the
+ * image, i.e. the tensor the user passes; the reference flips rows before
+ * flattening (torch_psdr.py:250) and the library applies the same flip when it
+ * indexes. Constant textures hold `channels` floats. */
+typedef struct {
+  int32_t kind;     /* PSDR_TEX_* */
+  int32_t channels; /* 1 or 3 */
+  int32_t height, width;
+  const float* data;
+} psdr_texture_desc;
+
+/* A triangle mesh with its material (mesh.cc:5-95 TriangleMesh; torch_psdr.py:343-379). */
+typedef struct {
+  const float* vertices;  int32_t num_vertices; /* (V,3) */
+  const int32_t* faces;   int32_t num_faces;    /* (F,3) */
+  const float* uvs;       int32_t num_uvs;      /* (T,2) or NULL */
+  const int32_t* uv_indices;                    /* (F,3) or NULL */
+  int32_t material;                             /* PSDR_MAT_* */
+  psdr_texture_desc color;                      /* diffuse reflectance (3 channels) */
+  psdr_texture_desc roughness;                  /* DiffuseBsdf only (1 channel) */
+  psdr_texture_desc normal;                     /* DiffuseBsdf only, kind NONE if absent */
+} psdr_mesh_desc;
+
+/* An area light (emitter.cc:4-14 AreaLight; torch_psdr.py:388-414). emit is host data. */
+typedef struct {
+  const float* vertices; int32_t num_vertices;
+  const int32_t* faces;  int32_t num_faces;
+  float emit[3];
+} psdr_area_light_desc;
+
+typedef struct {
+  const psdr_mesh_desc* meshes;       int32_t num_meshes;
+  const psdr_area_light_desc* lights; int32_t num_lights;
+} psdr_scene_desc;
+
+/* A camera (camera.h:208-362; psdr.cc:22-37). Host data. For PERSPECTIVE, fov is
+ * the vertical field of view in radians; for ORTHOGRAPHIC it is the view width. */
+typedef struct {
+  int32_t type;
+  float look_from[3], look_at[3], up[3];
+  float fov;
+  int32_t height, width;
+} psdr_camera_desc;
+
+/* PathIntegrator::Config (path_integrator.h:8-21; torch_psdr.py:478-536) plus the
+ * B200 extensions: estimator (REFERENCE reproduces the reference's renderD tape;
+ * UNBIASED uses the corrected boundary normalisation), tile_paths (wavefront tile,
+ * 0 = autotuned), leaf_size (BVH leaf collapse, 0 = default), terms, and seed
+ * (0 = the reference's sample streams). */
+typedef struct {
+  int32_t n_pass, spp_interior, enable_light_visable, spp_primary_edge, spp_secondary_edge;
+  int32_t max_bounce, mis_light_samples, mis_bsdf_samples;
+  int32_t primary_edge_preprocess_rounds, secondary_edge_preprocess_rounds;
+  int32_t primary_edge_hypercube_resolution, secondary_edge_hypercube_resolution[3];
+  int32_t estimator;
+  int32_t tile_paths;
+  int32_t leaf_size;
+  int32_t terms;  /* gradient terms of psdr_render_bwd: bit 0 interior, bit 1 primary
+                     edges, bit 2 direct edges; 0 = all (what renderD differentiates) */
+  uint64_t seed;
+} psdr_config;
+
+/* Gradient outputs of psdr_render_bwd (caller-owned device buffers, fp32).
+ * vertices: one buffer per mesh followed by one per light, each (V,3), may be NULL.
+ * textures: one per mesh (same shape as its color texture), may be NULL.
+ * emit: one (3,) buffer per light, may be NULL. camera_origin: one (3,) per camera.
+ * With accumulate = 0 the outputs are overwritten, otherwise added to. */
+typedef struct {
+  float** vertices;
+  float** textures;
+  float** emit;
+  float** camera_origin;
+  int32_t accumulate;
+} psdr_grad_targets;
+
+/* ---------------------------------------------------------------- general */
+PSDR_API const char* psdr_last_error(void);
+PSDR_API const char* psdr_version(void);
+PSDR_API int32_t psdr_abi_version(void);
+
+/* ---------------------------------------------------------------- scene
+ * Replaces Scene::Scene (scene.cc:3-104) + SceneOptix ctor / build_accel
+ * (scene_optix.cc:10-46, 187-238) + TriangleMesh edge build (mesh.cc:97-204):
+ * flattens the meshes, builds the edge list and the sampling CDFs and an LBVH,
+ * all on `stream`. Texture data pointers are borrowed and must outlive the scene. */
+PSDR_API psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_scene** out);
+PSDR_API psdr_status psdr_scene_destroy(psdr_scene* scene);
+/* Rebuild the acceleration structure, triangle attributes and edges after the
+ * vertex buffers changed in place (same topology). */
+PSDR_API psdr_status psdr_scene_update(psdr_scene* scene, void* stream);
+/* Synchronous query: [0] triangles, [1] vertices, [2] edges, [3] bvh nodes,
+ * [4] lights, [5] objects. */
+PSDR_API psdr_status psdr_scene_info(psdr_scene* scene, int64_t* info6);
+/* Synchronous: copies the edge list (v0,v1 global vertex ids; 16 floats per edge:
+ * p0, p1, out_direction, n_left, n_right, length) into DEVICE buffers of capacity cap. */
+PSDR_API psdr_status psdr_scene_edges(psdr_scene* scene, int32_t* v01, float* geo, int64_t cap, int64_t* n_out, void* stream);
+
+/* Closest hit for n rays (device, 8 floats per ray: ox oy oz tmin dx dy dz tmax).
+ * Outputs the global triangle id (-1 on miss), OptiX-convention barycentrics
+ * (weights of p1, p2) and t. brute_force != 0 tests every triangle (the KAT path).
+ * Replaces SceneOptix::hit (scene_optix.cc:240-277) + device_programs.cu:13-47. */
+PSDR_API psdr_status psdr_intersect(psdr_scene* scene, const float* rays, int64_t n, int32_t* tri, float* bary,
+                           float* t, int32_t brute_force, void* stream);
+
+/* ---------------------------------------------------------------- rendering
+ * psdr_render_fwd replaces PathIntegrator::renderC / the forward of renderD
+ * (path_integrator.cc:381-414; torch_psdr.py:538-556). images[c] is a device
+ * (H,W,3) fp32 buffer per camera. */
+PSDR_API psdr_status psdr_workspace_create(psdr_workspace** out);
+PSDR_API psdr_status psdr_workspace_destroy(psdr_workspace* ws);
+PSDR_API psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
+                            const psdr_config* cfg, float** images, void* stream);
+/* Per-sample interior radiance of one camera ((H*W*spp, 3) device buffer), the
+ * values the film averages; used by the parity tests. */
+PSDR_API psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cam,
+                                const psdr_config* cfg, float* samples, void* stream);
+/* Path-replay adjoint of renderD (replaces Wrap2torch.backward + enoki's reverse
+ * sweep, torch_psdr.py:48-72): interior term + primary-edge and direct-edge
+ * boundary terms. d_images[c] is dLoss/dImage (H,W,3) per camera. */
+PSDR_API psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
+                            const psdr_config* cfg, const float** d_images, const psdr_grad_targets* grads,
+                            void* stream);
+
+/* ---------------------------------------------------------------- batching
+ * Many views over one or more scenes in one work list, captured into CUDA graphs
+ * (one for the forward, one for the backward) on first launch and replayed after.
+ * cam_scene[c] selects the scene of camera c. images / d_images / grads are bound
+ * at creation and must stay valid. grads has one entry per scene. */
+PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scenes, const psdr_camera_desc* cams,
+                              const int32_t* cam_scene, int32_t n_cams, const psdr_config* cfg, float** images,
+                              const float** d_images, const psdr_grad_targets* grads, psdr_batch** out);
+PSDR_API psdr_status psdr_batch_forward(psdr_batch* batch, void* stream);
+PSDR_API psdr_status psdr_batch_backward(psdr_batch* batch, void* stream);
+PSDR_API psdr_status psdr_batch_destroy(psdr_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSDR_H_ */

@@ -375,6 +375,19 @@ static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, cons
 extern "C" {
 
 int orc_num_threads() { return omp_get_max_threads(); }
+
+// Raw PCG32 outputs for (initstate, initseq) (pins the restatement to the published
+// pcg-basic demo vector).
+void orc_pcg32(uint64_t initstate, uint64_t initseq, int n, uint32_t* out) {
+  Pcg32 p;
+  p.seed(initstate, initseq);
+  for (int i = 0; i < n; ++i) out[i] = p.next();
+}
+// First n floats of sampler stream i (sampler.h:11-17 seeding).
+void orc_sampler_floats(uint64_t i, int n, float* out) {
+  Pcg32 p = make_sampler(i);
+  for (int k = 0; k < n; ++k) out[k] = p.next_float();
+}
 void orc_set_threads(int n) { omp_set_num_threads(n); }
 
 // Image render (interior term). precision 0 = float, 1 = double.

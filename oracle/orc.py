@@ -57,6 +57,8 @@ def lib():
         _lib.orc_intersect.argtypes = [P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, P, P, P]
         _lib.orc_edges.argtypes = [P, C.c_int, P, C.c_int, C.c_int, P, P]
         _lib.orc_set_threads.argtypes = [C.c_int]
+        _lib.orc_pcg32.argtypes = [C.c_uint64, C.c_uint64, C.c_int, P]
+        _lib.orc_sampler_floats.argtypes = [C.c_uint64, C.c_int, P]
     return _lib
 
 
@@ -173,3 +175,15 @@ def edges(spec, cap=None):
     geo = np.zeros((cap, 16), np.float32)
     n = L.orc_edges(*m.args()[:4], cap, _ptr(v01), _ptr(geo))
     return v01[:n], geo[:n]
+
+
+def pcg32(initstate, initseq, n):
+    out = np.zeros(n, np.uint32)
+    lib().orc_pcg32(initstate, initseq, n, _ptr(out))
+    return out
+
+
+def sampler_floats(i, n):
+    out = np.zeros(n, np.float32)
+    lib().orc_sampler_floats(i, n, _ptr(out))
+    return out

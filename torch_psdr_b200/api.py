@@ -1,0 +1,459 @@
+"""PyTorch API of the B200 path tracer: a drop-in for torch_psdr's Python surface.
+
+Mirrors src/python/torch_psdr.py (class names, constructor arguments, asserts and
+the renderC / renderD contract). Tensors are borrowed as CUDA buffers and handed to
+the native library through the C ABI; the only PyTorch machinery is the
+torch.autograd.Function below, whose forward calls psdr_render_fwd and whose backward
+calls psdr_render_bwd (the path-replay adjoint).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Union
+
+import torch
+from torch import Tensor
+
+from . import _lib as L
+
+
+def _dev_tensor(t: Tensor, dtype) -> Tensor:
+    if not isinstance(t, Tensor):
+        t = torch.as_tensor(t)
+    if not t.is_cuda:
+        raise ValueError("torch_psdr_b200 renders on the GPU: tensors must be CUDA tensors")
+    return t.detach().to(dtype).contiguous().clone()
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _host3(t: Tensor):
+    v = t.detach().reshape(-1).float().cpu().tolist()
+    return (C.c_float * 3)(*v[:3])
+
+
+class VarContex:
+    """Collects the tensors that require grad, in the order torch_psdr.py:84-103 does."""
+
+    def __init__(self):
+        self.torch_vars: List[Tensor] = []
+
+    def append_variable(self, torch_var: Tensor):
+        if isinstance(torch_var, Tensor) and torch_var.requires_grad:
+            self.torch_vars.append(torch_var)
+
+    def merge_variables(self, torch_vars):
+        for t in torch_vars:
+            if t.requires_grad:
+                self.torch_vars.append(t)
+
+    def get_variables(self):
+        return self.torch_vars
+
+
+class BaseCamera(VarContex):
+    """Base class of PerspectiveCamera and OrthographicCamera (torch_psdr.py:106-110)."""
+
+
+class PerspectiveCamera(BaseCamera):
+    def __init__(self, look_from: Tensor, look_at: Tensor, up: Tensor, vfov: Tensor, height: int, width: int):
+        """Pinhole camera (torch_psdr.py:113-158; camera.h:208-277).
+
+        Args:
+            look_from: (3,) camera position.  look_at: (3,) target.  up: (3,) up vector.
+            vfov: (1,) vertical field of view in radians.  height, width: image size.
+        """
+        super().__init__()
+        assert look_from.size() == (3,)
+        assert look_at.size() == (3,)
+        assert up.size() == (3,)
+        assert vfov.size() == (1,)
+        assert height > 0 and width > 0
+        self.look_from, self.look_at, self.up, self.vfov = look_from, look_at, up, vfov
+        for t in (look_from, look_at, up, vfov):
+            self.append_variable(t)
+        self.height = int(height)
+        self.width = int(width)
+
+    def _desc(self):
+        d = L.CameraDesc()
+        d.type = L.CAM_PERSPECTIVE
+        d.look_from = _host3(self.look_from)
+        d.look_at = _host3(self.look_at)
+        d.up = _host3(self.up)
+        d.fov = float(self.vfov.detach().reshape(-1)[0].item())
+        d.height, d.width = self.height, self.width
+        return d
+
+
+Camera = PerspectiveCamera  # example/optimize_texture.py:76 uses dr.Camera
+
+
+class OrthographicCamera(BaseCamera):
+    def __init__(self, look_from, look_at, up, view_width, height: int, width: int):
+        """Orthographic camera (torch_psdr.py:161-206). Not built on this path yet."""
+        super().__init__()
+        assert look_from.size() == (3,)
+        assert look_at.size() == (3,)
+        assert up.size() == (3,)
+        assert view_width.size() == (1,)
+        assert height > 0 and width > 0
+        raise NotImplementedError("OrthographicCamera is not available in torch_psdr_b200 yet")
+
+
+class Texture(VarContex):
+    def __init__(self, tex: Tensor):
+        """Constant (1,)/(3,) or image (H,W,1)/(H,W,3) texture (torch_psdr.py:209-269).
+
+        The image keeps the caller's row order; the library applies the row flip of
+        torch_psdr.py:250 when it indexes (nearest texel, texture.h:65-74).
+        """
+        super().__init__()
+        tex_type = None
+        size = tuple(tex.size())
+        if tex.dim() == 1:
+            if size == (1,):
+                tex_type = "Constant1f"
+            elif size == (3,):
+                tex_type = "Constant3f"
+        elif tex.dim() == 2:
+            # torch_psdr.py:232-234 tests `tex_type == "UV1f"` (a comparison, not an
+            # assignment), so a (H, W) texture fails its assert; kept as is.
+            pass
+        elif tex.dim() == 3:
+            if size[-1] == 1:
+                tex_type = "UV1f"
+            elif size[-1] == 3:
+                tex_type = "UV3f"
+        assert tex_type is not None
+        self.tex_type = tex_type
+        self.tensor = tex
+        self.append_variable(tex)
+        self.data = _dev_tensor(tex, torch.float32)
+
+    def _desc(self):
+        d = L.TextureDesc()
+        if self.tex_type.startswith("Constant"):
+            d.kind = L.TEX_CONSTANT
+            d.channels = 1 if self.tex_type == "Constant1f" else 3
+            d.height = d.width = 1
+        else:
+            d.kind = L.TEX_UV
+            d.height, d.width = int(self.data.shape[0]), int(self.data.shape[1])
+            d.channels = int(self.data.shape[2])
+        d.data = self.data.data_ptr()
+        return d
+
+
+class Material(VarContex):
+    """Base class of the materials (torch_psdr.py:272-277)."""
+
+
+class DiffuseMaterial(Material):
+    def __init__(self, tex: Union[Tensor, Texture]):
+        """Lambertian reflectance (torch_psdr.py:280-295; diffuse_material.cc:3-45)."""
+        super().__init__()
+        if isinstance(tex, Tensor):
+            tex = Texture(tex)
+        assert tex.tex_type == "Constant3f" or tex.tex_type == "UV3f"
+        self.texture = tex
+        self.merge_variables(tex.get_variables())
+        self.mat_type = L.MAT_DIFFUSE
+
+
+class DiffuseBsdfMaterial(Material):
+    def __init__(self, color, roughness, normal=None):
+        """Oren-Nayar style diffuse BSDF (torch_psdr.py:298-335). Not built on this path yet."""
+        super().__init__()
+        if isinstance(color, Tensor):
+            color = Texture(color)
+        if isinstance(roughness, Tensor):
+            roughness = Texture(roughness)
+        if isinstance(normal, Tensor):
+            normal = Texture(normal)
+        assert color.tex_type == "Constant3f" or color.tex_type == "UV3f"
+        assert roughness.tex_type == "Constant1f" or roughness.tex_type == "UV1f"
+        assert normal is None or normal.tex_type == "Constant3f" or normal.tex_type == "UV3f"
+        raise NotImplementedError("DiffuseBsdfMaterial is not available in torch_psdr_b200 yet")
+
+
+class PrincipledMaterial(Material):
+    pass
+
+
+class Mesh(VarContex):
+    def __init__(self, vertices: Tensor, uvs, face_indices: Tensor, uv_indices, material: Material):
+        """Triangle mesh with its material (torch_psdr.py:343-379; mesh.cc:5-95)."""
+        super().__init__()
+        assert vertices.dim() == 2 and vertices.size(-1) == 3
+        assert uvs is None or (uvs.dim() == 2 and uvs.size(-1) == 2)
+        assert face_indices.dim() == 2 and face_indices.size(-1) == 3
+        assert uv_indices is None or (uv_indices.dim() == 2 and uv_indices.size(-1) == 3)
+        self.vertices = vertices
+        self.v = _dev_tensor(vertices, torch.float32)
+        self.f = _dev_tensor(face_indices, torch.int32)
+        no_uvs = uvs is None or uv_indices is None
+        self.uv = None if no_uvs else _dev_tensor(uvs, torch.float32)
+        self.uvi = None if no_uvs else _dev_tensor(uv_indices, torch.int32)
+        self.material = material
+        self.append_variable(vertices)
+        self.merge_variables(material.get_variables())
+
+    def _desc(self):
+        d = L.MeshDesc()
+        d.vertices, d.num_vertices = self.v.data_ptr(), int(self.v.shape[0])
+        d.faces, d.num_faces = self.f.data_ptr(), int(self.f.shape[0])
+        if self.uv is not None:
+            d.uvs, d.num_uvs, d.uv_indices = self.uv.data_ptr(), int(self.uv.shape[0]), self.uvi.data_ptr()
+        d.material = self.material.mat_type
+        d.color = self.material.texture._desc()
+        d.roughness = L.TextureDesc(L.TEX_NONE, 0, 0, 0, None)
+        d.normal = L.TextureDesc(L.TEX_NONE, 0, 0, 0, None)
+        return d
+
+
+class Light(VarContex):
+    """Base class of the lights (torch_psdr.py:382-385)."""
+
+
+class AreaLight(Light):
+    def __init__(self, vertices: Tensor, face_indices: Tensor, emit: Tensor):
+        """Triangle-mesh emitter with constant radiance (torch_psdr.py:388-414; emitter.cc:4-92)."""
+        super().__init__()
+        assert vertices.dim() == 2 and vertices.size(-1) == 3
+        assert face_indices.dim() == 2 and face_indices.size(-1) == 3
+        assert emit.dim() == 1 and emit.size(0) == 3
+        self.vertices, self.emit = vertices, emit
+        self.v = _dev_tensor(vertices, torch.float32)
+        self.f = _dev_tensor(face_indices, torch.int32)
+        self.append_variable(vertices)
+        self.append_variable(emit)
+
+    def _desc(self):
+        d = L.AreaLightDesc()
+        d.vertices, d.num_vertices = self.v.data_ptr(), int(self.v.shape[0])
+        d.faces, d.num_faces = self.f.data_ptr(), int(self.f.shape[0])
+        d.emit = _host3(self.emit)
+        return d
+
+
+class EnvLight(Light):
+    def __init__(self, cube_map: Texture):
+        """Cube-map environment light (torch_psdr.py:417-430). Not built on this path."""
+        super().__init__()
+        assert cube_map.tex_type == "UV3f"
+        raise NotImplementedError("EnvLight is not available in torch_psdr_b200")
+
+
+class SH9Light(Light):
+    def __init__(self, sh9_coeff: Tensor):
+        """Spherical-harmonics light (torch_psdr.py:433-447). Not built on this path."""
+        super().__init__()
+        assert sh9_coeff.size() == (9, 3)
+        raise NotImplementedError("SH9Light is not available in torch_psdr_b200")
+
+
+class Scene(VarContex):
+    def __init__(self, cameras: List[BaseCamera], meshes: List[Mesh], lights: List[Light]):
+        """Cameras, meshes and lights (torch_psdr.py:450-474). Builds the native scene
+        (triangle records, edge list, sampling CDFs, LBVH) on the current stream."""
+        super().__init__()
+        self.cameras = list(cameras)
+        self.meshes = list(meshes)
+        self.lights = list(lights)
+        for c in self.cameras:
+            self.merge_variables(c.get_variables())
+        for m in self.meshes:
+            self.merge_variables(m.get_variables())
+        for lt in self.lights:
+            self.merge_variables(lt.get_variables())
+        lib = L.load()
+        md = (L.MeshDesc * max(1, len(self.meshes)))(*[m._desc() for m in self.meshes])
+        ld = (L.AreaLightDesc * max(1, len(self.lights)))(*[lt._desc() for lt in self.lights])
+        desc = L.SceneDesc(md, len(self.meshes), ld, len(self.lights))
+        handle = C.c_void_p()
+        L.check(lib.psdr_scene_create(C.byref(desc), _stream(), C.byref(handle)), "psdr_scene_create")
+        self._handle = handle
+        self._lib = lib
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def info(self):
+        out = (C.c_int64 * 6)()
+        L.check(self._lib.psdr_scene_info(self._handle, out), "psdr_scene_info")
+        return dict(zip(["triangles", "vertices", "edges", "bvh_nodes", "lights", "objects"], list(out)))
+
+    def _camera_descs(self):
+        return (L.CameraDesc * len(self.cameras))(*[c._desc() for c in self.cameras])
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.psdr_scene_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+
+class _RenderD(torch.autograd.Function):
+    """Replaces Wrap2torch (torch_psdr.py:29-72): forward renders, backward runs the
+    path-replay adjoint and returns the gradient of every input tensor."""
+
+    @staticmethod
+    def forward(ctx, integrator, scene, *torch_vars):
+        imgs = integrator._render(scene)
+        ctx.integrator = integrator
+        ctx.scene = scene
+        ctx.n_vars = len(torch_vars)
+        ctx.vars = torch_vars
+        return tuple(imgs)
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx, *grads):
+        grads = [g if g is not None else None for g in grads]
+        out = ctx.integrator._backward(ctx.scene, grads, ctx.vars)
+        return (None, None) + tuple(out)
+
+
+class PathIntegrator:
+    def __init__(self, enable_light_visable: bool = False, n_pass: int = 1, spp_interior: int = 1,
+                 max_bounce: int = 3, mis_light_samples: int = 1, mis_bsdf_samples: int = 1,
+                 spp_primary_edge: int = 1, spp_secondary_edge: int = 1, primary_edge_preprocess_rounds: int = 1,
+                 secondary_edge_preprocess_rounds: int = 1, primary_edge_hypercube_resolution: int = 10000,
+                 secondary_edge_hypercube_resolution: List[int] = [10000, 6, 6], estimator: str = "reference",
+                 seed: int = 0, tile_paths: int = 0, gradient_terms: int = 0):
+        """Path-space differentiable integrator (torch_psdr.py:477-536; path_integrator.h:8-21).
+
+        B200 extensions: estimator ("reference" reproduces renderD exactly), seed (0 =
+        the reference's sample streams), tile_paths (wavefront tile, 0 = automatic),
+        gradient_terms (bitmask: 1 interior, 2 primary edges, 4 direct edges; 0 = all).
+        """
+        assert n_pass > 0
+        assert spp_interior > 0
+        assert spp_primary_edge > 0
+        assert spp_secondary_edge > 0
+        assert max_bounce > 0
+        assert mis_light_samples >= 0
+        assert mis_bsdf_samples >= 0
+        assert primary_edge_preprocess_rounds > 0
+        assert secondary_edge_preprocess_rounds > 0
+        assert primary_edge_hypercube_resolution > 0
+        assert len(secondary_edge_hypercube_resolution) == 3
+        for reso in secondary_edge_hypercube_resolution:
+            assert reso > 0
+        assert estimator in ("reference", "unbiased")
+        cfg = L.Config()
+        cfg.n_pass = n_pass
+        cfg.spp_interior = spp_interior
+        cfg.enable_light_visable = int(bool(enable_light_visable))
+        cfg.spp_primary_edge = spp_primary_edge
+        cfg.spp_secondary_edge = spp_secondary_edge
+        cfg.max_bounce = max_bounce
+        cfg.mis_light_samples = mis_light_samples
+        cfg.mis_bsdf_samples = mis_bsdf_samples
+        cfg.primary_edge_preprocess_rounds = primary_edge_preprocess_rounds
+        cfg.secondary_edge_preprocess_rounds = secondary_edge_preprocess_rounds
+        cfg.primary_edge_hypercube_resolution = primary_edge_hypercube_resolution
+        cfg.secondary_edge_hypercube_resolution = (C.c_int32 * 3)(*secondary_edge_hypercube_resolution)
+        cfg.estimator = L.EST_REFERENCE if estimator == "reference" else L.EST_UNBIASED
+        cfg.tile_paths = tile_paths
+        cfg.terms = gradient_terms
+        cfg.seed = seed
+        self.cfg = cfg
+        self._lib = L.load()
+        self._ws = None
+
+    def _workspace(self):
+        if self._ws is None:
+            h = C.c_void_p()
+            L.check(self._lib.psdr_workspace_create(C.byref(h)), "psdr_workspace_create")
+            self._ws = h
+        return self._ws
+
+    def __del__(self):
+        if getattr(self, "_ws", None) is not None:
+            try:
+                self._lib.psdr_workspace_destroy(self._ws)
+            except Exception:
+                pass
+
+    def _render(self, scene: Scene) -> List[Tensor]:
+        imgs = [torch.empty((c.height, c.width, 3), dtype=torch.float32, device="cuda") for c in scene.cameras]
+        ptrs = (C.c_void_p * len(imgs))(*[i.data_ptr() for i in imgs])
+        cams = scene._camera_descs()
+        L.check(self._lib.psdr_render_fwd(scene.handle, self._workspace(), cams, len(imgs), C.byref(self.cfg),
+                                          ptrs, _stream()), "psdr_render_fwd")
+        return imgs
+
+    def render_samples(self, scene: Scene, camera_index: int = 0) -> Tensor:
+        """Per-sample interior radiance (H*W*spp, 3) of one camera (the values the film averages)."""
+        c = scene.cameras[camera_index]
+        out = torch.empty((c.height * c.width * self.cfg.spp_interior, 3), dtype=torch.float32, device="cuda")
+        cams = scene._camera_descs()
+        L.check(self._lib.psdr_render_samples(scene.handle, self._workspace(), C.byref(cams[camera_index]),
+                                              C.byref(self.cfg), out.data_ptr(), _stream()), "psdr_render_samples")
+        return out
+
+    def _backward(self, scene: Scene, grads, torch_vars):
+        dev = "cuda"
+        dimgs = []
+        for g, c in zip(grads, scene.cameras):
+            if g is None:
+                g = torch.zeros((c.height, c.width, 3), dtype=torch.float32, device=dev)
+            dimgs.append(g.detach().float().contiguous())
+        nm, nl = len(scene.meshes), len(scene.lights)
+        vert_g = [torch.zeros_like(m.v) for m in scene.meshes] + [torch.zeros_like(lt.v) for lt in scene.lights]
+        tex_g = [torch.zeros_like(m.material.texture.data) for m in scene.meshes]
+        emit_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.lights]
+        cam_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.cameras]
+        P = C.c_void_p
+        vp = (P * (nm + nl))(*[t.data_ptr() for t in vert_g])
+        tp = (P * max(1, nm))(*[t.data_ptr() for t in tex_g])
+        ep = (P * max(1, nl))(*[t.data_ptr() for t in emit_g])
+        cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
+        tg = L.GradTargets(vp, tp, ep, cp, 0)
+        dp = (P * len(dimgs))(*[d.data_ptr() for d in dimgs])
+        cams = scene._camera_descs()
+        L.check(self._lib.psdr_render_bwd(scene.handle, self._workspace(), cams, len(dimgs), C.byref(self.cfg), dp,
+                                          C.byref(tg), _stream()), "psdr_render_bwd")
+        # map the accumulators onto the input tensors (a tensor may play several roles)
+        acc = {}
+
+        def add(t, g):
+            if t is None or not isinstance(t, Tensor) or not t.requires_grad:
+                return
+            g = g.reshape(t.shape).to(t.dtype)
+            key = id(t)
+            acc[key] = g if key not in acc else acc[key] + g
+
+        for i, m in enumerate(scene.meshes):
+            add(m.vertices, vert_g[i])
+            add(m.material.texture.tensor, tex_g[i])
+        for j, lt in enumerate(scene.lights):
+            add(lt.vertices, vert_g[nm + j])
+            add(lt.emit, emit_g[j])
+        for k, c in enumerate(scene.cameras):
+            add(c.look_from, cam_g[k])
+            for t in (c.look_at, c.up, c.vfov):
+                add(t, torch.zeros_like(t, dtype=torch.float32))
+        return [acc.get(id(t), torch.zeros_like(t)) for t in torch_vars]
+
+    def renderC(self, scene: Scene) -> List[Tensor]:
+        """Plain render (path_integrator.cc:408-410): one (H, W, 3) image per camera."""
+        with torch.no_grad():
+            return self._render(scene)
+
+    def renderD(self, scene: Scene) -> List[Tensor]:
+        """Differentiable render (torch_psdr.py:547-556): images requiring grad; their
+        backward runs the path-replay adjoint with both edge-sampling terms."""
+        torch_vars = scene.get_variables()
+        if not torch_vars:
+            return self._render(scene)
+        imgs = _RenderD.apply(self, scene, *torch_vars)
+        return list(imgs)

@@ -1,0 +1,371 @@
+// capi.cu -- the extern "C" entry points declared in include/psdr.h.
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "render.h"
+
+namespace psdr {
+
+thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+
+void scene_build_geometry(psdr_scene* s);
+void psdr_scene_alloc(psdr_scene* s);
+
+namespace {
+
+__global__ void k_intersect(DevScene sc, const float* __restrict__ rays, long long n, int* __restrict__ tri,
+                            float* __restrict__ bary, float* __restrict__ tout, int brute) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float* r = rays + 8 * i;
+    const float3 o = f3(r[0], r[1], r[2]), d = f3(r[4], r[5], r[6]);
+    const float tmin = r[3], tmax = r[7];
+    HitRec h;
+    if (!brute) {
+      h = trace_closest(sc, o, d, tmin, tmax);
+    } else {
+      h.tri = -1; h.t = tmax; h.b1 = h.b2 = 0.f;
+      const RayPre rp = ray_pre(o, d);
+      for (int t = 0; t < sc.ntri; ++t) {
+        const float4* q = sc.tri + 6 * (size_t)t;
+        float tt, b1, b2;
+        if (tri_test(rp, xyz(q[0]), xyz(q[1]), xyz(q[2]), tmin, h.t, tt, b1, b2))
+          if (tt < h.t || h.tri < 0 || t < h.tri) { h.t = tt; h.tri = t; h.b1 = b1; h.b2 = b2; }
+      }
+    }
+    tri[i] = h.tri;
+    if (bary) { bary[2 * i] = h.tri >= 0 ? h.b1 : -1.f; bary[2 * i + 1] = h.tri >= 0 ? h.b2 : -1.f; }
+    if (tout) tout[i] = h.tri >= 0 ? h.t : -1.f;
+  }
+}
+
+__global__ void k_edges_out(const float4* __restrict__ e, const int2* __restrict__ ev, int n, int* __restrict__ v01,
+                            float* __restrict__ geo) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 a = e[4 * i], b = e[4 * i + 1], c = e[4 * i + 2], d = e[4 * i + 3];
+  const float g[16] = {a.x, a.y, a.z, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w, a.w};
+  for (int k = 0; k < 16; ++k) geo[16 * i + k] = g[k];
+  v01[2 * i] = ev[i].x;
+  v01[2 * i + 1] = ev[i].y;
+}
+
+void check_tex(const psdr_texture_desc& t, const char* what, bool allow_none) {
+  if (t.kind == PSDR_TEX_NONE && allow_none) return;
+  PSDR_CHECK(t.kind == PSDR_TEX_CONSTANT || t.kind == PSDR_TEX_UV, std::string(what) + ": bad texture kind");
+  PSDR_CHECK(t.channels == 1 || t.channels == 3, std::string(what) + ": channels must be 1 or 3");
+  PSDR_CHECK(t.data != nullptr, std::string(what) + ": null texture data");
+  if (t.kind == PSDR_TEX_UV) PSDR_CHECK(t.height > 0 && t.width > 0, std::string(what) + ": empty texture");
+}
+
+void check_cfg(const psdr_config* c) {
+  PSDR_CHECK(c != nullptr, "null config");
+  PSDR_CHECK(c->n_pass > 0, "n_pass must be > 0");
+  PSDR_CHECK(c->spp_interior > 0, "spp_interior must be > 0");
+  PSDR_CHECK(c->spp_primary_edge > 0, "spp_primary_edge must be > 0");
+  PSDR_CHECK(c->spp_secondary_edge > 0, "spp_secondary_edge must be > 0");
+  PSDR_CHECK(c->max_bounce > 0 && c->max_bounce <= kMaxDepth, "max_bounce must be in [1, 16]");
+  PSDR_CHECK(c->mis_light_samples >= 0 && c->mis_bsdf_samples >= 0, "mis sample counts must be >= 0");
+  PSDR_CHECK(c->mis_light_samples + std::max(c->mis_bsdf_samples, 1) + 1 <= kMaxRays, "too many mis samples");
+  PSDR_CHECK(c->primary_edge_preprocess_rounds > 0 && c->secondary_edge_preprocess_rounds > 0,
+             "preprocess rounds must be > 0");
+  PSDR_CHECK(c->primary_edge_hypercube_resolution > 0, "primary hypercube resolution must be > 0");
+  for (int k = 0; k < 3; ++k)
+    PSDR_CHECK(c->secondary_edge_hypercube_resolution[k] > 0, "secondary hypercube resolution must be > 0");
+  PSDR_CHECK(c->estimator == PSDR_EST_REFERENCE || c->estimator == PSDR_EST_UNBIASED, "bad estimator");
+  PSDR_CHECK(c->tile_paths >= 0, "tile_paths must be >= 0");
+}
+
+void check_cams(const psdr_camera_desc* cams, int n) {
+  PSDR_CHECK(cams != nullptr && n > 0, "no cameras");
+  for (int i = 0; i < n; ++i) {
+    PSDR_CHECK(cams[i].type == PSDR_CAM_PERSPECTIVE, "only perspective cameras are supported");
+    PSDR_CHECK(cams[i].height > 0 && cams[i].width > 0, "camera height and width must be > 0");
+  }
+}
+
+DevScene* dev_scene(psdr_scene* s) { return s->d_dev.as<DevScene>(); }
+
+SceneGradInfo grad_info(const psdr_scene* s) {
+  SceneGradInfo gi;
+  const int nm = (int)s->meshes.size();
+  if (s->nlight == 1) {
+    gi.emit_hot = 1;
+    if (s->obj_nvert[nm] <= kMaxLightVerts) {
+      gi.hot_lv0 = s->obj_vert_off[nm];
+      gi.hot_nlv = s->obj_nvert[nm];
+    }
+  }
+  return gi;
+}
+
+}  // namespace
+}  // namespace psdr
+
+using namespace psdr;
+
+#define API_BEGIN try {
+#define API_END                                                          \
+  }                                                                      \
+  catch (const psdr::Error& e) {                                         \
+    psdr::set_error(e.msg);                                              \
+    return e.code;                                                       \
+  }                                                                      \
+  catch (const std::bad_alloc&) {                                        \
+    psdr::set_error("host allocation failed");                          \
+    return PSDR_ERR_OOM;                                                 \
+  }                                                                      \
+  catch (const std::exception& e) {                                      \
+    psdr::set_error(e.what());                                           \
+    return PSDR_ERR_CUDA;                                                \
+  }                                                                      \
+  return PSDR_OK;
+
+extern "C" {
+
+const char* psdr_last_error(void) { return psdr::g_err.c_str(); }
+const char* psdr_version(void) { return "torch_psdr_b200 0.1.0 (sm_100a)"; }
+int32_t psdr_abi_version(void) { return 1; }
+
+psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_scene** out) {
+  API_BEGIN
+  PSDR_CHECK(desc != nullptr && out != nullptr, "null argument");
+  PSDR_CHECK(desc->num_meshes >= 0 && desc->num_lights >= 0, "negative counts");
+  PSDR_CHECK(desc->num_meshes + desc->num_lights > 0, "scene has no geometry");
+  PSDR_CHECK(desc->num_meshes == 0 || desc->meshes != nullptr, "null mesh array");
+  PSDR_CHECK(desc->num_lights == 0 || desc->lights != nullptr, "null light array");
+  *out = nullptr;
+  psdr_scene* s = new psdr_scene();
+  s->stream = (cudaStream_t)stream;
+  try {
+    const int nm = desc->num_meshes, nl = desc->num_lights;
+    s->meshes.assign(desc->meshes, desc->meshes + nm);
+    s->lights.assign(desc->lights, desc->lights + nl);
+    s->nobj = nm + nl;
+    s->nlight = nl;
+    int voff = 0, toff = 0;
+    size_t texoff = 0;
+    for (int o = 0; o < s->nobj; ++o) {
+      const bool is_mesh = o < nm;
+      const float* V = is_mesh ? s->meshes[o].vertices : s->lights[o - nm].vertices;
+      const int* F = is_mesh ? s->meshes[o].faces : s->lights[o - nm].faces;
+      const int nV = is_mesh ? s->meshes[o].num_vertices : s->lights[o - nm].num_vertices;
+      const int nF = is_mesh ? s->meshes[o].num_faces : s->lights[o - nm].num_faces;
+      PSDR_CHECK(V != nullptr && F != nullptr, "null vertex or face buffer");
+      PSDR_CHECK(nV > 0 && nF > 0, "empty mesh");
+      s->obj_vert_off.push_back(voff);
+      s->obj_tri_off.push_back(toff);
+      s->obj_nvert.push_back(nV);
+      s->obj_ntri.push_back(nF);
+      DevObj ob{};
+      ob.mat = 0;
+      ob.light = is_mesh ? -1 : o - nm;
+      ob.color.kind = -1;
+      ob.rough.kind = -1;
+      ob.normal.kind = -1;
+      if (is_mesh) {
+        const psdr_mesh_desc& m = s->meshes[o];
+        PSDR_CHECK(m.material == PSDR_MAT_DIFFUSE, "only DiffuseMaterial is supported by this build");
+        check_tex(m.color, "color", false);
+        PSDR_CHECK(m.color.channels == 3, "color texture must have 3 channels");
+        PSDR_CHECK((m.uvs == nullptr) == (m.uv_indices == nullptr) || m.uvs == nullptr || m.uv_indices == nullptr,
+                   "uvs / uv_indices mismatch");
+        ob.mat = m.material;
+        ob.color = DevTex{m.color.kind, m.color.channels, m.color.kind == PSDR_TEX_UV ? m.color.height : 1,
+                          m.color.kind == PSDR_TEX_UV ? m.color.width : 1, m.color.data, nullptr};
+        const size_t cnt = (size_t)ob.color.h * ob.color.w * ob.color.ch;
+        s->tex_grad_off.push_back(texoff);
+        texoff += cnt;
+      } else {
+        s->tex_grad_off.push_back(SIZE_MAX);
+      }
+      s->h_objs.push_back(ob);
+      voff += nV;
+      toff += nF;
+    }
+    s->nvert = voff;
+    s->ntri = toff;
+    for (int l = 0; l < nl; ++l) {
+      DevLight L{};
+      L.tri0 = s->obj_tri_off[nm + l];
+      L.ntri = s->obj_ntri[nm + l];
+      for (int k = 0; k < 3; ++k) L.emit[k] = s->lights[l].emit[k];
+      s->h_lights.push_back(L);
+    }
+    s->dev.ltri_base = nl > 0 ? s->obj_tri_off[nm] : 0;
+    psdr_scene_alloc(s);
+    // fp64 gradient accumulators live with the scene
+    cudaStream_t st = s->stream;
+    s->g_verts.alloc(sizeof(double) * 3 * s->nvert, st);
+    s->g_tex.alloc(sizeof(double) * std::max<size_t>(1, texoff), st);
+    s->g_emit.alloc(sizeof(double) * 3 * std::max(1, nl), st);
+    s->dev.grad_verts = s->g_verts.as<double>();
+    for (int o = 0; o < nm; ++o) s->h_objs[o].color.grad = s->g_tex.as<double>() + s->tex_grad_off[o];
+    for (int l = 0; l < nl; ++l) s->h_lights[l].grad_emit = s->g_emit.as<double>() + 3 * l;
+    s->upload_tables();
+    scene_build_geometry(s);
+  } catch (...) {
+    delete s;
+    throw;
+  }
+  *out = s;
+  API_END
+}
+
+psdr_status psdr_scene_destroy(psdr_scene* scene) {
+  API_BEGIN
+  delete scene;
+  API_END
+}
+
+psdr_status psdr_scene_update(psdr_scene* scene, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene != nullptr, "null scene");
+  if (stream) scene->stream = (cudaStream_t)stream;
+  scene_build_geometry(scene);
+  API_END
+}
+
+psdr_status psdr_scene_info(psdr_scene* scene, int64_t* info) {
+  API_BEGIN
+  PSDR_CHECK(scene != nullptr && info != nullptr, "null argument");
+  int ne = 0;
+  PSDR_CUDA(cudaMemcpyAsync(&ne, scene->n_edges.p, sizeof(int), cudaMemcpyDeviceToHost, scene->stream));
+  PSDR_CUDA(cudaStreamSynchronize(scene->stream));
+  info[0] = scene->ntri;
+  info[1] = scene->nvert;
+  info[2] = ne;
+  info[3] = std::max(0, scene->ntri - 1);
+  info[4] = scene->nlight;
+  info[5] = scene->nobj;
+  API_END
+}
+
+psdr_status psdr_scene_edges(psdr_scene* scene, int32_t* v01, float* geo, int64_t cap, int64_t* n_out, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene && v01 && geo && n_out, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  int ne = 0;
+  PSDR_CUDA(cudaStreamSynchronize(scene->stream));
+  PSDR_CUDA(cudaMemcpy(&ne, scene->n_edges.p, sizeof(int), cudaMemcpyDeviceToHost));
+  *n_out = ne;
+  const int n = (int)std::min<int64_t>(ne, cap);
+  if (n > 0)
+    k_edges_out<<<(n + 255) / 256, 256, 0, st>>>(scene->edge.as<float4>(), scene->edge_v.as<int2>(), n, v01, geo);
+  PSDR_CUDA(cudaGetLastError());
+  PSDR_CUDA(cudaStreamSynchronize(st));
+  API_END
+}
+
+psdr_status psdr_intersect(psdr_scene* scene, const float* rays, int64_t n, int32_t* tri, float* bary, float* t,
+                           int32_t brute_force, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene && (rays || n == 0) && (tri || n == 0), "null argument");
+  PSDR_CHECK(n >= 0, "negative ray count");
+  if (n == 0) return PSDR_OK;
+  const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)num_sms() * 16);
+  k_intersect<<<blocks, 128, 0, (cudaStream_t)stream>>>(scene->dev, rays, n, tri, bary, t, brute_force);
+  PSDR_CUDA(cudaGetLastError());
+  API_END
+}
+
+psdr_status psdr_workspace_create(psdr_workspace** out) {
+  API_BEGIN
+  PSDR_CHECK(out != nullptr, "null argument");
+  *out = new psdr_workspace();
+  API_END
+}
+
+psdr_status psdr_workspace_destroy(psdr_workspace* ws) {
+  API_BEGIN
+  delete ws;
+  API_END
+}
+
+psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
+                            const psdr_config* cfg, float** images, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene && ws && images, "null argument");
+  check_cfg(cfg);
+  check_cams(cams, n_cams);
+  PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
+  std::vector<DevView> views(n_cams);
+  for (int i = 0; i < n_cams; ++i) {
+    PSDR_CHECK(images[i] != nullptr, "null image buffer");
+    make_view(cams[i], cfg->spp_interior, views[i]);
+    views[i].image = images[i];
+  }
+  render_forward_impl(dev_scene(scene), views, *cfg, ws, (cudaStream_t)stream, nullptr);
+  API_END
+}
+
+psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cam,
+                                const psdr_config* cfg, float* samples, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene && ws && samples, "null argument");
+  check_cfg(cfg);
+  check_cams(cam, 1);
+  PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
+  std::vector<DevView> views(1);
+  make_view(*cam, cfg->spp_interior, views[0]);
+  render_forward_impl(dev_scene(scene), views, *cfg, ws, (cudaStream_t)stream, samples);
+  API_END
+}
+
+psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
+                            const psdr_config* cfg, const float** d_images, const psdr_grad_targets* grads,
+                            void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene && ws && d_images && grads, "null argument");
+  check_cfg(cfg);
+  check_cams(cams, n_cams);
+  PSDR_CHECK(scene->nlight > 0, "scene has no light");
+  PSDR_CHECK(cfg->estimator == PSDR_EST_REFERENCE, "only the reference estimator is available in this build");
+  cudaStream_t st = (cudaStream_t)stream;
+  PSDR_CUDA(cudaMemsetAsync(scene->g_verts.p, 0, scene->g_verts.bytes, st));
+  PSDR_CUDA(cudaMemsetAsync(scene->g_tex.p, 0, scene->g_tex.bytes, st));
+  PSDR_CUDA(cudaMemsetAsync(scene->g_emit.p, 0, scene->g_emit.bytes, st));
+  ws->campos_acc.alloc(sizeof(double) * 3 * n_cams, st);
+  PSDR_CUDA(cudaMemsetAsync(ws->campos_acc.p, 0, sizeof(double) * 3 * n_cams, st));
+  std::vector<DevView> views(n_cams);
+  for (int i = 0; i < n_cams; ++i) {
+    PSDR_CHECK(d_images[i] != nullptr, "null image gradient");
+    make_view(cams[i], cfg->spp_interior, views[i]);
+    views[i].dimage = d_images[i];
+    views[i].grad_pos = ws->campos_acc.as<double>() + 3 * i;
+  }
+  render_backward_impl(dev_scene(scene), views, *cfg, ws, grad_info(scene), st);
+  const int nm = (int)scene->meshes.size();
+  for (int o = 0; o < scene->nobj; ++o) {
+    if (grads->vertices && grads->vertices[o])
+      grad_out(scene->g_verts.as<double>() + 3 * (size_t)scene->obj_vert_off[o], grads->vertices[o],
+               3 * (long long)scene->obj_nvert[o], grads->accumulate, st);
+    if (o < nm && grads->textures && grads->textures[o]) {
+      const DevObj& ob = scene->h_objs[o];
+      grad_out(scene->g_tex.as<double>() + scene->tex_grad_off[o], grads->textures[o],
+               (long long)ob.color.h * ob.color.w * ob.color.ch, grads->accumulate, st);
+    }
+  }
+  for (int l = 0; l < scene->nlight; ++l)
+    if (grads->emit && grads->emit[l]) grad_out(scene->g_emit.as<double>() + 3 * l, grads->emit[l], 3, grads->accumulate, st);
+  for (int i = 0; i < n_cams; ++i)
+    if (grads->camera_origin && grads->camera_origin[i])
+      grad_out(ws->campos_acc.as<double>() + 3 * i, grads->camera_origin[i], 3, grads->accumulate, st);
+  PSDR_CUDA(cudaGetLastError());
+  API_END
+}
+
+psdr_status psdr_batch_create(psdr_scene* const*, int32_t, const psdr_camera_desc*, const int32_t*, int32_t,
+                              const psdr_config*, float**, const float**, const psdr_grad_targets*, psdr_batch** out) {
+  if (out) *out = nullptr;
+  psdr::set_error("batching is not available in this build");
+  return PSDR_ERR_UNSUPPORTED;
+}
+psdr_status psdr_batch_forward(psdr_batch*, void*) { return PSDR_ERR_UNSUPPORTED; }
+psdr_status psdr_batch_backward(psdr_batch*, void*) { return PSDR_ERR_UNSUPPORTED; }
+psdr_status psdr_batch_destroy(psdr_batch*) { return PSDR_OK; }
+
+}  // extern "C"

@@ -1,0 +1,393 @@
+// psdr_common.cuh -- device-side building blocks shared by every kernel file:
+// vector math, the PCG32/TEA sampler streams, scene records in HBM, the watertight
+// ray/triangle test and the LBVH traversal.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#define PSDR_HD __host__ __device__ __forceinline__
+#define PSDR_D __device__ __forceinline__
+
+namespace psdr {
+
+// ------------------------------------------------------------------ float3 math
+PSDR_HD float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+PSDR_HD float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+PSDR_HD float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+PSDR_HD float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+PSDR_HD float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+PSDR_HD float3 operator*(float s, float3 a) { return f3(a.x * s, a.y * s, a.z * s); }
+PSDR_HD float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+PSDR_HD float3 mul(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+PSDR_HD float3& operator+=(float3& a, float3 b) { a = a + b; return a; }
+PSDR_HD float3& operator-=(float3& a, float3 b) { a = a - b; return a; }
+PSDR_HD float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+PSDR_HD float3 cross(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+PSDR_HD float sqnorm(float3 a) { return dot(a, a); }
+PSDR_HD float norm(float3 a) { return sqrtf(sqnorm(a)); }
+PSDR_HD float3 normalize(float3 a) { return a * (1.0f / sqrtf(sqnorm(a))); }
+PSDR_HD float3 xyz(float4 a) { return f3(a.x, a.y, a.z); }
+PSDR_HD float sel3(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+PSDR_HD float comp(float3 v, int k) { return sel3(v, k); }
+PSDR_HD bool finite3(float3 v) { return isfinite(sqnorm(v)); }
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kInvPi = 0.318309886183790671538f;
+constexpr float k2Pi = 6.28318530717958647692f;
+constexpr float kEps = 1e-5f;       // types.h:114 REAL_EPS
+constexpr float kTmin = 1e-3f;      // device_programs.cu:8 tmin of every trace
+
+// ------------------------------------------------------------------ PCG32 + TEA
+// One PCG32 stream per sample index (sampler.h:8-84), seeded through 4-round TEA.
+constexpr uint64_t kPcgState = 0x853c49e6748fea9bULL;
+constexpr uint64_t kPcgMult = 0x5851f42d4c957f2dULL;
+
+PSDR_HD uint64_t tea64(uint32_t v0, uint32_t v1) {
+  uint32_t sum = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    sum += 0x9e3779b9u;
+    v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + sum) ^ ((v1 >> 5) + 0xc8013ea4u);
+    v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + sum) ^ ((v0 >> 5) + 0x7e95761eu);
+  }
+  return (uint64_t)v0 + ((uint64_t)v1 << 32);
+}
+
+struct Rng {
+  uint64_t state, inc;
+  PSDR_HD uint32_t next(bool advance) {
+    uint64_t old = state;
+    if (advance) state = old * kPcgMult + inc;
+    uint32_t xs = (uint32_t)(((old >> 18) ^ old) >> 27);
+    uint32_t rot = (uint32_t)(old >> 59);
+    return (xs >> rot) | (xs << ((32u - rot) & 31u));
+  }
+  PSDR_HD float next_float(bool advance = true) {
+    uint32_t bits = (next(advance) >> 9) | 0x3f800000u;
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(bits) - 1.0f;
+#else
+    float f;
+    __builtin_memcpy(&f, &bits, 4);
+    return f - 1.0f;
+#endif
+  }
+};
+
+// sampler.h:11-17; `seed` != 0 shifts the stream index (an extension: 0 reproduces
+// the reference's streams).
+PSDR_HD Rng make_rng(uint64_t i) {
+  uint32_t a = (uint32_t)(i + kPcgState), b = (uint32_t)i;
+  uint64_t initstate = tea64(a, b), initseq = tea64(b, a);
+  Rng r;
+  r.state = 0;
+  r.inc = (initseq << 1) | 1u;
+  r.next(true);
+  r.state += initstate;
+  r.next(true);
+  return r;
+}
+
+// ------------------------------------------------------------------ scene records
+struct DevTex {
+  int kind;  // -1 none, 0 constant, 1 uv
+  int ch;
+  int h, w;
+  const float* data;
+  double* grad;  // fp64 accumulator with the same layout, or null
+};
+struct DevObj {
+  int mat;
+  int light;  // light index or -1
+  DevTex color, rough, normal;
+};
+struct DevLight {
+  int tri0, ntri;
+  float emit[3];
+  float area, inv_area, power;
+  double* grad_emit;  // 3 doubles or null
+};
+
+// Per-triangle shading record, 6 x float4 (96 B) in original triangle order:
+//  [0] p0.xyz, area   [1] p1.xyz, obj(bits)   [2] p2.xyz, uv0.x
+//  [3] n.xyz, uv0.y   [4] t.xyz, uv1.x        [5] uv1.y, uv2.x, uv2.y, 0
+// BVH node (BVH2, child boxes stored in the parent), 4 x float4 (64 B):
+//  [0] L.lo.xyz L.hi.x [1] L.hi.yz R.lo.xy [2] R.lo.z R.hi.xyz [3] left, right (int)
+// child >= 0: internal node; child < 0: leaf ~((first << 3) | (count-1)).
+// Leaf triangles, 3 x float4 (48 B) in BVH order: p0.xyz + id(bits), p1.xyz, p2.xyz.
+struct DevScene {
+  int ntri, nvert, nobj, nlight;
+  const float4* tri;
+  const int4* tri_v;       // global vertex ids (x,y,z) + object (w)
+  const float* verts;      // (nvert, 3)
+  const DevObj* objs;
+  const DevLight* lights;
+  const float* light_pmf;
+  const float* light_cmf;
+  const float* ltri_pmf;   // per-light triangle CDFs, indexed by tri - ltri_base
+  const float* ltri_cmf;
+  int ltri_base;
+  int edge_cap;
+  const int* n_edges;      // device scalar
+  const float4* edge;      // 4 x float4: (p0,len) (p1,out.x) (out.yz,nl.xy) (nl.z,nr)
+  const int2* edge_v;
+  const float* edge_pmf;
+  const float* edge_cmf;
+  int root;
+  const float4* nodes;
+  const float4* leaf;
+  double* grad_verts;      // (nvert, 3) or null
+  int* err;                // device error word (bit 0: traversal stack overflow)
+};
+
+// ------------------------------------------------------------------ discrete sampling
+// sampler.h:98-117 DiscreteSampler::sample_reuse with enoki::binary_search's fixed
+// floor(log2(n-1))+1 bisection steps; rescales s in place.
+PSDR_D int discrete_sample(const float* __restrict__ pmf, const float* __restrict__ cmf, int n, float& s,
+                           float& pdf) {
+  if (n <= 1) { pdf = 1.0f; return 0; }
+  int start = 0, end = n - 1;
+  int iters = 32 - __clz(end);
+  for (int it = 0; it < iters; ++it) {
+    int mid = (start + end) >> 1;
+    if (__ldg(cmf + mid) < s) start = min(mid + 1, end);
+    else end = mid;
+  }
+  pdf = __ldg(pmf + start);
+  float prev = start > 0 ? __ldg(cmf + start - 1) : 0.0f;
+  s = (s - prev) / pdf;
+  return start;
+}
+
+// ------------------------------------------------------------------ watertight test
+// Woop, Benthin & Wald (JCGT 2013). Every arithmetic step is an explicitly rounded
+// IEEE operation so the device result is bit-identical to the float oracle.
+struct RayPre {
+  float3 o;
+  int kx, ky, kz;
+  float Sx, Sy, Sz;
+};
+PSDR_D RayPre ray_pre(float3 o, float3 d) {
+  RayPre r;
+  r.o = o;
+  float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  int kx = kz + 1 == 3 ? 0 : kz + 1;
+  int ky = kx + 1 == 3 ? 0 : kx + 1;
+  float dz = sel3(d, kz);
+  if (dz < 0.0f) { int t = kx; kx = ky; ky = t; }
+  r.kx = kx; r.ky = ky; r.kz = kz;
+  r.Sx = __fdiv_rn(sel3(d, kx), dz);
+  r.Sy = __fdiv_rn(sel3(d, ky), dz);
+  r.Sz = __fdiv_rn(1.0f, dz);
+  return r;
+}
+PSDR_D bool tri_test(const RayPre& r, float3 p0, float3 p1, float3 p2, float tmin, float tmax, float& t,
+                     float& b1, float& b2) {
+  float3 A = f3(__fsub_rn(p0.x, r.o.x), __fsub_rn(p0.y, r.o.y), __fsub_rn(p0.z, r.o.z));
+  float3 B = f3(__fsub_rn(p1.x, r.o.x), __fsub_rn(p1.y, r.o.y), __fsub_rn(p1.z, r.o.z));
+  float3 C = f3(__fsub_rn(p2.x, r.o.x), __fsub_rn(p2.y, r.o.y), __fsub_rn(p2.z, r.o.z));
+  float Akz = sel3(A, r.kz), Bkz = sel3(B, r.kz), Ckz = sel3(C, r.kz);
+  float Ax = __fsub_rn(sel3(A, r.kx), __fmul_rn(r.Sx, Akz)), Ay = __fsub_rn(sel3(A, r.ky), __fmul_rn(r.Sy, Akz));
+  float Bx = __fsub_rn(sel3(B, r.kx), __fmul_rn(r.Sx, Bkz)), By = __fsub_rn(sel3(B, r.ky), __fmul_rn(r.Sy, Bkz));
+  float Cx = __fsub_rn(sel3(C, r.kx), __fmul_rn(r.Sx, Ckz)), Cy = __fsub_rn(sel3(C, r.ky), __fmul_rn(r.Sy, Ckz));
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float det = __fadd_rn(__fadd_rn(U, V), W);
+  if (det == 0.0f) return false;
+  float Az = __fmul_rn(r.Sz, Akz), Bz = __fmul_rn(r.Sz, Bkz), Cz = __fmul_rn(r.Sz, Ckz);
+  float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+  float tt = __fdiv_rn(T, det);
+  if (!(tt > tmin && tt <= tmax)) return false;
+  t = tt;
+  b1 = __fdiv_rn(V, det);
+  b2 = __fdiv_rn(W, det);
+  return true;
+}
+
+// ------------------------------------------------------------------ traversal
+constexpr int kStack = 64;
+
+struct HitRec {
+  int tri;
+  float b1, b2, t;
+};
+
+PSDR_D float safe_inv(float d) { return 1.0f / (fabsf(d) > 1e-30f ? d : copysignf(1e-30f, d)); }
+
+// Closest hit in (tmin, tmax], ties broken by the smaller triangle id. Node boxes are
+// expanded at build time and the cull bound is relaxed by 1e-5 relative so that no
+// triangle the exact test would accept is culled (the KAT checks this against brute
+// force on every ray).
+PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, float tmax) {
+  RayPre rp = ray_pre(o, d);
+  const float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+  const float3 oi = f3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+  HitRec h;
+  h.tri = -1; h.b1 = 0.f; h.b2 = 0.f; h.t = tmax;
+  int stack[kStack];
+  int sp = 0;
+  int node = sc.root;
+  if (sc.ntri <= 0) return h;
+  while (true) {
+    if (node >= 0) {
+      const float4* nd = sc.nodes + 4 * (size_t)node;
+      const float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
+      const int4 e = __ldg(reinterpret_cast<const int4*>(nd + 3));
+      const float cull = h.t * 1.00001f + 1e-12f;
+      // left child box
+      float l0x = fmaf(a.x, inv.x, -oi.x), l1x = fmaf(a.w, inv.x, -oi.x);
+      float l0y = fmaf(a.y, inv.y, -oi.y), l1y = fmaf(b.x, inv.y, -oi.y);
+      float l0z = fmaf(a.z, inv.z, -oi.z), l1z = fmaf(b.y, inv.z, -oi.z);
+      float ln = fmaxf(fmaxf(fminf(l0x, l1x), fminf(l0y, l1y)), fmaxf(fminf(l0z, l1z), tmin));
+      float lf = fminf(fminf(fmaxf(l0x, l1x), fmaxf(l0y, l1y)), fminf(fmaxf(l0z, l1z), cull));
+      // right child box
+      float r0x = fmaf(b.z, inv.x, -oi.x), r1x = fmaf(c.y, inv.x, -oi.x);
+      float r0y = fmaf(b.w, inv.y, -oi.y), r1y = fmaf(c.z, inv.y, -oi.y);
+      float r0z = fmaf(c.x, inv.z, -oi.z), r1z = fmaf(c.w, inv.z, -oi.z);
+      float rn = fmaxf(fmaxf(fminf(r0x, r1x), fminf(r0y, r1y)), fmaxf(fminf(r0z, r1z), tmin));
+      float rf = fminf(fminf(fmaxf(r0x, r1x), fmaxf(r0y, r1y)), fminf(fmaxf(r0z, r1z), cull));
+      const bool hl = ln <= lf * 1.0000005f, hr = rn <= rf * 1.0000005f;
+      if (hl && hr) {
+        int nearc = ln <= rn ? e.x : e.y, farc = ln <= rn ? e.y : e.x;
+        if (sp < kStack) stack[sp++] = farc;
+        else atomicOr(sc.err, 1);
+        node = nearc;
+      } else if (hl) {
+        node = e.x;
+      } else if (hr) {
+        node = e.y;
+      } else {
+        if (sp == 0) break;
+        node = stack[--sp];
+      }
+    } else {
+      const int code = ~node;
+      const int first = code >> 3, cnt = (code & 7) + 1;
+      for (int k = 0; k < cnt; ++k) {
+        const float4* lt = sc.leaf + 3 * (size_t)(first + k);
+        const float4 q0 = __ldg(lt), q1 = __ldg(lt + 1), q2 = __ldg(lt + 2);
+        float tt, b1, b2;
+        if (tri_test(rp, xyz(q0), xyz(q1), xyz(q2), tmin, h.t, tt, b1, b2)) {
+          const int id = __float_as_int(q0.w);
+          if (tt < h.t || h.tri < 0 || id < h.tri) { h.t = tt; h.tri = id; h.b1 = b1; h.b2 = b2; }
+        }
+      }
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  }
+  return h;
+}
+
+// ------------------------------------------------------------------ surface points
+// scene.cc:106-161 Scene::hit: the point is re-formed from the triangle and the
+// barycentrics; the normal and tangent face the incoming ray (is_front flip).
+struct Surf {
+  float3 p, n, t;
+  float u, v;
+  float area;
+  float sqd;     // squared distance to the ray origin
+  int tri, obj, light;
+  bool valid, is_light, front;
+};
+
+PSDR_D Surf make_surf(const DevScene& sc, int tri, float b1, float b2, float3 org) {
+  Surf s;
+  s.valid = tri >= 0;
+  s.tri = tri;
+  s.is_light = false;
+  s.light = -1;
+  s.obj = -1;
+  if (!s.valid) return s;
+  const float4* r = sc.tri + 6 * (size_t)tri;
+  const float4 q0 = __ldg(r), q1 = __ldg(r + 1), q2 = __ldg(r + 2), q3 = __ldg(r + 3), q4 = __ldg(r + 4),
+               q5 = __ldg(r + 5);
+  const float3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2);
+  s.p = p0 + b1 * (p1 - p0) + b2 * (p2 - p0);
+  const float u0 = q2.w, v0 = q3.w, u1 = q4.w, v1 = q5.x, u2 = q5.y, v2 = q5.z;
+  s.u = u0 + b1 * (u1 - u0) + b2 * (u2 - u0);
+  s.v = v0 + b1 * (v1 - v0) + b2 * (v2 - v0);
+  const float3 wun = s.p - org;
+  s.sqd = sqnorm(wun);
+  const float3 wi = -normalize(wun);
+  const float3 n = xyz(q3), t = xyz(q4);
+  s.front = dot(wi, n) > 0.0f;
+  s.n = s.front ? n : -n;
+  s.t = s.front ? t : -t;
+  s.area = q0.w;
+  s.obj = __float_as_int(q1.w);
+  s.light = __ldg(&sc.objs[s.obj].light);
+  s.is_light = s.light >= 0;
+  return s;
+}
+
+// texture.h:65-74 UVTexture::at_nearest on the caller's (H,W,C) tensor with the row
+// flip of torch_psdr.py:250; returns the element offset of the texel.
+PSDR_D int texel_offset(const DevTex& tx, float u, float v) {
+  if (tx.kind != 1) return 0;
+  float uu = rintf(fminf(fmaxf(u * (float)tx.w - 0.5f, -1.0f), (float)tx.w));
+  float vv = rintf(fminf(fmaxf(v * (float)tx.h - 0.5f, -1.0f), (float)tx.h));
+  int u0 = min(max((int)uu, 0), tx.w - 1);
+  int v0 = min(max((int)vv, 0), tx.h - 1);
+  return tx.ch * ((tx.h - 1 - v0) * tx.w + u0);
+}
+PSDR_D float3 tex_rgb(const DevTex& tx, int off) {
+  if (tx.kind < 0) return f3(0.f, 0.f, 0.f);
+  const float* p = tx.data + off;
+  if (tx.ch == 1) { float x = __ldg(p); return f3(x, x, x); }
+  return f3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+}
+
+// diffuse_material.cc:3-30: cosine-weighted direction in the (T, N x T, N) frame.
+PSDR_D float3 diffuse_dir(float3 N, float3 T, float ru, float rv, float& cos_theta, float& sin_theta,
+                          float& sphi, float& cphi) {
+  const float3 B = cross(N, T);
+  cos_theta = ru > 0.f ? sqrtf(ru) : 0.f;
+  sin_theta = (1.0f - ru) > 0.f ? sqrtf(1.0f - ru) : 0.f;
+  sincosf(rv * k2Pi, &sphi, &cphi);
+  const float uu = cphi * sin_theta, vv = sphi * sin_theta;
+  return normalize(T * uu + B * vv + N * cos_theta);
+}
+
+PSDR_D float mis_power(float w1, float w2, float n1, float n2) {
+  const float a = (n1 * w1) * (n1 * w1), b = (n2 * w2) * (n2 * w2);
+  return a / (a + b);
+}
+
+// emitter.cc:29-59 AreaLight::sample_light_point (triangle by area, sqrt warp).
+struct LightSample {
+  float3 y;
+  float pdf;     // pdf_light * pdf_choose (detached)
+  int light;
+  int tri;       // global triangle id the point lies on
+  float su, sv;  // y = p0 + (p1-p0) su + (p2-p0) sv
+};
+PSDR_D LightSample sample_light(const DevScene& sc, float rx, float ry) {
+  LightSample ls;
+  float pch = 1.0f;
+  int l = discrete_sample(sc.light_pmf, sc.light_cmf, sc.nlight, rx, pch);
+  const DevLight& L = sc.lights[l];
+  float ptri;
+  const int base = L.tri0 - sc.ltri_base;
+  int k = discrete_sample(sc.ltri_pmf + base, sc.ltri_cmf + base, L.ntri, rx, ptri);
+  const int tri = L.tri0 + k;
+  const float4* r = sc.tri + 6 * (size_t)tri;
+  const float3 p0 = xyz(__ldg(r)), p1 = xyz(__ldg(r + 1)), p2 = xyz(__ldg(r + 2));
+  const float sq = ry > 0.f ? sqrtf(ry) : 0.f;
+  ls.su = rx * sq;
+  ls.sv = 1.0f - sq;
+  ls.y = p0 + (p1 - p0) * ls.su + (p2 - p0) * ls.sv;
+  ls.pdf = L.inv_area * pch;
+  ls.light = l;
+  ls.tri = tri;
+  return ls;
+}
+
+}  // namespace psdr

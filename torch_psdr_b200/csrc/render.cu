@@ -1,0 +1,1386 @@
+// render.cu -- wavefront path tracing, path-replay adjoint and edge sampling.
+//
+// Forward (path_integrator.cc:80-186 trace2light, :355-372 render_interior,
+// camera.h:75-87 Film::add) as wavefront kernels over a tile of path samples:
+//   k_camera  : sampler stream, pixel jitter, camera ray, primary closest hit
+//   per depth : k_shade (hit-light test, light / BSDF / indirect sampling, ray write
+//               with warp-aggregated compaction) -> k_trace (closest hit per ray)
+//               -> k_accum (NEE + MIS contributions, throughput, compaction)
+//   k_film    : per-pixel average of its spp paths (deterministic, no atomics).
+// Backward (Wrap2torch.backward + enoki reverse sweep, torch_psdr.py:48-72): the tile
+// is re-traced from the stored seeds recording only hit records, then k_adjoint
+// replays every path's sampler stream and applies the hand-written adjoint of the
+// estimator, scattering into fp64 accumulators (warp-aggregated where a warp shares
+// the target). Primary-edge (path_integrator.cc:188-272) and direct-edge (:274-353)
+// boundary terms follow the reference formulas (PSDR_EST_REFERENCE).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "render.h"
+
+namespace psdr {
+
+// ------------------------------------------------------------------ helpers
+PSDR_D unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Warp-aggregated append: all lanes of the warp must call it together.
+PSDR_D int warp_append(int* counter, bool pred) {
+  const unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (!m) return -1;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return pred ? base + __popc(m & lanemask_lt()) : -1;
+}
+
+PSDR_D void xform_pos(const float* m, float3 p, float3& out) {
+  const float w = m[12] * p.x + m[13] * p.y + m[14] * p.z + m[15];
+  out = f3((m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3]) / w, (m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7]) / w,
+           (m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]) / w);
+}
+PSDR_D float3 xform_dir(const float* m, float3 p) {
+  return f3(m[0] * p.x + m[1] * p.y + m[2] * p.z, m[4] * p.x + m[5] * p.y + m[6] * p.z,
+            m[8] * p.x + m[9] * p.y + m[10] * p.z);
+}
+
+// camera.h:260-276 gen_camera_ray_with_point: visibility in the raster + pixel.
+PSDR_D bool project(const DevView& V, float3 pt, int& px, int& py) {
+  float3 pc, p;
+  xform_pos(V.w2c, pt, pc);
+  xform_pos(V.c2r, pc, p);
+  px = (int)floorf(p.x);
+  py = (int)floorf(p.y);
+  return pc.z < 0.f && p.x > 0.f && p.x < (float)V.W && p.y > 0.f && p.y < (float)V.H;
+}
+
+PSDR_D int find_view(const DevView* __restrict__ views, int nv, long long g) {
+  int lo = 0, hi = nv - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (views[mid].sample_off <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+PSDR_D int find_view_pix(const DevView* __restrict__ views, int nv, long long g) {
+  int lo = 0, hi = nv - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (views[mid].pix_off <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+PSDR_D float4 hit4(const HitRec& h) { return make_float4(__int_as_float(h.tri), h.b1, h.b2, h.t); }
+
+PSDR_D void atomic_add3(double* p, float3 v) {
+  atomicAdd(p, (double)v.x);
+  atomicAdd(p + 1, (double)v.y);
+  atomicAdd(p + 2, (double)v.z);
+}
+
+// ------------------------------------------------------------------ camera kernel
+template <int MODE>
+__global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict__ scenes,
+                                                const DevView* __restrict__ views, Tile tile) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (tile.n + 31) & ~31;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool alive = false;
+    if (s < tile.n) {
+      const long long g = tile.begin + s;
+      const int v = find_view(views, w.nviews, g);
+      const DevView& V = views[v];
+      const DevScene& sc = scenes[V.scene];
+      const long long i = g - V.sample_off;
+      Rng rng = make_rng((unsigned long long)i + w.seed);
+      const float jx = rng.next_float(), jy = rng.next_float();
+      const int pix = V.spp > 1 ? (int)(i / V.spp) : (int)i;
+      const int x = pix % V.W, y = pix / V.W;
+      float3 pc;
+      xform_pos(V.r2c, f3(jx + (float)x, jy + (float)y, 1.0f), pc);
+      const float3 d = normalize(xform_dir(V.c2w, pc));
+      const HitRec h = trace_closest(sc, V.pos, d, kTmin, INFINITY);
+      w.rs[s] = rng.state;
+      w.ri[s] = rng.inc;
+      w.view[s] = v;
+      w.pix[s] = pix;
+      w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
+      w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      w.cur[s] = hit4(h);
+      w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      if (MODE == MODE_REPLAY) w.rec[(size_t)s * w.rec_stride] = hit4(h);
+      alive = h.tri >= 0;
+    }
+    const int k = warp_append(&w.cnt[0], alive);
+    if (alive) w.q0[k] = s;
+  }
+}
+
+// ------------------------------------------------------------------ shade kernel
+// Hit-light test and all samples of one depth; rays are written to the shaded slot.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict__ scenes,
+                                               const DevView* __restrict__ views, int d) {
+  const int* qin = (d & 1) ? w.q1 : w.q0;
+  const int n = w.cnt[2 * d];
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const bool last = d == w.D - 1;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n32; q += stride) {
+    bool go = false;
+    int s = -1;
+    Surf x;
+    const DevScene* sc = nullptr;
+    if (q < n) {
+      s = qin[q];
+      sc = &scenes[views[w.view[s]].scene];
+      const float4 c = w.cur[s];
+      x = make_surf(*sc, __float_as_int(c.x), c.y, c.z, xyz(w.org[s]));
+      if (x.is_light) {
+        if (MODE == MODE_FWD && w.light_vis && d == 0) {
+          const DevLight& Lt = sc->lights[x.light];
+          float4 L = w.L[s];
+          const float4 T = w.T[s];
+          L.x += T.x * Lt.emit[0]; L.y += T.y * Lt.emit[1]; L.z += T.z * Lt.emit[2];
+          w.L[s] = L;
+        }
+      } else {
+        go = true;
+      }
+    }
+    const int k = warp_append(&w.cnt[2 * d + 1], go);
+    if (!go) continue;
+    w.qs[k] = s;
+    Rng rng{w.rs[s], w.ri[s]};
+    const size_t base = (size_t)k * w.R;
+    for (int i = 0; i < w.nL; ++i) {
+      const float rx = rng.next_float(), ry = rng.next_float();
+      const LightSample ls = sample_light(*sc, rx, ry);
+      const float3 dv = ls.y - x.p;
+      const float3 dir = normalize(dv);
+      const float dist = norm(dv);
+      w.ro[base + i] = make_float4(x.p.x, x.p.y, x.p.z, dist * 1.0001f + 4e-3f);
+      w.rd[base + i] = make_float4(dir.x, dir.y, dir.z, __int_as_float(ls.light));
+      w.ra[base + i] = make_float4(ls.y.x, ls.y.y, ls.y.z, ls.pdf);
+    }
+    for (int j = 0; j < w.nB; ++j) {
+      const float rx = rng.next_float(), ry = rng.next_float();
+      float ct, st, sp, cp;
+      const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+      w.ro[base + w.nL + j] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
+      w.rd[base + w.nL + j] = make_float4(wo.x, wo.y, wo.z, 0.f);
+      w.ra[base + w.nL + j] = make_float4(ct, 0.f, 0.f, 0.f);
+    }
+    {
+      const float rx = rng.next_float(), ry = rng.next_float();
+      if (!last) {
+        float ct, st, sp, cp;
+        const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+        const int r = w.nL + w.nB;
+        w.ro[base + r] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
+        w.rd[base + r] = make_float4(wo.x, wo.y, wo.z, 0.f);
+        w.ra[base + r] = make_float4(ct, 0.f, 0.f, 0.f);
+      }
+    }
+    w.rs[s] = rng.state;
+  }
+}
+
+// ------------------------------------------------------------------ trace kernel
+__global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict__ scenes,
+                                               const DevView* __restrict__ views, int d) {
+  const int nk = w.cnt[2 * d + 1];
+  const int Rd = (d == w.D - 1) ? w.R - 1 : w.R;
+  const long long total = (long long)nk * Rd;
+  const int stride = gridDim.x * blockDim.x;
+  for (long long idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+    const int k = (int)(idx / Rd);
+    const int r = (int)(idx - (long long)k * Rd);
+    const size_t slot = (size_t)k * w.R + r;
+    const int s = w.qs[k];
+    const DevScene& sc = scenes[views[w.view[s]].scene];
+    const float4 o = w.ro[slot], dd = w.rd[slot];
+    const HitRec h = trace_closest(sc, xyz(o), xyz(dd), kTmin, o.w);
+    w.hit[slot] = hit4(h);
+  }
+}
+
+// ------------------------------------------------------------------ accumulate kernel
+template <int MODE>
+__global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict__ scenes,
+                                               const DevView* __restrict__ views, int d) {
+  const int n = w.cnt[2 * d + 1];
+  int* qout = (d & 1) ? w.q0 : w.q1;
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const bool last = d == w.D - 1;
+  const float fL = (float)w.nL, fB = (float)w.nB;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n32; k += stride) {
+    bool cont = false;
+    int s = -1;
+    if (k < n) {
+      s = w.qs[k];
+      const DevScene& sc = scenes[views[w.view[s]].scene];
+      const size_t base = (size_t)k * w.R;
+      const float4 c = w.cur[s];
+      const Surf x = make_surf(sc, __float_as_int(c.x), c.y, c.z, xyz(w.org[s]));
+      if (MODE == MODE_REPLAY) {
+        float4* rec = w.rec + (size_t)s * w.rec_stride + 1 + (size_t)d * w.R;
+        const int Rd = last ? w.R - 1 : w.R;
+        for (int r = 0; r < Rd; ++r) rec[r] = w.hit[base + r];
+        if (!last) {
+          const float4 h = w.hit[base + w.nL + w.nB];
+          if (__float_as_int(h.x) >= 0) {
+            w.cur[s] = h;
+            w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
+            cont = true;
+          }
+        }
+      } else {
+        float4 T4 = w.T[s], L4 = w.L[s];
+        float3 T = xyz(T4), L = xyz(L4);
+        const DevObj& ob = sc.objs[x.obj];
+        const float3 bsdf = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v)) * kInvPi;
+        for (int i = 0; i < w.nL; ++i) {
+          const float4 h = w.hit[base + i];
+          const int tri = __float_as_int(h.x);
+          if (tri < 0) continue;
+          const float4 dd = w.rd[base + i], aux = w.ra[base + i];
+          const float3 dir = xyz(dd);
+          const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
+          if (!(q.is_light && sqnorm(q.p - xyz(aux)) < kEps)) continue;
+          const DevLight& Lt = sc.lights[__float_as_int(dd.w)];
+          const float tmp = dot(q.n, -dir) / q.sqd;
+          const float G = dot(x.n, dir) * tmp;
+          const float pdf_l = aux.w;
+          float wgt = 1.0f / fL;
+          if (w.nB > 0) wgt *= mis_power(pdf_l, dot(x.n, dir) * kInvPi * tmp, fL, fB);
+          const float sc_ = G / pdf_l * wgt;
+          L += mul(T, f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z)) * sc_;
+        }
+        for (int j = 0; j < w.nB; ++j) {
+          const float4 h = w.hit[base + w.nL + j];
+          const int tri = __float_as_int(h.x);
+          if (tri < 0) continue;
+          const float3 wo = xyz(w.rd[base + w.nL + j]);
+          const float ct = w.ra[base + w.nL + j].x;
+          const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
+          if (!q.is_light) continue;
+          const DevLight& Lt = sc.lights[q.light];
+          const float tmp = dot(q.n, -wo) / q.sqd;
+          const float G = dot(x.n, wo) * tmp;
+          const float pdf_b = ct * kInvPi * tmp;
+          float wgt = 1.0f / fB;
+          if (w.nL > 0) wgt *= mis_power(pdf_b, __ldg(sc.light_pmf + q.light) * Lt.inv_area, fB, fL);
+          const float sc_ = G / pdf_b * wgt;
+          L += mul(T, f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z)) * sc_;
+        }
+        if (!last) {
+          const int r = w.nL + w.nB;
+          const float4 h = w.hit[base + r];
+          const int tri = __float_as_int(h.x);
+          if (tri >= 0) {
+            const float3 wo = xyz(w.rd[base + r]);
+            const float ct = w.ra[base + r].x;
+            const Surf nx = make_surf(sc, tri, h.y, h.z, x.p);
+            const float tmp = dot(nx.n, -wo) / nx.sqd;
+            const float G = dot(x.n, wo) * tmp;
+            const float pdf = ct * kInvPi * tmp;
+            T = mul(T, bsdf) * (G / pdf);
+            w.cur[s] = h;
+            w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
+            cont = true;
+          }
+        }
+        w.T[s] = make_float4(T.x, T.y, T.z, 0.f);
+        w.L[s] = make_float4(L.x, L.y, L.z, 0.f);
+      }
+    }
+    const int kk = warp_append(&w.cnt[2 * (d + 1)], cont);
+    if (cont) qout[kk] = s;
+  }
+}
+
+// ------------------------------------------------------------------ film
+// Per pixel: sum of its spp path radiances (non-finite paths count as 0), / spp,
+// then the n_pass average of identical passes (path_integrator.cc:381-406).
+__global__ void k_film(WF w, const DevView* __restrict__ views, Tile tile, int n_pass, float* samples_out) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < tile.npix; p += gridDim.x * blockDim.x) {
+    const long long gp = tile.pix_begin + p;
+    const int v = find_view_pix(views, w.nviews, gp);
+    const DevView& V = views[v];
+    const long long lp = gp - V.pix_off;
+    const long long s0 = V.sample_off + lp * V.spp - tile.begin;
+    float3 acc = f3(0.f, 0.f, 0.f);
+    for (int k = 0; k < V.spp; ++k) {
+      const long long s = s0 + k;
+      float3 L = xyz(w.L[s]);
+      if (!finite3(L) || __float_as_int(w.cur[s].x) == -2) L = f3(0.f, 0.f, 0.f);
+      if (samples_out) {
+        samples_out[3 * (lp * V.spp + k)] = L.x;
+        samples_out[3 * (lp * V.spp + k) + 1] = L.y;
+        samples_out[3 * (lp * V.spp + k) + 2] = L.z;
+      }
+      acc += L;
+    }
+    float3 val = acc / (float)V.spp;
+    if (n_pass > 1) {
+      float3 a = f3(0.f, 0.f, 0.f);
+      for (int i = 0; i < n_pass; ++i) a += val;
+      val = a / (float)n_pass;
+    }
+    if (V.image) {
+      float* o = V.image + 3 * lp;
+      o[0] = val.x; o[1] = val.y; o[2] = val.z;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ adjoint helpers
+struct SurfAdj {
+  float3 p, n, t;
+  float area;
+};
+PSDR_D SurfAdj zero_adj() {
+  SurfAdj a;
+  a.p = a.n = a.t = f3(0.f, 0.f, 0.f);
+  a.area = 0.f;
+  return a;
+}
+
+// Light vertices accumulated in registers (single area light with <= 8 vertices).
+struct HotAcc {
+  int lv0, nlv;   // vertex range of the light mesh; nlv = 0 disables
+  bool emit_hot;  // single light: accumulate its emission gradient in e[]
+  float g[kMaxLightVerts * 3];
+  float e[3];
+};
+
+PSDR_D void add_emit(HotAcc& hot, double* grad_emit, float3 a) {
+  if (!grad_emit) return;
+  if (hot.emit_hot) { hot.e[0] += a.x; hot.e[1] += a.y; hot.e[2] += a.z; }
+  else atomic_add3(grad_emit, a);
+}
+
+PSDR_D void add_vertex(const DevScene& sc, HotAcc& hot, int v, float3 a) {
+  if (!sc.grad_verts) return;
+  const int rel = v - hot.lv0;
+  if (hot.nlv > 0 && rel >= 0 && rel < hot.nlv) {
+#pragma unroll
+    for (int k = 0; k < kMaxLightVerts; ++k)
+      if (k == rel) { hot.g[3 * k] += a.x; hot.g[3 * k + 1] += a.y; hot.g[3 * k + 2] += a.z; }
+    return;
+  }
+  atomic_add3(sc.grad_verts + 3 * (size_t)v, a);
+}
+
+// Adjoint of Scene::hit's surface attributes (point, flipped normal and tangent,
+// area) w.r.t. the triangle vertices (mesh.cc:27-67; area via |cross|/2, the same
+// function as Heron's formula).
+PSDR_D void surf_vertex_adj(const DevScene& sc, int tri, float b1, float b2, bool front, const SurfAdj& a,
+                            float3& g0, float3& g1, float3& g2) {
+  const float4* r = sc.tri + 6 * (size_t)tri;
+  const float4 q0 = __ldg(r), q1 = __ldg(r + 1), q2 = __ldg(r + 2), q3 = __ldg(r + 3), q5 = __ldg(r + 5);
+  const float3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2);
+  const float sgn = front ? 1.f : -1.f;
+  g0 = a.p * (1.f - b1 - b2);
+  g1 = a.p * b1;
+  g2 = a.p * b2;
+  const float3 c = p1 - p0, b = p0 - p2;
+  const float3 cr = cross(c, b);
+  const float crn = norm(cr);
+  const float3 n = cr / crn;
+  const float3 an = a.n * sgn;
+  float3 acr = (an - n * dot(n, an)) / crn + n * (0.5f * a.area);
+  // tangent
+  const float du1y = q5.x - q3.w, du2y = q5.z - q3.w;
+  const float3 tw = c * du2y + b * du1y;
+  const float twn = norm(tw);
+  const float3 t = tw / twn;
+  const float3 at = a.t * sgn;
+  const float3 atw = (at - t * dot(t, at)) / twn;
+  float3 ac = cross(b, acr) + atw * du2y;
+  float3 ab = cross(acr, c) + atw * du1y;
+  g1 += ac; g0 -= ac;
+  g0 += ab; g2 -= ab;
+}
+
+PSDR_D void scatter_surf(const DevScene& sc, HotAcc& hot, int tri, float b1, float b2, bool front,
+                         const SurfAdj& a) {
+  if (!sc.grad_verts) return;
+  float3 g0, g1, g2;
+  surf_vertex_adj(sc, tri, b1, b2, front, a, g0, g1, g2);
+  const int4 tv = __ldg(sc.tri_v + tri);
+  add_vertex(sc, hot, tv.x, g0);
+  add_vertex(sc, hot, tv.y, g1);
+  add_vertex(sc, hot, tv.z, g2);
+}
+
+PSDR_D void scatter_tex(const DevTex& tx, int off, float3 a, bool /*unused*/) {
+  if (!tx.grad) return;
+  if (tx.ch == 1) atomicAdd(tx.grad + off, (double)(a.x + a.y + a.z));
+  else atomic_add3(tx.grad + off, a);
+}
+
+// Adjoint of G = dot(Nx, w) dot(Nq, -w) / d2 with d2 = |q - x|^2, w given.
+PSDR_D void geom_adj(float adjG, float3 Nx, float3 Nq, float3 w, float3 xp, float3 qp, float d2, float G,
+                     SurfAdj& ax, SurfAdj& aq, float3& adj_w) {
+  const float a = dot(Nx, w), bq = -dot(Nq, w);
+  const float adj_a = adjG * bq / d2, adj_b = adjG * a / d2, adj_d2 = -adjG * G / d2;
+  ax.n += w * adj_a;
+  aq.n += w * (-adj_b);
+  adj_w = Nx * adj_a - Nq * adj_b;
+  const float3 dq = (qp - xp) * (2.f * adj_d2);
+  aq.p += dq;
+  ax.p -= dq;
+}
+
+// Adjoint of wo = normalize(u T + v B + ct N), B = N x T, w.r.t. N and T.
+PSDR_D void dir_adj(float3 adj_wo, float3 wo, float3 N, float3 T, float u, float v, float ct, SurfAdj& ax) {
+  const float3 B = cross(N, T);
+  const float3 m = T * u + B * v + N * ct;
+  const float3 am = (adj_wo - wo * dot(wo, adj_wo)) / norm(m);
+  const float3 aB = am * v;
+  ax.t += am * u + cross(aB, N);
+  ax.n += am * ct + cross(T, aB);
+}
+
+struct DepthVals {
+  float3 C, beta;
+  bool has_next;
+};
+
+// One depth of trace2light, recomputed from the sampler stream and the hit records.
+// ADJ=false returns the contribution C and the throughput factor beta; ADJ=true
+// back-propagates adjC / adjB into the surfaces, the texture, the emission and the
+// light vertices (carry = adjoint of the next vertex, passed to the next depth).
+template <bool ADJ>
+PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng& rng, const float4* rec, bool last,
+                            float3 adjC, float3 adjB, SurfAdj& ax, SurfAdj& carry, HotAcc& hot, float3& adj_tex) {
+  DepthVals out;
+  out.C = f3(0.f, 0.f, 0.f);
+  out.beta = f3(0.f, 0.f, 0.f);
+  out.has_next = false;
+  const float fL = (float)w.nL, fB = (float)w.nB;
+  const DevObj& ob = sc.objs[x.obj];
+  const float3 tex = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v));
+  const float3 bsdf = tex * kInvPi;
+  for (int i = 0; i < w.nL; ++i) {
+    const float rx = rng.next_float(), ry = rng.next_float();
+    const LightSample ls = sample_light(sc, rx, ry);
+    const float4 h = rec[i];
+    const int tri = __float_as_int(h.x);
+    if (tri < 0) continue;
+    const float3 rv = ls.y - x.p;
+    const float3 dir = normalize(rv);
+    const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
+    if (!(q.is_light && sqnorm(q.p - ls.y) < kEps)) continue;
+    const DevLight& Lt = sc.lights[ls.light];
+    const float3 emit = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+    const float tmp = dot(q.n, -dir) / q.sqd;
+    const float G = dot(x.n, dir) * tmp;
+    float wgt = 1.0f / fL;
+    if (w.nB > 0) wgt *= mis_power(ls.pdf, dot(x.n, dir) * kInvPi * tmp, fL, fB);
+    const float k = G / ls.pdf * wgt;
+    const float3 eb = mul(emit, bsdf);
+    if (!ADJ) {
+      out.C += eb * k;
+    } else {
+      const float3 av = adjC * wgt;
+      const float s_ = G / ls.pdf;
+      const float3 ae = mul(av, bsdf) * s_;
+      add_emit(hot, sc.lights[ls.light].grad_emit, ae);
+      adj_tex += mul(av, emit) * (s_ * kInvPi);
+      const float adj_gam = dot(av, eb) / ls.pdf;
+      SurfAdj aq = zero_adj();
+      aq.area = adj_gam * G / q.area;
+      float3 adj_dir;
+      geom_adj(adj_gam, x.n, q.n, dir, x.p, q.p, q.sqd, G, ax, aq, adj_dir);
+      const float3 ar = (adj_dir - dir * dot(dir, adj_dir)) / norm(rv);
+      ax.p -= ar;
+      // light sample point y = p0 + (p1-p0) su + (p2-p0) sv
+      if (sc.grad_verts) {
+        const int4 tv = __ldg(sc.tri_v + ls.tri);
+        add_vertex(sc, hot, tv.x, ar * (1.f - ls.su - ls.sv));
+        add_vertex(sc, hot, tv.y, ar * ls.su);
+        add_vertex(sc, hot, tv.z, ar * ls.sv);
+      }
+      scatter_surf(sc, hot, tri, h.y, h.z, q.front, aq);
+    }
+  }
+  for (int j = 0; j < w.nB; ++j) {
+    const float rx = rng.next_float(), ry = rng.next_float();
+    float ct, st, sp, cp;
+    const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+    const float4 h = rec[w.nL + j];
+    const int tri = __float_as_int(h.x);
+    if (tri < 0) continue;
+    const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
+    if (!q.is_light) continue;
+    const DevLight& Lt = sc.lights[q.light];
+    const float3 emit = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+    const float tmp = dot(q.n, -wo) / q.sqd;
+    const float G = dot(x.n, wo) * tmp;
+    const float pdf_b = ct * kInvPi * tmp;
+    float wgt = 1.0f / fB;
+    if (w.nL > 0) wgt *= mis_power(pdf_b, __ldg(sc.light_pmf + q.light) * Lt.inv_area, fB, fL);
+    const float3 eb = mul(emit, bsdf);
+    if (!ADJ) {
+      out.C += eb * (G / pdf_b * wgt);
+    } else {
+      const float3 av = adjC * wgt;
+      const float s_ = G / pdf_b;
+      const float3 ae = mul(av, bsdf) * s_;
+      add_emit(hot, Lt.grad_emit, ae);
+      adj_tex += mul(av, emit) * (s_ * kInvPi);
+      const float adj_gam = dot(av, eb) / pdf_b;
+      SurfAdj aq = zero_adj();
+      aq.area = adj_gam * G / q.area;
+      float3 adj_wo;
+      geom_adj(adj_gam, x.n, q.n, wo, x.p, q.p, q.sqd, G, ax, aq, adj_wo);
+      dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+      scatter_surf(sc, hot, tri, h.y, h.z, q.front, aq);
+    }
+  }
+  {
+    const float rx = rng.next_float(), ry = rng.next_float();
+    if (!last) {
+      float ct, st, sp, cp;
+      const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+      const float4 h = rec[w.nL + w.nB];
+      const int tri = __float_as_int(h.x);
+      if (tri >= 0) {
+        out.has_next = true;
+        const Surf nx = make_surf(sc, tri, h.y, h.z, x.p);
+        const float tmp = dot(nx.n, -wo) / nx.sqd;
+        const float G = dot(x.n, wo) * tmp;
+        const float pdf = ct * kInvPi * tmp;
+        const float s_ = G / pdf;
+        if (!ADJ) {
+          out.beta = bsdf * s_;
+        } else {
+          adj_tex += adjB * (s_ * kInvPi);
+          const float adj_gam = dot(adjB, bsdf) / pdf;
+          carry = zero_adj();
+          carry.area = adj_gam * G / nx.area;
+          float3 adj_wo;
+          geom_adj(adj_gam, x.n, nx.n, wo, x.p, nx.p, nx.sqd, G, ax, carry, adj_wo);
+          dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+        }
+      }
+    }
+  }
+  return out;
+}
+
+
+// Warp-aggregated scatter of a surface adjoint: reduced over the warp when every
+// lane targets the same triangle of the same scene (the spp samples of a pixel).
+PSDR_D void scatter_surf_warp(const DevScene* scp, HotAcc& hot, int tri, float b1, float b2, bool front,
+                              const SurfAdj& a, bool active) {
+  const int t0 = __shfl_sync(0xffffffffu, active ? tri : -1, 0);
+  const unsigned long long p0 = __shfl_sync(0xffffffffu, (unsigned long long)scp, 0);
+  const bool uni = __all_sync(0xffffffffu, active && tri == t0 && (unsigned long long)scp == p0);
+  if (!uni) {
+    if (active) scatter_surf(*scp, hot, tri, b1, b2, front, a);
+    return;
+  }
+  if (!scp->grad_verts) return;
+  float3 g0, g1, g2;
+  surf_vertex_adj(*scp, tri, b1, b2, front, a, g0, g1, g2);
+  float v[9] = {g0.x, g0.y, g0.z, g1.x, g1.y, g1.z, g2.x, g2.y, g2.z};
+#pragma unroll
+  for (int o = 16; o; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0) {
+    const int4 tv = __ldg(scp->tri_v + tri);
+    add_vertex(*scp, hot, tv.x, f3(v[0], v[1], v[2]));
+    add_vertex(*scp, hot, tv.y, f3(v[3], v[4], v[5]));
+    add_vertex(*scp, hot, tv.z, f3(v[6], v[7], v[8]));
+  }
+}
+
+PSDR_D void scatter_tex_warp(const DevTex* tx, int off, float3 a, bool active) {
+  const bool has = active && tx && tx->grad;
+  const unsigned long long key = has ? (unsigned long long)(tx->grad + off) : 0ull;
+  const unsigned long long k0 = __shfl_sync(0xffffffffu, key, 0);
+  const bool uni = __all_sync(0xffffffffu, has && key == k0);
+  if (!uni) {
+    if (has) scatter_tex(*tx, off, a, false);
+    return;
+  }
+  float v0 = a.x, v1 = a.y, v2 = a.z;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+    v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+    v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+  }
+  if ((threadIdx.x & 31) == 0) scatter_tex(*tx, off, f3(v0, v1, v2), false);
+}
+
+// ------------------------------------------------------------------ adjoint kernel
+// One thread per path of the tile: re-evaluates the path from its sampler stream and
+// hit records, forms the suffix radiances S_d = C_d + beta_d S_{d+1}, then runs the
+// reverse-mode adjoint depth by depth (PSDR_EST_REFERENCE: pdfs and MIS weights are
+// constants, jacobi = area/detach(area), barycentrics are not differentiated).
+__global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restrict__ scenes,
+                                                 const DevView* __restrict__ views, Tile tile, int hot_lv0,
+                                                 int hot_nlv, int emit_hot) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (tile.n + 31) & ~31;
+  HotAcc hot;
+  hot.lv0 = hot_lv0;
+  hot.nlv = hot_nlv;
+  hot.emit_hot = emit_hot != 0;
+#pragma unroll
+  for (int k = 0; k < kMaxLightVerts * 3; ++k) hot.g[k] = 0.f;
+  hot.e[0] = hot.e[1] = hot.e[2] = 0.f;
+  const DevScene* flush_sc = nullptr;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool has0 = false;
+    int tri0 = -1;
+    float b10 = 0.f, b20 = 0.f;
+    bool front0 = true;
+    SurfAdj ax0 = zero_adj();
+    float3 atex0 = f3(0.f, 0.f, 0.f);
+    const DevTex* tx0 = nullptr;
+    int toff0 = 0;
+    const DevScene* scp = nullptr;
+    if (s < tile.n) {
+      const DevView& V = views[w.view[s]];
+      scp = &scenes[V.scene];
+      const float4 h0 = w.rec[(size_t)s * w.rec_stride];
+      tri0 = __float_as_int(h0.x);
+      if (tri0 >= 0 && V.dimage) {
+        const DevScene& sc = *scp;
+        flush_sc = scp;
+        const float* gp = V.dimage + 3 * (size_t)w.pix[s];
+        const float3 g = f3(gp[0], gp[1], gp[2]) / (float)V.spp;
+        const long long i = tile.begin + s - V.sample_off;
+        Rng rng0 = make_rng((unsigned long long)i + w.seed);
+        rng0.next_float();
+        rng0.next_float();
+        const Surf x0 = make_surf(sc, tri0, h0.y, h0.z, V.pos);
+        b10 = h0.y; b20 = h0.z; front0 = x0.front;
+        const float4* rec = w.rec + (size_t)s * w.rec_stride + 1;
+        // pass 1: per-depth contributions and throughput factors
+        float3 C[kMaxDepth], B[kMaxDepth];
+        int De = 0;
+        bool lightstop = false;
+        {
+          Rng rng = rng0;
+          Surf x = x0;
+          SurfAdj d1 = zero_adj(), d2 = zero_adj();
+          HotAcc hd;
+          hd.nlv = 0;
+          hd.emit_hot = false;
+          float3 at = f3(0.f, 0.f, 0.f);
+          for (int d = 0; d < w.D; ++d) {
+            if (x.is_light) {
+              if (w.light_vis && d == 0) {
+                const DevLight& Lt = sc.lights[x.light];
+                C[0] = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+                B[0] = f3(0.f, 0.f, 0.f);
+                De = 1;
+                lightstop = true;
+              }
+              break;
+            }
+            const DepthVals dv = depth_eval<false>(w, sc, x, rng, rec + (size_t)d * w.R, d == w.D - 1,
+                                                   f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f), d1, d2, hd, at);
+            C[d] = dv.C;
+            B[d] = dv.beta;
+            De = d + 1;
+            if (!dv.has_next) break;
+            const float4 hn = rec[(size_t)d * w.R + w.nL + w.nB];
+            x = make_surf(sc, __float_as_int(hn.x), hn.y, hn.z, x.p);
+          }
+        }
+        float3 Ssuf[kMaxDepth + 1];
+        Ssuf[De] = f3(0.f, 0.f, 0.f);
+        for (int d = De - 1; d >= 0; --d) Ssuf[d] = C[d] + mul(B[d], Ssuf[d + 1]);
+        const float3 L = Ssuf[0];
+        if (De > 0 && finite3(L)) {
+          has0 = true;
+          SurfAdj ax = zero_adj();
+          ax.area = dot(g, L) / x0.area;  // jacobi of the primary hit
+          if (lightstop) {
+            add_emit(hot, sc.lights[x0.light].grad_emit, g);
+            ax0 = ax;
+          } else {
+            Rng rng = rng0;
+            Surf xc = x0;
+            int tric = tri0;
+            float4 hc = h0;
+            float3 T = f3(1.f, 1.f, 1.f);
+            for (int d = 0; d < De; ++d) {
+              const float3 adjC = mul(g, T);
+              const float3 adjB = mul(adjC, Ssuf[d + 1]);
+              SurfAdj nextc = zero_adj();
+              float3 atx = f3(0.f, 0.f, 0.f);
+              depth_eval<true>(w, sc, xc, rng, rec + (size_t)d * w.R, d == w.D - 1, adjC, adjB, ax, nextc, hot, atx);
+              const DevObj& ob = sc.objs[xc.obj];
+              const int off = texel_offset(ob.color, xc.u, xc.v);
+              if (d == 0) {
+                ax0 = ax;
+                atex0 = atx;
+                tx0 = &ob.color;
+                toff0 = off;
+              } else {
+                if (ob.color.grad) scatter_tex(ob.color, off, atx, false);
+                scatter_surf(sc, hot, tric, hc.y, hc.z, xc.front, ax);
+              }
+              T = mul(T, B[d]);
+              if (d + 1 >= De) break;
+              hc = rec[(size_t)d * w.R + w.nL + w.nB];
+              tric = __float_as_int(hc.x);
+              const float3 org = xc.p;
+              xc = make_surf(sc, tric, hc.y, hc.z, org);
+              ax = nextc;
+            }
+          }
+        }
+      }
+    }
+    scatter_surf_warp(scp, hot, tri0, b10, b20, front0, ax0, has0);
+    scatter_tex_warp(tx0, toff0, atex0, has0);
+  }
+  // flush register accumulators: warp reduce, one atomic per warp
+#pragma unroll
+  for (int k = 0; k < kMaxLightVerts * 3; ++k) {
+    float v = hot.g[k];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    hot.g[k] = v;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float v = hot.e[k];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    hot.e[k] = v;
+  }
+  const unsigned have = __ballot_sync(0xffffffffu, flush_sc != nullptr);
+  if (!have) return;
+  const unsigned long long addr = __shfl_sync(0xffffffffu, (unsigned long long)flush_sc, __ffs(have) - 1);
+  const DevScene* fsc = reinterpret_cast<const DevScene*>(addr);
+  if ((threadIdx.x & 31) == 0) {
+    if (hot_nlv > 0 && fsc->grad_verts)
+      for (int k = 0; k < hot_nlv * 3; ++k)
+        if (hot.g[k] != 0.f) atomicAdd(fsc->grad_verts + 3 * (size_t)hot_lv0 + k, (double)hot.g[k]);
+    if (emit_hot && fsc->nlight > 0 && fsc->lights[0].grad_emit)
+      for (int k = 0; k < 3; ++k)
+        if (hot.e[k] != 0.f) atomicAdd(fsc->lights[0].grad_emit + k, (double)hot.e[k]);
+  }
+}
+
+// ------------------------------------------------------------------ hypercube
+struct HCube {
+  const float* pmf;
+  const float* cmf;
+  int ncells;
+  int res[3];
+  float unit[3];
+};
+
+// ------------------------------------------------------------------ primary edges
+// path_integrator.cc:188-272. PRE=true is the preprocess pass over the hypercube
+// cells (sample index = cell, the sampler stream persists across rounds); PRE=false
+// samples the cell from the preprocessed mass.
+template <bool PRE>
+__global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restrict__ scenes,
+                                                   const DevView* __restrict__ views, int v, EdgeBuf eb,
+                                                   long long begin, int n, HCube hc, int round) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool alive = false;
+    if (s < n) {
+      const long long i = begin + s;
+      const DevView& V = views[v];
+      const DevScene& sc = scenes[V.scene];
+      Rng rng;
+      float s1, hpdf = 1.f;
+      bool ok = true;
+      if (PRE) {
+        if (round == 0) rng = make_rng((unsigned long long)i);
+        else { rng.state = w.rs[s]; rng.inc = w.ri[s]; }
+        s1 = ((float)i + rng.next_float()) * hc.unit[0];
+      } else {
+        rng = make_rng((unsigned long long)i + w.seed);
+        s1 = rng.next_float();
+        const int cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s1, hpdf);
+        ok = hpdf > 0.f;
+        s1 = (s1 + (float)cell) * hc.unit[0];
+      }
+      const int ne = *sc.n_edges;
+      float ss = s1, pe;
+      const int e = discrete_sample(sc.edge_pmf, sc.edge_cmf, ne, ss, pe);
+      const float4 E0 = __ldg(sc.edge + 4 * (size_t)e), E1 = __ldg(sc.edge + 4 * (size_t)e + 1);
+      const float3 p0 = xyz(E0), p1 = xyz(E1);
+      const float3 xe = p0 + (p1 - p0) * ss;
+      const float pdf_e = pe / E0.w;
+      int px = 0, py = 0;
+      bool valid = ok && project(V, xe, px, py);
+      const float3 rd = normalize(xe - V.pos);
+      const float3 nrm = cross(rd, normalize(p1 - p0));
+      HitRec ha, hb;
+      ha.tri = hb.tri = -1;
+      ha.b1 = ha.b2 = hb.b1 = hb.b2 = 0.f;
+      if (valid) {
+        ha = trace_closest(sc, V.pos, rd - nrm * kEps, kTmin, INFINITY);
+        hb = trace_closest(sc, V.pos, rd + nrm * kEps, kTmin, INFINITY);
+      }
+      const Surf a = make_surf(sc, ha.tri, ha.b1, ha.b2, V.pos);
+      const Surf b = make_surf(sc, hb.tri, hb.b1, hb.b2, V.pos);
+      valid = valid && a.valid && b.valid && (norm(a.p - xe) < 10.f * kEps || norm(b.p - xe) < 10.f * kEps);
+      eb.a[s] = make_float4(__int_as_float(e), ss, pdf_e, hpdf);
+      eb.n[s] = make_float4(nrm.x, nrm.y, nrm.z, __int_as_float(py * V.W + px));
+      eb.hb[s] = make_float4(__int_as_float(hb.tri), hb.b1, hb.b2, __int_as_float(valid ? 1 : 0));
+      w.rs[s] = rng.state;
+      w.ri[s] = rng.inc;
+      w.view[s] = v;
+      w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
+      w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      w.cur[s] = hit4(ha);
+      w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      alive = valid;
+    }
+    const int k = warp_append(&w.cnt[0], alive);
+    if (alive) w.q0[k] = s;
+  }
+}
+
+// Between the two trace2light calls: keep L_a, restart the slot at the +eps hit with
+// the sampler stream continuing where the first path left it.
+__global__ void __launch_bounds__(256) k_edge_mid(WF w, const DevView* __restrict__ views, int v, EdgeBuf eb, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool alive = false;
+    if (s < n) {
+      const float4 hb = eb.hb[s];
+      alive = __float_as_int(hb.w) != 0;
+      if (alive) {
+        const DevView& V = views[v];
+        eb.La[s] = w.L[s];
+        w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
+        w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        w.cur[s] = make_float4(hb.x, hb.y, hb.z, 0.f);
+        w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      }
+    }
+    const int k = warp_append(&w.cnt[0], alive);
+    if (alive) w.q0[k] = s;
+  }
+}
+
+// PRE: mass[cell] += |dL / pdf_e|. Otherwise the gradient of the zero-valued term
+// (x_e - detach(x_e)).n + (o - detach(o)).(n*[1,1,-1]) times dL / pdf_e / pdf_hc / spp.
+template <bool PRE>
+__global__ void __launch_bounds__(256) k_edge_final(WF w, const DevScene* __restrict__ scenes,
+                                                    const DevView* __restrict__ views, int v, EdgeBuf eb,
+                                                    long long begin, int n, float* mass, int spp) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  float3 go = f3(0.f, 0.f, 0.f);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    if (s >= n) continue;
+    const float4 hb = eb.hb[s];
+    if (__float_as_int(hb.w) == 0) continue;
+    const float3 La = xyz(eb.La[s]), Lb = xyz(w.L[s]);
+    const float3 dL = La - Lb;
+    const float4 a = eb.a[s];
+    const float pdf_e = a.z;
+    if (PRE) {
+      const float3 val = dL / pdf_e;
+      if (finite3(val)) mass[begin + s] = mass[begin + s] + norm(val);
+    } else {
+      if (!finite3(dL * 0.0f)) continue;
+      const float4 nn = eb.n[s];
+      const int pix = __float_as_int(nn.w);
+      if (!V.dimage) continue;
+      const float* gp = V.dimage + 3 * (size_t)pix;
+      const float K = (gp[0] * dL.x + gp[1] * dL.y + gp[2] * dL.z) / (pdf_e * a.w * (float)spp);
+      const float3 nrm = xyz(nn);
+      const float3 ax = nrm * K;
+      const int e = __float_as_int(a.x);
+      const float ss = a.y;
+      if (sc.grad_verts) {
+        const int2 ev = __ldg(sc.edge_v + e);
+        atomic_add3(sc.grad_verts + 3 * (size_t)ev.x, ax * (1.f - ss));
+        atomic_add3(sc.grad_verts + 3 * (size_t)ev.y, ax * ss);
+      }
+      go += f3(nrm.x, nrm.y, -nrm.z) * K;
+    }
+  }
+  if (!PRE && V.grad_pos) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      go.x += __shfl_xor_sync(0xffffffffu, go.x, o);
+      go.y += __shfl_xor_sync(0xffffffffu, go.y, o);
+      go.z += __shfl_xor_sync(0xffffffffu, go.z, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (go.x != 0.f || go.y != 0.f || go.z != 0.f)) atomic_add3(V.grad_pos, go);
+  }
+}
+
+// ------------------------------------------------------------------ direct edges
+// path_integrator.cc:274-353 and the boundary_term / hit_triangle adjoint (:11-78).
+template <bool PRE>
+__global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict__ scenes,
+                                                const DevView* __restrict__ views, int v, long long n, HCube hc,
+                                                int round, float* mass, int spp) {
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+    Rng rng;
+    float s3[3], hpdf = 1.f;
+    if (PRE) {
+      if (round == 0) rng = make_rng((unsigned long long)i);
+      else { rng.state = w.rs[i]; rng.inc = w.ri[i]; }
+      const int r12 = hc.res[1] * hc.res[2];
+      const int c0 = (int)(i / r12);
+      const int rem = (int)(i - (long long)c0 * r12);
+      const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
+      const float d0 = rng.next_float(), d1 = rng.next_float(), d2 = rng.next_float();
+      s3[0] = ((float)c0 + d0) * hc.unit[0];
+      s3[1] = ((float)c1 + d1) * hc.unit[1];
+      s3[2] = ((float)c2 + d2) * hc.unit[2];
+      w.rs[i] = rng.state;
+      w.ri[i] = rng.inc;
+    } else {
+      rng = make_rng((unsigned long long)i + w.seed);
+      s3[0] = rng.next_float(); s3[1] = rng.next_float(); s3[2] = rng.next_float();
+      const int cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s3[2], hpdf);
+      if (!(hpdf > 0.f)) continue;
+      const int r12 = hc.res[1] * hc.res[2];
+      const int c0 = cell / r12, rem = cell - c0 * r12;
+      const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
+      s3[0] = (s3[0] + (float)c0) * hc.unit[0];
+      s3[1] = (s3[1] + (float)c1) * hc.unit[1];
+      s3[2] = (s3[2] + (float)c2) * hc.unit[2];
+    }
+    const int ne = *sc.n_edges;
+    float sx = s3[0], pe;
+    const int e = discrete_sample(sc.edge_pmf, sc.edge_cmf, ne, sx, pe);
+    const float4 E0 = __ldg(sc.edge + 4 * (size_t)e), E1 = __ldg(sc.edge + 4 * (size_t)e + 1),
+                 E2 = __ldg(sc.edge + 4 * (size_t)e + 2), E3 = __ldg(sc.edge + 4 * (size_t)e + 3);
+    const float3 p0 = xyz(E0), p1 = xyz(E1);
+    const float3 out = f3(E1.w, E2.x, E2.y), nl = f3(E2.z, E2.w, E3.x), nr = f3(E3.y, E3.z, E3.w);
+    const float3 xb = p0 + (p1 - p0) * sx;
+    const float pdf_e = pe / E0.w;
+    const LightSample ls = sample_light(sc, s3[1], s3[2]);
+    const float3 dir = normalize(xb - ls.y);
+    bool valid = dot(nl, dir) * dot(nr, dir) < 0.f && norm(nl - nr) > kEps;
+    if (!valid) continue;
+    const HitRec hs = trace_closest(sc, xb, -dir, kTmin, INFINITY);
+    const Surf s0 = make_surf(sc, hs.tri, hs.b1, hs.b2, xb);
+    if (!(s0.valid && s0.is_light && sqnorm(s0.p - ls.y) < kEps)) continue;
+    const HitRec hd = trace_closest(sc, xb, dir, kTmin, INFINITY);
+    const Surf d0 = make_surf(sc, hd.tri, hd.b1, hd.b2, xb);
+    if (!(d0.valid && !d0.is_light)) continue;
+    int px, py;
+    if (!project(V, d0.p, px, py)) continue;
+    const float3 cd = normalize(d0.p - V.pos);
+    const HitRec h2 = trace_closest(sc, V.pos, cd, kTmin, INFINITY);
+    const Surf i2 = make_surf(sc, h2.tri, h2.b1, h2.b2, V.pos);
+    if (!(i2.valid && !i2.is_light && sqnorm(i2.p - d0.p) < kEps)) continue;
+    const float pdf_xw = s0.sqd * pdf_e * ls.pdf / dot(s0.n, dir);
+    // boundary_term (detached quantities)
+    const float3 xs = s0.p, xd = d0.p, ns = s0.n, nd = d0.n;
+    const float3 rb = xb - xs;
+    const float3 db = normalize(rb);
+    float3 ev = normalize(p1 - p0);
+    if (dot(cross(db, ev), out) < 0.f) ev = -ev;
+    const float3 npl = cross(db, ev);
+    const float3 ep = cross(nd, npl);
+    const float cos_s = fabsf(dot(ns, db));
+    const float cos_b = dot(ev, db), cos_d = dot(ep, db);
+    const float sb2 = 1.f - cos_b * cos_b, sd2 = 1.f - cos_d * cos_d;
+    const float sin_b = sb2 > 0.f ? sqrtf(sb2) : 0.f, sin_d = sd2 > 0.f ? sqrtf(sd2) : 0.f;
+    const float len_sb = norm(xb - xs), len_sd = norm(xd - xs);
+    const float Jb = len_sd * len_sb * sin_b / (sin_d * cos_s);
+    const float dG = cos_s * dot(nd, -db) / (len_sd * len_sd);
+    const DevLight& Lt = sc.lights[s0.light];
+    const float3 Ts = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+    const DevObj& ob = sc.objs[d0.obj];
+    const float3 Td = tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi;
+    if (PRE) {
+      float3 val = mul(mul(f3(dG, dG, dG) * Jb / pdf_xw, Ts), Td);
+      if (!finite3(val)) continue;
+      val.x = val.x < kEps ? kEps : val.x;
+      val.y = val.y < kEps ? kEps : val.y;
+      val.z = val.z < kEps ? kEps : val.z;
+      mass[i] = mass[i] + norm(val);
+    } else {
+      const float3 nep = cross(nd, ep);
+      const float3 z = mul(mul(mul(f3(0.f, 0.f, 0.f), nep * dG) * Jb / pdf_xw, Ts), Td);
+      if (!finite3(z) || !V.dimage || !sc.grad_verts) continue;
+      const float* gp = V.dimage + 3 * ((size_t)py * V.W + px);
+      const float c = Jb / pdf_xw * dG / (hpdf * (float)spp);
+      const float3 wv = f3(gp[0] * nep.x * Ts.x * Td.x, gp[1] * nep.y * Ts.y * Td.y, gp[2] * nep.z * Ts.z * Td.z) * c;
+      // hit_triangle(xs, d, xd, ep, nep) adjoint w.r.t. d
+      const float3 e1 = ep, e2 = nep;
+      const float3 T = xs - xd;
+      const float3 P = cross(db, e2), Q = cross(T, e1);
+      const float det = dot(P, e1);
+      const float dcl = fminf(fmaxf(det, kEps), 1.f - kEps);
+      const float inv = 1.f / dcl;
+      const float u = dot(P, T) * inv, vv = dot(Q, db) * inv;
+      const float au = dot(wv, e1), avv = dot(wv, e2);
+      float3 ad = cross(e2, T) * (au * inv) + Q * (avv * inv);
+      if (det > kEps && det < 1.f - kEps) ad += cross(e2, e1) * (-(au * u + avv * vv) * inv);
+      const float3 axb = (ad - db * dot(db, ad)) / norm(rb);
+      const int2 evv = __ldg(sc.edge_v + e);
+      atomic_add3(sc.grad_verts + 3 * (size_t)evv.x, axb * (1.f - sx));
+      atomic_add3(sc.grad_verts + 3 * (size_t)evv.y, axb * sx);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ small utilities
+__global__ void k_mass_cdf(const float* __restrict__ mass, int n, double* __restrict__ w) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) w[i] = (double)mass[i];
+}
+__global__ void k_mass_finalize(const double* __restrict__ w, const double* __restrict__ pre, int n,
+                                float* __restrict__ pmf, float* __restrict__ cmf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double tot = pre[n - 1];
+  if (!(tot > 0.0)) { pmf[i] = 0.f; cmf[i] = 1.f; return; }
+  pmf[i] = (float)(w[i] / tot);
+  cmf[i] = (float)(pre[i] / tot);
+}
+__global__ void k_grad_out(const double* __restrict__ acc, float* __restrict__ out, long long n, int accumulate) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = (accumulate ? out[i] : 0.f) + (float)acc[i];
+}
+
+
+// ================================================================== host side
+namespace {
+inline int grid_for(long long n, int threads, int per_sm) {
+  const long long want = (n + threads - 1) / threads;
+  const long long cap = (long long)num_sms() * per_sm;
+  return (int)std::max<long long>(1, std::min(want, cap));
+}
+}  // namespace
+
+// camera.h:7-64, :111-124; psdr.cc:24-29 (near -0.01, far -1000). Row-major floats.
+void make_view(const psdr_camera_desc& c, int spp, DevView& v) {
+  auto nrm = [](double* a) { double n = std::sqrt(a[0]*a[0]+a[1]*a[1]+a[2]*a[2]); a[0]/=n; a[1]/=n; a[2]/=n; };
+  auto crs = [](const double* a, const double* b, double* r) {
+    r[0] = a[1]*b[2]-a[2]*b[1]; r[1] = a[2]*b[0]-a[0]*b[2]; r[2] = a[0]*b[1]-a[1]*b[0]; };
+  double o[3] = {c.look_from[0], c.look_from[1], c.look_from[2]};
+  double t[3] = {c.look_at[0], c.look_at[1], c.look_at[2]};
+  double u[3] = {c.up[0], c.up[1], c.up[2]};
+  double dir[3] = {o[0]-t[0], o[1]-t[1], o[2]-t[2]};
+  nrm(dir); nrm(u);
+  double right[3], nup[3];
+  crs(u, dir, right);
+  crs(dir, right, nup);
+  double cw[4][4] = {{0}}, cs[4][4] = {{0}}, sr[4][4] = {{0}}, tr[4][4] = {{0}};
+  for (int i = 0; i < 3; ++i) { cw[i][0] = right[i]; cw[i][1] = nup[i]; cw[i][2] = dir[i]; cw[i][3] = o[i]; }
+  cw[3][3] = 1;
+  const double nearv = -0.01, farv = -1000.0, inv_nf = 1.0 / (nearv - farv);
+  const double cot = 1.0 / std::tan((double)c.fov * 0.5);
+  cs[0][0] = -cot; cs[1][1] = -cot; cs[2][2] = (nearv + farv) * inv_nf; cs[2][3] = -2 * farv * nearv * inv_nf; cs[3][2] = 1;
+  sr[0][0] = 0.5 * c.width; sr[1][1] = -0.5 * c.height; sr[2][2] = 1; sr[3][3] = 1;
+  tr[0][0] = tr[1][1] = tr[2][2] = tr[3][3] = 1; tr[0][3] = 1; tr[1][3] = -1;
+  auto mm = [](const double a[4][4], const double b[4][4], double r[4][4]) {
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) { double s = 0; for (int k = 0; k < 4; ++k) s += a[i][k] * b[k][j]; r[i][j] = s; } };
+  auto inv = [](const double a[4][4], double r[4][4]) {
+    double m[4][8];
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 8; ++j) m[i][j] = j < 4 ? a[i][j] : (j - 4 == i ? 1.0 : 0.0);
+    for (int col = 0; col < 4; ++col) {
+      int p = col;
+      for (int rr = col + 1; rr < 4; ++rr) if (std::fabs(m[rr][col]) > std::fabs(m[p][col])) p = rr;
+      for (int j = 0; j < 8; ++j) std::swap(m[col][j], m[p][j]);
+      const double iv = 1.0 / m[col][col];
+      for (int j = 0; j < 8; ++j) m[col][j] *= iv;
+      for (int rr = 0; rr < 4; ++rr) { if (rr == col) continue; const double f = m[rr][col]; for (int j = 0; j < 8; ++j) m[rr][j] -= f * m[col][j]; }
+    }
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) r[i][j] = m[i][j + 4];
+  };
+  double t1[4][4], c2r[4][4], r2c[4][4], w2c[4][4];
+  mm(sr, tr, t1);
+  mm(t1, cs, c2r);
+  inv(c2r, r2c);
+  inv(cw, w2c);
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) {
+      v.r2c[4 * i + j] = (float)r2c[i][j];
+      v.c2w[4 * i + j] = (float)cw[i][j];
+      v.w2c[4 * i + j] = (float)w2c[i][j];
+      v.c2r[4 * i + j] = (float)c2r[i][j];
+    }
+  v.pos = make_float3(c.look_from[0], c.look_from[1], c.look_from[2]);
+  v.H = c.height;
+  v.W = c.width;
+  v.spp = spp;
+  v.scene = 0;
+  v.image = nullptr;
+  v.dimage = nullptr;
+  v.grad_pos = nullptr;
+}
+
+std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap) {
+  std::vector<Tile> tiles;
+  Tile cur{0, 0, 0, 0};
+  for (const DevView& v : views) {
+    long long rem = (long long)v.H * v.W;
+    while (rem > 0) {
+      const long long room = (cap - cur.n) / v.spp;
+      if (room <= 0) {
+        tiles.push_back(cur);
+        cur = Tile{cur.begin + cur.n, 0, cur.pix_begin + cur.npix, 0};
+        continue;
+      }
+      const long long take = std::min(room, rem);
+      cur.n += (int)(take * v.spp);
+      cur.npix += (int)take;
+      rem -= take;
+    }
+  }
+  if (cur.n > 0) tiles.push_back(cur);
+  return tiles;
+}
+
+void assign_offsets(std::vector<DevView>& views) {
+  long long so = 0, po = 0;
+  for (DevView& v : views) {
+    v.sample_off = so;
+    v.pix_off = po;
+    so += (long long)v.H * v.W * v.spp;
+    po += (long long)v.H * v.W;
+  }
+}
+
+static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int mode, cudaStream_t st) {
+  const int cap = w.cap;
+  for (int d = 0; d < w.D; ++d) {
+    if (mode == MODE_REPLAY) k_shade<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
+    else k_shade<MODE_FWD><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
+    k_trace<<<grid_for((long long)cap * w.R, 128, 16), 128, 0, st>>>(w, scenes, views, d);
+    if (mode == MODE_REPLAY) k_accum<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
+    else k_accum<MODE_FWD><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
+  }
+  PSDR_CUDA(cudaGetLastError());
+}
+
+static void run_tile(WF& w, const DevScene* scenes, const DevView* views, const Tile& tile, int mode,
+                     cudaStream_t st) {
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  if (mode == MODE_REPLAY) k_camera<MODE_REPLAY><<<grid_for(tile.n, 256, 8), 256, 0, st>>>(w, scenes, views, tile);
+  else k_camera<MODE_FWD><<<grid_for(tile.n, 256, 8), 256, 0, st>>>(w, scenes, views, tile);
+  depth_loop(w, scenes, views, mode, st);
+}
+
+int choose_cap(const psdr_config& cfg, const std::vector<DevView>& views, bool backward) {
+  int maxspp = 1;
+  long long total = 0;
+  for (auto& v : views) { maxspp = std::max(maxspp, v.spp); total += (long long)v.H * v.W * v.spp; }
+  long long cap = cfg.tile_paths > 0 ? cfg.tile_paths : (1 << 20);
+  if (backward) {
+    long long cells = std::max<long long>(cfg.primary_edge_hypercube_resolution,
+                                          (long long)cfg.secondary_edge_hypercube_resolution[0] *
+                                              cfg.secondary_edge_hypercube_resolution[1] *
+                                              cfg.secondary_edge_hypercube_resolution[2]);
+    cap = std::max(cap, cells);
+  } else {
+    cap = std::min<long long>(cap, std::max<long long>(total, maxspp));
+  }
+  cap = std::max<long long>(cap, maxspp);
+  cap = (cap + 31) / 32 * 32;
+  return (int)cap;
+}
+
+}  // namespace psdr
+
+void psdr_workspace::ensure(int c, int r, int d, int nv, int rec_needed, cudaStream_t st) {
+  using namespace psdr;
+  stream = st;
+  if (c > cap || r > R || d > D) {
+    cap = std::max(c, cap);
+    R = std::max(r, R);
+    D = std::max(d, D);
+    const size_t n = (size_t)cap;
+    rs.alloc(8 * n, st); ri.alloc(8 * n, st); view.alloc(4 * n, st); pix.alloc(4 * n, st);
+    T.alloc(16 * n, st); L.alloc(16 * n, st); cur.alloc(16 * n, st); org.alloc(16 * n, st);
+    q0.alloc(4 * n, st); q1.alloc(4 * n, st); qs.alloc(4 * n, st);
+    cnt.alloc(sizeof(int) * 2 * (kMaxDepth + 2), st);
+    ro.alloc(16 * n * R, st); rd.alloc(16 * n * R, st); ra.alloc(16 * n * R, st); hit.alloc(16 * n * R, st);
+    eb_a.alloc(16 * n, st); eb_n.alloc(16 * n, st); eb_hb.alloc(16 * n, st); eb_La.alloc(16 * n, st);
+    mass.alloc(4 * n, st); mass_d.alloc(8 * n, st); mass_pre.alloc(8 * n, st);
+    hc_pmf.alloc(4 * n, st); hc_cmf.alloc(4 * n, st);
+    scan_tmp.alloc(8 * (scan_tmp_doubles((int)n) + 64), st);
+  }
+  if (rec_needed) rec.alloc(16 * (size_t)cap * (1 + (size_t)D * R), st);
+  if (nv > nviews_cap) {
+    nviews_cap = nv;
+    views.alloc(sizeof(DevView) * nv, st);
+  }
+  wf.cap = cap;
+  wf.rs = rs.as<unsigned long long>(); wf.ri = ri.as<unsigned long long>();
+  wf.view = view.as<int>(); wf.pix = pix.as<int>();
+  wf.T = T.as<float4>(); wf.L = L.as<float4>(); wf.cur = cur.as<float4>(); wf.org = org.as<float4>();
+  wf.q0 = q0.as<int>(); wf.q1 = q1.as<int>(); wf.qs = qs.as<int>(); wf.cnt = cnt.as<int>();
+  wf.ro = ro.as<float4>(); wf.rd = rd.as<float4>(); wf.ra = ra.as<float4>(); wf.hit = hit.as<float4>();
+  wf.rec = rec.as<float4>();
+}
+
+namespace psdr {
+
+void upload_views(psdr_workspace* ws, const std::vector<DevView>& views, cudaStream_t st) {
+  ws->h_views = views;
+  PSDR_CUDA(cudaMemcpyAsync(ws->views.p, ws->h_views.data(), sizeof(DevView) * views.size(), cudaMemcpyHostToDevice, st));
+}
+
+void set_wf(WF& w, const psdr_config& cfg, int nviews, int nB_override, int light_vis) {
+  w.D = cfg.max_bounce;
+  w.nL = cfg.mis_light_samples;
+  w.nB = nB_override >= 0 ? nB_override : cfg.mis_bsdf_samples;
+  w.R = w.nL + w.nB + 1;
+  w.light_vis = light_vis;
+  w.nviews = nviews;
+  w.seed = cfg.seed;
+  w.rec_stride = 1 + w.D * w.R;
+}
+
+// Forward: the interior estimate of every view into V.image (and per-sample radiance
+// of view 0 into samples_out when given).
+void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
+                         psdr_workspace* ws, cudaStream_t st, float* samples_out) {
+  assign_offsets(views);
+  const int cap = choose_cap(cfg, views, false);
+  const int R = cfg.mis_light_samples + cfg.mis_bsdf_samples + 1;
+  ws->ensure(cap, R, cfg.max_bounce, (int)views.size(), 0, st);
+  upload_views(ws, views, st);
+  WF w = ws->wf;
+  w.cap = ws->cap;
+  set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
+  const DevView* vd = ws->views.as<DevView>();
+  for (const Tile& t : plan_tiles(views, cap)) {
+    run_tile(w, scenes_dev, vd, t, MODE_FWD, st);
+    k_film<<<grid_for(t.npix, 256, 8), 256, 0, st>>>(w, vd, t, std::max(1, cfg.n_pass), samples_out);
+  }
+  PSDR_CUDA(cudaGetLastError());
+}
+
+static void edge_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb, long long begin,
+                       int n, const HCube& hc, int round, bool pre, float* mass, int spp, cudaStream_t st) {
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  if (pre) k_edge_init<true><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round);
+  else k_edge_init<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round);
+  depth_loop(w, scenes, vd, MODE_FWD, st);
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  k_edge_mid<<<grid_for(n, 256, 8), 256, 0, st>>>(w, vd, v, eb, n);
+  depth_loop(w, scenes, vd, MODE_FWD, st);
+  if (pre) k_edge_final<true><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, mass, spp);
+  else k_edge_final<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, mass, spp);
+  PSDR_CUDA(cudaGetLastError());
+}
+
+static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, cudaStream_t st) {
+  HCube hc;
+  const int b = (ncells + 255) / 256;
+  k_mass_cdf<<<b, 256, 0, st>>>(ws->mass.as<float>(), ncells, ws->mass_d.as<double>());
+  inclusive_scan_double(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), ncells, ws->scan_tmp.as<double>(), st);
+  k_mass_finalize<<<b, 256, 0, st>>>(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), ncells,
+                                     ws->hc_pmf.as<float>(), ws->hc_cmf.as<float>());
+  PSDR_CUDA(cudaGetLastError());
+  hc.pmf = ws->hc_pmf.as<float>();
+  hc.cmf = ws->hc_cmf.as<float>();
+  hc.ncells = ncells;
+  for (int k = 0; k < 3; ++k) {
+    hc.res[k] = k < N ? res[k] : 1;
+    hc.unit[k] = 1.0f / (float)hc.res[k];
+  }
+  return hc;
+}
+
+// Backward: interior path replay + adjoint, then the primary- and direct-edge terms
+// of every view. Views must carry dimage (and grad_pos when wanted).
+void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
+                          psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
+  assign_offsets(views);
+  const int cap = choose_cap(cfg, views, true);
+  const int nL = cfg.mis_light_samples;
+  const int Rmax = nL + std::max(cfg.mis_bsdf_samples, 1) + 1;
+  ws->ensure(cap, Rmax, cfg.max_bounce, (int)views.size(), 1, st);
+  upload_views(ws, views, st);
+  const DevView* vd = ws->views.as<DevView>();
+  const int terms = cfg.terms ? cfg.terms : 7;
+  // ---- interior
+  if (terms & 1) {
+    WF w = ws->wf;
+    w.cap = ws->cap;
+    set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
+    for (const Tile& t : plan_tiles(views, cap)) {
+      run_tile(w, scenes_dev, vd, t, MODE_REPLAY, st);
+      k_adjoint<<<grid_for(t.n, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+    }
+    PSDR_CUDA(cudaGetLastError());
+  }
+  // ---- boundary terms per view
+  WF w = ws->wf;
+  w.cap = ws->cap;
+  set_wf(w, cfg, (int)views.size(), 1, 0);
+  EdgeBuf eb{ws->eb_a.as<float4>(), ws->eb_n.as<float4>(), ws->eb_hb.as<float4>(), ws->eb_La.as<float4>(), nullptr};
+  for (int v = 0; v < (int)views.size(); ++v) {
+    const DevView& V = views[v];
+    // primary edges: preprocess over the hypercube cells, then the edge samples
+    if (terms & 2) {
+      const int cells = cfg.primary_edge_hypercube_resolution;
+      PSDR_CUDA(cudaMemsetAsync(ws->mass.p, 0, sizeof(float) * cells, st));
+      HCube none{};
+      none.unit[0] = 1.0f / (float)cells;
+      for (int r = 0; r < cfg.primary_edge_preprocess_rounds; ++r)
+        edge_phase(w, scenes_dev, vd, v, eb, 0, cells, none, r, true, ws->mass.as<float>(), 1, st);
+      const int res[1] = {cells};
+      const HCube hc = build_hcube(ws, cells, res, 1, st);
+      const long long N = (long long)V.H * V.W * cfg.spp_primary_edge;
+      for (long long b = 0; b < N; b += cap)
+        edge_phase(w, scenes_dev, vd, v, eb, b, (int)std::min<long long>(cap, N - b), hc, 0, false, nullptr,
+                   cfg.spp_primary_edge, st);
+    }
+    // direct edges
+    if (terms & 4) {
+      const int* r3 = cfg.secondary_edge_hypercube_resolution;
+      const int cells = r3[0] * r3[1] * r3[2];
+      PSDR_CUDA(cudaMemsetAsync(ws->mass.p, 0, sizeof(float) * cells, st));
+      HCube pre{};
+      for (int k = 0; k < 3; ++k) { pre.res[k] = r3[k]; pre.unit[k] = 1.0f / (float)r3[k]; }
+      for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r)
+        k_direct<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
+                                                                 ws->mass.as<float>(), 1);
+      const HCube hc = build_hcube(ws, cells, r3, 3, st);
+      const long long N = (long long)V.H * V.W * cfg.spp_secondary_edge;
+      k_direct<false><<<grid_for(N, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, N, hc, 0, nullptr,
+                                                            cfg.spp_secondary_edge);
+      PSDR_CUDA(cudaGetLastError());
+    }
+  }
+}
+
+void grad_out(const double* acc, float* out, long long n, int accumulate, cudaStream_t st) {
+  if (!out || n <= 0) return;
+  k_grad_out<<<(int)((n + 255) / 256), 256, 0, st>>>(acc, out, n, accumulate);
+}
+
+}  // namespace psdr

@@ -1,0 +1,95 @@
+// render.h -- wavefront state shared by the render kernels and the host orchestration.
+#pragma once
+
+#include <vector>
+
+#include "psdr_internal.h"
+
+namespace psdr {
+
+constexpr int kMaxDepth = 16;
+constexpr int kMaxRays = 18;          // rays per path per depth: light + bsdf + indirect
+constexpr int kMaxLightVerts = 8;     // light vertices accumulated in registers by the adjoint
+
+// One camera view of a job. Matrices are row-major 4x4 (camera.h:108-124).
+struct DevView {
+  float r2c[16], c2w[16], w2c[16], c2r[16];
+  float3 pos;
+  int H, W, spp, scene;
+  long long sample_off;  // first sample of this view in the job's sample space
+  long long pix_off;     // first pixel of this view in the job's pixel space
+  float* image;          // (H,W,3) or null
+  const float* dimage;   // (H,W,3) or null
+  double* grad_pos;      // 3 doubles or null
+};
+
+// Path states and ray queues of one tile (structure of arrays, capacity `cap`).
+struct WF {
+  int cap, R, D, nL, nB, light_vis, nviews, spp_pass;
+  unsigned long long seed;
+  unsigned long long* rs;
+  unsigned long long* ri;
+  int* view;
+  int* pix;
+  float4* T;
+  float4* L;
+  float4* cur;   // current vertex: tri(bits), b1, b2, -
+  float4* org;   // origin of the ray that reached it
+  int* q0;
+  int* q1;
+  int* qs;
+  int* cnt;      // per depth: [2d] live paths, [2d+1] shaded paths
+  float4* ro;    // ray origin + tmax
+  float4* rd;    // ray direction + aux (light index bits)
+  float4* ra;    // aux: NEE target point + pdf / bsdf cos(theta)
+  float4* hit;   // tri(bits), b1, b2, t
+  float4* rec;   // replay records: 1 + D*R per path
+  int rec_stride;
+};
+
+struct Tile {
+  long long begin;  // first sample (job sample space)
+  int n;            // samples in the tile
+  long long pix_begin;
+  int npix;
+};
+
+// Side buffers of the primary-edge term (one entry per edge sample of a tile).
+struct EdgeBuf {
+  float4* a;     // edge id(bits), s, pdf_e, hc_pdf
+  float4* n;     // edge normal, pixel(bits)
+  float4* hb;    // hit of the +eps ray: tri(bits), b1, b2, valid(bits)
+  float4* La;    // radiance of the -eps path
+  unsigned long long* rng_keep;  // preprocess: sampler state across rounds
+};
+
+enum Mode { MODE_FWD = 0, MODE_REPLAY = 1 };
+
+struct psdr_ws_impl;
+
+}  // namespace psdr
+
+struct psdr_workspace {
+  int cap = 0, R = 0, D = 0, nviews_cap = 0;
+  psdr::DBuf rs, ri, view, pix, T, L, cur, org, q0, q1, qs, cnt, ro, rd, ra, hit, rec;
+  psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
+  psdr::DBuf campos_acc;
+  cudaStream_t stream = nullptr;
+  std::vector<psdr::DevView> h_views;
+  psdr::WF wf{};
+  void ensure(int cap, int R, int D, int nviews, int rec_needed, cudaStream_t st);
+};
+
+namespace psdr {
+struct SceneGradInfo;
+void make_view(const psdr_camera_desc& c, int spp, DevView& v);
+void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
+                         psdr_workspace* ws, cudaStream_t st, float* samples_out);
+struct SceneGradInfo {
+  int hot_lv0 = 0, hot_nlv = 0, emit_hot = 0;
+};
+void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
+                          psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
+void grad_out(const double* acc, float* out, long long n, int accumulate, cudaStream_t st);
+std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap);
+}  // namespace psdr
