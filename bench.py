@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Throughput of the B200 differentiable path tracer on the geometry-gradient workload.
+
+Workload (the reference's headline configuration for fwd+bwd at 512^2): a level-5
+icosphere (20,480 triangles, radial vertex noise N(0, 0.02), seed 2, 256^2 texture
+seed 0) on a 10x10 ground quad under a 1x1 area light (20,484 triangles in all);
+512x512, 32 spp interior, 4 spp primary-edge and 4 spp secondary-edge samples,
+max_bounce 3, one light and one BSDF MIS sample. One step = rebuild the scene from
+the (translated) vertices, renderD forward, L2 loss against a fixed target, and
+the full backward (interior path replay + both edge-sampling terms).
+
+Metric: interior path samples (512*512*32 per view) per second of fwd+bwd.
+`value` is device time with inputs resident in HBM; `e2e` adds the host->device
+copies of the vertices and texture from pinned memory and the device->host read
+of the vertex gradient and the loss, through the public Python API.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Under torchrun every rank renders its own replica (weak scaling, replicas only).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd path samples/s at 512² (batched vs plain) at matched grad error vs FD"
+UNIT = "path samples/s"
+H = W = 512
+SPP = 32
+CFG = dict(spp_interior=SPP, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=3, mis_light_samples=1,
+           mis_bsdf_samples=1)
+WORKLOAD = ("geometry gradient: level-5 icosphere 20,480 tris (+ground, light = 20,484), 512x512, 32 spp interior "
+            "+ 4 spp primary edges + 4 spp secondary edges, depth 3, L2 loss, fwd+bwd incl. scene rebuild")
+TRACE_BYTES_PER_RAY = 40  # ray read 24 B + hit write 16 B (per-ray share of the trace kernel)
+STEP_BYTES_PER_SAMPLE = 2628  # fwd+bwd algorithmic bytes per path sample at depth 3
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def make_spec():
+    from torch_psdr_b200 import synth
+    return synth.sphere_scene(level=5, tex_hw=256, tex_seed=0, noise_sigma=0.02, noise_seed=2, height=H, width=W)
+
+
+# ---------------------------------------------------------------- reference (CPU) arm
+def cpu_rate(spec, seconds_budget=20.0, rows=None):
+    """Oracle FP32 forward (interior) on a band of rows, all host threads: path samples/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import copy
+    import orc
+    orc.lib()
+    nthreads = os.cpu_count() or 1
+    orc.set_threads(nthreads)
+    s = copy.deepcopy(spec)
+    # `rows` full-width rows spanning the same view (the projection uses cot(fov/2) for
+    # both axes, so fewer rows subsample the whole 512^2 view vertically).
+    rows = rows or 16
+    s.cameras[0].height = rows
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        orc.render(s, precision=0, **CFG)
+        n += rows * W * SPP
+        if time.perf_counter() - t0 > seconds_budget * 0.5:
+            break
+    dt = time.perf_counter() - t0
+    return n / dt, nthreads, f"oracle FP32 forward (interior term; the CPU port has no reverse-mode adjoint), " \
+                             f"{rows} rows x {W} of the same view at {SPP} spp, {n} samples in {dt:.1f} s"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    spec = make_spec()
+    vals = []
+    cores = 1
+    sample = ""
+    for _ in range(args.warmup):
+        cpu_rate(spec, seconds_budget=4.0)
+    for _ in range(args.steps):
+        v, cores, sample = cpu_rate(spec, seconds_budget=8.0)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * H * W * SPP / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded icosphere scene)", "config": {"workload": WORKLOAD},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_index):
+        self.p = None
+        self.dev = dev_index
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev_index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- B200 arm
+def run_b200(args):
+    import torch
+    import torch_psdr_b200 as dr
+    from torch_psdr_b200 import _lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = tdist
+    dev = torch.device("cuda", local)
+    lib = L.load()
+    spec = make_spec()
+    sphere, ground = spec.meshes
+    light = spec.lights[0]
+    c = spec.cameras[0]
+
+    def tens(a, dt=torch.float32, rg=False):
+        return torch.tensor(np.asarray(a), dtype=dt, device=dev, requires_grad=rg)
+
+    base = tens(sphere.vertices)
+    faces = tens(sphere.faces, torch.int32)
+    uvs, uvi = tens(sphere.uvs), tens(sphere.uv_indices, torch.int32)
+    tex = tens(sphere.texture)
+    gV, gF, gT = tens(ground.vertices), tens(ground.faces, torch.int32), tens(ground.texture)
+    lV, lF, lE = tens(light.vertices), tens(light.faces, torch.int32), tens(light.emit)
+    cam = dr.PerspectiveCamera(tens(c.look_from), tens(c.look_at), tens(c.up), tens([c.vfov]), H, W)
+    integ = dr.PathIntegrator(**CFG)
+
+    def build_scene(verts, texture):
+        return dr.Scene([cam], [dr.Mesh(verts, uvs, faces, uvi, dr.DiffuseMaterial(texture)),
+                                dr.Mesh(gV, None, gF, None, dr.DiffuseMaterial(gT))],
+                        [dr.AreaLight(lV, lF, lE)])
+
+    with torch.no_grad():
+        target = integ.renderC(build_scene(base + torch.tensor([0.05, 0.0, 0.0], device=dev), tex))[0].clone()
+    t = torch.zeros(3, device=dev, requires_grad=True)
+
+    def step(verts_base, texture):
+        if t.grad is not None:
+            t.grad = None
+        v = verts_base + t
+        scene = build_scene(v, texture)
+        img = integ.renderD(scene)[0]
+        loss = ((img - target) ** 2).sum()
+        loss.backward()
+        return loss
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        step(base, tex)
+    torch.cuda.synchronize()
+
+    # ---------------- device-resident timing
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    L.check(lib.psdr_profile_enable(1), "profile")
+    L.check(lib.psdr_profile_reset(), "profile")
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(float(k))  # evicts L2 between steps, outside the timed events
+        ev[k][0].record(stream)
+        step(base, tex)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    prof = (ctypes.c_int64 * 3)()
+    trace_ms = ctypes.c_double()
+    L.check(lib.psdr_profile_read(prof, ctypes.byref(trace_ms)), "profile")
+    launches, trace_launches, rays = int(prof[0]), int(prof[1]), int(prof[2])
+    L.check(lib.psdr_profile_enable(0), "profile")
+    if dist:
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    samples = H * W * SPP
+    value = world * samples * args.steps / (total_ms / 1e3)
+
+    # ---------------- end-to-end through the public API with host buffers
+    h_base = torch.tensor(sphere.vertices, dtype=torch.float32).pin_memory()
+    h_tex = torch.tensor(sphere.texture, dtype=torch.float32).pin_memory()
+    h_grad = torch.empty((sphere.vertices.shape[0], 3), dtype=torch.float32).pin_memory()
+    h_loss = torch.empty((), dtype=torch.float32).pin_memory()
+    vb = torch.empty_like(base)
+    vt = torch.empty_like(tex)
+
+    def e2e_step():
+        vb.copy_(h_base, non_blocking=True)
+        vt.copy_(h_tex, non_blocking=True)
+        vv = vb.detach().requires_grad_(True)
+        scene = build_scene(vv + t, vt)
+        img = integ.renderD(scene)[0]
+        loss = ((img - target) ** 2).sum()
+        loss.backward()
+        h_grad.copy_(vv.grad, non_blocking=True)
+        h_loss.copy_(loss.detach(), non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ee[k][0].record(stream)
+        e2e_step()
+        ee[k][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in ee)
+    if dist:
+        tt = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_value = world * samples * args.steps / (e2e_ms / 1e3)
+    h2d = h_base.numel() * 4 + h_tex.numel() * 4
+    d2h = h_grad.numel() * 4 + 4
+
+    peak, peak_kind = peaks()
+    trace_avg_ms = trace_ms.value / max(1, trace_launches)
+    achieved = (rays / max(1, trace_launches)) * TRACE_BYTES_PER_RAY / (trace_avg_ms / 1e3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded icosphere scene)",
+            "config": {"workload": WORKLOAD, "mode": "plain (per-view launch sequence, no graph)",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": "k_trace (LBVH closest hit)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "bytes_per_unit": f"{TRACE_BYTES_PER_RAY} B/ray", "rays_per_launch": rays / max(1, trace_launches),
+                         "trace_share_of_step": trace_ms.value / max(total_ms / world if world == 1 else total_ms, 1e-9),
+                         "step_algorithmic_gbs": samples * STEP_BYTES_PER_SAMPLE / (total_ms / args.steps / 1e3) / 1e9},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "clocks": clk,
+            "rays_per_s": rays / (total_ms / 1e3)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_rate(spec, seconds_budget=20.0)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference", "ours"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

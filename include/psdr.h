@@ -182,6 +182,17 @@ PSDR_API psdr_status psdr_batch_forward(psdr_batch* batch, void* stream);
 PSDR_API psdr_status psdr_batch_backward(psdr_batch* batch, void* stream);
 PSDR_API psdr_status psdr_batch_destroy(psdr_batch* batch);
 
+/* ---------------------------------------------------------------- profiling
+ * Extension with no counterpart in the reference. When enabled, the library
+ * brackets every trace-kernel launch with CUDA events on the launching stream,
+ * counts the kernels it launches and the rays it traces. psdr_profile_read
+ * synchronises on the recorded events. */
+PSDR_API psdr_status psdr_profile_enable(int32_t on);
+PSDR_API psdr_status psdr_profile_reset(void);
+/* out[0] kernel launches, out[1] trace launches, out[2] rays traced (all since the
+ * last reset); *trace_ms = summed duration of the trace launches. */
+PSDR_API psdr_status psdr_profile_read(int64_t* out3, double* trace_ms);
+
 #ifdef __cplusplus
 }
 #endif

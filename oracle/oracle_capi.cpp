@@ -7,6 +7,7 @@
 #include <omp.h>
 
 #include <cstdio>
+#include <memory>
 
 #include "psdr_oracle.hpp"
 
@@ -19,6 +20,11 @@ template <class S, bool AD> struct Ctx {
   Camera<R> cam;
   V3<S> cam_pos;
   OrcConfig cfg;
+  // Float scene/camera for the primary-edge term: its +-1e-5 rays graze silhouette
+  // edges, so they are formed in float exactly as the GPU forms them.
+  const Scene<float>* scf = nullptr;
+  Camera<float> camf;
+  V3<float> posf;
 };
 
 // camera.h:235-258 PerspectiveCamera::gen_camera_ray_ for sample i.
@@ -52,40 +58,41 @@ inline void project(const Camera<R>& cam, const V3<S>& pt, bool& valid, int& rx,
   ry = (int)std::floor(py);
 }
 
-// path_integrator.cc:203-251 eval_primary_boundary.
+// path_integrator.cc:203-251 eval_primary_boundary. The sampled point, the offset
+// rays and the two trace2light<false> paths are evaluated in float; in AD mode the
+// zero-valued x_dot_n carries the derivatives of the edge vertices and camera origin.
 template <class S, bool AD>
-inline V3<S> eval_primary(const Ctx<S, AD>& c, Pcg32& rng, typename Traits<S>::R s1, int& rx, int& ry, bool& valid) {
-  using R = typename Traits<S>::R;
-  const Scene<S>& sc = c.sc;
-  R s = s1, pe;
-  int ei = sc.edge_cdf.sample_reuse(s, pe);
-  const Edge<S>& E = sc.edges[ei];
-  V3<S> xe = E.p0 + (E.p1 - E.p0) * S(s);
-  S pdf_e = S(pe) / E.len;
+inline V3<S> eval_primary(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx, int& ry, bool& valid) {
+  const Scene<float>& sf = *c.scf;
+  float s = s1, pe;
+  int ei = sf.edge_cdf.sample_reuse(s, pe);
+  const Edge<float>& E = sf.edges[ei];
+  V3<float> xe = E.p0 + (E.p1 - E.p0) * s;
+  float pdf_e = pe / E.len;
   valid = true;
-  project(c.cam, xe, valid, rx, ry);
-  V3<S> rd = normalize(xe - c.cam_pos);
-  V3<R> n = valv(cross(rd, normalize(detach(E.p1 - E.p0))));
-  V3<R> o = valv(c.cam_pos), d = valv(rd);
-  const R eps = R(1e-5);
-  V3<R> da = d - n * eps, db = d + n * eps;
-  Its<R> ia = scene_hit<R, false>(c.scv, o, da, valid);
-  Its<R> ib = scene_hit<R, false>(c.scv, o, db, valid);
-  V3<R> xev = valv(xe);
-  valid = valid && ia.valid && ib.valid &&
-          (double(norm(ia.p - xev)) < 1e-4 || double(norm(ib.p - xev)) < 1e-4);
-  V3<R> La = trace2light<R, false>(c.scv, rng, ia, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
-  V3<R> Lb = trace2light<R, false>(c.scv, rng, ib, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
-  V3<R> dL = La - Lb;
+  project(c.camf, xe, valid, rx, ry);
+  V3<float> rd = normalize(xe - c.posf);
+  V3<float> n = cross(rd, normalize(E.p1 - E.p0));
+  const float eps = 1e-5f;
+  V3<float> da = rd - n * eps, db = rd + n * eps;
+  Its<float> ia = scene_hit<float, false>(sf, c.posf, da, valid);
+  Its<float> ib = scene_hit<float, false>(sf, c.posf, db, valid);
+  valid = valid && ia.valid && ib.valid && (norm(ia.p - xe) < 1e-4f || norm(ib.p - xe) < 1e-4f);
+  V3<float> La = trace2light<float, false>(sf, rng, ia, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
+  V3<float> Lb = trace2light<float, false>(sf, rng, ib, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
+  V3<float> dL = La - Lb;
   V3<S> value;
   if (AD) {
+    const Edge<S>& Es = c.sc.edges[ei];
+    V3<S> xes = Es.p0 + (Es.p1 - Es.p0) * S(s);
     V3<S> ns(S(n.x), S(n.y), S(n.z));
     V3<S> nflip(S(n.x), S(n.y), S(-n.z));
-    S xdn = dot(xe - detach(xe), ns) + dot(c.cam_pos - detach(c.cam_pos), nflip);
+    S xdn = dot(xes - detach(xes), ns) + dot(c.cam_pos - detach(c.cam_pos), nflip);
     V3<S> dLs(S(dL.x), S(dL.y), S(dL.z));
-    value = dLs * (xdn / detach(pdf_e));
+    value = dLs * (xdn / S(pdf_e));
   } else {
-    value = V3<S>(S(dL.x), S(dL.y), S(dL.z)) / pdf_e;
+    V3<float> v = dL / pdf_e;
+    value = V3<S>(S(v.x), S(v.y), S(v.z));
   }
   valid = valid && finite3(value);
   return value;
@@ -193,9 +200,10 @@ template <class R> struct HyperCube {
   }
 };
 
-// path_integrator.cc:253-272 preprocess_primary_boundary (value mode)
+// path_integrator.cc:253-272 preprocess_primary_boundary (value mode, float)
 template <class R>
 inline HyperCube<R> preprocess_primary(const Ctx<R, false>& c) {
+  static_assert(std::is_same<R, float>::value, "the primary-edge term is evaluated in float");
   HyperCube<R> hc;
   int r = c.cfg.pe_res;
   hc.init(1, &r);
@@ -254,7 +262,8 @@ using namespace orc;
 // Film::add (camera.h:75-87): per pixel sum of the samples, divided by spp.
 template <class S, bool AD>
 static void render_camera(const Ctx<S, AD>& c, int which, double* img, const double* dLdI, double* dphi,
-                          double* per_sample, const Ctx<typename Traits<S>::R, false>* cv) {
+                          double* per_sample, const Ctx<typename Traits<S>::R, false>* cv,
+                          const Ctx<float, false>* cf) {
   using R = typename Traits<S>::R;
   const int H = c.cam.H, W = c.cam.W;
   const size_t npix = (size_t)H * W;
@@ -288,15 +297,15 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
   }
   // ---- primary boundary (renderD only; zero-valued, gradient only)
   if (which & 2) {
-    HyperCube<R> hc = preprocess_primary<R>(*cv);
+    HyperCube<float> hc = preprocess_primary<float>(*cf);
     const int spp = c.cfg.spp_primary_edge;
     const uint64_t N = (uint64_t)npix * spp;
     std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < (int64_t)N; ++i) {
       Pcg32 rng = make_sampler((uint64_t)i);
-      R s1 = rng.next_float();
-      R hp = hc.sample_reuse(&s1);
+      float s1 = rng.next_float();
+      float hp = hc.sample_reuse(&s1);
       int rx, ry;
       bool valid;
       V3<S> v = eval_primary<S, AD>(c, rng, s1, rx, ry, valid);
@@ -351,12 +360,28 @@ static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, cons
   const Scene<R>* scv;
   if constexpr (std::is_same<S, R>::value) scv = &sc;
   else { scv_own = mk_scene<R>(m, nm, l, nl, none); scv = &scv_own; }
+  Scene<float> scf_own;
+  const Scene<float>* scf = nullptr;
+  if (which & 2) {
+    if constexpr (std::is_same<S, float>::value) scf = &sc;
+    else { scf_own = mk_scene<float>(m, nm, l, nl, Seeds<float>{}); scf = &scf_own; }
+  }
   size_t off = 0;
   for (int ci = 0; ci < nc; ++ci) {
     Ctx<S, AD> c{sc, *scv, {}, {}, *cfg};
     c.cam.setup(cams[ci]);
     Ctx<R, false> cv{*scv, *scv, {}, {}, *cfg};
     cv.cam = c.cam;
+    Camera<float> camf;
+    camf.setup(cams[ci]);
+    V3<float> posf(cams[ci].look_from[0], cams[ci].look_from[1], cams[ci].look_from[2]);
+    c.scf = scf; c.camf = camf; c.posf = posf;
+    cv.scf = scf; cv.camf = camf; cv.posf = posf;
+    std::unique_ptr<Ctx<float, false>> cf;
+    if (scf) {
+      cf.reset(new Ctx<float, false>{*scf, *scf, camf, posf, *cfg});
+      cf->scf = scf; cf->camf = camf; cf->posf = posf;
+    }
     for (int k = 0; k < 3; ++k) {
       c.cam_pos[k] = Seeder<S>::make(cams[ci].look_from[k], seeds.campos, 3 * ci + k);
       cv.cam_pos[k] = R(cams[ci].look_from[k]);
@@ -364,7 +389,7 @@ static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, cons
     size_t npix = (size_t)c.cam.H * c.cam.W;
     std::vector<double> img(3 * npix, 0.0);
     for (int pass = 0; pass < std::max(1, cfg->n_pass); ++pass)
-      render_camera<S, AD>(c, which, img.data(), dLdI ? dLdI + off : nullptr, dphi, per_sample, &cv);
+      render_camera<S, AD>(c, which, img.data(), dLdI ? dLdI + off : nullptr, dphi, per_sample, &cv, cf.get());
     if (images) for (size_t i = 0; i < 3 * npix; ++i) images[off + i] = img[i] / std::max(1, cfg->n_pass);
     off += 3 * npix;
     if (per_sample) per_sample += 3 * npix * cfg->spp_interior;

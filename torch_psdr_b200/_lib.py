@@ -88,6 +88,9 @@ SIGNATURES = {
     "psdr_batch_forward": ([P, P], C.c_int),
     "psdr_batch_backward": ([P, P], C.c_int),
     "psdr_batch_destroy": ([P], C.c_int),
+    "psdr_profile_enable": ([C.c_int32], C.c_int),
+    "psdr_profile_reset": ([], C.c_int),
+    "psdr_profile_read": ([C.POINTER(C.c_int64), C.POINTER(C.c_double)], C.c_int),
 }
 
 _lib = None

@@ -211,6 +211,34 @@ PSDR_D bool tri_test(const RayPre& r, float3 p0, float3 p1, float3 p2, float tmi
   return true;
 }
 
+// ------------------------------------------------------------------ explicitly rounded ops
+// Used where a result must be bit-identical to the float oracle (the edge-sample rays
+// of the primary boundary term graze silhouettes, so their construction is exact).
+PSDR_D float3 sub_rn(float3 a, float3 b) { return f3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+PSDR_D float3 add_rn(float3 a, float3 b) { return f3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)); }
+PSDR_D float3 scale_rn(float3 a, float s) { return f3(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)); }
+PSDR_D float dot_rn(float3 a, float3 b) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+PSDR_D float norm_rn(float3 a) { return __fsqrt_rn(dot_rn(a, a)); }
+PSDR_D float3 normalize_rn(float3 a) {
+  const float n = norm_rn(a);
+  return f3(__fdiv_rn(a.x, n), __fdiv_rn(a.y, n), __fdiv_rn(a.z, n));
+}
+PSDR_D float3 cross_rn(float3 a, float3 b) {
+  return f3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+// row-major 4x4 affine/projective transform of a point, summed left to right
+PSDR_D float3 xform_pos_rn(const float* m, float3 p) {
+  auto row = [&](int r) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[4 * r], p.x), __fmul_rn(m[4 * r + 1], p.y)),
+                               __fmul_rn(m[4 * r + 2], p.z)), m[4 * r + 3]);
+  };
+  const float w = row(3);
+  return f3(__fdiv_rn(row(0), w), __fdiv_rn(row(1), w), __fdiv_rn(row(2), w));
+}
+
 // ------------------------------------------------------------------ traversal
 constexpr int kStack = 64;
 

@@ -54,6 +54,7 @@ struct DBuf {
 };
 
 int num_sms();
+void count_launches(int n);  // profiler launch counter (psdr_profile_read)
 
 // Scan / sort primitives (sort.cu).
 void exclusive_scan_int(const int* in, int* out, int n, int* tmp_blocks, cudaStream_t st);

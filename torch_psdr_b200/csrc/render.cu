@@ -195,10 +195,12 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
 
 // ------------------------------------------------------------------ trace kernel
 __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict__ scenes,
-                                               const DevView* __restrict__ views, int d) {
+                                               const DevView* __restrict__ views, int d,
+                                               unsigned long long* __restrict__ ray_count) {
   const int nk = w.cnt[2 * d + 1];
   const int Rd = (d == w.D - 1) ? w.R - 1 : w.R;
   const long long total = (long long)nk * Rd;
+  if (ray_count && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ray_count, (unsigned long long)total);
   const int stride = gridDim.x * blockDim.x;
   for (long long idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
     const int k = (int)(idx / Rd);
@@ -826,19 +828,22 @@ __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restr
       float ss = s1, pe;
       const int e = discrete_sample(sc.edge_pmf, sc.edge_cmf, ne, ss, pe);
       const float4 E0 = __ldg(sc.edge + 4 * (size_t)e), E1 = __ldg(sc.edge + 4 * (size_t)e + 1);
+      // ray construction in explicitly rounded ops (bit-identical to the float oracle)
       const float3 p0 = xyz(E0), p1 = xyz(E1);
-      const float3 xe = p0 + (p1 - p0) * ss;
-      const float pdf_e = pe / E0.w;
-      int px = 0, py = 0;
-      bool valid = ok && project(V, xe, px, py);
-      const float3 rd = normalize(xe - V.pos);
-      const float3 nrm = cross(rd, normalize(p1 - p0));
+      const float3 xe = add_rn(p0, scale_rn(sub_rn(p1, p0), ss));
+      const float pdf_e = __fdiv_rn(pe, E0.w);
+      const float3 pc = xform_pos_rn(V.w2c, xe);
+      const float3 pr = xform_pos_rn(V.c2r, pc);
+      const int px = (int)floorf(pr.x), py = (int)floorf(pr.y);
+      bool valid = ok && pc.z < 0.f && pr.x > 0.f && pr.x < (float)V.W && pr.y > 0.f && pr.y < (float)V.H;
+      const float3 rd = normalize_rn(sub_rn(xe, V.pos));
+      const float3 nrm = cross_rn(rd, normalize_rn(sub_rn(p1, p0)));
       HitRec ha, hb;
       ha.tri = hb.tri = -1;
       ha.b1 = ha.b2 = hb.b1 = hb.b2 = 0.f;
       if (valid) {
-        ha = trace_closest(sc, V.pos, rd - nrm * kEps, kTmin, INFINITY);
-        hb = trace_closest(sc, V.pos, rd + nrm * kEps, kTmin, INFINITY);
+        ha = trace_closest(sc, V.pos, sub_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
+        hb = trace_closest(sc, V.pos, add_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
       }
       const Surf a = make_surf(sc, ha.tri, ha.b1, ha.b2, V.pos);
       const Surf b = make_surf(sc, hb.tri, hb.b1, hb.b2, V.pos);
@@ -900,12 +905,12 @@ __global__ void __launch_bounds__(256) k_edge_final(WF w, const DevScene* __rest
     const float4 hb = eb.hb[s];
     if (__float_as_int(hb.w) == 0) continue;
     const float3 La = xyz(eb.La[s]), Lb = xyz(w.L[s]);
-    const float3 dL = La - Lb;
+    const float3 dL = sub_rn(La, Lb);
     const float4 a = eb.a[s];
     const float pdf_e = a.z;
     if (PRE) {
-      const float3 val = dL / pdf_e;
-      if (finite3(val)) mass[begin + s] = mass[begin + s] + norm(val);
+      const float3 val = f3(__fdiv_rn(dL.x, pdf_e), __fdiv_rn(dL.y, pdf_e), __fdiv_rn(dL.z, pdf_e));
+      if (finite3(val)) mass[begin + s] = __fadd_rn(mass[begin + s], norm_rn(val));
     } else {
       if (!finite3(dL * 0.0f)) continue;
       const float4 nn = eb.n[s];
@@ -1171,12 +1176,39 @@ void assign_offsets(std::vector<DevView>& views) {
   }
 }
 
+Profiler& profiler() {
+  static Profiler p;
+  return p;
+}
+void Profiler::begin_trace(cudaStream_t st) {
+  if (!on) return;
+  if (used == ev.size()) {
+    cudaEvent_t a, b;
+    PSDR_CUDA(cudaEventCreate(&a));
+    PSDR_CUDA(cudaEventCreate(&b));
+    ev.emplace_back(a, b);
+  }
+  PSDR_CUDA(cudaEventRecord(ev[used].first, st));
+}
+void Profiler::end_trace(cudaStream_t st) {
+  if (!on) return;
+  PSDR_CUDA(cudaEventRecord(ev[used].second, st));
+  ++used;
+  ++trace_launches;
+}
+#define PSDR_LAUNCHED(n) (profiler().launches += (n))
+void count_launches(int n) { profiler().launches += n; }
+
 static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int mode, cudaStream_t st) {
   const int cap = w.cap;
+  Profiler& pf = profiler();
   for (int d = 0; d < w.D; ++d) {
     if (mode == MODE_REPLAY) k_shade<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
     else k_shade<MODE_FWD><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
-    k_trace<<<grid_for((long long)cap * w.R, 128, 16), 128, 0, st>>>(w, scenes, views, d);
+    pf.begin_trace(st);
+    k_trace<<<grid_for((long long)cap * w.R, 128, 16), 128, 0, st>>>(w, scenes, views, d, pf.on ? pf.d_rays : nullptr);
+    pf.end_trace(st);
+    PSDR_LAUNCHED(3);
     if (mode == MODE_REPLAY) k_accum<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
     else k_accum<MODE_FWD><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
   }
@@ -1188,6 +1220,7 @@ static void run_tile(WF& w, const DevScene* scenes, const DevView* views, const 
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
   if (mode == MODE_REPLAY) k_camera<MODE_REPLAY><<<grid_for(tile.n, 256, 8), 256, 0, st>>>(w, scenes, views, tile);
   else k_camera<MODE_FWD><<<grid_for(tile.n, 256, 8), 256, 0, st>>>(w, scenes, views, tile);
+  PSDR_LAUNCHED(1);
   depth_loop(w, scenes, views, mode, st);
 }
 
@@ -1278,6 +1311,7 @@ void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views
   for (const Tile& t : plan_tiles(views, cap)) {
     run_tile(w, scenes_dev, vd, t, MODE_FWD, st);
     k_film<<<grid_for(t.npix, 256, 8), 256, 0, st>>>(w, vd, t, std::max(1, cfg.n_pass), samples_out);
+    PSDR_LAUNCHED(1);
   }
   PSDR_CUDA(cudaGetLastError());
 }
@@ -1287,12 +1321,15 @@ static void edge_phase(WF w, const DevScene* scenes, const DevView* vd, int v, c
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
   if (pre) k_edge_init<true><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round);
   else k_edge_init<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round);
+  PSDR_LAUNCHED(1);
   depth_loop(w, scenes, vd, MODE_FWD, st);
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
   k_edge_mid<<<grid_for(n, 256, 8), 256, 0, st>>>(w, vd, v, eb, n);
+  PSDR_LAUNCHED(1);
   depth_loop(w, scenes, vd, MODE_FWD, st);
   if (pre) k_edge_final<true><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, mass, spp);
   else k_edge_final<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, mass, spp);
+  PSDR_LAUNCHED(1);
   PSDR_CUDA(cudaGetLastError());
 }
 
@@ -1300,6 +1337,7 @@ static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, 
   HCube hc;
   const int b = (ncells + 255) / 256;
   k_mass_cdf<<<b, 256, 0, st>>>(ws->mass.as<float>(), ncells, ws->mass_d.as<double>());
+  PSDR_LAUNCHED(5);
   inclusive_scan_double(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), ncells, ws->scan_tmp.as<double>(), st);
   k_mass_finalize<<<b, 256, 0, st>>>(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), ncells,
                                      ws->hc_pmf.as<float>(), ws->hc_cmf.as<float>());
@@ -1334,6 +1372,7 @@ void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& view
     for (const Tile& t : plan_tiles(views, cap)) {
       run_tile(w, scenes_dev, vd, t, MODE_REPLAY, st);
       k_adjoint<<<grid_for(t.n, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+      PSDR_LAUNCHED(1);
     }
     PSDR_CUDA(cudaGetLastError());
   }
@@ -1366,6 +1405,7 @@ void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& view
       PSDR_CUDA(cudaMemsetAsync(ws->mass.p, 0, sizeof(float) * cells, st));
       HCube pre{};
       for (int k = 0; k < 3; ++k) { pre.res[k] = r3[k]; pre.unit[k] = 1.0f / (float)r3[k]; }
+      PSDR_LAUNCHED(cfg.secondary_edge_preprocess_rounds + 1);
       for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r)
         k_direct<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
                                                                  ws->mass.as<float>(), 1);
@@ -1381,6 +1421,59 @@ void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& view
 void grad_out(const double* acc, float* out, long long n, int accumulate, cudaStream_t st) {
   if (!out || n <= 0) return;
   k_grad_out<<<(int)((n + 255) / 256), 256, 0, st>>>(acc, out, n, accumulate);
+  PSDR_LAUNCHED(1);
 }
 
 }  // namespace psdr
+
+// ---------------------------------------------------------------- profiler C entry points
+using psdr::profiler;
+extern "C" {
+PSDR_API psdr_status psdr_profile_enable(int32_t on) {
+  try {
+    psdr::Profiler& p = profiler();
+    if (on && !p.d_rays) {
+      PSDR_CUDA(cudaMalloc(&p.d_rays, sizeof(unsigned long long)));
+      PSDR_CUDA(cudaMemset(p.d_rays, 0, sizeof(unsigned long long)));
+    }
+    p.on = on != 0;
+  } catch (const psdr::Error& e) {
+    psdr::set_error(e.msg);
+    return e.code;
+  }
+  return PSDR_OK;
+}
+PSDR_API psdr_status psdr_profile_reset(void) {
+  try {
+    psdr::Profiler& p = profiler();
+    p.used = 0;
+    p.launches = 0;
+    p.trace_launches = 0;
+    if (p.d_rays) PSDR_CUDA(cudaMemset(p.d_rays, 0, sizeof(unsigned long long)));
+  } catch (const psdr::Error& e) {
+    psdr::set_error(e.msg);
+    return e.code;
+  }
+  return PSDR_OK;
+}
+PSDR_API psdr_status psdr_profile_read(int64_t* out3, double* trace_ms) {
+  try {
+    psdr::Profiler& p = profiler();
+    double ms = 0;
+    for (size_t i = 0; i < p.used; ++i) {
+      PSDR_CUDA(cudaEventSynchronize(p.ev[i].second));
+      float t = 0;
+      PSDR_CUDA(cudaEventElapsedTime(&t, p.ev[i].first, p.ev[i].second));
+      ms += t;
+    }
+    unsigned long long rays = 0;
+    if (p.d_rays) PSDR_CUDA(cudaMemcpy(&rays, p.d_rays, sizeof(rays), cudaMemcpyDeviceToHost));
+    if (out3) { out3[0] = p.launches; out3[1] = p.trace_launches; out3[2] = (int64_t)rays; }
+    if (trace_ms) *trace_ms = ms;
+  } catch (const psdr::Error& e) {
+    psdr::set_error(e.msg);
+    return e.code;
+  }
+  return PSDR_OK;
+}
+}

@@ -81,6 +81,17 @@ struct psdr_workspace {
 };
 
 namespace psdr {
+// In-library profiler (psdr_profile_*): launch counts and trace-kernel event timing.
+struct Profiler {
+  bool on = false;
+  long long launches = 0, trace_launches = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  size_t used = 0;
+  unsigned long long* d_rays = nullptr;
+  void begin_trace(cudaStream_t st);
+  void end_trace(cudaStream_t st);
+};
+Profiler& profiler();
 struct SceneGradInfo;
 void make_view(const psdr_camera_desc& c, int spp, DevView& v);
 void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,

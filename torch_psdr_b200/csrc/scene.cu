@@ -143,7 +143,7 @@ __global__ void k_edge_build(const uint64_t* __restrict__ keys, const uint32_t* 
   float3 out = shared ? normalize(nl + nr) : normalize(cross(p1 - p0, nl));
   const float3 cp = normalize((p0 + p1) - (p2l + p2r));
   if (dot(cp, out) < 0.f && shared && norm(nl - nr) > kEps) { nl = -nl; nr = -nr; out = -out; }
-  const float len = norm(p0 - p1);
+  const float len = norm_rn(sub_rn(p0, p1));  // exact: the edge CDF matches the float oracle
   const int e = eidx[i];
   edge[4 * e + 0] = make_float4(p0.x, p0.y, p0.z, len);
   edge[4 * e + 1] = make_float4(p1.x, p1.y, p1.z, out.x);
@@ -449,6 +449,8 @@ void scene_build_geometry(psdr_scene* s) {
     s->dev.root = ~0;  // single triangle: the root is a leaf
   }
   k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), s->leaf.as<float4>());
+  // records + lights + half-edge sort (2 x passes x 5) + edge build/CDF (8) + BVH (9 + morton sort)
+  count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 9 + 3 * 4);
   PSDR_CUDA(cudaGetLastError());
   PSDR_CUDA(cudaMemcpyAsync(s->d_dev.p, &s->dev, sizeof(DevScene), cudaMemcpyHostToDevice, st));
 }
