@@ -159,6 +159,21 @@ PSDR_API psdr_status psdr_workspace_create(psdr_workspace** out);
 PSDR_API psdr_status psdr_workspace_destroy(psdr_workspace* ws);
 PSDR_API psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
                             const psdr_config* cfg, float** images, void* stream);
+/* Allocation-free variant of psdr_render_fwd for one camera; no counterpart in the
+ * reference. For callers that cannot allocate device memory at render time (a host
+ * that gives the library a fixed budget up front, a loop that cannot afford
+ * cudaMalloc's implicit device synchronisation, code that must not add allocation
+ * nodes to a stream being recorded). The wavefront tiles use one file-scope 32 MiB
+ * __device__ array per GPU, held until the process exits; tiles shrink to fit it, so
+ * any image size works, but spp_interior must not exceed the tile (about 100k paths
+ * with one light and one BSDF sample; larger values return PSDR_ERR_INVALID_ARG).
+ * The first call on a device resolves the array's address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture. All calls share the array and it
+ * keeps the last call's contents: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller. The scene is an input
+ * created earlier by psdr_scene_create; image is the (H,W,3) output. */
+PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const psdr_camera_desc* cam, const psdr_config* cfg,
+                                             float* image, void* stream);
 /* Per-sample interior radiance of one camera ((H*W*spp, 3) device buffer), the
  * values the film averages; used by the parity tests. */
 PSDR_API psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cam,

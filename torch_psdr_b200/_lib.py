@@ -80,6 +80,7 @@ SIGNATURES = {
     "psdr_workspace_destroy": ([P], C.c_int),
     "psdr_render_fwd": ([P, P, C.POINTER(CameraDesc), C.c_int32, C.POINTER(Config), C.POINTER(P), P], C.c_int),
     "psdr_render_samples": ([P, P, C.POINTER(CameraDesc), C.POINTER(Config), P, P], C.c_int),
+    "psdr_render_fwd_noalloc": ([P, C.POINTER(CameraDesc), C.POINTER(Config), P, P], C.c_int),
     "psdr_render_bwd": ([P, P, C.POINTER(CameraDesc), C.c_int32, C.POINTER(Config), C.POINTER(P),
                          C.POINTER(GradTargets), P], C.c_int),
     "psdr_batch_create": ([C.POINTER(P), C.c_int32, C.POINTER(CameraDesc), C.POINTER(C.c_int32), C.c_int32,

@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "render.h"
 
@@ -1476,4 +1478,130 @@ PSDR_API psdr_status psdr_profile_read(int64_t* out3, double* trace_ms) {
   }
   return PSDR_OK;
 }
+}
+
+// ================================================================== allocation-free forward
+// psdr_render_fwd_noalloc renders one camera without allocating device memory: the
+// wavefront buffers of each tile live in one file-scope __device__ array that every
+// GPU loading this library holds until the process exits. It exists for callers that
+// cannot call cudaMalloc at render time -- hosts that hand the library a fixed memory
+// budget up front (plugin hosts, engines with their own pools), latency-critical loops
+// where cudaMalloc's implicit device synchronisation is not acceptable, and code that
+// must not add allocation nodes while a stream is being recorded.
+namespace psdr {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of the scratch array for the current device. The first call on a
+// device looks it up with cudaGetSymbolAddress (the host-side symbol is only a
+// stand-in and must never be passed to a kernel).
+unsigned char* noalloc_scratch() {
+  int dev = 0;
+  PSDR_CUDA(cudaGetDevice(&dev));
+  PSDR_CHECK(dev >= 0 && dev < kNoAllocMaxDevices, "device index out of range for the allocation-free path");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    PSDR_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Bytes of scratch a tile of `cap` paths needs with R rays per path and depth D.
+size_t noalloc_bytes(size_t cap, int R, int D) {
+  size_t b = align256(sizeof(DevView));
+  b += align256(sizeof(int) * 2 * (D + 2));
+  b += 2 * align256(8 * cap);              // sampler state, stream increment
+  b += 2 * align256(4 * cap);              // view, pixel
+  b += 4 * align256(16 * cap);             // T, L, current vertex, origin
+  b += 3 * align256(4 * cap);              // queues
+  b += 4 * align256(16 * cap * (size_t)R); // ray origin/direction/aux, hits
+  return b;
+}
+
+}  // namespace
+}  // namespace psdr
+
+extern "C" PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const psdr_camera_desc* cam,
+                                                        const psdr_config* cfg, float* image, void* stream) {
+  using namespace psdr;
+  try {
+    PSDR_CHECK(scene != nullptr && cam != nullptr && cfg != nullptr && image != nullptr, "null argument");
+    PSDR_CHECK(cfg->n_pass > 0 && cfg->spp_interior > 0, "n_pass and spp_interior must be > 0");
+    PSDR_CHECK(cfg->max_bounce > 0 && cfg->max_bounce <= kMaxDepth, "max_bounce must be in [1, 16]");
+    PSDR_CHECK(cfg->mis_light_samples >= 0 && cfg->mis_bsdf_samples >= 0, "mis sample counts must be >= 0");
+    PSDR_CHECK(cam->type == PSDR_CAM_PERSPECTIVE, "only perspective cameras are supported");
+    PSDR_CHECK(cam->height > 0 && cam->width > 0, "camera height and width must be > 0");
+    PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
+    const int R = cfg->mis_light_samples + cfg->mis_bsdf_samples + 1;
+    PSDR_CHECK(R <= kMaxRays, "too many mis samples");
+    const int D = cfg->max_bounce;
+    // largest tile (multiple of 32 paths) that fits the fixed scratch
+    size_t cap = kNoAllocScratchBytes / (100 + 64 * (size_t)R);
+    cap &= ~size_t(31);
+    while (cap > 32 && noalloc_bytes(cap, R, D) > kNoAllocScratchBytes) cap -= 32;
+    if ((size_t)cfg->spp_interior > cap) {
+      set_error("psdr_render_fwd_noalloc: spp_interior " + std::to_string(cfg->spp_interior) +
+                " exceeds the allocation-free tile of " + std::to_string(cap) + " paths (32 MiB scratch)");
+      return PSDR_ERR_INVALID_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned char* base = noalloc_scratch();
+    size_t off = 0;
+    auto take = [&](size_t bytes) { unsigned char* p = base + off; off += align256(bytes); return p; };
+    DevView* vd = reinterpret_cast<DevView*>(take(sizeof(DevView)));
+    WF w{};
+    w.cap = (int)cap;
+    w.cnt = reinterpret_cast<int*>(take(sizeof(int) * 2 * (D + 2)));
+    w.rs = reinterpret_cast<unsigned long long*>(take(8 * cap));
+    w.ri = reinterpret_cast<unsigned long long*>(take(8 * cap));
+    w.view = reinterpret_cast<int*>(take(4 * cap));
+    w.pix = reinterpret_cast<int*>(take(4 * cap));
+    w.T = reinterpret_cast<float4*>(take(16 * cap));
+    w.L = reinterpret_cast<float4*>(take(16 * cap));
+    w.cur = reinterpret_cast<float4*>(take(16 * cap));
+    w.org = reinterpret_cast<float4*>(take(16 * cap));
+    w.q0 = reinterpret_cast<int*>(take(4 * cap));
+    w.q1 = reinterpret_cast<int*>(take(4 * cap));
+    w.qs = reinterpret_cast<int*>(take(4 * cap));
+    w.ro = reinterpret_cast<float4*>(take(16 * cap * R));
+    w.rd = reinterpret_cast<float4*>(take(16 * cap * R));
+    w.ra = reinterpret_cast<float4*>(take(16 * cap * R));
+    w.hit = reinterpret_cast<float4*>(take(16 * cap * R));
+    w.rec = nullptr;
+    set_wf(w, *cfg, 1, -1, cfg->enable_light_visable);
+    // the view record goes into the scratch too (the previous call's view is overwritten)
+    DevView V;
+    make_view(*cam, cfg->spp_interior, V);
+    V.sample_off = 0;
+    V.pix_off = 0;
+    V.image = image;
+    PSDR_CUDA(cudaMemcpyAsync(vd, &V, sizeof(DevView), cudaMemcpyHostToDevice, st));
+    // tiles of whole pixels, walked without building a host-side list
+    const long long npix = (long long)cam->height * cam->width;
+    const long long pix_per_tile = (long long)cap / cfg->spp_interior;
+    for (long long p0 = 0; p0 < npix; p0 += pix_per_tile) {
+      const long long np = std::min(pix_per_tile, npix - p0);
+      Tile t{p0 * cfg->spp_interior, (int)(np * cfg->spp_interior), p0, (int)np};
+      run_tile(w, scene->d_dev.as<DevScene>(), vd, t, MODE_FWD, st);  // clears the queue counters first
+      k_film<<<grid_for(t.npix, 256, 8), 256, 0, st>>>(w, vd, t, std::max(1, cfg->n_pass), nullptr);
+    }
+    PSDR_CUDA(cudaGetLastError());
+  } catch (const psdr::Error& e) {
+    psdr::set_error(e.msg);
+    return e.code;
+  } catch (const std::exception& e) {
+    psdr::set_error(e.what());
+    return PSDR_ERR_CUDA;
+  }
+  return PSDR_OK;
 }
