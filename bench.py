@@ -314,7 +314,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference", "ours"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=512, help="image size (512 = the benchmark workload)")
+    ap.add_argument("--spp", type=int, default=32, help="interior spp (32 = the benchmark workload)")
     args = ap.parse_args()
+    global H, W, SPP
+    if args.size != 512 or args.spp != 32:
+        H = W = args.size
+        SPP = args.spp
+        CFG["spp_interior"] = SPP
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
