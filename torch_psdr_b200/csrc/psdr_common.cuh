@@ -253,8 +253,16 @@ PSDR_D float safe_inv(float d) { return 1.0f / (fabsf(d) > 1e-30f ? d : copysign
 // expanded at build time and the cull bound is relaxed by 1e-5 relative so that no
 // triangle the exact test would accept is culled (the KAT checks this against brute
 // force on every ray).
-PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, float tmax) {
-  RayPre rp = ray_pre(o, d);
+//
+// t_occ turns the query into an occlusion test below t_occ: the first triangle hit
+// with t < t_occ ends the traversal and the ray reports a miss. Shadow rays use it
+// with t_occ = |y - x| - 4e-3: any such hit lies >= 4e-3 from the light point y, so
+// the reference's test |hit - y|^2 < 1e-5 (path_integrator.cc:114-116) fails for it
+// exactly as it would for the true closest hit; hits at or beyond t_occ are resolved
+// as closest hits.
+PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, float tmax,
+                            float t_occ = -INFINITY) {
+  const RayPre rp = ray_pre(o, d);
   const float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
   const float3 oi = f3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
   HitRec h;
@@ -303,6 +311,11 @@ PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, 
         const float4 q0 = __ldg(lt), q1 = __ldg(lt + 1), q2 = __ldg(lt + 2);
         float tt, b1, b2;
         if (tri_test(rp, xyz(q0), xyz(q1), xyz(q2), tmin, h.t, tt, b1, b2)) {
+          if (tt < t_occ) {  // occluded before the target: report a miss
+            h.tri = -1;
+            h.t = tt;
+            return h;
+          }
           const int id = __float_as_int(q0.w);
           if (tt < h.t || h.tri < 0 || id < h.tri) { h.t = tt; h.tri = id; h.b1 = b1; h.b2 = b2; }
         }

@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/psdr.h"
+#include "psdr.h"
 #include "psdr_common.cuh"
 
 namespace psdr {

@@ -161,34 +161,38 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
     if (!go) continue;
     w.qs[k] = s;
     Rng rng{w.rs[s], w.ri[s]};
-    const size_t base = (size_t)k * w.R;
+    // rays are stored type-major (slot r * cap + k): a warp of k_trace then traces
+    // rays of one kind from neighbouring paths
+    const size_t cs = (size_t)w.cap;
     for (int i = 0; i < w.nL; ++i) {
       const float rx = rng.next_float(), ry = rng.next_float();
       const LightSample ls = sample_light(*sc, rx, ry);
       const float3 dv = ls.y - x.p;
       const float3 dir = normalize(dv);
       const float dist = norm(dv);
-      w.ro[base + i] = make_float4(x.p.x, x.p.y, x.p.z, dist * 1.0001f + 4e-3f);
-      w.rd[base + i] = make_float4(dir.x, dir.y, dir.z, __int_as_float(ls.light));
-      w.ra[base + i] = make_float4(ls.y.x, ls.y.y, ls.y.z, ls.pdf);
+      const size_t slot = i * cs + k;
+      w.ro[slot] = make_float4(x.p.x, x.p.y, x.p.z, dist * 1.0001f + 4e-3f);
+      w.rd[slot] = make_float4(dir.x, dir.y, dir.z, __int_as_float(ls.light));
+      w.ra[slot] = make_float4(ls.y.x, ls.y.y, ls.y.z, ls.pdf);
     }
     for (int j = 0; j < w.nB; ++j) {
       const float rx = rng.next_float(), ry = rng.next_float();
       float ct, st, sp, cp;
       const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
-      w.ro[base + w.nL + j] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
-      w.rd[base + w.nL + j] = make_float4(wo.x, wo.y, wo.z, 0.f);
-      w.ra[base + w.nL + j] = make_float4(ct, 0.f, 0.f, 0.f);
+      const size_t slot = (w.nL + j) * cs + k;
+      w.ro[slot] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
+      w.rd[slot] = make_float4(wo.x, wo.y, wo.z, 0.f);
+      w.ra[slot] = make_float4(ct, 0.f, 0.f, 0.f);
     }
     {
       const float rx = rng.next_float(), ry = rng.next_float();
       if (!last) {
         float ct, st, sp, cp;
         const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
-        const int r = w.nL + w.nB;
-        w.ro[base + r] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
-        w.rd[base + r] = make_float4(wo.x, wo.y, wo.z, 0.f);
-        w.ra[base + r] = make_float4(ct, 0.f, 0.f, 0.f);
+        const size_t slot = (w.nL + w.nB) * cs + k;
+        w.ro[slot] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
+        w.rd[slot] = make_float4(wo.x, wo.y, wo.z, 0.f);
+        w.ra[slot] = make_float4(ct, 0.f, 0.f, 0.f);
       }
     }
     w.rs[s] = rng.state;
@@ -205,13 +209,15 @@ __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict_
   if (ray_count && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ray_count, (unsigned long long)total);
   const int stride = gridDim.x * blockDim.x;
   for (long long idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
-    const int k = (int)(idx / Rd);
-    const int r = (int)(idx - (long long)k * Rd);
-    const size_t slot = (size_t)k * w.R + r;
+    const int r = (int)(idx / nk);
+    const int k = (int)(idx - (long long)r * nk);
+    const size_t slot = (size_t)r * w.cap + k;
     const int s = w.qs[k];
     const DevScene& sc = scenes[views[w.view[s]].scene];
     const float4 o = w.ro[slot], dd = w.rd[slot];
-    const HitRec h = trace_closest(sc, xyz(o), xyz(dd), kTmin, o.w);
+    // light-sample rays (r < nL) are occlusion tests below the target point
+    const float t_occ = r < w.nL ? (o.w - 4e-3f) / 1.0001f - 4e-3f : -INFINITY;
+    const HitRec h = trace_closest(sc, xyz(o), xyz(dd), kTmin, o.w, t_occ);
     w.hit[slot] = hit4(h);
   }
 }
@@ -232,15 +238,15 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
     if (k < n) {
       s = w.qs[k];
       const DevScene& sc = scenes[views[w.view[s]].scene];
-      const size_t base = (size_t)k * w.R;
+      const size_t cs = (size_t)w.cap;
       const float4 c = w.cur[s];
       const Surf x = make_surf(sc, __float_as_int(c.x), c.y, c.z, xyz(w.org[s]));
       if (MODE == MODE_REPLAY) {
         float4* rec = w.rec + (size_t)s * w.rec_stride + 1 + (size_t)d * w.R;
         const int Rd = last ? w.R - 1 : w.R;
-        for (int r = 0; r < Rd; ++r) rec[r] = w.hit[base + r];
+        for (int r = 0; r < Rd; ++r) rec[r] = w.hit[r * cs + k];
         if (!last) {
-          const float4 h = w.hit[base + w.nL + w.nB];
+          const float4 h = w.hit[(w.nL + w.nB) * cs + k];
           if (__float_as_int(h.x) >= 0) {
             w.cur[s] = h;
             w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
@@ -253,10 +259,10 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
         const DevObj& ob = sc.objs[x.obj];
         const float3 bsdf = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v)) * kInvPi;
         for (int i = 0; i < w.nL; ++i) {
-          const float4 h = w.hit[base + i];
+          const float4 h = w.hit[i * cs + k];
           const int tri = __float_as_int(h.x);
           if (tri < 0) continue;
-          const float4 dd = w.rd[base + i], aux = w.ra[base + i];
+          const float4 dd = w.rd[i * cs + k], aux = w.ra[i * cs + k];
           const float3 dir = xyz(dd);
           const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
           if (!(q.is_light && sqnorm(q.p - xyz(aux)) < kEps)) continue;
@@ -270,11 +276,12 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
           L += mul(T, f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z)) * sc_;
         }
         for (int j = 0; j < w.nB; ++j) {
-          const float4 h = w.hit[base + w.nL + j];
+          const size_t slot = (w.nL + j) * cs + k;
+          const float4 h = w.hit[slot];
           const int tri = __float_as_int(h.x);
           if (tri < 0) continue;
-          const float3 wo = xyz(w.rd[base + w.nL + j]);
-          const float ct = w.ra[base + w.nL + j].x;
+          const float3 wo = xyz(w.rd[slot]);
+          const float ct = w.ra[slot].x;
           const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
           if (!q.is_light) continue;
           const DevLight& Lt = sc.lights[q.light];
@@ -287,12 +294,12 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
           L += mul(T, f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z)) * sc_;
         }
         if (!last) {
-          const int r = w.nL + w.nB;
-          const float4 h = w.hit[base + r];
+          const size_t slot = (w.nL + w.nB) * cs + k;
+          const float4 h = w.hit[slot];
           const int tri = __float_as_int(h.x);
           if (tri >= 0) {
-            const float3 wo = xyz(w.rd[base + r]);
-            const float ct = w.ra[base + r].x;
+            const float3 wo = xyz(w.rd[slot]);
+            const float ct = w.ra[slot].x;
             const Surf nx = make_surf(sc, tri, h.y, h.z, x.p);
             const float tmp = dot(nx.n, -wo) / nx.sqd;
             const float G = dot(x.n, wo) * tmp;
@@ -993,7 +1000,10 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     const float3 dir = normalize(xb - ls.y);
     bool valid = dot(nl, dir) * dot(nr, dir) < 0.f && norm(nl - nr) > kEps;
     if (!valid) continue;
-    const HitRec hs = trace_closest(sc, xb, -dir, kTmin, INFINITY);
+    // edge -> light: the same occlusion shortcut as the NEE rays (valid needs the
+    // closest hit to be the light within sqrt(1e-5) of y)
+    const float dist_l = norm(xb - ls.y);
+    const HitRec hs = trace_closest(sc, xb, -dir, kTmin, dist_l * 1.0001f + 4e-3f, dist_l - 4e-3f);
     const Surf s0 = make_surf(sc, hs.tri, hs.b1, hs.b2, xb);
     if (!(s0.valid && s0.is_light && sqnorm(s0.p - ls.y) < kEps)) continue;
     const HitRec hd = trace_closest(sc, xb, dir, kTmin, INFINITY);

@@ -241,8 +241,16 @@ __global__ void k_morton(int n, const float4* __restrict__ tri, const unsigned i
     float t = e > 0.f ? (x - l) / e : 0.5f;
     return (unsigned int)fminf(fmaxf(t * 1024.0f, 0.0f), 1023.0f);
   };
-  const unsigned int m = (expand_bits(q(c.x, lo.x, ext.x)) << 2) | (expand_bits(q(c.y, lo.y, ext.y)) << 1) |
-                         expand_bits(q(c.z, lo.z, ext.z));
+  unsigned int m = (expand_bits(q(c.x, lo.x, ext.x)) << 2) | (expand_bits(q(c.y, lo.y, ext.y)) << 1) |
+                   expand_bits(q(c.z, lo.z, ext.z));
+  // Triangles whose box spans more than a quarter of the scene (ground planes, walls)
+  // get the top key bit, so the root splits them off instead of letting them inflate
+  // the box of whatever small-triangle cluster shares their centroid cell.
+  const float3 glo = f3(ord2f(cbox[6]), ord2f(cbox[7]), ord2f(cbox[8]));
+  const float3 ghi = f3(ord2f(cbox[9]), ord2f(cbox[10]), ord2f(cbox[11]));
+  const float sext = fmaxf(fmaxf(ghi.x - glo.x, ghi.y - glo.y), ghi.z - glo.z);
+  const float text = fmaxf(fmaxf(bh.x - bl.x, bh.y - bl.y), bh.z - bl.z);
+  if (text > 0.25f * sext) m |= 1u << 30;
   keys[i] = m;
   vals[i] = (uint32_t)i;
 }
@@ -433,7 +441,7 @@ void scene_build_geometry(psdr_scene* s) {
   k_cbox_init<<<1, 32, 0, st>>>(cbox);
   k_centroid_box<<<nblk(n), 256, 0, st>>>(n, s->tri.as<float4>(), cbox);
   k_morton<<<nblk(n), 256, 0, st>>>(n, s->tri.as<float4>(), cbox, keys, vals);
-  radix_sort_pairs(keys, vals, n, 30, s->sort_tmp, st);
+  radix_sort_pairs(keys, vals, n, 31, s->sort_tmp, st);
   int2* child = s->aux_i.as<int2>();
   int2* range = s->range.as<int2>();
   int* parent = s->parent.as<int>();
