@@ -186,10 +186,16 @@ PSDR_API psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, cons
                             void* stream);
 
 /* ---------------------------------------------------------------- batching
- * Many views over one or more scenes in one work list, captured into CUDA graphs
- * (one for the forward, one for the backward) on first launch and replayed after.
+ * Many views over one or more scenes in one work list (small views share tiles),
+ * recorded into two CUDA graphs on first use and replayed with one launch each
+ * (no counterpart in the reference, which renders cameras one by one with a device
+ * synchronisation per ray query, path_integrator.cc:381-406).
  * cam_scene[c] selects the scene of camera c. images / d_images / grads are bound
- * at creation and must stay valid. grads has one entry per scene. */
+ * at creation and must stay valid; d_images may be NULL for a forward-only batch.
+ * grads has one entry per scene; its camera_origin array is indexed by the global
+ * camera index. psdr_batch_forward first rebuilds every scene's geometry from its
+ * vertex buffers (so vertices changed in place are picked up), then renders;
+ * psdr_batch_backward runs the full adjoint. Both need a non-default stream. */
 PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scenes, const psdr_camera_desc* cams,
                               const int32_t* cam_scene, int32_t n_cams, const psdr_config* cfg, float** images,
                               const float** d_images, const psdr_grad_targets* grads, psdr_batch** out);

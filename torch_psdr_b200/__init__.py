@@ -7,10 +7,10 @@
 The renderer is the native library libpsdr_b200.so (include/psdr.h): an LBVH and
 wavefront path-tracing kernels for sm_100a with a path-replay adjoint.
 """
-from .api import (AreaLight, BaseCamera, Camera, DiffuseBsdfMaterial, DiffuseMaterial, EnvLight, Light, Material,
+from .api import (AreaLight, BaseCamera, BatchRender, Camera, DiffuseBsdfMaterial, DiffuseMaterial, EnvLight, Light, Material,
                   Mesh, OrthographicCamera, PathIntegrator, PerspectiveCamera, PrincipledMaterial, Scene, SH9Light,
                   Texture, VarContex)
 
-__all__ = ["AreaLight", "BaseCamera", "Camera", "DiffuseBsdfMaterial", "DiffuseMaterial", "EnvLight", "Light",
+__all__ = ["AreaLight", "BaseCamera", "BatchRender", "Camera", "DiffuseBsdfMaterial", "DiffuseMaterial", "EnvLight", "Light",
            "Material", "Mesh", "OrthographicCamera", "PathIntegrator", "PerspectiveCamera", "PrincipledMaterial",
            "Scene", "SH9Light", "Texture", "VarContex"]

@@ -201,6 +201,18 @@ class Mesh(VarContex):
         self.append_variable(vertices)
         self.merge_variables(material.get_variables())
 
+    def set_vertices(self, vertices: Tensor):
+        """Copy new vertex positions (same count) into the buffer the native scene reads
+        when it rebuilds (psdr_scene_update, or the forward graph of a BatchRender); the
+        given tensor becomes the one that receives the vertex gradient."""
+        assert tuple(vertices.shape) == tuple(self.v.shape)
+        self.v.copy_(vertices.detach())
+        self.vertices = vertices
+
+    def get_variables(self):
+        out = [self.vertices] if self.vertices.requires_grad else []
+        return out + self.material.get_variables()
+
     def _desc(self):
         d = L.MeshDesc()
         d.vertices, d.num_vertices = self.v.data_ptr(), int(self.v.shape[0])
@@ -263,12 +275,6 @@ class Scene(VarContex):
         self.cameras = list(cameras)
         self.meshes = list(meshes)
         self.lights = list(lights)
-        for c in self.cameras:
-            self.merge_variables(c.get_variables())
-        for m in self.meshes:
-            self.merge_variables(m.get_variables())
-        for lt in self.lights:
-            self.merge_variables(lt.get_variables())
         lib = L.load()
         md = (L.MeshDesc * max(1, len(self.meshes)))(*[m._desc() for m in self.meshes])
         ld = (L.AreaLightDesc * max(1, len(self.lights)))(*[lt._desc() for lt in self.lights])
@@ -282,10 +288,21 @@ class Scene(VarContex):
     def handle(self):
         return self._handle
 
+    def get_variables(self):
+        """Tensors requiring grad, cameras then meshes then lights (torch_psdr.py:469-471)."""
+        out = []
+        for part in self.cameras + self.meshes + self.lights:
+            out += [t for t in part.get_variables() if t.requires_grad]
+        return out
+
     def info(self):
         out = (C.c_int64 * 6)()
         L.check(self._lib.psdr_scene_info(self._handle, out), "psdr_scene_info")
         return dict(zip(["triangles", "vertices", "edges", "bvh_nodes", "lights", "objects"], list(out)))
+
+    def update(self):
+        """Rebuild triangle records, edges, CDFs and the BVH after Mesh.set_vertices."""
+        L.check(self._lib.psdr_scene_update(self._handle, _stream()), "psdr_scene_update")
 
     def _camera_descs(self):
         return (L.CameraDesc * len(self.cameras))(*[c._desc() for c in self.cameras])
@@ -457,3 +474,138 @@ class PathIntegrator:
             return self._render(scene)
         imgs = _RenderD.apply(self, scene, *torch_vars)
         return list(imgs)
+
+
+class BatchRender:
+    """All cameras of one or more scenes rendered as one work list from CUDA graphs.
+
+    The forward graph rebuilds every scene's geometry from its meshes' vertex buffers
+    (update them in place with `Mesh.set_vertices`) and renders every camera; the
+    backward graph runs the path-replay adjoint and both edge terms for all views.
+    Images, image gradients and gradient buffers are allocated once and bound to the
+    graphs. Extension: the reference has no batching.
+    """
+
+    def __init__(self, integrator: PathIntegrator, scenes: List[Scene], differentiable: bool = True):
+        self.integrator = integrator
+        self.scenes = list(scenes)
+        self.lib = L.load()
+        self.stream = torch.cuda.Stream()
+        dev = "cuda"
+        cams, cam_scene = [], []
+        for si, sc in enumerate(self.scenes):
+            for c in sc.cameras:
+                cams.append(c)
+                cam_scene.append(si)
+        self.cams = cams
+        self.images = [torch.zeros((c.height, c.width, 3), dtype=torch.float32, device=dev) for c in cams]
+        self.d_images = [torch.zeros_like(i) for i in self.images] if differentiable else None
+        P = C.c_void_p
+        self._keep = []
+        targets = []
+        self.grads = []
+        cam_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in cams]
+        cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
+        self.cam_grads = cam_g
+        for sc in self.scenes:
+            vg = [torch.zeros_like(m.v) for m in sc.meshes] + [torch.zeros_like(lt.v) for lt in sc.lights]
+            tg = [torch.zeros_like(m.material.texture.data) for m in sc.meshes]
+            eg = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in sc.lights]
+            self.grads.append((vg, tg, eg))
+            vp = (P * max(1, len(vg)))(*[t.data_ptr() for t in vg])
+            tp = (P * max(1, len(tg)))(*[t.data_ptr() for t in tg])
+            ep = (P * max(1, len(eg)))(*[t.data_ptr() for t in eg])
+            self._keep += [vp, tp, ep]
+            targets.append(L.GradTargets(vp, tp, ep, cp, 0))
+        self._keep.append(cp)
+        tgt = (L.GradTargets * len(targets))(*targets)
+        sh = (P * len(self.scenes))(*[s.handle for s in self.scenes])
+        cd = (L.CameraDesc * len(cams))(*[c._desc() for c in cams])
+        csc = (C.c_int32 * len(cams))(*cam_scene)
+        ip = (P * len(cams))(*[t.data_ptr() for t in self.images])
+        dp = (P * len(cams))(*[t.data_ptr() for t in self.d_images]) if differentiable else None
+        self._keep += [tgt, sh, cd, csc, ip, dp]
+        h = C.c_void_p()
+        torch.cuda.synchronize()
+        L.check(self.lib.psdr_batch_create(sh, len(self.scenes), cd, csc, len(cams), C.byref(integrator.cfg), ip, dp,
+                                           tgt, C.byref(h)), "psdr_batch_create")
+        self._handle = h
+
+    def forward(self) -> List[Tensor]:
+        """Rebuild geometry and render every camera (returns the bound image buffers)."""
+        cur = torch.cuda.current_stream()
+        self.stream.wait_stream(cur)
+        L.check(self.lib.psdr_batch_forward(self._handle, C.c_void_p(self.stream.cuda_stream)), "psdr_batch_forward")
+        cur.wait_stream(self.stream)
+        return self.images
+
+    def backward(self, d_images: List[Tensor]):
+        """Run the adjoint for dLoss/dImage of every camera; fills the bound gradient buffers."""
+        for dst, g in zip(self.d_images, d_images):
+            if g is None:
+                dst.zero_()
+            else:
+                dst.copy_(g)
+        cur = torch.cuda.current_stream()
+        self.stream.wait_stream(cur)
+        L.check(self.lib.psdr_batch_backward(self._handle, C.c_void_p(self.stream.cuda_stream)),
+                "psdr_batch_backward")
+        cur.wait_stream(self.stream)
+
+    def renderD(self) -> List[Tensor]:
+        """Differentiable batched render: images whose backward fills .grad of the
+        scenes' input tensors, like PathIntegrator.renderD."""
+        torch_vars = []
+        for sc in self.scenes:
+            torch_vars += sc.get_variables()
+        return list(_BatchRenderD.apply(self, *torch_vars))
+
+    def _map_grads(self, torch_vars):
+        acc = {}
+
+        def add(t, g):
+            if t is None or not isinstance(t, Tensor) or not t.requires_grad:
+                return
+            g = g.reshape(t.shape).to(t.dtype)
+            acc[id(t)] = g if id(t) not in acc else acc[id(t)] + g
+
+        k = 0
+        for sc, (vg, tg, eg) in zip(self.scenes, self.grads):
+            nm = len(sc.meshes)
+            for i, m in enumerate(sc.meshes):
+                add(m.vertices, vg[i])
+                add(m.material.texture.tensor, tg[i])
+            for j, lt in enumerate(sc.lights):
+                add(lt.vertices, vg[nm + j])
+                add(lt.emit, eg[j])
+            for c in sc.cameras:
+                add(c.look_from, self.cam_grads[k])
+                for t in (c.look_at, c.up, c.vfov):
+                    add(t, torch.zeros_like(t, dtype=torch.float32))
+                k += 1
+        return [acc.get(id(t), torch.zeros_like(t)) for t in torch_vars]
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                torch.cuda.synchronize()
+                self.lib.psdr_batch_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+
+class _BatchRenderD(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, batch, *torch_vars):
+        imgs = batch.forward()
+        ctx.batch = batch
+        ctx.vars = torch_vars
+        return tuple(i.clone() for i in imgs)
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx, *grads):
+        ctx.batch.backward(list(grads))
+        return (None,) + tuple(ctx.batch._map_grads(ctx.vars))

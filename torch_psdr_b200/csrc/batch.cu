@@ -1,0 +1,227 @@
+// batch.cu -- many views over one or more scenes as one work list, replayed from CUDA
+// graphs (psdr_batch_*). The reference renders cameras one after another with a
+// device synchronisation per ray query (path_integrator.cc:381-406,
+// scene_optix.cc:240-277); here all views share the wavefront tiles (small views
+// are packed together), and the whole forward (optionally preceded by the scenes'
+// geometry rebuild) and the whole backward are each recorded once into a graph and
+// replayed with a single launch.
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "render.h"
+
+struct psdr_batch {
+  std::vector<psdr_scene*> scenes;
+  std::vector<psdr::DevView> views;
+  psdr_config cfg{};
+  psdr_workspace ws;
+  psdr::DBuf scenes_dev;  // DevScene array, one entry per scene
+  psdr::DBuf campos;      // fp64 camera-origin accumulators, 3 per view
+  int cap = 0;
+  bool backward = false;
+  bool rebuild = true;
+  psdr::SceneGradInfo gi;
+  // gradient targets, deep-copied pointer arrays per scene
+  std::vector<std::vector<float*>> gv, gt, ge;
+  std::vector<float*> gc;
+  std::vector<int> gacc;
+  cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
+  long long fwd_launches = 0, bwd_launches = 0;
+  ~psdr_batch() {
+    if (fwd_exec) cudaGraphExecDestroy(fwd_exec);
+    if (bwd_exec) cudaGraphExecDestroy(bwd_exec);
+  }
+};
+
+namespace psdr {
+namespace {
+
+// Records `body` on `st` into a graph and instantiates it.
+template <class F>
+cudaGraphExec_t capture(cudaStream_t st, F body, long long& launches) {
+  Profiler& pf = profiler();
+  const bool was_on = pf.on;
+  pf.on = false;  // no timing events inside graphs
+  const long long l0 = pf.launches;
+  PSDR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    body();
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(st, &g);
+    if (g) cudaGraphDestroy(g);
+    pf.on = was_on;
+    throw;
+  }
+  cudaGraph_t graph = nullptr;
+  PSDR_CUDA(cudaStreamEndCapture(st, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  pf.on = was_on;
+  PSDR_CUDA(e);
+  launches = pf.launches - l0;
+  pf.launches = l0;
+  return exec;
+}
+
+}  // namespace
+}  // namespace psdr
+
+using namespace psdr;
+
+extern "C" {
+
+PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scenes, const psdr_camera_desc* cams,
+                                       const int32_t* cam_scene, int32_t n_cams, const psdr_config* cfg,
+                                       float** images, const float** d_images, const psdr_grad_targets* grads,
+                                       psdr_batch** out) {
+  psdr_batch* b = nullptr;
+  try {
+    PSDR_CHECK(out != nullptr && scenes != nullptr && n_scenes > 0 && cam_scene != nullptr && images != nullptr,
+               "null argument");
+    *out = nullptr;
+    check_config(cfg);
+    check_cameras(cams, n_cams);
+    for (int i = 0; i < n_scenes; ++i) {
+      PSDR_CHECK(scenes[i] != nullptr, "null scene");
+      PSDR_CHECK(scenes[i]->nlight > 0 || cfg->mis_light_samples == 0, "a scene has no light to sample");
+    }
+    b = new psdr_batch();
+    b->scenes.assign(scenes, scenes + n_scenes);
+    b->cfg = *cfg;
+    b->backward = d_images != nullptr;
+    if (b->backward) {
+      PSDR_CHECK(grads != nullptr, "d_images given without gradient targets");
+      PSDR_CHECK(cfg->estimator == PSDR_EST_REFERENCE, "only the reference estimator is available in this build");
+    }
+    cudaStream_t st = nullptr;
+    b->campos.alloc(sizeof(double) * 3 * n_cams, st);
+    b->views.resize(n_cams);
+    for (int i = 0; i < n_cams; ++i) {
+      PSDR_CHECK(cam_scene[i] >= 0 && cam_scene[i] < n_scenes, "camera scene index out of range");
+      PSDR_CHECK(images[i] != nullptr, "null image buffer");
+      make_view(cams[i], cfg->spp_interior, b->views[i]);
+      b->views[i].scene = cam_scene[i];
+      b->views[i].image = images[i];
+      b->views[i].dimage = b->backward ? d_images[i] : nullptr;
+      b->views[i].grad_pos = b->campos.as<double>() + 3 * i;
+      if (b->backward) PSDR_CHECK(d_images[i] != nullptr, "null image gradient");
+    }
+    assign_offsets(b->views);
+    b->cap = choose_cap(*cfg, b->views, true);
+    const int Rmax = cfg->mis_light_samples + std::max(cfg->mis_bsdf_samples, 1) + 1;
+    b->ws.ensure(b->cap, Rmax, cfg->max_bounce, n_cams, b->backward ? 1 : 0, st);
+    upload_views(&b->ws, b->views, st);
+    std::vector<DevScene> ds(n_scenes);
+    for (int i = 0; i < n_scenes; ++i) ds[i] = scenes[i]->dev;
+    b->scenes_dev.alloc(sizeof(DevScene) * n_scenes, st);
+    PSDR_CUDA(cudaMemcpyAsync(b->scenes_dev.p, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice, st));
+    if (n_scenes == 1) b->gi = grad_info(scenes[0]);
+    if (b->backward) {
+      b->gv.resize(n_scenes);
+      b->gt.resize(n_scenes);
+      b->ge.resize(n_scenes);
+      b->gacc.resize(n_scenes);
+      for (int i = 0; i < n_scenes; ++i) {
+        const psdr_scene* s = scenes[i];
+        const psdr_grad_targets& g = grads[i];
+        const int nm = (int)s->meshes.size();
+        for (int o = 0; o < s->nobj; ++o) b->gv[i].push_back(g.vertices ? g.vertices[o] : nullptr);
+        for (int m = 0; m < nm; ++m) b->gt[i].push_back(g.textures ? g.textures[m] : nullptr);
+        for (int l = 0; l < s->nlight; ++l) b->ge[i].push_back(g.emit ? g.emit[l] : nullptr);
+        b->gacc[i] = g.accumulate;
+      }
+      for (int c = 0; c < n_cams; ++c) {
+        const psdr_grad_targets& g = grads[cam_scene[c]];
+        b->gc.push_back(g.camera_origin ? g.camera_origin[c] : nullptr);
+      }
+    }
+    PSDR_CUDA(cudaStreamSynchronize(st));
+    *out = b;
+  } catch (const psdr::Error& e) {
+    delete b;
+    psdr::set_error(e.msg);
+    return e.code;
+  } catch (const std::exception& e) {
+    delete b;
+    psdr::set_error(e.what());
+    return PSDR_ERR_CUDA;
+  }
+  return PSDR_OK;
+}
+
+// Forward of every view: geometry rebuild of each scene from its vertex buffers (the
+// caller may have changed them in place), then the interior render into the images.
+PSDR_API psdr_status psdr_batch_forward(psdr_batch* b, void* stream) {
+  try {
+    PSDR_CHECK(b != nullptr, "null batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    PSDR_CHECK(st != nullptr, "batches need a non-default stream (graph capture)");
+    if (!b->fwd_exec) {
+      b->fwd_exec = capture(st, [&] {
+        if (b->rebuild)
+          for (psdr_scene* s : b->scenes) scene_build_geometry(s, st);
+        forward_launch(b->scenes_dev.as<DevScene>(), b->views, b->cfg, b->cap, &b->ws, st, nullptr);
+      }, b->fwd_launches);
+    }
+    PSDR_CUDA(cudaGraphLaunch(b->fwd_exec, st));
+    profiler().launches += b->fwd_launches;
+  } catch (const psdr::Error& e) {
+    psdr::set_error(e.msg);
+    return e.code;
+  }
+  return PSDR_OK;
+}
+
+// Backward of every view (interior replay + adjoint, both edge terms), fp64
+// accumulation, then the fp32 gradient outputs bound at creation.
+PSDR_API psdr_status psdr_batch_backward(psdr_batch* b, void* stream) {
+  try {
+    PSDR_CHECK(b != nullptr, "null batch");
+    PSDR_CHECK(b->backward, "the batch was created without image gradients");
+    cudaStream_t st = (cudaStream_t)stream;
+    PSDR_CHECK(st != nullptr, "batches need a non-default stream (graph capture)");
+    if (!b->bwd_exec) {
+      b->bwd_exec = capture(st, [&] {
+        for (psdr_scene* s : b->scenes) {
+          PSDR_CUDA(cudaMemsetAsync(s->g_verts.p, 0, s->g_verts.bytes, st));
+          PSDR_CUDA(cudaMemsetAsync(s->g_tex.p, 0, s->g_tex.bytes, st));
+          PSDR_CUDA(cudaMemsetAsync(s->g_emit.p, 0, s->g_emit.bytes, st));
+        }
+        PSDR_CUDA(cudaMemsetAsync(b->campos.p, 0, sizeof(double) * 3 * b->views.size(), st));
+        backward_launch(b->scenes_dev.as<DevScene>(), b->views, b->cfg, b->cap, &b->ws, b->gi, st);
+        for (size_t i = 0; i < b->scenes.size(); ++i) {
+          psdr_scene* s = b->scenes[i];
+          const int nm = (int)s->meshes.size();
+          for (int o = 0; o < s->nobj; ++o)
+            grad_out(s->g_verts.as<double>() + 3 * (size_t)s->obj_vert_off[o], b->gv[i][o],
+                     3 * (long long)s->obj_nvert[o], b->gacc[i], st);
+          for (int m = 0; m < nm; ++m) {
+            const DevObj& ob = s->h_objs[m];
+            grad_out(s->g_tex.as<double>() + s->tex_grad_off[m], b->gt[i][m],
+                     (long long)ob.color.h * ob.color.w * ob.color.ch, b->gacc[i], st);
+          }
+          for (int l = 0; l < s->nlight; ++l)
+            grad_out(s->g_emit.as<double>() + 3 * l, b->ge[i][l], 3, b->gacc[i], st);
+        }
+        for (size_t c = 0; c < b->views.size(); ++c)
+          grad_out(b->campos.as<double>() + 3 * c, b->gc[c], 3, b->gacc[b->views[c].scene], st);
+      }, b->bwd_launches);
+    }
+    PSDR_CUDA(cudaGraphLaunch(b->bwd_exec, st));
+    profiler().launches += b->bwd_launches;
+  } catch (const psdr::Error& e) {
+    psdr::set_error(e.msg);
+    return e.code;
+  }
+  return PSDR_OK;
+}
+
+PSDR_API psdr_status psdr_batch_destroy(psdr_batch* b) {
+  delete b;
+  return PSDR_OK;
+}
+
+}  // extern "C"

@@ -12,7 +12,7 @@ namespace psdr {
 thread_local std::string g_err;
 void set_error(const std::string& m) { g_err = m; }
 
-void scene_build_geometry(psdr_scene* s);
+void scene_build_geometry(psdr_scene* s, cudaStream_t st);
 void psdr_scene_alloc(psdr_scene* s);
 
 namespace {
@@ -89,6 +89,8 @@ void check_cams(const psdr_camera_desc* cams, int n) {
 
 DevScene* dev_scene(psdr_scene* s) { return s->d_dev.as<DevScene>(); }
 
+}  // namespace
+
 SceneGradInfo grad_info(const psdr_scene* s) {
   SceneGradInfo gi;
   const int nm = (int)s->meshes.size();
@@ -102,7 +104,9 @@ SceneGradInfo grad_info(const psdr_scene* s) {
   return gi;
 }
 
-}  // namespace
+void check_config(const psdr_config* c) { check_cfg(c); }
+void check_cameras(const psdr_camera_desc* cams, int n) { check_cams(cams, n); }
+
 }  // namespace psdr
 
 using namespace psdr;
@@ -206,7 +210,7 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
     for (int o = 0; o < nm; ++o) s->h_objs[o].color.grad = s->g_tex.as<double>() + s->tex_grad_off[o];
     for (int l = 0; l < nl; ++l) s->h_lights[l].grad_emit = s->g_emit.as<double>() + 3 * l;
     s->upload_tables();
-    scene_build_geometry(s);
+    scene_build_geometry(s, s->stream);
   } catch (...) {
     delete s;
     throw;
@@ -224,8 +228,7 @@ psdr_status psdr_scene_destroy(psdr_scene* scene) {
 psdr_status psdr_scene_update(psdr_scene* scene, void* stream) {
   API_BEGIN
   PSDR_CHECK(scene != nullptr, "null scene");
-  if (stream) scene->stream = (cudaStream_t)stream;
-  scene_build_geometry(scene);
+  scene_build_geometry(scene, stream ? (cudaStream_t)stream : scene->stream);
   API_END
 }
 
@@ -358,14 +361,6 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   API_END
 }
 
-psdr_status psdr_batch_create(psdr_scene* const*, int32_t, const psdr_camera_desc*, const int32_t*, int32_t,
-                              const psdr_config*, float**, const float**, const psdr_grad_targets*, psdr_batch** out) {
-  if (out) *out = nullptr;
-  psdr::set_error("batching is not available in this build");
-  return PSDR_ERR_UNSUPPORTED;
-}
-psdr_status psdr_batch_forward(psdr_batch*, void*) { return PSDR_ERR_UNSUPPORTED; }
-psdr_status psdr_batch_backward(psdr_batch*, void*) { return PSDR_ERR_UNSUPPORTED; }
-psdr_status psdr_batch_destroy(psdr_batch*) { return PSDR_OK; }
+
 
 }  // extern "C"

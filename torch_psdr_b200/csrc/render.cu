@@ -1309,13 +1309,10 @@ void set_wf(WF& w, const psdr_config& cfg, int nviews, int nB_override, int ligh
 
 // Forward: the interior estimate of every view into V.image (and per-sample radiance
 // of view 0 into samples_out when given).
-void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
-                         psdr_workspace* ws, cudaStream_t st, float* samples_out) {
-  assign_offsets(views);
-  const int cap = choose_cap(cfg, views, false);
-  const int R = cfg.mis_light_samples + cfg.mis_bsdf_samples + 1;
-  ws->ensure(cap, R, cfg.max_bounce, (int)views.size(), 0, st);
-  upload_views(ws, views, st);
+// Device work of a forward job whose views are already in ws->views (tiles of `cap`
+// paths). Makes no allocation and no host copy, so it can be recorded into a graph.
+void forward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg, int cap,
+                    psdr_workspace* ws, cudaStream_t st, float* samples_out) {
   WF w = ws->wf;
   w.cap = ws->cap;
   set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
@@ -1326,6 +1323,16 @@ void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views
     PSDR_LAUNCHED(1);
   }
   PSDR_CUDA(cudaGetLastError());
+}
+
+void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
+                         psdr_workspace* ws, cudaStream_t st, float* samples_out) {
+  assign_offsets(views);
+  const int cap = choose_cap(cfg, views, false);
+  const int R = cfg.mis_light_samples + cfg.mis_bsdf_samples + 1;
+  ws->ensure(cap, R, cfg.max_bounce, (int)views.size(), 0, st);
+  upload_views(ws, views, st);
+  forward_launch(scenes_dev, views, cfg, cap, ws, st, samples_out);
 }
 
 static void edge_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb, long long begin,
@@ -1366,14 +1373,22 @@ static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, 
 
 // Backward: interior path replay + adjoint, then the primary- and direct-edge terms
 // of every view. Views must carry dimage (and grad_pos when wanted).
+void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg,
+                     int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
+
 void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
                           psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
   assign_offsets(views);
   const int cap = choose_cap(cfg, views, true);
-  const int nL = cfg.mis_light_samples;
-  const int Rmax = nL + std::max(cfg.mis_bsdf_samples, 1) + 1;
+  const int Rmax = cfg.mis_light_samples + std::max(cfg.mis_bsdf_samples, 1) + 1;
   ws->ensure(cap, Rmax, cfg.max_bounce, (int)views.size(), 1, st);
   upload_views(ws, views, st);
+  backward_launch(scenes_dev, views, cfg, cap, ws, gi, st);
+}
+
+// Device work of a backward job (views already uploaded); no allocation, no host copy.
+void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg,
+                     int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
   const DevView* vd = ws->views.as<DevView>();
   const int terms = cfg.terms ? cfg.terms : 7;
   // ---- interior

@@ -102,5 +102,16 @@ struct SceneGradInfo {
 void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
                           psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
 void grad_out(const double* acc, float* out, long long n, int accumulate, cudaStream_t st);
+void assign_offsets(std::vector<DevView>& views);
+int choose_cap(const psdr_config& cfg, const std::vector<DevView>& views, bool backward);
+void upload_views(psdr_workspace* ws, const std::vector<DevView>& views, cudaStream_t st);
+void forward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg, int cap,
+                    psdr_workspace* ws, cudaStream_t st, float* samples_out);
+void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg,
+                     int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
+SceneGradInfo grad_info(const psdr_scene* s);
+void check_config(const psdr_config* c);
+void check_cameras(const psdr_camera_desc* cams, int n);
+void scene_build_geometry(psdr_scene* s, cudaStream_t st);
 std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap);
 }  // namespace psdr

@@ -385,9 +385,10 @@ int num_sms() {
   return n;
 }
 
-// Builds everything that depends on vertex positions (records, edges, CDFs, BVH).
-void scene_build_geometry(psdr_scene* s) {
-  cudaStream_t st = s->stream;
+// Builds everything that depends on vertex positions (records, edges, CDFs, BVH) on
+// stream `st`. Device work only (after the first build sized the scratch), so it can
+// also be recorded into a graph.
+void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
   // vertices
   for (int o = 0; o < s->nobj; ++o) {
     const float* src = o < (int)s->meshes.size() ? s->meshes[o].vertices : s->lights[o - s->meshes.size()].vertices;
@@ -406,10 +407,8 @@ void scene_build_geometry(psdr_scene* s) {
                                             uvs, uvi, s->tri.as<float4>(), s->tri_v.as<int4>());
   }
   PSDR_CUDA(cudaGetLastError());
-  // lights
+  // lights (the table was uploaded at creation; area, power and CDFs are recomputed)
   if (s->nlight > 0) {
-    PSDR_CUDA(cudaMemcpyAsync(s->lights_buf.p, s->h_lights.data(), sizeof(DevLight) * s->nlight,
-                              cudaMemcpyHostToDevice, st));
     k_light_setup<<<1, 1, 0, st>>>(s->lights_buf.as<DevLight>(), s->nlight, s->tri.as<float4>(), s->ltri_pmf.as<float>(),
                                    s->ltri_cmf.as<float>(), s->dev.ltri_base, s->light_pmf.as<float>(),
                                    s->light_cmf.as<float>());
@@ -450,17 +449,11 @@ void scene_build_geometry(psdr_scene* s) {
   PSDR_CUDA(cudaMemsetAsync(bflags, 0, sizeof(int) * std::max(1, n), st));
   if (n > 1) k_karras<<<nblk(n - 1), 256, 0, st>>>(n, keys, child, range, parent);
   k_bottom_up<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), child, parent, aabb, bflags);
-  if (n > 1) {
-    k_layout<<<nblk(n - 1), 256, 0, st>>>(n, s->leaf_size, child, range, aabb, cbox, s->nodes.as<float4>());
-    s->dev.root = 0;
-  } else {
-    s->dev.root = ~0;  // single triangle: the root is a leaf
-  }
+  if (n > 1) k_layout<<<nblk(n - 1), 256, 0, st>>>(n, s->leaf_size, child, range, aabb, cbox, s->nodes.as<float4>());
   k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), s->leaf.as<float4>());
   // records + lights + half-edge sort (2 x passes x 5) + edge build/CDF (8) + BVH (9 + morton sort)
   count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 9 + 3 * 4);
   PSDR_CUDA(cudaGetLastError());
-  PSDR_CUDA(cudaMemcpyAsync(s->d_dev.p, &s->dev, sizeof(DevScene), cudaMemcpyHostToDevice, st));
 }
 
 void psdr_scene_alloc(psdr_scene* s) {
@@ -507,15 +500,22 @@ void psdr_scene_alloc(psdr_scene* s) {
   d.edge_cap = nh; d.n_edges = s->n_edges.as<int>(); d.edge = s->edge.as<float4>(); d.edge_v = s->edge_v.as<int2>();
   d.edge_pmf = s->edge_pmf.as<float>(); d.edge_cmf = s->edge_cmf.as<float>();
   d.nodes = s->nodes.as<float4>(); d.leaf = s->leaf.as<float4>();
+  d.root = s->ntri > 1 ? 0 : ~0;  // a single triangle makes the root a leaf
   d.grad_verts = nullptr;
   d.err = s->err.as<int>();
 }
 
 }  // namespace psdr
 
+// Host -> device uploads of the object and light tables and the scene record; done
+// once at creation so that the geometry rebuild (psdr_scene_update, or a rebuild
+// recorded into a batch graph) is made of device work only.
 void psdr_scene::upload_tables() {
   using namespace psdr;
   PSDR_CUDA(cudaMemcpyAsync(objs.p, h_objs.data(), sizeof(DevObj) * std::max<size_t>(1, h_objs.size()),
                             cudaMemcpyHostToDevice, stream));
+  if (nlight > 0)
+    PSDR_CUDA(cudaMemcpyAsync(lights_buf.p, h_lights.data(), sizeof(DevLight) * nlight, cudaMemcpyHostToDevice,
+                              stream));
   PSDR_CUDA(cudaMemcpyAsync(d_dev.p, &dev, sizeof(DevScene), cudaMemcpyHostToDevice, stream));
 }
