@@ -28,21 +28,27 @@ struct psdr_batch {
   std::vector<int> gacc;
   cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
   long long fwd_launches = 0, bwd_launches = 0;
+  std::vector<psdr::Profiler::EvPair> fwd_ev, bwd_ev;  // trace timing events recorded in the graphs
   ~psdr_batch() {
     if (fwd_exec) cudaGraphExecDestroy(fwd_exec);
     if (bwd_exec) cudaGraphExecDestroy(bwd_exec);
+    auto& reps = psdr::profiler().replays;
+    for (size_t i = reps.size(); i-- > 0;)
+      if (reps[i].first == &fwd_ev || reps[i].first == &bwd_ev) reps.erase(reps.begin() + i);
+    for (auto* v : {&fwd_ev, &bwd_ev})
+      for (auto& e : *v) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   }
 };
 
 namespace psdr {
 namespace {
 
-// Records `body` on `st` into a graph and instantiates it.
+// Records `body` on `st` into a graph and instantiates it. With profiling on, the
+// trace kernels' timing events are recorded into the graph (list `gev`).
 template <class F>
-cudaGraphExec_t capture(cudaStream_t st, F body, long long& launches) {
+cudaGraphExec_t capture(cudaStream_t st, F body, long long& launches, std::vector<Profiler::EvPair>* gev) {
   Profiler& pf = profiler();
-  const bool was_on = pf.on;
-  pf.on = false;  // no timing events inside graphs
+  pf.capture_ev = gev;
   const long long l0 = pf.launches;
   PSDR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   try {
@@ -51,15 +57,15 @@ cudaGraphExec_t capture(cudaStream_t st, F body, long long& launches) {
     cudaGraph_t g = nullptr;
     cudaStreamEndCapture(st, &g);
     if (g) cudaGraphDestroy(g);
-    pf.on = was_on;
+    pf.capture_ev = nullptr;
     throw;
   }
   cudaGraph_t graph = nullptr;
+  pf.capture_ev = nullptr;
   PSDR_CUDA(cudaStreamEndCapture(st, &graph));
   cudaGraphExec_t exec = nullptr;
   const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
-  pf.on = was_on;
   PSDR_CUDA(e);
   launches = pf.launches - l0;
   pf.launches = l0;
@@ -164,10 +170,11 @@ PSDR_API psdr_status psdr_batch_forward(psdr_batch* b, void* stream) {
         if (b->rebuild)
           for (psdr_scene* s : b->scenes) scene_build_geometry(s, st);
         forward_launch(b->scenes_dev.as<DevScene>(), b->views, b->cfg, b->cap, &b->ws, st, nullptr);
-      }, b->fwd_launches);
+      }, b->fwd_launches, &b->fwd_ev);
     }
     PSDR_CUDA(cudaGraphLaunch(b->fwd_exec, st));
     profiler().launches += b->fwd_launches;
+    profiler().replayed(&b->fwd_ev, (long long)b->fwd_ev.size());
   } catch (const psdr::Error& e) {
     psdr::set_error(e.msg);
     return e.code;
@@ -208,10 +215,11 @@ PSDR_API psdr_status psdr_batch_backward(psdr_batch* b, void* stream) {
         }
         for (size_t c = 0; c < b->views.size(); ++c)
           grad_out(b->campos.as<double>() + 3 * c, b->gc[c], 3, b->gacc[b->views[c].scene], st);
-      }, b->bwd_launches);
+      }, b->bwd_launches, &b->bwd_ev);
     }
     PSDR_CUDA(cudaGraphLaunch(b->bwd_exec, st));
     profiler().launches += b->bwd_launches;
+    profiler().replayed(&b->bwd_ev, (long long)b->bwd_ev.size());
   } catch (const psdr::Error& e) {
     psdr::set_error(e.msg);
     return e.code;

@@ -1194,6 +1194,14 @@ Profiler& profiler() {
 }
 void Profiler::begin_trace(cudaStream_t st) {
   if (!on) return;
+  if (capture_ev) {
+    cudaEvent_t a, b;
+    PSDR_CUDA(cudaEventCreate(&a));
+    PSDR_CUDA(cudaEventCreate(&b));
+    capture_ev->emplace_back(a, b);
+    PSDR_CUDA(cudaEventRecord(a, st));
+    return;
+  }
   if (used == ev.size()) {
     cudaEvent_t a, b;
     PSDR_CUDA(cudaEventCreate(&a));
@@ -1204,9 +1212,20 @@ void Profiler::begin_trace(cudaStream_t st) {
 }
 void Profiler::end_trace(cudaStream_t st) {
   if (!on) return;
+  if (capture_ev) {
+    PSDR_CUDA(cudaEventRecord(capture_ev->back().second, st));
+    return;
+  }
   PSDR_CUDA(cudaEventRecord(ev[used].second, st));
   ++used;
   ++trace_launches;
+}
+void Profiler::replayed(std::vector<EvPair>* graph_ev, long long n_trace) {
+  if (!on || graph_ev->empty()) return;
+  trace_launches += n_trace;
+  for (auto& r : replays)
+    if (r.first == graph_ev) { ++r.second; return; }
+  replays.emplace_back(graph_ev, 1);
 }
 #define PSDR_LAUNCHED(n) (profiler().launches += (n))
 void count_launches(int n) { profiler().launches += n; }
@@ -1476,6 +1495,7 @@ PSDR_API psdr_status psdr_profile_reset(void) {
     p.used = 0;
     p.launches = 0;
     p.trace_launches = 0;
+    p.replays.clear();
     if (p.d_rays) PSDR_CUDA(cudaMemset(p.d_rays, 0, sizeof(unsigned long long)));
   } catch (const psdr::Error& e) {
     psdr::set_error(e.msg);
@@ -1492,6 +1512,16 @@ PSDR_API psdr_status psdr_profile_read(int64_t* out3, double* trace_ms) {
       float t = 0;
       PSDR_CUDA(cudaEventElapsedTime(&t, p.ev[i].first, p.ev[i].second));
       ms += t;
+    }
+    for (auto& r : p.replays) {
+      double g = 0;
+      for (auto& e : *r.first) {
+        PSDR_CUDA(cudaEventSynchronize(e.second));
+        float t = 0;
+        PSDR_CUDA(cudaEventElapsedTime(&t, e.first, e.second));
+        g += t;
+      }
+      ms += g * (double)r.second;
     }
     unsigned long long rays = 0;
     if (p.d_rays) PSDR_CUDA(cudaMemcpy(&rays, p.d_rays, sizeof(rays), cudaMemcpyDeviceToHost));

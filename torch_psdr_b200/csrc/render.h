@@ -83,13 +83,20 @@ struct psdr_workspace {
 namespace psdr {
 // In-library profiler (psdr_profile_*): launch counts and trace-kernel event timing.
 struct Profiler {
+  using EvPair = std::pair<cudaEvent_t, cudaEvent_t>;
   bool on = false;
   long long launches = 0, trace_launches = 0;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  std::vector<EvPair> ev;  // events of directly launched trace kernels
   size_t used = 0;
+  // While a graph is being recorded, trace events go to the graph's own list; every
+  // replay re-records them, and psdr_profile_read weights the last replay's times by
+  // the number of replays since the last reset.
+  std::vector<EvPair>* capture_ev = nullptr;
+  std::vector<std::pair<std::vector<EvPair>*, long long>> replays;
   unsigned long long* d_rays = nullptr;
   void begin_trace(cudaStream_t st);
   void end_trace(cudaStream_t st);
+  void replayed(std::vector<EvPair>* graph_ev, long long n_trace);
 };
 Profiler& profiler();
 struct SceneGradInfo;
