@@ -1199,7 +1199,8 @@ void Profiler::begin_trace(cudaStream_t st) {
     PSDR_CUDA(cudaEventCreate(&a));
     PSDR_CUDA(cudaEventCreate(&b));
     capture_ev->emplace_back(a, b);
-    PSDR_CUDA(cudaEventRecord(a, st));
+    // External: becomes an event-record node of the graph (re-recorded every replay)
+    PSDR_CUDA(cudaEventRecordWithFlags(a, st, cudaEventRecordExternal));
     return;
   }
   if (used == ev.size()) {
@@ -1213,7 +1214,7 @@ void Profiler::begin_trace(cudaStream_t st) {
 void Profiler::end_trace(cudaStream_t st) {
   if (!on) return;
   if (capture_ev) {
-    PSDR_CUDA(cudaEventRecord(capture_ev->back().second, st));
+    PSDR_CUDA(cudaEventRecordWithFlags(capture_ev->back().second, st, cudaEventRecordExternal));
     return;
   }
   PSDR_CUDA(cudaEventRecord(ev[used].second, st));
