@@ -115,9 +115,9 @@ struct DevLight {
 // Per-triangle shading record, 6 x float4 (96 B) in original triangle order:
 //  [0] p0.xyz, area   [1] p1.xyz, obj(bits)   [2] p2.xyz, uv0.x
 //  [3] n.xyz, uv0.y   [4] t.xyz, uv1.x        [5] uv1.y, uv2.x, uv2.y, 0
-// BVH node (BVH2, child boxes stored in the parent), 4 x float4 (64 B):
-//  [0] L.lo.xyz L.hi.x [1] L.hi.yz R.lo.xy [2] R.lo.z R.hi.xyz [3] left, right (int)
-// child >= 0: internal node; child < 0: leaf ~((first << 3) | (count-1)).
+// BVH node (4-wide, child boxes stored in the parent), 7 x float4 (112 B):
+//  [0] lo.x of children 0..3 [1] hi.x [2] lo.y [3] hi.y [4] lo.z [5] hi.z [6] links (int)
+// link >= 0: internal node; link < 0: leaf ~((first << 3) | (count-1)); 0x7fffffff: empty.
 // Leaf triangles, 3 x float4 (48 B) in BVH order: p0.xyz + id(bits), p1.xyz, p2.xyz.
 struct DevScene {
   int ntri, nvert, nobj, nlight;
@@ -240,7 +240,7 @@ PSDR_D float3 xform_pos_rn(const float* m, float3 p) {
 }
 
 // ------------------------------------------------------------------ traversal
-constexpr int kStack = 64;
+constexpr int kStack = 96;
 
 struct HitRec {
   int tri;
@@ -260,6 +260,13 @@ PSDR_D float safe_inv(float d) { return 1.0f / (fabsf(d) > 1e-30f ? d : copysign
 // the reference's test |hit - y|^2 < 1e-5 (path_integrator.cc:114-116) fails for it
 // exactly as it would for the true closest hit; hits at or beyond t_occ are resolved
 // as closest hits.
+PSDR_D void cswap(float& ka, int& va, float& kb, int& vb) {
+  if (kb < ka) {
+    const float tk = ka; ka = kb; kb = tk;
+    const int tv = va; va = vb; vb = tv;
+  }
+}
+
 PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, float tmax,
                             float t_occ = -INFINITY) {
   const RayPre rp = ray_pre(o, d);
@@ -273,35 +280,43 @@ PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, 
   if (sc.ntri <= 0) return h;
   while (true) {
     if (node >= 0) {
-      const float4* nd = sc.nodes + 4 * (size_t)node;
-      const float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2);
-      const int4 e = __ldg(reinterpret_cast<const int4*>(nd + 3));
+      // 4-wide node: six float4 of child bounds (SoA) + the four child links
+      const float4* nd = sc.nodes + 7 * (size_t)node;
+      const float4 lx = __ldg(nd), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
+      const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5);
+      const int4 e = __ldg(reinterpret_cast<const int4*>(nd + 6));
       const float cull = h.t * 1.00001f + 1e-12f;
-      // left child box
-      float l0x = fmaf(a.x, inv.x, -oi.x), l1x = fmaf(a.w, inv.x, -oi.x);
-      float l0y = fmaf(a.y, inv.y, -oi.y), l1y = fmaf(b.x, inv.y, -oi.y);
-      float l0z = fmaf(a.z, inv.z, -oi.z), l1z = fmaf(b.y, inv.z, -oi.z);
-      float ln = fmaxf(fmaxf(fminf(l0x, l1x), fminf(l0y, l1y)), fmaxf(fminf(l0z, l1z), tmin));
-      float lf = fminf(fminf(fmaxf(l0x, l1x), fmaxf(l0y, l1y)), fminf(fmaxf(l0z, l1z), cull));
-      // right child box
-      float r0x = fmaf(b.z, inv.x, -oi.x), r1x = fmaf(c.y, inv.x, -oi.x);
-      float r0y = fmaf(b.w, inv.y, -oi.y), r1y = fmaf(c.z, inv.y, -oi.y);
-      float r0z = fmaf(c.x, inv.z, -oi.z), r1z = fmaf(c.w, inv.z, -oi.z);
-      float rn = fmaxf(fmaxf(fminf(r0x, r1x), fminf(r0y, r1y)), fmaxf(fminf(r0z, r1z), tmin));
-      float rf = fminf(fminf(fmaxf(r0x, r1x), fmaxf(r0y, r1y)), fminf(fmaxf(r0z, r1z), cull));
-      const bool hl = ln <= lf * 1.0000005f, hr = rn <= rf * 1.0000005f;
-      if (hl && hr) {
-        int nearc = ln <= rn ? e.x : e.y, farc = ln <= rn ? e.y : e.x;
-        if (sp < kStack) stack[sp++] = farc;
-        else atomicOr(sc.err, 1);
-        node = nearc;
-      } else if (hl) {
-        node = e.x;
-      } else if (hr) {
-        node = e.y;
-      } else {
+      auto slab = [&](float l_x, float h_x, float l_y, float h_y, float l_z, float h_z, int c) {
+        const float ax = fmaf(l_x, inv.x, -oi.x), bx = fmaf(h_x, inv.x, -oi.x);
+        const float ay = fmaf(l_y, inv.y, -oi.y), by = fmaf(h_y, inv.y, -oi.y);
+        const float az = fmaf(l_z, inv.z, -oi.z), bz = fmaf(h_z, inv.z, -oi.z);
+        const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), tmin));
+        const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), cull));
+        return (c != 0x7fffffff && tn <= tf * 1.0000005f) ? tn : INFINITY;
+      };
+      float k0 = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, e.x);
+      float k1 = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, e.y);
+      float k2 = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, e.z);
+      float k3 = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, e.w);
+      int c0 = e.x, c1 = e.y, c2 = e.z, c3 = e.w;
+      // sort the four (distance, child) pairs, nearest first
+      cswap(k0, c0, k1, c1);
+      cswap(k2, c2, k3, c3);
+      cswap(k0, c0, k2, c2);
+      cswap(k1, c1, k3, c3);
+      cswap(k1, c1, k2, c2);
+      if (k0 == INFINITY) {
         if (sp == 0) break;
         node = stack[--sp];
+        continue;
+      }
+      node = c0;
+      if (sp + 3 <= kStack) {
+        if (k3 != INFINITY) stack[sp++] = c3;
+        if (k2 != INFINITY) stack[sp++] = c2;
+        if (k1 != INFINITY) stack[sp++] = c1;
+      } else {
+        atomicOr(sc.err, 1);
       }
     } else {
       const int code = ~node;

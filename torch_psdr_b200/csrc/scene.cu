@@ -7,9 +7,10 @@
 //    reference hashes them on the host; grouping by sorted key gives the same
 //    left/right face assignment, in (min,max) order per mesh),
 //  * discrete CDFs over edges (length), lights (power) and light triangles (area),
-//  * an LBVH: 30-bit Morton codes of triangle-box centres, radix sort, Karras (2012)
-//    hierarchy, bottom-up boxes, then a BVH2 layout with child boxes in the parent
-//    and leaves collapsed up to `leaf_size` triangles.
+//  * an LBVH: 30-bit Morton codes of triangle-box centres (large triangles split off
+//    by a top key bit), radix sort, Karras (2012) hierarchy, bottom-up boxes, then a
+//    4-wide layout (pairwise collapse of the binary tree) with child boxes in the
+//    parent and leaves of up to `leaf_size` triangles.
 #include <algorithm>
 #include <cmath>
 
@@ -321,41 +322,78 @@ __global__ void k_bottom_up(int n, const uint32_t* __restrict__ order, const flo
   }
 }
 
-// Final BVH2 layout with conservative (padded) child boxes.
-__global__ void k_layout(int n, int leaf_size, const int2* __restrict__ child, const int2* __restrict__ range,
-                         const float* __restrict__ aabb, const unsigned int* __restrict__ cbox,
-                         float4* __restrict__ nodes) {
+// ---- 4-wide BVH: every internal node at even depth of the binary tree becomes a
+// 4-wide node whose children are its grandchildren (or its children where those are
+// leaves), i.e. a pairwise collapse of two binary levels.
+__global__ void k_depth_flags(int n, const int* __restrict__ parent, const int2* __restrict__ range, int leaf_size,
+                              int* __restrict__ flag) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
+  int d = 0;
+  bool inside = false;
+  for (int a = i; a != 0; ++d) {
+    a = parent[a];
+    const int2 r = range[a];
+    if (r.y - r.x + 1 <= leaf_size) inside = true;
+  }
+  const int2 r = range[i];
+  const bool leafy = r.y - r.x + 1 <= leaf_size;
+  flag[i] = (!inside && !leafy && (d & 1) == 0) ? 1 : 0;
+}
+
+__global__ void k_layout4(int n, int leaf_size, const int2* __restrict__ child, const int2* __restrict__ range,
+                          const float* __restrict__ aabb, const unsigned int* __restrict__ cbox,
+                          const int* __restrict__ flag, const int* __restrict__ idx4, float4* __restrict__ nodes4) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1 || !flag[i]) return;
   const float3 glo = f3(ord2f(cbox[6]), ord2f(cbox[7]), ord2f(cbox[8]));
   const float3 ghi = f3(ord2f(cbox[9]), ord2f(cbox[10]), ord2f(cbox[11]));
   const float ext = fmaxf(fmaxf(ghi.x - glo.x, ghi.y - glo.y), ghi.z - glo.z);
   const float apad = ext * 2e-6f + 1e-20f;
-  const int2 c = child[i];
-  int enc[2];
-  float bx[2][6];
+  auto is_leaf = [&](int c) {
+    if (c >= n - 1) return true;
+    const int2 r = range[c];
+    return r.y - r.x + 1 <= leaf_size;
+  };
+  auto leaf_code = [&](int c) {
+    if (c >= n - 1) return ~((c - (n - 1)) << 3);
+    const int2 r = range[c];
+    return ~((r.x << 3) | (r.y - r.x));
+  };
+  int slot[4];
+  int ns = 0;
+  const int2 ch = child[i];
   for (int s = 0; s < 2; ++s) {
-    const int ch = s == 0 ? c.x : c.y;
-    const float* b = aabb + 6 * (size_t)ch;
-    for (int q = 0; q < 3; ++q) {
-      float lo = b[q], hi = b[3 + q];
-      bx[s][q] = lo - (fabsf(lo) * 2e-6f + apad);
-      bx[s][3 + q] = hi + (fabsf(hi) * 2e-6f + apad);
-    }
-    if (ch >= n - 1) {
-      const int k = ch - (n - 1);
-      enc[s] = ~((k << 3) | 0);
-    } else {
-      const int2 rg = range[ch];
-      const int cnt = rg.y - rg.x + 1;
-      enc[s] = cnt <= leaf_size ? ~((rg.x << 3) | (cnt - 1)) : ch;
-    }
+    const int c = s == 0 ? ch.x : ch.y;
+    if (is_leaf(c)) { slot[ns++] = c; continue; }
+    const int2 g = child[c];
+    slot[ns++] = g.x;
+    slot[ns++] = g.y;
   }
-  float4* o = nodes + 4 * (size_t)i;
-  o[0] = make_float4(bx[0][0], bx[0][1], bx[0][2], bx[0][3]);
-  o[1] = make_float4(bx[0][4], bx[0][5], bx[1][0], bx[1][1]);
-  o[2] = make_float4(bx[1][2], bx[1][3], bx[1][4], bx[1][5]);
-  o[3] = make_float4(__int_as_float(enc[0]), __int_as_float(enc[1]), 0.f, 0.f);
+  float lo[3][4], hi[3][4];
+  int enc[4];
+  for (int k = 0; k < 4; ++k) {
+    if (k >= ns) {
+      for (int q = 0; q < 3; ++q) { lo[q][k] = INFINITY; hi[q][k] = -INFINITY; }
+      enc[k] = 0x7fffffff;
+      continue;
+    }
+    const int c = slot[k];
+    const float* b = aabb + 6 * (size_t)c;
+    for (int q = 0; q < 3; ++q) {
+      lo[q][k] = b[q] - (fabsf(b[q]) * 2e-6f + apad);
+      hi[q][k] = b[3 + q] + (fabsf(b[3 + q]) * 2e-6f + apad);
+    }
+    enc[k] = is_leaf(c) ? leaf_code(c) : idx4[c];
+  }
+  float4* o = nodes4 + 7 * (size_t)idx4[i];
+  o[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+  o[1] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+  o[2] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+  o[3] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+  o[4] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+  o[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+  o[6] = make_float4(__int_as_float(enc[0]), __int_as_float(enc[1]), __int_as_float(enc[2]), __int_as_float(enc[3]));
 }
 
 __global__ void k_leaf_tris(int n, const uint32_t* __restrict__ order, const float4* __restrict__ tri,
@@ -449,7 +487,14 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
   PSDR_CUDA(cudaMemsetAsync(bflags, 0, sizeof(int) * std::max(1, n), st));
   if (n > 1) k_karras<<<nblk(n - 1), 256, 0, st>>>(n, keys, child, range, parent);
   k_bottom_up<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), child, parent, aabb, bflags);
-  if (n > 1) k_layout<<<nblk(n - 1), 256, 0, st>>>(n, s->leaf_size, child, range, aabb, cbox, s->nodes.as<float4>());
+  if (n > 1) {
+    // 4-wide nodes: flags (even depth), exclusive scan for their indices, layout
+    int* f4 = s->aux_i2.as<int>();
+    int* idx4 = s->aux_i2.as<int>() + n;
+    k_depth_flags<<<nblk(n - 1), 256, 0, st>>>(n, parent, range, s->leaf_size, f4);
+    exclusive_scan_int(f4, idx4, n - 1, s->flags.as<int>() + 2 * (size_t)n, st);
+    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, s->leaf_size, child, range, aabb, cbox, f4, idx4, s->nodes.as<float4>());
+  }
   k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), s->leaf.as<float4>());
   // records + lights + half-edge sort (2 x passes x 5) + edge build/CDF (8) + BVH (9 + morton sort)
   count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 9 + 3 * 4);
@@ -475,19 +520,19 @@ void psdr_scene_alloc(psdr_scene* s) {
   s->edge_v.alloc(sizeof(int2) * nh, st);
   s->edge_pmf.alloc(sizeof(float) * nh, st);
   s->edge_cmf.alloc(sizeof(float) * nh, st);
-  s->nodes.alloc(sizeof(float4) * 4 * n, st);
+  s->nodes.alloc(sizeof(float4) * 7 * n, st);
   s->leaf.alloc(sizeof(float4) * 3 * n, st);
   s->err.alloc(sizeof(int), st);
   s->keys.alloc(sizeof(uint64_t) * nh, st);
   s->vals.alloc(sizeof(uint32_t) * nh, st);
   s->aux_i.alloc(sizeof(int2) * nh, st);
-  s->aux_i2.alloc(sizeof(int) * nh, st);
+  s->aux_i2.alloc(sizeof(int) * std::max<size_t>(nh, 2 * (size_t)n), st);
   s->aux_d.alloc(sizeof(double) * nh, st);
   s->aux_d2.alloc(sizeof(double) * nh + sizeof(float) * nh, st);
   s->aabb.alloc(sizeof(float) * 6 * (2 * (size_t)n), st);
   s->parent.alloc(sizeof(int) * 2 * (size_t)n, st);
   s->range.alloc(sizeof(int2) * n, st);
-  s->flags.alloc(sizeof(int) * std::max<size_t>(2 * (size_t)n, 2 * scan_tmp_ints(nh) + 64), st);
+  s->flags.alloc(sizeof(int) * (2 * (size_t)n + std::max<size_t>(2 * (size_t)n, 2 * scan_tmp_ints(nh) + 64)), st);
   s->cbox.alloc(sizeof(unsigned int) * 12, st);
   s->d_dev.alloc(sizeof(DevScene), st);
   PSDR_CUDA(cudaMemsetAsync(s->err.p, 0, sizeof(int), st));
