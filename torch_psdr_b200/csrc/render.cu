@@ -117,7 +117,12 @@ __global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict
       w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       w.cur[s] = hit4(h);
       w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
-      if (MODE == MODE_REPLAY) w.rec[(size_t)s * w.rec_stride] = hit4(h);
+      if (MODE == MODE_REPLAY) {
+        float4* rec = w.rec + (size_t)s * w.rec_stride;
+        rec[0] = hit4(h);
+        float4* cb = rec + 1 + (size_t)w.D * w.R;
+        for (int q = 0; q < 2 * w.D; ++q) cb[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
       alive = h.tri >= 0;
     }
     const int k = warp_append(&w.cnt[0], alive);
@@ -223,6 +228,10 @@ __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict_
 }
 
 // ------------------------------------------------------------------ accumulate kernel
+// Per shaded path: the depth's contribution C (light samples + MIS-weighted BSDF
+// samples, path_integrator.cc:103-160) and throughput factor beta (indirect bounce,
+// :163-181). FWD folds them into L and T; REPLAY also stores the hit records and
+// (C, beta) of the depth, which is all the adjoint needs besides the sampler stream.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict__ scenes,
                                                const DevView* __restrict__ views, int d) {
@@ -241,76 +250,73 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
       const size_t cs = (size_t)w.cap;
       const float4 c = w.cur[s];
       const Surf x = make_surf(sc, __float_as_int(c.x), c.y, c.z, xyz(w.org[s]));
-      if (MODE == MODE_REPLAY) {
-        float4* rec = w.rec + (size_t)s * w.rec_stride + 1 + (size_t)d * w.R;
-        const int Rd = last ? w.R - 1 : w.R;
-        for (int r = 0; r < Rd; ++r) rec[r] = w.hit[r * cs + k];
-        if (!last) {
-          const float4 h = w.hit[(w.nL + w.nB) * cs + k];
-          if (__float_as_int(h.x) >= 0) {
-            w.cur[s] = h;
-            w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
-            cont = true;
-          }
-        }
-      } else {
-        float4 T4 = w.T[s], L4 = w.L[s];
-        float3 T = xyz(T4), L = xyz(L4);
-        const DevObj& ob = sc.objs[x.obj];
-        const float3 bsdf = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v)) * kInvPi;
-        for (int i = 0; i < w.nL; ++i) {
-          const float4 h = w.hit[i * cs + k];
-          const int tri = __float_as_int(h.x);
-          if (tri < 0) continue;
-          const float4 dd = w.rd[i * cs + k], aux = w.ra[i * cs + k];
-          const float3 dir = xyz(dd);
-          const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
-          if (!(q.is_light && sqnorm(q.p - xyz(aux)) < kEps)) continue;
-          const DevLight& Lt = sc.lights[__float_as_int(dd.w)];
-          const float tmp = dot(q.n, -dir) / q.sqd;
-          const float G = dot(x.n, dir) * tmp;
-          const float pdf_l = aux.w;
-          float wgt = 1.0f / fL;
-          if (w.nB > 0) wgt *= mis_power(pdf_l, dot(x.n, dir) * kInvPi * tmp, fL, fB);
-          const float sc_ = G / pdf_l * wgt;
-          L += mul(T, f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z)) * sc_;
-        }
-        for (int j = 0; j < w.nB; ++j) {
-          const size_t slot = (w.nL + j) * cs + k;
-          const float4 h = w.hit[slot];
-          const int tri = __float_as_int(h.x);
-          if (tri < 0) continue;
+      const DevObj& ob = sc.objs[x.obj];
+      const float3 bsdf = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v)) * kInvPi;
+      float3 C = f3(0.f, 0.f, 0.f), beta = f3(0.f, 0.f, 0.f);
+      for (int i = 0; i < w.nL; ++i) {
+        const float4 h = w.hit[i * cs + k];
+        const int tri = __float_as_int(h.x);
+        if (tri < 0) continue;
+        const float4 dd = w.rd[i * cs + k], aux = w.ra[i * cs + k];
+        const float3 dir = xyz(dd);
+        const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
+        if (!(q.is_light && sqnorm(q.p - xyz(aux)) < kEps)) continue;
+        const DevLight& Lt = sc.lights[__float_as_int(dd.w)];
+        const float tmp = dot(q.n, -dir) / q.sqd;
+        const float G = dot(x.n, dir) * tmp;
+        const float pdf_l = aux.w;
+        float wgt = 1.0f / fL;
+        if (w.nB > 0) wgt *= mis_power(pdf_l, dot(x.n, dir) * kInvPi * tmp, fL, fB);
+        C += f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z) * (G / pdf_l * wgt);
+      }
+      for (int j = 0; j < w.nB; ++j) {
+        const size_t slot = (w.nL + j) * cs + k;
+        const float4 h = w.hit[slot];
+        const int tri = __float_as_int(h.x);
+        if (tri < 0) continue;
+        const float3 wo = xyz(w.rd[slot]);
+        const float ct = w.ra[slot].x;
+        const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
+        if (!q.is_light) continue;
+        const DevLight& Lt = sc.lights[q.light];
+        const float tmp = dot(q.n, -wo) / q.sqd;
+        const float G = dot(x.n, wo) * tmp;
+        const float pdf_b = ct * kInvPi * tmp;
+        float wgt = 1.0f / fB;
+        if (w.nL > 0) wgt *= mis_power(pdf_b, __ldg(sc.light_pmf + q.light) * Lt.inv_area, fB, fL);
+        C += f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z) * (G / pdf_b * wgt);
+      }
+      float4 hn = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f);
+      if (!last) {
+        const size_t slot = (w.nL + w.nB) * cs + k;
+        hn = w.hit[slot];
+        const int tri = __float_as_int(hn.x);
+        if (tri >= 0) {
           const float3 wo = xyz(w.rd[slot]);
           const float ct = w.ra[slot].x;
-          const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
-          if (!q.is_light) continue;
-          const DevLight& Lt = sc.lights[q.light];
-          const float tmp = dot(q.n, -wo) / q.sqd;
+          const Surf nx = make_surf(sc, tri, hn.y, hn.z, x.p);
+          const float tmp = dot(nx.n, -wo) / nx.sqd;
           const float G = dot(x.n, wo) * tmp;
-          const float pdf_b = ct * kInvPi * tmp;
-          float wgt = 1.0f / fB;
-          if (w.nL > 0) wgt *= mis_power(pdf_b, __ldg(sc.light_pmf + q.light) * Lt.inv_area, fB, fL);
-          const float sc_ = G / pdf_b * wgt;
-          L += mul(T, f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z)) * sc_;
+          const float pdf = ct * kInvPi * tmp;
+          beta = bsdf * (G / pdf);
+          w.cur[s] = hn;
+          w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
+          cont = true;
         }
-        if (!last) {
-          const size_t slot = (w.nL + w.nB) * cs + k;
-          const float4 h = w.hit[slot];
-          const int tri = __float_as_int(h.x);
-          if (tri >= 0) {
-            const float3 wo = xyz(w.rd[slot]);
-            const float ct = w.ra[slot].x;
-            const Surf nx = make_surf(sc, tri, h.y, h.z, x.p);
-            const float tmp = dot(nx.n, -wo) / nx.sqd;
-            const float G = dot(x.n, wo) * tmp;
-            const float pdf = ct * kInvPi * tmp;
-            T = mul(T, bsdf) * (G / pdf);
-            w.cur[s] = h;
-            w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
-            cont = true;
-          }
-        }
-        w.T[s] = make_float4(T.x, T.y, T.z, 0.f);
+      }
+      if (MODE == MODE_REPLAY) {
+        float4* rec = w.rec + (size_t)s * w.rec_stride;
+        float4* rh = rec + 1 + (size_t)d * w.R;
+        const int Rd = last ? w.R - 1 : w.R;
+        for (int r = 0; r < Rd; ++r) rh[r] = w.hit[r * cs + k];
+        float4* cb = rec + 1 + (size_t)w.D * w.R + 2 * d;
+        cb[0] = make_float4(C.x, C.y, C.z, 0.f);
+        cb[1] = make_float4(beta.x, beta.y, beta.z, 0.f);
+      } else {
+        const float3 T = xyz(w.T[s]);
+        const float3 L = xyz(w.L[s]) + mul(T, C);
+        const float3 Tn = mul(T, beta);
+        w.T[s] = make_float4(Tn.x, Tn.y, Tn.z, 0.f);
         w.L[s] = make_float4(L.x, L.y, L.z, 0.f);
       }
     }
@@ -639,10 +645,18 @@ PSDR_D void scatter_tex_warp(const DevTex* tx, int off, float3 a, bool active) {
 }
 
 // ------------------------------------------------------------------ adjoint kernel
-// One thread per path of the tile: re-evaluates the path from its sampler stream and
-// hit records, forms the suffix radiances S_d = C_d + beta_d S_{d+1}, then runs the
-// reverse-mode adjoint depth by depth (PSDR_EST_REFERENCE: pdfs and MIS weights are
-// constants, jacobi = area/detach(area), barycentrics are not differentiated).
+// One thread per path of the tile: the replay stored each depth's contribution C_d
+// and throughput factor beta_d, so the suffix radiances S_d = C_d + beta_d S_{d+1}
+// come straight from the records; the path is then walked forward once, replaying
+// its sampler stream, and every depth's reverse-mode adjoint is applied
+// (PSDR_EST_REFERENCE: pdfs and MIS weights are constants, jacobi = area/detach(area),
+// barycentrics are not differentiated), scattering into fp64 accumulators.
+PSDR_D float3 suffix_radiance(const float4* __restrict__ cb, int from, int D) {
+  float3 S = f3(0.f, 0.f, 0.f);
+  for (int k = D - 1; k >= from; --k) S = xyz(cb[2 * k]) + mul(xyz(cb[2 * k + 1]), S);
+  return S;
+}
+
 __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restrict__ scenes,
                                                  const DevView* __restrict__ views, Tile tile, int hot_lv0,
                                                  int hot_nlv, int emit_hot) {
@@ -669,76 +683,48 @@ __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restric
     if (s < tile.n) {
       const DevView& V = views[w.view[s]];
       scp = &scenes[V.scene];
-      const float4 h0 = w.rec[(size_t)s * w.rec_stride];
+      const float4* rec = w.rec + (size_t)s * w.rec_stride;
+      const float4 h0 = rec[0];
       tri0 = __float_as_int(h0.x);
       if (tri0 >= 0 && V.dimage) {
         const DevScene& sc = *scp;
         flush_sc = scp;
         const float* gp = V.dimage + 3 * (size_t)w.pix[s];
         const float3 g = f3(gp[0], gp[1], gp[2]) / (float)V.spp;
-        const long long i = tile.begin + s - V.sample_off;
-        Rng rng0 = make_rng((unsigned long long)i + w.seed);
-        rng0.next_float();
-        rng0.next_float();
         const Surf x0 = make_surf(sc, tri0, h0.y, h0.z, V.pos);
         b10 = h0.y; b20 = h0.z; front0 = x0.front;
-        const float4* rec = w.rec + (size_t)s * w.rec_stride + 1;
-        // pass 1: per-depth contributions and throughput factors
-        float3 C[kMaxDepth], B[kMaxDepth];
-        int De = 0;
-        bool lightstop = false;
-        {
-          Rng rng = rng0;
-          Surf x = x0;
-          SurfAdj d1 = zero_adj(), d2 = zero_adj();
-          HotAcc hd;
-          hd.nlv = 0;
-          hd.emit_hot = false;
-          float3 at = f3(0.f, 0.f, 0.f);
-          for (int d = 0; d < w.D; ++d) {
-            if (x.is_light) {
-              if (w.light_vis && d == 0) {
-                const DevLight& Lt = sc.lights[x.light];
-                C[0] = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
-                B[0] = f3(0.f, 0.f, 0.f);
-                De = 1;
-                lightstop = true;
-              }
-              break;
-            }
-            const DepthVals dv = depth_eval<false>(w, sc, x, rng, rec + (size_t)d * w.R, d == w.D - 1,
-                                                   f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f), d1, d2, hd, at);
-            C[d] = dv.C;
-            B[d] = dv.beta;
-            De = d + 1;
-            if (!dv.has_next) break;
-            const float4 hn = rec[(size_t)d * w.R + w.nL + w.nB];
-            x = make_surf(sc, __float_as_int(hn.x), hn.y, hn.z, x.p);
+        const float4* hits = rec + 1;
+        const float4* cb = rec + 1 + (size_t)w.D * w.R;
+        if (x0.is_light) {
+          // camera ray on a light: L = emit at depth 0 when lights are visible
+          if (w.light_vis) {
+            const DevLight& Lt = sc.lights[x0.light];
+            const float3 L = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+            has0 = true;
+            ax0.area = dot(g, L) / x0.area;
+            add_emit(hot, Lt.grad_emit, g);
           }
-        }
-        float3 Ssuf[kMaxDepth + 1];
-        Ssuf[De] = f3(0.f, 0.f, 0.f);
-        for (int d = De - 1; d >= 0; --d) Ssuf[d] = C[d] + mul(B[d], Ssuf[d + 1]);
-        const float3 L = Ssuf[0];
-        if (De > 0 && finite3(L)) {
-          has0 = true;
-          SurfAdj ax = zero_adj();
-          ax.area = dot(g, L) / x0.area;  // jacobi of the primary hit
-          if (lightstop) {
-            add_emit(hot, sc.lights[x0.light].grad_emit, g);
-            ax0 = ax;
-          } else {
-            Rng rng = rng0;
+        } else {
+          const float3 L = suffix_radiance(cb, 0, w.D);
+          if (finite3(L)) {
+            has0 = true;
+            const long long i = tile.begin + s - V.sample_off;
+            Rng rng = make_rng((unsigned long long)i + w.seed);
+            rng.next_float();
+            rng.next_float();
+            SurfAdj ax = zero_adj();
+            ax.area = dot(g, L) / x0.area;  // jacobi of the primary hit
             Surf xc = x0;
             int tric = tri0;
             float4 hc = h0;
             float3 T = f3(1.f, 1.f, 1.f);
-            for (int d = 0; d < De; ++d) {
+            for (int d = 0; d < w.D; ++d) {
               const float3 adjC = mul(g, T);
-              const float3 adjB = mul(adjC, Ssuf[d + 1]);
+              const float3 adjB = mul(adjC, suffix_radiance(cb, d + 1, w.D));
               SurfAdj nextc = zero_adj();
               float3 atx = f3(0.f, 0.f, 0.f);
-              depth_eval<true>(w, sc, xc, rng, rec + (size_t)d * w.R, d == w.D - 1, adjC, adjB, ax, nextc, hot, atx);
+              const DepthVals dv = depth_eval<true>(w, sc, xc, rng, hits + (size_t)d * w.R, d == w.D - 1, adjC, adjB,
+                                                    ax, nextc, hot, atx);
               const DevObj& ob = sc.objs[xc.obj];
               const int off = texel_offset(ob.color, xc.u, xc.v);
               if (d == 0) {
@@ -750,12 +736,13 @@ __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restric
                 if (ob.color.grad) scatter_tex(ob.color, off, atx, false);
                 scatter_surf(sc, hot, tric, hc.y, hc.z, xc.front, ax);
               }
-              T = mul(T, B[d]);
-              if (d + 1 >= De) break;
-              hc = rec[(size_t)d * w.R + w.nL + w.nB];
+              if (!dv.has_next) break;
+              T = mul(T, xyz(cb[2 * d + 1]));
+              hc = hits[(size_t)d * w.R + w.nL + w.nB];
               tric = __float_as_int(hc.x);
               const float3 org = xc.p;
               xc = make_surf(sc, tric, hc.y, hc.z, org);
+              if (xc.is_light) break;  // the path ends on a light: nothing downstream
               ax = nextc;
             }
           }
@@ -1295,7 +1282,7 @@ void psdr_workspace::ensure(int c, int r, int d, int nv, int rec_needed, cudaStr
     hc_pmf.alloc(4 * n, st); hc_cmf.alloc(4 * n, st);
     scan_tmp.alloc(8 * (scan_tmp_doubles((int)n) + 64), st);
   }
-  if (rec_needed) rec.alloc(16 * (size_t)cap * (1 + (size_t)D * R), st);
+  if (rec_needed) rec.alloc(16 * (size_t)cap * (1 + (size_t)D * R + 2 * (size_t)D), st);
   if (nv > nviews_cap) {
     nviews_cap = nv;
     views.alloc(sizeof(DevView) * nv, st);
@@ -1324,7 +1311,7 @@ void set_wf(WF& w, const psdr_config& cfg, int nviews, int nB_override, int ligh
   w.light_vis = light_vis;
   w.nviews = nviews;
   w.seed = cfg.seed;
-  w.rec_stride = 1 + w.D * w.R;
+  w.rec_stride = 1 + w.D * w.R + 2 * w.D;  // primary hit, hits per depth, (C, beta) per depth
 }
 
 // Forward: the interior estimate of every view into V.image (and per-sample radiance
