@@ -25,7 +25,34 @@ template <class S, bool AD> struct Ctx {
   const Scene<float>* scf = nullptr;
   Camera<float> camf;
   V3<float> posf;
+  float fov = 0.f;        // vertical field of view (radians)
+  double hc_cells = 1.0;  // hypercube cell count of the term being evaluated
 };
+
+// Raster area per unit surface area at x with normal n (up to fx*fy): |n.(x-o)|/z^3.
+template <class S, class R>
+inline S cam_jacobian(const Camera<R>& cam, const V3<S>& x, const V3<S>& n, const V3<S>& o) {
+  V3<S> rel = x - o;
+  V3<S> look(S(-cam.c2w[0][2]), S(-cam.c2w[1][2]), S(-cam.c2w[2][2]));
+  S z = dot(rel, look);
+  return abs_(dot(n, rel)) / (z * z * z);
+}
+
+// fx*fy of the raster map (camera.h: x scaled by W/2*cot(fov/2), y by H/2*cot(fov/2)).
+inline double raster_fxfy(double fov, int H, int W) {
+  double cot = 1.0 / std::tan(fov * 0.5);
+  return 0.25 * double(W) * double(H) * cot * cot;
+}
+
+// Raster position of x seen from o (camera rotation fixed, translation o).
+template <class S, class R>
+inline V3<S> raster_of(const Camera<R>& cam, const V3<S>& x, const V3<S>& o) {
+  V3<S> rel = x - o;
+  V3<S> pc(S(cam.c2w[0][0]) * rel.x + S(cam.c2w[1][0]) * rel.y + S(cam.c2w[2][0]) * rel.z,
+           S(cam.c2w[0][1]) * rel.x + S(cam.c2w[1][1]) * rel.y + S(cam.c2w[2][1]) * rel.z,
+           S(cam.c2w[0][2]) * rel.x + S(cam.c2w[1][2]) * rel.y + S(cam.c2w[2][2]) * rel.z);
+  return Camera<R>::xpos(cam.c2r, pc);
+}
 
 // camera.h:235-258 PerspectiveCamera::gen_camera_ray_ for sample i.
 template <class S, bool AD>
@@ -43,9 +70,16 @@ inline V3<S> interior_sample(const Ctx<S, AD>& c, uint64_t i, int& pix, bool& va
   V3<S> ds(S(d.x), S(d.y), S(d.z));
   Its<S> its = scene_hit<S, AD>(c.sc, c.cam_pos, ds, true);
   valid = its.valid;
+  const bool unb = c.cfg.mode == 1;
   V3<S> L = trace2light<S, AD>(c.sc, rng, its, its.valid, c.cfg.mis_light_samples, c.cfg.mis_bsdf_samples,
-                               c.cfg.max_bounce, c.cfg.enable_light_visable != 0);
-  return L * its.jac;
+                               c.cfg.max_bounce, c.cfg.enable_light_visable != 0, unb && AD);
+  S jac = its.jac;
+  if (unb && AD && its.valid) {
+    // raster area per surface area at the primary vertex, as a ratio with its detached value
+    S J = cam_jacobian(c.cam, its.p, its.n, c.cam_pos);
+    jac = jac * (J / detach(J));
+  }
+  return L * jac;
 }
 
 template <class S, class R>
@@ -174,6 +208,176 @@ inline V3<S> eval_direct(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], int& 
   return value;
 }
 
+// ---------------------------------------------------------------- unbiased estimator
+// The derivative of the image in the material form of the path integral: every path
+// vertex moves with its triangle (fixed barycentrics), so the interior term differentiates
+// the measurement contribution times the area and camera Jacobians. Three boundary terms
+// complete it: material crossing the pixel borders, silhouettes sliding over the
+// background, and shadow boundaries sliding over the receivers of direct light. All are
+// zero-valued in the forward image; only their derivatives are used.
+
+// Material point of a hit found in the value scene, in the differentiated scene.
+template <class S, class T>
+inline V3<S> material_point(const Scene<S>& sc, const Its<T>& h) {
+  const Tri<S>& t = sc.tris[h.tri];
+  return t.p0 + (t.p1 - t.p0) * S(h.b1) + (t.p2 - t.p0) * S(h.b2);
+}
+
+// True when triangle tri is one of the faces of edge E.
+template <class S, class T>
+inline bool tri_has_edge(const Scene<S>& sc, int tri, const Edge<T>& E) {
+  if (tri < 0) return false;
+  const auto& f = sc.faces[tri];
+  const bool h0 = f[0] == E.v0 || f[1] == E.v0 || f[2] == E.v0;
+  const bool h1 = f[0] == E.v1 || f[1] == E.v1 || f[2] == E.v1;
+  return h0 && h1;
+}
+
+// Silhouette term. The edge sample and its two offset rays are those of eval_primary;
+// one side must land on a face of the edge (foreground), the other side (background,
+// possibly empty) changes visibility at the raster velocity of the edge relative to the
+// background point: -L_bg (v_edge - v_bg).n_bg per unit raster length.
+template <class S, bool AD>
+inline V3<S> eval_primary_unb(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx, int& ry, bool& valid) {
+  const Scene<float>& sf = *c.scf;
+  float s = s1, pe;
+  int ei = sf.edge_cdf.sample_reuse(s, pe);
+  const Edge<float>& E = sf.edges[ei];
+  V3<float> xe = E.p0 + (E.p1 - E.p0) * s;
+  float pdf_e = pe / E.len;
+  valid = true;
+  project(c.camf, xe, valid, rx, ry);
+  V3<float> rd = normalize(xe - c.posf);
+  V3<float> n = cross(rd, normalize(E.p1 - E.p0));
+  const float eps = 1e-5f;
+  V3<float> da = rd - n * eps, db = rd + n * eps;
+  Its<float> ia = scene_hit<float, false>(sf, c.posf, da, valid);
+  Its<float> ib = scene_hit<float, false>(sf, c.posf, db, valid);
+  const bool na = ia.valid && tri_has_edge(sf, ia.tri, E), nb = ib.valid && tri_has_edge(sf, ib.tri, E);
+  valid = valid && na != nb;
+  const Its<float>& ig = na ? ib : ia;
+  valid = valid && ig.valid;
+  V3<float> Lg = trace2light<float, false>(sf, rng, ig, valid, c.cfg.mis_light_samples, c.cfg.mis_bsdf_samples,
+                                           c.cfg.max_bounce, c.cfg.enable_light_visable != 0);
+  V3<S> value;
+  if (!valid) return value;
+  if constexpr (AD) {
+    const Edge<S>& Es = c.sc.edges[ei];
+    V3<S> xes = Es.p0 + (Es.p1 - Es.p0) * S(s);
+    V3<S> xg = material_point(c.sc, ig);
+    V3<double> o(c.posf.x, c.posf.y, c.posf.z);
+    V3<double> rel_e(double(xe.x) - o.x, double(xe.y) - o.y, double(xe.z) - o.z);
+    V3<double> rel_g(double(ig.p.x) - o.x, double(ig.p.y) - o.y, double(ig.p.z) - o.z);
+    double re = norm(rel_e), rg = norm(rel_g);
+    V3<double> look(-double(c.camf.c2w[0][2]), -double(c.camf.c2w[1][2]), -double(c.camf.c2w[2][2]));
+    double z = dot(rel_e, look);
+    double k = raster_fxfy(c.fov, c.cam.H, c.cam.W) * re / (z * z * z) / (double(pdf_e) * c.cam.H * c.cam.W);
+    V3<S> dso = c.cam_pos - detach(c.cam_pos);
+    V3<S> vrel = (xes - detach(xes) - dso) - (xg - detach(xg) - dso) * S(re / rg);
+    V3<S> ns(S(n.x), S(n.y), S(n.z));
+    S vn = dot(vrel, ns) * S(na ? 1.0 : -1.0);
+    value = V3<S>(S(Lg.x), S(Lg.y), S(Lg.z)) * (vn * S(-k));
+  }
+  valid = valid && finite3(value);
+  return value;
+}
+
+// Shadow-boundary term of direct light at the primary vertex. Sampling and visibility
+// tests are those of eval_direct; the edge point x_b, light point y and receiver x_d
+// lie on one line. The shadow boundary moves over the receiver's material at the
+// relative velocity d_eff = dx_b - dx_d/lam - dy (1 - 1/lam), lam = |x_d-y|/|x_b-y|;
+// the occluding faces lie on the side opposite the edge's outward vector.
+template <class S, bool AD>
+inline V3<S> eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], int& rx, int& ry, bool& valid) {
+  using R = typename Traits<S>::R;
+  const Scene<S>& sc = c.sc;
+  R s = s3[0], pe;
+  int ei = sc.edge_cdf.sample_reuse(s, pe);
+  const Edge<S>& E = sc.edges[ei];
+  V3<S> xb = E.p0 + (E.p1 - E.p0) * S(s);
+  double pdf_e = double(pe) / val(E.len);
+  R sy = s3[1], sz = s3[2], pch = R(1);
+  int l = sc.light_cdf.sample_reuse(sy, pch);
+  R pl;
+  V3<S> yl = light_sample_point(sc, l, sy, sz, pl);
+  double pdf_l = double(pl) * double(pch);
+  V3<S> dir = normalize(xb - yl);
+  valid = val(dot(E.nl, dir)) * val(dot(E.nr, dir)) < 0 && val(norm(E.nl - E.nr)) > 1e-5;
+  rx = ry = 0;
+  Its<S> is0 = scene_hit<S, AD>(sc, xb, -dir, valid);
+  valid = valid && is0.valid && is0.is_light && val(sqnorm(is0.p - yl)) < double(R(1e-5));
+  Its<S> id0 = scene_hit<S, AD>(sc, xb, dir, valid);
+  valid = valid && id0.valid && !id0.is_light;
+  project(c.cam, id0.p, valid, rx, ry);
+  V3<S> cd = normalize(id0.p - c.cam_pos);
+  Its<S> i2 = scene_hit<S, AD>(sc, c.cam_pos, cd, valid);
+  valid = valid && i2.valid && !i2.is_light && val(sqnorm(i2.p - id0.p)) < double(R(1e-5));
+  V3<S> value;
+  if (!valid) return value;
+  if constexpr (AD) {
+    V3<double> xbv = val3(xb), yv = val3(yl), xdv = val3(id0.p);
+    V3<double> w = normalize(xbv - yv);
+    V3<double> ev = normalize(val3(E.p1) - val3(E.p0));
+    if (dot(cross(w, ev), val3(E.out)) < 0) ev = -ev;
+    V3<double> ns = cross(w, ev);
+    double dby = norm(xbv - yv), lam = norm(xdv - yv) / dby;
+    V3<S> deff = (xb - detach(xb)) - (id0.p - detach(id0.p)) * S(1.0 / lam) - (yl - detach(yl)) * S(1.0 - 1.0 / lam);
+    S dn = dot(deff, V3<S>(S(ns.x), S(ns.y), S(ns.z)));
+    double cos_y = std::fabs(dot(val3(is0.n), w));
+    V3<double> o = val3(c.cam_pos);
+    double Jc = raster_fxfy(c.fov, c.cam.H, c.cam.W) * val(cam_jacobian(c.cam, xdv, val3(id0.n), o));
+    double k = cos_y / (dby * dby) * Jc / (pdf_e * pdf_l * c.cam.H * c.cam.W);
+    V3<S> fr = detach(tex_at(sc, id0.obj, id0.u, id0.v) * inv_pi<S>());
+    V3<S> Le = detach(sc.emit[is0.light]);
+    value = mul(fr, Le) * (dn * S(-k));
+  }
+  valid = valid && finite3(value);
+  return value;
+}
+
+// Pixel-border term: border sample i on the (W+1) x H vertical and W x (H+1) horizontal
+// unit segments of the pixel grid (spp_pixel_boundary samples each). The radiance L
+// seen through the border point flows across it at the raster velocity of its primary
+// vertex; the pixel it enters gains L v, the one it leaves loses it. Adds
+// dPhi/dtheta . seed_k to dphi.
+template <class S, bool AD>
+inline void pixel_border_sample(const Ctx<S, AD>& c, uint64_t i, const double* dLdI, double* dphi) {
+  using R = typename Traits<S>::R;
+  if constexpr (AD) {
+    constexpr int KD = sizeof(S) / sizeof(double) - 1;
+    const int H = c.cam.H, W = c.cam.W, spp = c.cfg.spp_pixel_boundary;
+    const uint64_t slot = i / (uint64_t)spp, nv = (uint64_t)(W + 1) * H;
+    Pcg32 rng = make_sampler(i);
+    R t = rng.next_float();
+    const bool vert = slot < nv;
+    int k, j;
+    V3<R> fp;
+    if (vert) { k = int(slot % (W + 1)); j = int(slot / (W + 1)); fp = V3<R>(R(k), t + R(j), R(1)); }
+    else { uint64_t q = slot - nv; k = int(q % W); j = int(q / W); fp = V3<R>(t + R(k), R(j), R(1)); }
+    V3<R> pc = Camera<R>::xpos(c.cam.r2c, fp);
+    V3<R> d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
+    V3<R> o(R(val(c.cam_pos.x)), R(val(c.cam_pos.y)), R(val(c.cam_pos.z)));
+    Its<R> its = scene_hit<R, false>(c.scv, o, d, true);
+    if (!its.valid) return;
+    V3<R> L = trace2light<R, false>(c.scv, rng, its, true, c.cfg.mis_light_samples, c.cfg.mis_bsdf_samples,
+                                    c.cfg.max_bounce, c.cfg.enable_light_visable != 0);
+    V3<S> x = material_point(c.sc, its);
+    V3<S> r = raster_of(c.cam, x, c.cam_pos);
+    S vel = vert ? r.x - detach(r.x) : r.y - detach(r.y);
+    // pixels on the two sides of the border (outside the image: no pixel)
+    int p_lo = -1, p_hi = -1;
+    if (vert) { if (k >= 1) p_lo = j * W + k - 1; if (k < W) p_hi = j * W + k; }
+    else { if (j >= 1) p_lo = (j - 1) * W + k; if (j < H) p_hi = j * W + k; }
+    double w = 0;
+    for (int ch = 0; ch < 3; ++ch) {
+      double g = (p_hi >= 0 ? dLdI[3 * p_hi + ch] : 0.0) - (p_lo >= 0 ? dLdI[3 * p_lo + ch] : 0.0);
+      w += g * double(L[ch]);
+    }
+    if (!std::isfinite(w)) return;
+    for (int q = 0; q < KD; ++q) dphi[q] += w * vel.d[q] / spp;
+  }
+}
+
 // sampler.h:201-247 HyperCubeSampler: cells in row-major order of the resolution.
 template <class R> struct HyperCube {
   int N = 1;
@@ -200,6 +404,15 @@ template <class R> struct HyperCube {
   }
 };
 
+// The unbiased estimator mixes a uniform share into the guiding masses so that no cell
+// whose preprocessing sample happened to be invalid is left unsampled.
+inline void mass_floor(std::vector<double>& m) {
+  double tot = 0;
+  for (double x : m) tot += x;
+  const double f = tot > 0 ? 0.05 * tot / double(m.size()) : 1.0;
+  for (double& x : m) x = double(float(float(x) + float(f)));
+}
+
 // path_integrator.cc:253-272 preprocess_primary_boundary (value mode, float)
 template <class R>
 inline HyperCube<R> preprocess_primary(const Ctx<R, false>& c) {
@@ -222,6 +435,7 @@ inline HyperCube<R> preprocess_primary(const Ctx<R, false>& c) {
     }
     for (int i = 0; i < hc.cells; ++i) rst[i] = double(R(R(rst[i]) + R(add[i])));
   }
+  if (c.cfg.mode == 1) mass_floor(rst);
   hc.d.build(rst);
   return hc;
 }
@@ -251,6 +465,7 @@ inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
     }
     for (int i = 0; i < hc.cells; ++i) rst[i] = double(R(R(rst[i]) + R(add[i])));
   }
+  if (c.cfg.mode == 1) mass_floor(rst);
   hc.d.build(rst);
   return hc;
 }
@@ -268,6 +483,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
   const int H = c.cam.H, W = c.cam.W;
   const size_t npix = (size_t)H * W;
   constexpr int KD = std::is_same<S, R>::value ? 0 : sizeof(S) / sizeof(double) - 1;
+  const bool unb = c.cfg.mode == 1;
   // ---- interior
   if (which & 1) {
     const int spp = c.cfg.spp_interior;
@@ -308,12 +524,13 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
       float hp = hc.sample_reuse(&s1);
       int rx, ry;
       bool valid;
-      V3<S> v = eval_primary<S, AD>(c, rng, s1, rx, ry, valid);
+      V3<S> v = unb ? eval_primary_unb<S, AD>(c, rng, s1, rx, ry, valid) : eval_primary<S, AD>(c, rng, s1, rx, ry, valid);
       if (!valid) continue;
+      const double dens = double(hp) * (unb ? double(hc.cells) : 1.0);
       if constexpr (KD > 0) {
         size_t pix = (size_t)ry * W + rx;
         for (int k = 0; k < 3; ++k)
-          for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += dLdI[3 * pix + k] * v[k].d[j] / double(hp) / spp;
+          for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += dLdI[3 * pix + k] * v[k].d[j] / dens / spp;
       }
     }
     if constexpr (KD > 0) for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
@@ -332,14 +549,24 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
       R hp = hc.sample_reuse(s3);
       int rx, ry;
       bool valid;
-      V3<S> v = eval_direct<S, AD>(c, s3, rx, ry, valid);
+      V3<S> v = unb ? eval_direct_unb<S, AD>(c, s3, rx, ry, valid) : eval_direct<S, AD>(c, s3, rx, ry, valid);
       if (!valid) continue;
+      const double dens = double(hp) * (unb ? double(hc.cells) : 1.0);
       if constexpr (KD > 0) {
         size_t pix = (size_t)ry * W + rx;
         for (int k = 0; k < 3; ++k)
-          for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += dLdI[3 * pix + k] * v[k].d[j] / double(hp) / spp;
+          for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += dLdI[3 * pix + k] * v[k].d[j] / dens / spp;
       }
     }
+    if constexpr (KD > 0) for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+  }
+  // ---- pixel borders (unbiased estimator only)
+  if ((which & 8) && unb && c.cfg.spp_pixel_boundary > 0) {
+    const uint64_t N = ((uint64_t)(W + 1) * H + (uint64_t)W * (H + 1)) * c.cfg.spp_pixel_boundary;
+    std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)N; ++i)
+      if constexpr (KD > 0) pixel_border_sample<S, AD>(c, (uint64_t)i, dLdI, &phi_s[i * KD]);
     if constexpr (KD > 0) for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
   }
 }
@@ -375,7 +602,7 @@ static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, cons
     Camera<float> camf;
     camf.setup(cams[ci]);
     V3<float> posf(cams[ci].look_from[0], cams[ci].look_from[1], cams[ci].look_from[2]);
-    c.scf = scf; c.camf = camf; c.posf = posf;
+    c.scf = scf; c.camf = camf; c.posf = posf; c.fov = cams[ci].fov;
     cv.scf = scf; cv.camf = camf; cv.posf = posf;
     std::unique_ptr<Ctx<float, false>> cf;
     if (scf) {

@@ -112,6 +112,7 @@ template <class S> inline V3<typename Traits<S>::R> valv(const V3<S>& a) {
   using R = typename Traits<S>::R;
   return {R(val(a.x)), R(val(a.y)), R(val(a.z))};
 }
+template <class S> inline V3<double> val3(const V3<S>& a) { return {double(val(a.x)), double(val(a.y)), double(val(a.z))}; }
 template <class S, class T> inline V3<S> cvt(const V3<T>& a) { return {S(a.x), S(a.y), S(a.z)}; }
 template <class S> inline bool finite3(const V3<S>& a) { return std::isfinite(val(sqnorm(a))); }
 
@@ -283,7 +284,8 @@ struct OrcConfig {
   int n_pass, spp_interior, enable_light_visable, spp_primary_edge, spp_secondary_edge;
   int max_bounce, mis_light_samples, mis_bsdf_samples;
   int pe_rounds, se_rounds, pe_res, se_res[3];
-  int mode;  // 0: reference formulas
+  int mode;  // 0: reference formulas, 1: unbiased estimator
+  int spp_pixel_boundary;  // pixel-border samples per border segment (unbiased estimator)
 };
 }
 
@@ -671,7 +673,8 @@ template <class S> struct Its {
   bool valid = false, is_front = false, is_light = false;
   V3<S> p, n, t, wi;
   S sqd = S(0), jac = S(1), area = S(0);
-  double u = 0, v = 0;  // texture coordinates (no derivatives)
+  double u = 0, v = 0;    // texture coordinates (no derivatives)
+  double b1 = 0, b2 = 0;  // barycentrics of the hit
   int tri = -1, obj = -1, light = -1;
 };
 
@@ -689,6 +692,8 @@ inline Its<S> scene_hit(const Scene<S>& sc, const V3<S>& o, const V3<S>& d, bool
   const Tri<S>& tr = sc.tris[h.tri];
   its.valid = true;
   its.tri = h.tri;
+  its.b1 = double(h.b1);
+  its.b2 = double(h.b2);
   S bu = S(h.b1), bv = S(h.b2);
   its.p = tr.p0 + bu * (tr.p1 - tr.p0) + bv * (tr.p2 - tr.p0);
   R u0 = R(tr.uv[0]), v0 = R(tr.uv[1]);
@@ -776,8 +781,12 @@ inline V3<S> light_sample_point(const Scene<S>& sc, int l, typename Traits<S>::R
 // ------------------------------------------------------------------ trace2light
 // path_integrator.cc:80-186. AD=true reproduces renderD's tape semantics (detached
 // pdfs and MIS weights, jacobi = area/detach(area)); AD=false is the plain render.
+// geo_dirs (the unbiased estimator) forms the G terms of BSDF-sampled segments from
+// the segment's end points instead of the sampled direction (same value, the
+// derivative of the material-form path integral).
 template <class S, bool AD>
-inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid, int nL, int nB, int D, bool light_vis) {
+inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid, int nL, int nB, int D, bool light_vis,
+                         bool geo_dirs = false) {
   using R = typename Traits<S>::R;
   V3<S> T(S(1), S(1), S(1)), L;
   valid = valid && its.valid;
@@ -823,6 +832,10 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
       V3<S> bsdf = tex_at(sc, its.obj, its.u, its.v) * inv_pi<S>();
       S tmp = dot(il.n, -wo) / il.sqd;
       S G = dot(its.n, wo) * tmp;
+      if (geo_dirs) {
+        const V3<S> wg = normalize(il.p - its.p);
+        G = dot(its.n, wg) * (dot(il.n, -wg) / il.sqd);
+      }
       R pdf_bsdf = R(ct) * R(1.0 / M_PI) * R(val(tmp));
       V3<S> value = mul(emit, bsdf) * (G * il.jac / S(pdf_bsdf));
       R weight = R(1) / R(nB);
@@ -845,6 +858,10 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
     V3<S> bsdf = tex_at(sc, its.obj, its.u, its.v) * inv_pi<S>();
     S tmp = dot(nx.n, -wo) / nx.sqd;
     S G = dot(its.n, wo) * tmp;
+    if (geo_dirs) {
+      const V3<S> wg = normalize(nx.p - its.p);
+      G = dot(its.n, wg) * (dot(nx.n, -wg) / nx.sqd);
+    }
     R pdf = R(ct) * R(1.0 / M_PI) * R(val(tmp));
     T = mul(T, bsdf) * (nx.jac * G / S(pdf));
     its = nx;

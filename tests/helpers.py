@@ -51,3 +51,86 @@ def rel_l2(a, b):
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+# ---------------------------------------------------------------- gradient-check scenes
+def wall_mesh(tex_hw=16, z=0.0, half=8.0, seed=5):
+    """Square facing +z at depth z (two triangles); textured (tex_hw^2) or constant grey."""
+    V = np.array([[-half, -half, z], [half, -half, z], [half, half, z], [-half, half, z]], np.float32)
+    F = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+    if not tex_hw:
+        return synth.MeshSpec(V, F, None, None, np.array([0.5, 0.5, 0.5], np.float32))
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    return synth.MeshSpec(V, F, uv, F.copy(), synth.uniform_texture(tex_hw, tex_hw, seed))
+
+
+def front_light():
+    """1x1 light at z = 3, y in [1.5, 2.5], facing -z, radiance 20."""
+    V = np.array([[-0.5, 1.5, 3.0], [0.5, 1.5, 3.0], [0.5, 2.5, 3.0], [-0.5, 2.5, 3.0]], np.float32)
+    F = np.array([[0, 2, 1], [0, 3, 2]], np.int32)
+    return synth.LightSpec(V, F, np.array([20, 20, 20], np.float32))
+
+
+def ball(level=2, textured=True, noise=0.02, scale=1.0, center=(0, 0, 0)):
+    V, F = synth.icosphere(level)
+    if noise:
+        V = synth.radial_noise(V, noise, 2)
+    V = (V * scale + np.asarray(center)).astype(np.float32)
+    if textured:
+        uvs, uvi = synth.spherical_uv(V, F)
+        return synth.MeshSpec(V, F, uvs, uvi, synth.uniform_texture(32, 32, 0))
+    return synth.MeshSpec(V, F, None, None, np.array([0.6, 0.4, 0.3], np.float32))
+
+
+def front_camera(h, w):
+    return synth.CameraSpec(np.array([0, 0.5, 4], np.float32), np.zeros(3, np.float32),
+                            np.array([0, 1, 0], np.float32), math.pi / 4, h, w)
+
+
+def gradient_case(name, h, w):
+    """(spec, index of the moving mesh) of the named translation-gradient case:
+    'ball'   - textured noisy ball before a textured wall (all four terms),
+    'shadow' - an occluder outside the view casting a shadow on a grey wall (direct term),
+    'wall'   - a textured wall filling the view (pixel borders)."""
+    cam = front_camera(h, w)
+    if name == "ball":
+        return synth.SceneSpec([ball(), wall_mesh(16, z=-2)], [front_light()], [cam]), 0
+    if name == "shadow":
+        occ = ball(textured=False, noise=0.0, scale=0.25, center=(0, 1.8, 2.2))
+        return synth.SceneSpec([occ, wall_mesh(0)], [front_light()], [cam]), 0
+    if name == "wall":
+        return synth.SceneSpec([wall_mesh(16)], [front_light()], [cam]), 0
+    raise ValueError(name)
+
+
+def smooth_weights(h, w):
+    """Smooth image-space loss gradient (keeps the loss nearly linear over the FD step)."""
+    yy, xx = np.meshgrid(np.arange(h) + 0.5, np.arange(w) + 0.5, indexing="ij")
+    return np.stack([np.sin(2 * np.pi * xx / w * 1.3 + c) * np.cos(2 * np.pi * yy / h * 0.7) + 0.3
+                     for c in range(3)], -1)
+
+
+def translation_seeds(spec, mesh):
+    """Directional seeds (V_total, 3, 8): directions 0..2 translate mesh `mesh` along x, y, z."""
+    nvt = sum(m.vertices.shape[0] for m in spec.meshes) + sum(l.vertices.shape[0] for l in spec.lights)
+    seeds = np.zeros((nvt, 3, 8))
+    off = sum(m.vertices.shape[0] for m in spec.meshes[:mesh])
+    n = spec.meshes[mesh].vertices.shape[0]
+    for k in range(3):
+        seeds[off:off + n, k, k] = 1.0
+    return seeds
+
+
+def fd_translation(render, spec, mesh, g, h):
+    """Central differences of sum(g * image) for translations of mesh `mesh` by +-h along
+    x, y, z; render(spec) -> image (H, W, 3) with fixed sample seeds (common random numbers)."""
+    V0 = spec.meshes[mesh].vertices.copy()
+    out = []
+    for k in range(3):
+        phi = []
+        for sgn in (1.0, -1.0):
+            spec.meshes[mesh].vertices = (V0 + np.float32(sgn * h) * np.eye(3, dtype=np.float32)[k]).astype(np.float32)
+            phi.append(float((g * render(spec)).sum()))
+        out.append((phi[0] - phi[1]) / (2 * h))
+    spec.meshes[mesh].vertices = V0
+    return np.array(out)

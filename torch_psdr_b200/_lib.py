@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libpsdr_b200.so")
+# PSDR_B200_LIB overrides the library location (e.g. a build installed elsewhere).
+LIB_PATH = os.environ.get("PSDR_B200_LIB", os.path.join(HERE, "_lib", "libpsdr_b200.so"))
 
 PSDR_OK = 0
 PSDR_ERR_INVALID_ARG = 1
