@@ -92,10 +92,20 @@ typedef struct {
 } psdr_camera_desc;
 
 /* PathIntegrator::Config (path_integrator.h:8-21; torch_psdr.py:478-536) plus the
- * B200 extensions: estimator (REFERENCE reproduces the reference's renderD tape;
- * UNBIASED uses the corrected boundary normalisation), tile_paths (wavefront tile,
- * 0 = autotuned), leaf_size (BVH leaf collapse, 0 = default), terms, and seed
- * (0 = the reference's sample streams). */
+ * B200 extensions: estimator, tile_paths (wavefront tile, 0 = autotuned), leaf_size
+ * (BVH leaf collapse, 0 = default), terms, spp_pixel_boundary and seed (0 = the
+ * reference's sample streams; seed s offsets every stream index by s * 2654435761
+ * modulo 2^32).
+ *
+ * estimator REFERENCE reproduces the reference's renderD tape (its boundary terms use
+ * world-space edge measures and per-pixel sample counts, so their scale is not that of
+ * the image derivative). UNBIASED is the derivative of the rendered image itself, in
+ * the material form of the path integral: the interior term differentiates the path
+ * contribution with the area and camera Jacobians of every vertex, and three boundary
+ * terms complete it - material crossing the pixel borders (spp_pixel_boundary samples
+ * per unit border segment), silhouettes sliding over the background, and shadow
+ * boundaries sliding over the receivers of direct light - with raster-space measures.
+ * The forward image is the same for both. */
 typedef struct {
   int32_t n_pass, spp_interior, enable_light_visable, spp_primary_edge, spp_secondary_edge;
   int32_t max_bounce, mis_light_samples, mis_bsdf_samples;
@@ -105,7 +115,9 @@ typedef struct {
   int32_t tile_paths;
   int32_t leaf_size;
   int32_t terms;  /* gradient terms of psdr_render_bwd: bit 0 interior, bit 1 primary
-                     edges, bit 2 direct edges; 0 = all (what renderD differentiates) */
+                     edges, bit 2 direct edges, bit 3 pixel borders (UNBIASED only);
+                     0 = all */
+  int32_t spp_pixel_boundary; /* UNBIASED: samples per unit pixel-border segment */
   uint64_t seed;
 } psdr_config;
 

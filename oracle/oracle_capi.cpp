@@ -1,7 +1,8 @@
 // oracle_capi.cpp -- TEST INFRASTRUCTURE ONLY (the oracle's C entry points for ctypes).
 //
 // Render drivers for the oracle: interior term (path_integrator.cc:355-372), primary
-// boundary (:188-272) and direct boundary (:274-353), in float, double or Dual<K>.
+// boundary (:188-272) and direct boundary (:274-353), in float, double or Dual<K>, with
+// the reference's derivative formulas (mode 0) or the unbiased estimator (mode 1).
 // PARITY UNPINNED (see psdr_oracle.hpp). Built by oracle/build.py into
 // oracle/_build/liborc.so; loaded only by tests, smoke() and the bench CPU baseline.
 #include <omp.h>
@@ -25,7 +26,6 @@ template <class S, bool AD> struct Ctx {
   const Scene<float>* scf = nullptr;
   Camera<float> camf;
   V3<float> posf;
-  float fov = 0.f;        // vertical field of view (radians)
   double hc_cells = 1.0;  // hypercube cell count of the term being evaluated
 };
 
@@ -38,19 +38,27 @@ inline S cam_jacobian(const Camera<R>& cam, const V3<S>& x, const V3<S>& n, cons
   return abs_(dot(n, rel)) / (z * z * z);
 }
 
-// fx*fy of the raster map (camera.h: x scaled by W/2*cot(fov/2), y by H/2*cot(fov/2)).
-inline double raster_fxfy(double fov, int H, int W) {
-  double cot = 1.0 / std::tan(fov * 0.5);
-  return 0.25 * double(W) * double(H) * cot * cot;
+// fx*fy of the map from world directions to raster coordinates. The camera's right
+// and up axes are not normalised (camera.h:7-40: right = up x dir), so the raster scale
+// of camera space (c2r) is divided by their lengths (the norms of w2c's first rows
+// are their inverses).
+template <class R>
+inline double raster_fxfy(const Camera<R>& cam) {
+  double r0 = 0, r1 = 0;
+  for (int j = 0; j < 3; ++j) {
+    r0 += double(cam.w2c[0][j]) * double(cam.w2c[0][j]);
+    r1 += double(cam.w2c[1][j]) * double(cam.w2c[1][j]);
+  }
+  return std::fabs(double(cam.c2r[0][0]) * double(cam.c2r[1][1])) * std::sqrt(r0 * r1);
 }
 
 // Raster position of x seen from o (camera rotation fixed, translation o).
 template <class S, class R>
 inline V3<S> raster_of(const Camera<R>& cam, const V3<S>& x, const V3<S>& o) {
   V3<S> rel = x - o;
-  V3<S> pc(S(cam.c2w[0][0]) * rel.x + S(cam.c2w[1][0]) * rel.y + S(cam.c2w[2][0]) * rel.z,
-           S(cam.c2w[0][1]) * rel.x + S(cam.c2w[1][1]) * rel.y + S(cam.c2w[2][1]) * rel.z,
-           S(cam.c2w[0][2]) * rel.x + S(cam.c2w[1][2]) * rel.y + S(cam.c2w[2][2]) * rel.z);
+  V3<S> pc(S(cam.w2c[0][0]) * rel.x + S(cam.w2c[0][1]) * rel.y + S(cam.w2c[0][2]) * rel.z,
+           S(cam.w2c[1][0]) * rel.x + S(cam.w2c[1][1]) * rel.y + S(cam.w2c[1][2]) * rel.z,
+           S(cam.w2c[2][0]) * rel.x + S(cam.w2c[2][1]) * rel.y + S(cam.w2c[2][2]) * rel.z);
   return Camera<R>::xpos(cam.c2r, pc);
 }
 
@@ -271,7 +279,7 @@ inline V3<S> eval_primary_unb(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx
     double re = norm(rel_e), rg = norm(rel_g);
     V3<double> look(-double(c.camf.c2w[0][2]), -double(c.camf.c2w[1][2]), -double(c.camf.c2w[2][2]));
     double z = dot(rel_e, look);
-    double k = raster_fxfy(c.fov, c.cam.H, c.cam.W) * re / (z * z * z) / (double(pdf_e) * c.cam.H * c.cam.W);
+    double k = raster_fxfy(c.cam) * re / (z * z * z) / (double(pdf_e) * c.cam.H * c.cam.W);
     V3<S> dso = c.cam_pos - detach(c.cam_pos);
     V3<S> vrel = (xes - detach(xes) - dso) - (xg - detach(xg) - dso) * S(re / rg);
     V3<S> ns(S(n.x), S(n.y), S(n.z));
@@ -325,7 +333,7 @@ inline V3<S> eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], i
     S dn = dot(deff, V3<S>(S(ns.x), S(ns.y), S(ns.z)));
     double cos_y = std::fabs(dot(val3(is0.n), w));
     V3<double> o = val3(c.cam_pos);
-    double Jc = raster_fxfy(c.fov, c.cam.H, c.cam.W) * val(cam_jacobian(c.cam, xdv, val3(id0.n), o));
+    double Jc = raster_fxfy(c.cam) * val(cam_jacobian(c.cam, xdv, val3(id0.n), o));
     double k = cos_y / (dby * dby) * Jc / (pdf_e * pdf_l * c.cam.H * c.cam.W);
     V3<S> fr = detach(tex_at(sc, id0.obj, id0.u, id0.v) * inv_pi<S>());
     V3<S> Le = detach(sc.emit[is0.light]);
@@ -335,25 +343,81 @@ inline V3<S> eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], i
   return value;
 }
 
-// Pixel-border term: border sample i on the (W+1) x H vertical and W x (H+1) horizontal
-// unit segments of the pixel grid (spp_pixel_boundary samples each). The radiance L
-// seen through the border point flows across it at the raster velocity of its primary
-// vertex; the pixel it enters gains L v, the one it leaves loses it. Adds
-// dPhi/dtheta . seed_k to dphi.
+// Pixel-border term. Segment q of the (W+1) x H vertical and W x (H+1) horizontal unit
+// segments of the pixel grid contributes (dI[hi] - dI[lo]) . Int L v dl: L is the
+// radiance seen through the border point, v the raster velocity of its primary vertex
+// across the segment (material flows into pixel hi and out of pixel lo; outside the
+// image dI = 0). Segments are importance-sampled by m_q = |dI[hi] - dI[lo]|_1 (float)
+// with stratified inversion of the double-precision CDF: sample i of N takes
+// u = (i + xi) / N, the first segment whose prefix sum exceeds u * total, and the
+// remainder as its position along the segment.
+struct Border {
+  int H = 0, W = 0;
+  long long S = 0;
+  std::vector<double> w, pre;
+  void pixels(long long q, bool& vert, int& k, int& j, int& lo, int& hi) const {
+    const long long nv = (long long)(W + 1) * H;
+    vert = q < nv;
+    lo = hi = -1;
+    if (vert) {
+      k = int(q % (W + 1)); j = int(q / (W + 1));
+      if (k >= 1) lo = j * W + k - 1;
+      if (k < W) hi = j * W + k;
+    } else {
+      const long long r = q - nv;
+      k = int(r % W); j = int(r / W);
+      if (j >= 1) lo = (j - 1) * W + k;
+      if (j < H) hi = j * W + k;
+    }
+  }
+  void build(int h, int wd, const double* dLdI) {
+    H = h; W = wd;
+    S = (long long)(W + 1) * H + (long long)W * (H + 1);
+    w.resize(S); pre.resize(S);
+    double acc = 0;
+    for (long long q = 0; q < S; ++q) {
+      bool vert; int k, j, lo, hi;
+      pixels(q, vert, k, j, lo, hi);
+      float d[3];
+      for (int c = 0; c < 3; ++c)
+        d[c] = (hi >= 0 ? float(dLdI[3 * hi + c]) : 0.f) - (lo >= 0 ? float(dLdI[3 * lo + c]) : 0.f);
+      const float m = std::fabs(d[0]) + std::fabs(d[1]) + std::fabs(d[2]);
+      w[q] = double(m);
+      acc += w[q];
+      pre[q] = acc;
+    }
+  }
+  long long locate(long long i, long long N, float xi, float& t, double& pmf) const {
+    const double tot = pre[S - 1];
+    const double u = (double(i) + double(xi)) / double(N);
+    const double tt = u * tot;
+    long long q = (long long)(std::upper_bound(pre.begin(), pre.end(), tt) - pre.begin());
+    if (q >= S) q = S - 1;
+    const double base = q > 0 ? pre[q - 1] : 0.0;
+    double r = (tt - base) / w[q];
+    r = r < 0.0 ? 0.0 : r;
+    t = std::min(float(r), 0.99999994f);
+    pmf = w[q] / tot;
+    return q;
+  }
+};
+
+// Border sample i of N: adds dPhi/dtheta . seed_k to dphi.
 template <class S, bool AD>
-inline void pixel_border_sample(const Ctx<S, AD>& c, uint64_t i, const double* dLdI, double* dphi) {
+inline void pixel_border_sample(const Ctx<S, AD>& c, const Border& B, uint64_t i, uint64_t N, const double* dLdI,
+                                double* dphi) {
   using R = typename Traits<S>::R;
   if constexpr (AD) {
     constexpr int KD = sizeof(S) / sizeof(double) - 1;
-    const int H = c.cam.H, W = c.cam.W, spp = c.cfg.spp_pixel_boundary;
-    const uint64_t slot = i / (uint64_t)spp, nv = (uint64_t)(W + 1) * H;
     Pcg32 rng = make_sampler(i);
-    R t = rng.next_float();
-    const bool vert = slot < nv;
-    int k, j;
-    V3<R> fp;
-    if (vert) { k = int(slot % (W + 1)); j = int(slot / (W + 1)); fp = V3<R>(R(k), t + R(j), R(1)); }
-    else { uint64_t q = slot - nv; k = int(q % W); j = int(q / W); fp = V3<R>(t + R(k), R(j), R(1)); }
+    const float xi = rng.next_float();
+    float t;
+    double pmf;
+    const long long q = B.locate((long long)i, (long long)N, xi, t, pmf);
+    if (!(pmf > 0)) return;
+    bool vert; int k, j, lo, hi;
+    B.pixels(q, vert, k, j, lo, hi);
+    V3<R> fp = vert ? V3<R>(R(float(k)), R(t + float(j)), R(1)) : V3<R>(R(t + float(k)), R(float(j)), R(1));
     V3<R> pc = Camera<R>::xpos(c.cam.r2c, fp);
     V3<R> d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
     V3<R> o(R(val(c.cam_pos.x)), R(val(c.cam_pos.y)), R(val(c.cam_pos.z)));
@@ -364,17 +428,14 @@ inline void pixel_border_sample(const Ctx<S, AD>& c, uint64_t i, const double* d
     V3<S> x = material_point(c.sc, its);
     V3<S> r = raster_of(c.cam, x, c.cam_pos);
     S vel = vert ? r.x - detach(r.x) : r.y - detach(r.y);
-    // pixels on the two sides of the border (outside the image: no pixel)
-    int p_lo = -1, p_hi = -1;
-    if (vert) { if (k >= 1) p_lo = j * W + k - 1; if (k < W) p_hi = j * W + k; }
-    else { if (j >= 1) p_lo = (j - 1) * W + k; if (j < H) p_hi = j * W + k; }
-    double w = 0;
+    double wgt = 0;
     for (int ch = 0; ch < 3; ++ch) {
-      double g = (p_hi >= 0 ? dLdI[3 * p_hi + ch] : 0.0) - (p_lo >= 0 ? dLdI[3 * p_lo + ch] : 0.0);
-      w += g * double(L[ch]);
+      double g = (hi >= 0 ? dLdI[3 * hi + ch] : 0.0) - (lo >= 0 ? dLdI[3 * lo + ch] : 0.0);
+      wgt += g * double(L[ch]);
     }
-    if (!std::isfinite(w)) return;
-    for (int q = 0; q < KD; ++q) dphi[q] += w * vel.d[q] / spp;
+    wgt /= double(N) * pmf;
+    if (!std::isfinite(wgt)) return;
+    for (int qd = 0; qd < KD; ++qd) dphi[qd] += wgt * vel.d[qd];
   }
 }
 
@@ -401,6 +462,28 @@ template <class R> struct HyperCube {
     cell_coords(idx, cc);
     for (int i = 0; i < N; ++i) s[i] = (s[i] + R(cc[i])) * unit[i];
     return pdf;
+  }
+  // Unbiased estimator: the cell is the first whose double-precision prefix sum exceeds
+  // s_last * total (a float CDF cannot resolve cells below 2^-24 of the mass nor place a
+  // sample inside them), and the position inside the cell along the last dimension is
+  // a fresh uniform. Returns the cell's probability.
+  std::vector<double> w, pre;
+  void build_unb(const std::vector<double>& m) {
+    w = m;
+    pre.resize(m.size());
+    double acc = 0;
+    for (size_t i = 0; i < m.size(); ++i) { acc += m[i]; pre[i] = acc; }
+  }
+  double sample_unb(R* s, Pcg32& rng) const {
+    const double tot = pre.back();
+    const double t = double(s[N - 1]) * tot;
+    int idx = int(std::upper_bound(pre.begin(), pre.end(), t) - pre.begin());
+    if (idx >= cells) idx = cells - 1;
+    int cc[3];
+    cell_coords(idx, cc);
+    s[N - 1] = R(rng.next_float());
+    for (int i = 0; i < N; ++i) s[i] = (s[i] + R(cc[i])) * unit[i];
+    return w[idx] / tot;
   }
 };
 
@@ -435,7 +518,10 @@ inline HyperCube<R> preprocess_primary(const Ctx<R, false>& c) {
     }
     for (int i = 0; i < hc.cells; ++i) rst[i] = double(R(R(rst[i]) + R(add[i])));
   }
-  if (c.cfg.mode == 1) mass_floor(rst);
+  if (c.cfg.mode == 1) {
+    mass_floor(rst);
+    hc.build_unb(rst);
+  }
   hc.d.build(rst);
   return hc;
 }
@@ -465,7 +551,10 @@ inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
     }
     for (int i = 0; i < hc.cells; ++i) rst[i] = double(R(R(rst[i]) + R(add[i])));
   }
-  if (c.cfg.mode == 1) mass_floor(rst);
+  if (c.cfg.mode == 1) {
+    mass_floor(rst);
+    hc.build_unb(rst);
+  }
   hc.d.build(rst);
   return hc;
 }
@@ -521,7 +610,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
     for (int64_t i = 0; i < (int64_t)N; ++i) {
       Pcg32 rng = make_sampler((uint64_t)i);
       float s1 = rng.next_float();
-      float hp = hc.sample_reuse(&s1);
+      const double hp = unb ? hc.sample_unb(&s1, rng) : double(hc.sample_reuse(&s1));
       int rx, ry;
       bool valid;
       V3<S> v = unb ? eval_primary_unb<S, AD>(c, rng, s1, rx, ry, valid) : eval_primary<S, AD>(c, rng, s1, rx, ry, valid);
@@ -546,7 +635,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
       Pcg32 rng = make_sampler((uint64_t)i);
       R s3[3];
       for (int k = 0; k < 3; ++k) s3[k] = rng.next_float();
-      R hp = hc.sample_reuse(s3);
+      const double hp = unb ? hc.sample_unb(s3, rng) : double(hc.sample_reuse(s3));
       int rx, ry;
       bool valid;
       V3<S> v = unb ? eval_direct_unb<S, AD>(c, s3, rx, ry, valid) : eval_direct<S, AD>(c, s3, rx, ry, valid);
@@ -562,12 +651,17 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
   }
   // ---- pixel borders (unbiased estimator only)
   if ((which & 8) && unb && c.cfg.spp_pixel_boundary > 0) {
-    const uint64_t N = ((uint64_t)(W + 1) * H + (uint64_t)W * (H + 1)) * c.cfg.spp_pixel_boundary;
-    std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
+    if constexpr (KD > 0) {
+      Border B;
+      B.build(H, W, dLdI);
+      if (B.pre[B.S - 1] > 0) {
+        const uint64_t N = (uint64_t)B.S * c.cfg.spp_pixel_boundary;
+        std::vector<double> phi_s(N * KD, 0.0);
 #pragma omp parallel for schedule(dynamic, 64)
-    for (int64_t i = 0; i < (int64_t)N; ++i)
-      if constexpr (KD > 0) pixel_border_sample<S, AD>(c, (uint64_t)i, dLdI, &phi_s[i * KD]);
-    if constexpr (KD > 0) for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+        for (int64_t i = 0; i < (int64_t)N; ++i) pixel_border_sample<S, AD>(c, B, (uint64_t)i, N, dLdI, &phi_s[i * KD]);
+        for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+      }
+    }
   }
 }
 
@@ -602,7 +696,7 @@ static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, cons
     Camera<float> camf;
     camf.setup(cams[ci]);
     V3<float> posf(cams[ci].look_from[0], cams[ci].look_from[1], cams[ci].look_from[2]);
-    c.scf = scf; c.camf = camf; c.posf = posf; c.fov = cams[ci].fov;
+    c.scf = scf; c.camf = camf; c.posf = posf;
     cv.scf = scf; cv.camf = camf; cv.posf = posf;
     std::unique_ptr<Ctx<float, false>> cf;
     if (scf) {

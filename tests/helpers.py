@@ -54,7 +54,7 @@ def rel_l2(a, b):
 
 
 # ---------------------------------------------------------------- gradient-check scenes
-def wall_mesh(tex_hw=16, z=0.0, half=8.0, seed=5):
+def wall_mesh(tex_hw=15, z=0.0, half=8.0, seed=5):
     """Square facing +z at depth z (two triangles); textured (tex_hw^2) or constant grey."""
     V = np.array([[-half, -half, z], [half, -half, z], [half, half, z], [-half, half, z]], np.float32)
     F = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
@@ -91,15 +91,21 @@ def gradient_case(name, h, w):
     """(spec, index of the moving mesh) of the named translation-gradient case:
     'ball'   - textured noisy ball before a textured wall (all four terms),
     'shadow' - an occluder outside the view casting a shadow on a grey wall (direct term),
-    'wall'   - a textured wall filling the view (pixel borders)."""
+    'wall'   - a textured wall filling the view (pixel borders).
+    Wall textures have an odd texel count: with an even one a texel edge lies on the
+    camera's centre line and so exactly on a pixel border, where the radiance that
+    crosses the border is that of the texel edge itself (a measure-zero alignment at
+    which the image is not differentiable and point samples on the border pick one
+    side)."""
     cam = front_camera(h, w)
     if name == "ball":
-        return synth.SceneSpec([ball(), wall_mesh(16, z=-2)], [front_light()], [cam]), 0
+        # off-centre for the same reason: the ball's uv seam texel edge faces the camera
+        return synth.SceneSpec([ball(center=(0.05, 0.02, 0.0)), wall_mesh(15, z=-2)], [front_light()], [cam]), 0
     if name == "shadow":
         occ = ball(textured=False, noise=0.0, scale=0.25, center=(0, 1.8, 2.2))
         return synth.SceneSpec([occ, wall_mesh(0)], [front_light()], [cam]), 0
     if name == "wall":
-        return synth.SceneSpec([wall_mesh(16)], [front_light()], [cam]), 0
+        return synth.SceneSpec([wall_mesh(15)], [front_light()], [cam]), 0
     raise ValueError(name)
 
 

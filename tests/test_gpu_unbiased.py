@@ -1,0 +1,132 @@
+"""The unbiased estimator on the GPU: every gradient term against the oracle's
+forward-mode derivatives, and whole-gradient translation checks against central finite
+differences of the GPU's own images (common random numbers)."""
+import numpy as np
+import pytest
+import torch
+
+import orc
+import torch_psdr_b200 as dr
+from torch_psdr_b200 import synth
+from helpers import fd_translation, gradient_case, rel_l2, smooth_weights, to_torch_scene, translation_seeds
+from test_gpu_parity import _gpu_dir_derivs, _seeds_for
+
+pytestmark = pytest.mark.gpu
+
+BASE = dict(spp_interior=4, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=3,
+            primary_edge_hypercube_resolution=500, secondary_edge_hypercube_resolution=[500, 3, 3])
+
+UNB_CASES = [
+    # (terms bitmask, parameters)
+    (1, ("verts",)),
+    (1, ("cam",)),
+    (1, ("tex", "emit")),
+    (2, ("verts",)),
+    (2, ("cam",)),
+    (4, ("verts",)),
+    (8, ("verts",)),
+    (8, ("cam",)),
+]
+
+
+@pytest.mark.parametrize("terms,kinds", UNB_CASES)
+def test_unbiased_terms_match_oracle(cuda, terms, kinds):
+    spec, _ = gradient_case("ball", 24, 24)
+    rng = np.random.default_rng(3)
+    gseeds, oseeds = _seeds_for(spec, kinds, rng)
+    params = set()
+    for k in kinds:
+        params |= {"verts": {"verts", "light_verts"}, "tex": {"tex"}, "emit": {"emit"}, "cam": {"cam"}}[k]
+    got, dLdI = _gpu_dir_derivs(spec, terms, gseeds, dict(BASE, estimator="unbiased", spp_pixel_boundary=4), params)
+    ocfg = dict(BASE, mode=1, spp_pixel_boundary=4,
+                secondary_edge_hypercube_resolution=tuple(BASE["secondary_edge_hypercube_resolution"]))
+    ref = orc.grad_dir(spec, [dLdI], which=terms, **oseeds, **ocfg)
+    err = np.abs(got - ref) / (np.abs(ref).max() + 1e-30)
+    print(f"unbiased terms={terms} {kinds}: gpu {got[:4]} oracle {ref[:4]} max rel {err.max():.2e}")
+    assert np.abs(ref).max() > 0
+    assert err.max() < 2e-3
+
+
+def _gpu_render(integ):
+    def render(spec):
+        scene, _ = to_torch_scene(spec)
+        return integ.renderC(scene)[0].double().cpu().numpy()
+    return render
+
+
+def _gpu_translation_grad(spec, mesh, integ, g):
+    scene, T = to_torch_scene(spec, requires_grad={"verts"})
+    img = integ.renderD(scene)[0]
+    img.backward(torch.tensor(g, dtype=torch.float32, device="cuda"))
+    return T[f"verts{mesh}"].grad.double().sum(0).cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["ball", "shadow", "wall"])
+def test_unbiased_translation_vs_fd(cuda, name):
+    size = 96
+    spec, mesh = gradient_case(name, size, size)
+    g = smooth_weights(size, size)
+    kw = dict(spp_interior=256, spp_primary_edge=64, spp_secondary_edge=8192, spp_pixel_boundary=64, max_bounce=2,
+              secondary_edge_hypercube_resolution=[20000, 6, 6], secondary_edge_preprocess_rounds=4,
+              estimator="unbiased")
+    ad = _gpu_translation_grad(spec, mesh, dr.PathIntegrator(**kw), g)
+    fd = fd_translation(_gpu_render(dr.PathIntegrator(**dict(kw, spp_interior=1024))), spec, mesh, g, 1e-2)
+    e = rel_l2(ad, fd)
+    print(f"{name}: AD {ad} FD {fd} rel L2 {e:.3f}")
+    assert e < 0.05
+
+
+def test_geometry_workload_translation_vs_fd(cuda):
+    """The 20k-triangle 512x512 workload at its own sample counts (32 spp interior, 4 spp
+    per edge kind and per pixel-border segment): gradient of the L2 loss against a
+    target with the sphere shifted, w.r.t. the sphere's translation."""
+    spec = synth.sphere_scene(level=5, tex_hw=256, noise_sigma=0.02, noise_seed=2, height=512, width=512)
+    kw = dict(spp_interior=32, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=3, estimator="unbiased")
+    integ = dr.PathIntegrator(**kw)
+    V0 = spec.meshes[0].vertices.copy()
+    spec.meshes[0].vertices = (V0 + np.array([0.03, -0.02, 0.02], np.float32)).astype(np.float32)
+    tgt = _gpu_render(dr.PathIntegrator(**dict(kw, spp_interior=64, seed=7)))(spec)
+    spec.meshes[0].vertices = V0
+    img0 = _gpu_render(integ)(spec)
+    g = 2.0 * (img0 - tgt)
+    ad = _gpu_translation_grad(spec, 0, integ, g)
+    fd_integ = dr.PathIntegrator(**dict(kw, spp_interior=1024))
+
+    def loss_image(s):
+        return _gpu_render(fd_integ)(s)
+
+    # central differences of the loss itself (not of sum(g * image))
+    h = 1e-3
+    fd = []
+    for k in range(3):
+        phi = []
+        for sgn in (1.0, -1.0):
+            spec.meshes[0].vertices = (V0 + np.float32(sgn * h) * np.eye(3, dtype=np.float32)[k]).astype(np.float32)
+            img = loss_image(spec)
+            phi.append(float(((img - tgt) ** 2).sum()))
+        fd.append((phi[0] - phi[1]) / (2 * h))
+    spec.meshes[0].vertices = V0
+    fd = np.array(fd)
+    e = rel_l2(ad, fd)
+    print(f"geometry workload: AD {ad} FD {fd} rel L2 {e:.3f}")
+    assert e < 0.05
+
+
+@pytest.mark.parametrize("terms", [1, 2, 4, 8])
+def test_unbiased_camera_translation_is_scene_translation(cuda, terms):
+    """Moving the camera by d is moving every mesh and light by -d: per term, the
+    camera-origin gradient equals minus the sum of all vertex gradients."""
+    spec, _ = gradient_case("ball", 32, 32)
+    scene, T = to_torch_scene(spec, requires_grad={"verts", "light_verts", "cam"})
+    integ = dr.PathIntegrator(**dict(BASE, estimator="unbiased", spp_pixel_boundary=4, gradient_terms=terms))
+    img = integ.renderD(scene)[0]
+    g = np.random.default_rng(5).normal(size=tuple(img.shape))
+    img.backward(torch.tensor(g, dtype=torch.float32, device="cuda"))
+    cam = T["cam0"].grad.double().cpu().numpy()
+    tot = sum(v.grad.double().sum(0).cpu().numpy() for k, v in T.items()
+              if (k.startswith("verts") or k.startswith("lverts")) and v.grad is not None)
+    scale = max(np.abs(v.grad.double().sum(0).cpu().numpy()).max() for k, v in T.items()
+                if (k.startswith("verts") or k.startswith("lverts")) and v.grad is not None)
+    print(f"terms={terms}: camera {cam} -sum(vertices) {-tot} (per-mesh scale {scale:.3g})")
+    assert scale > 0
+    np.testing.assert_allclose(cam, -tot, rtol=0, atol=2e-3 * scale)

@@ -14,9 +14,9 @@ CFG = dict(max_bounce=2, primary_edge_hypercube_resolution=2000, mode=1)
 
 
 @pytest.mark.parametrize("name,size,spp,se_res,tol", [
-    ("ball", 48, 1024, 2000, 0.08),
-    ("shadow", 48, 4096, 20000, 0.10),
-    ("wall", 48, 1024, 2000, 0.08),
+    ("ball", 48, 1024, 2000, 0.03),
+    ("shadow", 48, 4096, 20000, 0.06),
+    ("wall", 48, 1024, 2000, 0.03),
 ])
 def test_unbiased_translation_matches_fd(name, size, spp, se_res, tol):
     spec, mesh = gradient_case(name, size, size)

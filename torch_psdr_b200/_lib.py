@@ -56,7 +56,8 @@ class Config(C.Structure):
                 ("primary_edge_preprocess_rounds", C.c_int32), ("secondary_edge_preprocess_rounds", C.c_int32),
                 ("primary_edge_hypercube_resolution", C.c_int32),
                 ("secondary_edge_hypercube_resolution", C.c_int32 * 3), ("estimator", C.c_int32),
-                ("tile_paths", C.c_int32), ("leaf_size", C.c_int32), ("terms", C.c_int32), ("seed", C.c_uint64)]
+                ("tile_paths", C.c_int32), ("leaf_size", C.c_int32), ("terms", C.c_int32),
+                ("spp_pixel_boundary", C.c_int32), ("seed", C.c_uint64)]
 
 
 class GradTargets(C.Structure):

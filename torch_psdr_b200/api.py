@@ -9,7 +9,7 @@ calls psdr_render_bwd (the path-replay adjoint).
 from __future__ import annotations
 
 import ctypes as C
-from typing import List, Union
+from typing import List, Optional, Union
 
 import torch
 from torch import Tensor
@@ -344,12 +344,17 @@ class PathIntegrator:
                  spp_primary_edge: int = 1, spp_secondary_edge: int = 1, primary_edge_preprocess_rounds: int = 1,
                  secondary_edge_preprocess_rounds: int = 1, primary_edge_hypercube_resolution: int = 10000,
                  secondary_edge_hypercube_resolution: List[int] = [10000, 6, 6], estimator: str = "reference",
-                 seed: int = 0, tile_paths: int = 0, gradient_terms: int = 0):
+                 seed: int = 0, tile_paths: int = 0, gradient_terms: int = 0,
+                 spp_pixel_boundary: Optional[int] = None):
         """Path-space differentiable integrator (torch_psdr.py:477-536; path_integrator.h:8-21).
 
-        B200 extensions: estimator ("reference" reproduces renderD exactly), seed (0 =
-        the reference's sample streams), tile_paths (wavefront tile, 0 = automatic),
-        gradient_terms (bitmask: 1 interior, 2 primary edges, 4 direct edges; 0 = all).
+        B200 extensions: estimator ("reference" reproduces renderD exactly; "unbiased"
+        is the derivative of the rendered image: material-form interior term plus
+        pixel-border, silhouette and shadow-boundary terms), seed (0 = the reference's
+        sample streams), tile_paths (wavefront tile, 0 = automatic), gradient_terms
+        (bitmask: 1 interior, 2 primary edges, 4 direct edges, 8 pixel borders; 0 = all),
+        spp_pixel_boundary (unbiased: samples per unit pixel-border segment; default
+        spp_primary_edge).
         """
         assert n_pass > 0
         assert spp_interior > 0
@@ -381,6 +386,8 @@ class PathIntegrator:
         cfg.estimator = L.EST_REFERENCE if estimator == "reference" else L.EST_UNBIASED
         cfg.tile_paths = tile_paths
         cfg.terms = gradient_terms
+        cfg.spp_pixel_boundary = spp_primary_edge if spp_pixel_boundary is None else spp_pixel_boundary
+        assert cfg.spp_pixel_boundary >= 0
         cfg.seed = seed
         self.cfg = cfg
         self._lib = L.load()

@@ -100,7 +100,6 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     b->backward = d_images != nullptr;
     if (b->backward) {
       PSDR_CHECK(grads != nullptr, "d_images given without gradient targets");
-      PSDR_CHECK(cfg->estimator == PSDR_EST_REFERENCE, "only the reference estimator is available in this build");
     }
     cudaStream_t st = nullptr;
     b->campos.alloc(sizeof(double) * 3 * n_cams, st);
@@ -119,6 +118,7 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     b->cap = choose_cap(*cfg, b->views, true);
     const int Rmax = cfg->mis_light_samples + std::max(cfg->mis_bsdf_samples, 1) + 1;
     b->ws.ensure(b->cap, Rmax, cfg->max_bounce, n_cams, b->backward ? 1 : 0, st);
+    if (b->backward) ensure_border(&b->ws, *cfg, b->views, st);
     upload_views(&b->ws, b->views, st);
     std::vector<DevScene> ds(n_scenes);
     for (int i = 0; i < n_scenes; ++i) ds[i] = scenes[i]->dev;

@@ -77,6 +77,7 @@ void check_cfg(const psdr_config* c) {
     PSDR_CHECK(c->secondary_edge_hypercube_resolution[k] > 0, "secondary hypercube resolution must be > 0");
   PSDR_CHECK(c->estimator == PSDR_EST_REFERENCE || c->estimator == PSDR_EST_UNBIASED, "bad estimator");
   PSDR_CHECK(c->tile_paths >= 0, "tile_paths must be >= 0");
+  PSDR_CHECK(c->spp_pixel_boundary >= 0, "spp_pixel_boundary must be >= 0");
 }
 
 void check_cams(const psdr_camera_desc* cams, int n) {
@@ -132,7 +133,7 @@ extern "C" {
 
 const char* psdr_last_error(void) { return psdr::g_err.c_str(); }
 const char* psdr_version(void) { return "torch_psdr_b200 0.1.0 (sm_100a)"; }
-int32_t psdr_abi_version(void) { return 1; }
+int32_t psdr_abi_version(void) { return 2; }
 
 psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_scene** out) {
   API_BEGIN
@@ -326,7 +327,6 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   check_cfg(cfg);
   check_cams(cams, n_cams);
   PSDR_CHECK(scene->nlight > 0, "scene has no light");
-  PSDR_CHECK(cfg->estimator == PSDR_EST_REFERENCE, "only the reference estimator is available in this build");
   cudaStream_t st = (cudaStream_t)stream;
   PSDR_CUDA(cudaMemsetAsync(scene->g_verts.p, 0, scene->g_verts.bytes, st));
   PSDR_CUDA(cudaMemsetAsync(scene->g_tex.p, 0, scene->g_tex.bytes, st));

@@ -474,11 +474,29 @@ struct DepthVals {
   bool has_next;
 };
 
+// Adjoint of a BSDF-sampled segment's G in the unbiased estimator: the direction is
+// that of the segment's end points, w = normalize(q - x), so it back-propagates into
+// both points instead of the sampling frame.
+PSDR_D void geom_adj_points(float adjG, const Surf& x, const Surf& q, SurfAdj& ax, SurfAdj& aq) {
+  const float3 rv = q.p - x.p;
+  const float rn = norm(rv);
+  const float3 wg = rv / rn;
+  const float G = dot(x.n, wg) * (dot(q.n, -wg) / q.sqd);
+  float3 adj_w;
+  geom_adj(adjG, x.n, q.n, wg, x.p, q.p, q.sqd, G, ax, aq, adj_w);
+  const float3 ar = (adj_w - wg * dot(wg, adj_w)) / rn;
+  aq.p += ar;
+  ax.p -= ar;
+}
+
 // One depth of trace2light, recomputed from the sampler stream and the hit records.
 // ADJ=false returns the contribution C and the throughput factor beta; ADJ=true
 // back-propagates adjC / adjB into the surfaces, the texture, the emission and the
 // light vertices (carry = adjoint of the next vertex, passed to the next depth).
-template <bool ADJ>
+// UNB (unbiased estimator): BSDF-sampled segments differentiate G through their end
+// points (geom_adj_points); the reference differentiates it through the sampled
+// direction's frame.
+template <bool ADJ, bool UNB = false>
 PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng& rng, const float4* rec, bool last,
                             float3 adjC, float3 adjB, SurfAdj& ax, SurfAdj& carry, HotAcc& hot, float3& adj_tex) {
   DepthVals out;
@@ -560,9 +578,13 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
       const float adj_gam = dot(av, eb) / pdf_b;
       SurfAdj aq = zero_adj();
       aq.area = adj_gam * G / q.area;
-      float3 adj_wo;
-      geom_adj(adj_gam, x.n, q.n, wo, x.p, q.p, q.sqd, G, ax, aq, adj_wo);
-      dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+      if (UNB) {
+        geom_adj_points(adj_gam, x, q, ax, aq);
+      } else {
+        float3 adj_wo;
+        geom_adj(adj_gam, x.n, q.n, wo, x.p, q.p, q.sqd, G, ax, aq, adj_wo);
+        dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+      }
       scatter_surf(sc, hot, tri, h.y, h.z, q.front, aq);
     }
   }
@@ -587,9 +609,13 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
           const float adj_gam = dot(adjB, bsdf) / pdf;
           carry = zero_adj();
           carry.area = adj_gam * G / nx.area;
-          float3 adj_wo;
-          geom_adj(adj_gam, x.n, nx.n, wo, x.p, nx.p, nx.sqd, G, ax, carry, adj_wo);
-          dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+          if (UNB) {
+            geom_adj_points(adj_gam, x, nx, ax, carry);
+          } else {
+            float3 adj_wo;
+            geom_adj(adj_gam, x.n, nx.n, wo, x.p, nx.p, nx.sqd, G, ax, carry, adj_wo);
+            dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+          }
         }
       }
     }
@@ -657,10 +683,68 @@ PSDR_D float3 suffix_radiance(const float4* __restrict__ cb, int from, int D) {
   return S;
 }
 
+// Camera-origin adjoint kept in registers while consecutive samples share a view.
+struct CamAcc {
+  const DevView* v = nullptr;
+  float3 g;
+  PSDR_D void add(const DevView* view, float3 a) {
+    if (view != v) {
+      flush();
+      v = view;
+      g = f3(0.f, 0.f, 0.f);
+    }
+    g += a;
+  }
+  PSDR_D void flush() {
+    if (v && v->grad_pos && (g.x != 0.f || g.y != 0.f || g.z != 0.f)) atomic_add3(v->grad_pos, g);
+    v = nullptr;
+  }
+  // End of a kernel: one atomic per warp when the warp shares the view.
+  PSDR_D void flush_warp() {
+    const unsigned long long key = (unsigned long long)v;
+    const unsigned long long k0 = __shfl_sync(0xffffffffu, key, 0);
+    if (!__all_sync(0xffffffffu, key == k0) || !v) { flush(); return; }
+    float3 s = g;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+      s.z += __shfl_xor_sync(0xffffffffu, s.z, o);
+    }
+    if ((threadIdx.x & 31) == 0) { g = s; flush(); }
+    v = nullptr;
+  }
+};
+
+// Viewing direction (camera -z axis in world space) and fx*fy of the map from world
+// directions to raster coordinates: the camera's right and up axes are not normalised
+// (camera.h:7-40), so c2r's scale is multiplied by the norms of w2c's first two rows.
+PSDR_D float3 view_look(const DevView& V) { return f3(-V.c2w[2], -V.c2w[6], -V.c2w[10]); }
+PSDR_D float view_fxfy(const DevView& V) {
+  const float r0 = sqrtf(V.w2c[0] * V.w2c[0] + V.w2c[1] * V.w2c[1] + V.w2c[2] * V.w2c[2]);
+  const float r1 = sqrtf(V.w2c[4] * V.w2c[4] + V.w2c[5] * V.w2c[5] + V.w2c[6] * V.w2c[6]);
+  return fabsf(V.c2r[0] * V.c2r[5]) * r0 * r1;
+}
+
+// Unbiased estimator, primary vertex: adjoint of the camera Jacobian ratio J/detach(J),
+// J = |n.(x-o)| / z^3, z = (x-o).look, scaled by phi = dot(dI, L).
+PSDR_D void cam_jacobian_adj(const DevView& V, const Surf& x, float phi, SurfAdj& ax, CamAcc& cam) {
+  const float3 rel = x.p - V.pos;
+  const float nr = dot(x.n, rel);
+  const float3 look = view_look(V);
+  const float z = dot(rel, look);
+  ax.n += rel * (phi / nr);
+  const float3 ap = x.n * (phi / nr) - look * (3.f * phi / z);
+  ax.p += ap;
+  cam.add(&V, -ap);
+}
+
+template <bool UNB>
 __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restrict__ scenes,
                                                  const DevView* __restrict__ views, Tile tile, int hot_lv0,
                                                  int hot_nlv, int emit_hot) {
   const int stride = gridDim.x * blockDim.x;
+  CamAcc cam;
   const int n32 = (tile.n + 31) & ~31;
   HotAcc hot;
   hot.lv0 = hot_lv0;
@@ -702,6 +786,7 @@ __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restric
             const float3 L = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
             has0 = true;
             ax0.area = dot(g, L) / x0.area;
+            if (UNB) cam_jacobian_adj(V, x0, dot(g, L), ax0, cam);
             add_emit(hot, Lt.grad_emit, g);
           }
         } else {
@@ -714,6 +799,7 @@ __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restric
             rng.next_float();
             SurfAdj ax = zero_adj();
             ax.area = dot(g, L) / x0.area;  // jacobi of the primary hit
+            if (UNB) cam_jacobian_adj(V, x0, dot(g, L), ax, cam);
             Surf xc = x0;
             int tric = tri0;
             float4 hc = h0;
@@ -723,8 +809,8 @@ __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restric
               const float3 adjB = mul(adjC, suffix_radiance(cb, d + 1, w.D));
               SurfAdj nextc = zero_adj();
               float3 atx = f3(0.f, 0.f, 0.f);
-              const DepthVals dv = depth_eval<true>(w, sc, xc, rng, hits + (size_t)d * w.R, d == w.D - 1, adjC, adjB,
-                                                    ax, nextc, hot, atx);
+              const DepthVals dv = depth_eval<true, UNB>(w, sc, xc, rng, hits + (size_t)d * w.R, d == w.D - 1, adjC,
+                                                         adjB, ax, nextc, hot, atx);
               const DevObj& ob = sc.objs[xc.obj];
               const int off = texel_offset(ob.color, xc.u, xc.v);
               if (d == 0) {
@@ -752,6 +838,7 @@ __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restric
     scatter_surf_warp(scp, hot, tri0, b10, b20, front0, ax0, has0);
     scatter_tex_warp(tx0, toff0, atex0, has0);
   }
+  if (UNB) cam.flush_warp();
   // flush register accumulators: warp reduce, one atomic per warp
 #pragma unroll
   for (int k = 0; k < kMaxLightVerts * 3; ++k) {
@@ -785,19 +872,47 @@ __global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restric
 struct HCube {
   const float* pmf;
   const float* cmf;
+  const double* w;    // cell masses (double)
+  const double* pre;  // inclusive prefix sums of w
   int ncells;
   int res[3];
   float unit[3];
 };
 
+// Unbiased estimator: the cell is the first whose double-precision prefix sum exceeds
+// s * total (a float CDF cannot resolve cells below 2^-24 of the mass nor place a sample
+// inside them); the caller draws a fresh uniform for the position inside the cell.
+PSDR_D int hc_cell_unb(const HCube& hc, float s, double& pmf) {
+  const double tot = hc.pre[hc.ncells - 1];
+  const double t = (double)s * tot;
+  int lo = 0, hi = hc.ncells - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (hc.pre[mid] > t) hi = mid;
+    else lo = mid + 1;
+  }
+  pmf = hc.w[lo] / tot;
+  return lo;
+}
+
 // ------------------------------------------------------------------ primary edges
+// True when triangle tri is one of the faces of the edge with vertices ev.
+PSDR_D bool tri_has_edge(const DevScene& sc, int tri, int2 ev) {
+  if (tri < 0) return false;
+  const int4 tv = __ldg(sc.tri_v + tri);
+  return (tv.x == ev.x || tv.y == ev.x || tv.z == ev.x) && (tv.x == ev.y || tv.y == ev.y || tv.z == ev.y);
+}
+
 // path_integrator.cc:188-272. PRE=true is the preprocess pass over the hypercube
 // cells (sample index = cell, the sampler stream persists across rounds); PRE=false
 // samples the cell from the preprocessed mass.
+// unb (unbiased estimator, PRE=false): one offset ray must hit a face of the edge
+// (foreground); the path of the other side (background, possibly a miss) is traced,
+// and eb.hb keeps that background hit with flag 1 (background on the +eps side) or 2.
 template <bool PRE>
 __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restrict__ scenes,
                                                    const DevView* __restrict__ views, int v, EdgeBuf eb,
-                                                   long long begin, int n, HCube hc, int round) {
+                                                   long long begin, int n, HCube hc, int round, int unb) {
   const int stride = gridDim.x * blockDim.x;
   const int n32 = (n + 31) & ~31;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
@@ -816,9 +931,17 @@ __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restr
       } else {
         rng = make_rng((unsigned long long)i + w.seed);
         s1 = rng.next_float();
-        const int cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s1, hpdf);
-        ok = hpdf > 0.f;
-        s1 = (s1 + (float)cell) * hc.unit[0];
+        if (unb) {
+          double pm;
+          const int cell = hc_cell_unb(hc, s1, pm);
+          hpdf = (float)pm;
+          ok = pm > 0.0;
+          s1 = (rng.next_float() + (float)cell) * hc.unit[0];
+        } else {
+          const int cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s1, hpdf);
+          ok = hpdf > 0.f;
+          s1 = (s1 + (float)cell) * hc.unit[0];
+        }
       }
       const int ne = *sc.n_edges;
       float ss = s1, pe;
@@ -841,23 +964,94 @@ __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restr
         ha = trace_closest(sc, V.pos, sub_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
         hb = trace_closest(sc, V.pos, add_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
       }
-      const Surf a = make_surf(sc, ha.tri, ha.b1, ha.b2, V.pos);
-      const Surf b = make_surf(sc, hb.tri, hb.b1, hb.b2, V.pos);
-      valid = valid && a.valid && b.valid && (norm(a.p - xe) < 10.f * kEps || norm(b.p - xe) < 10.f * kEps);
+      int flag;
+      HitRec hcur = ha;
+      if (!PRE && unb) {
+        const int2 ev = __ldg(sc.edge_v + e);
+        const bool na = tri_has_edge(sc, ha.tri, ev), nb = tri_has_edge(sc, hb.tri, ev);
+        const HitRec& hg = na ? hb : ha;
+        valid = valid && na != nb && hg.tri >= 0;
+        flag = valid ? (na ? 1 : 2) : 0;
+        hcur = hg;
+        eb.hb[s] = make_float4(__int_as_float(hg.tri), hg.b1, hg.b2, __int_as_float(flag));
+      } else {
+        const Surf a = make_surf(sc, ha.tri, ha.b1, ha.b2, V.pos);
+        const Surf b = make_surf(sc, hb.tri, hb.b1, hb.b2, V.pos);
+        valid = valid && a.valid && b.valid && (norm(a.p - xe) < 10.f * kEps || norm(b.p - xe) < 10.f * kEps);
+        flag = valid ? 1 : 0;
+        eb.hb[s] = make_float4(__int_as_float(hb.tri), hb.b1, hb.b2, __int_as_float(flag));
+      }
       eb.a[s] = make_float4(__int_as_float(e), ss, pdf_e, hpdf);
       eb.n[s] = make_float4(nrm.x, nrm.y, nrm.z, __int_as_float(py * V.W + px));
-      eb.hb[s] = make_float4(__int_as_float(hb.tri), hb.b1, hb.b2, __int_as_float(valid ? 1 : 0));
       w.rs[s] = rng.state;
       w.ri[s] = rng.inc;
       w.view[s] = v;
       w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
       w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-      w.cur[s] = hit4(ha);
+      w.cur[s] = hit4(hcur);
       w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
       alive = valid;
     }
     const int k = warp_append(&w.cnt[0], alive);
     if (alive) w.q0[k] = s;
+  }
+}
+
+// Unbiased silhouette term: -sgn L_bg K (d_rel . n) with d_rel = (dx_e - do) -
+// (r_e / r_bg)(dx_bg - do), K = fx fy r_e / z_e^3 / (pdf_e hc_density H W spp); the
+// background point moves with its triangle, the edge point with the edge's vertices.
+__global__ void __launch_bounds__(256) k_edge_final_unb(WF w, const DevScene* __restrict__ scenes,
+                                                        const DevView* __restrict__ views, int v, EdgeBuf eb, int n,
+                                                        float cells, int spp) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  const float3 look = view_look(V);
+  const float fxfy = view_fxfy(V);
+  float3 go = f3(0.f, 0.f, 0.f);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    if (s >= n || !V.dimage) continue;
+    const float4 hg = eb.hb[s];
+    const int flag = __float_as_int(hg.w);
+    if (flag == 0) continue;
+    const float4 a = eb.a[s], nn = eb.n[s];
+    const float* gp = V.dimage + 3 * (size_t)__float_as_int(nn.w);
+    const float3 L = xyz(w.L[s]);
+    const float phi = gp[0] * L.x + gp[1] * L.y + gp[2] * L.z;
+    if (!(phi != 0.f) || !isfinite(phi)) continue;
+    const int e = __float_as_int(a.x);
+    const float ss = a.y;
+    const float4 E0 = __ldg(sc.edge + 4 * (size_t)e), E1 = __ldg(sc.edge + 4 * (size_t)e + 1);
+    const float3 xe = add_rn(xyz(E0), scale_rn(sub_rn(xyz(E1), xyz(E0)), ss));
+    const float3 re3 = xe - V.pos;
+    const float re = norm(re3), z = dot(re3, look);
+    const int tri = __float_as_int(hg.x);
+    const Surf g = make_surf(sc, tri, hg.y, hg.z, V.pos);
+    const float ratio = re / sqrtf(g.sqd);
+    const float K = fxfy * re / (z * z * z) / (a.z * a.w * cells * (float)V.H * (float)V.W * (float)spp);
+    const float3 av = xyz(nn) * (-(flag == 1 ? 1.f : -1.f) * phi * K);
+    if (!finite3(av)) continue;
+    if (sc.grad_verts) {
+      const int2 ev = __ldg(sc.edge_v + e);
+      atomic_add3(sc.grad_verts + 3 * (size_t)ev.x, av * (1.f - ss));
+      atomic_add3(sc.grad_verts + 3 * (size_t)ev.y, av * ss);
+      const int4 tv = __ldg(sc.tri_v + tri);
+      const float3 ag = av * (-ratio);
+      atomic_add3(sc.grad_verts + 3 * (size_t)tv.x, ag * (1.f - hg.y - hg.z));
+      atomic_add3(sc.grad_verts + 3 * (size_t)tv.y, ag * hg.y);
+      atomic_add3(sc.grad_verts + 3 * (size_t)tv.z, ag * hg.z);
+    }
+    go -= av * (1.f - ratio);
+  }
+  if (V.grad_pos) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      go.x += __shfl_xor_sync(0xffffffffu, go.x, o);
+      go.y += __shfl_xor_sync(0xffffffffu, go.y, o);
+      go.z += __shfl_xor_sync(0xffffffffu, go.z, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (go.x != 0.f || go.y != 0.f || go.z != 0.f)) atomic_add3(V.grad_pos, go);
   }
 }
 
@@ -937,9 +1131,180 @@ __global__ void __launch_bounds__(256) k_edge_final(WF w, const DevScene* __rest
   }
 }
 
+// ------------------------------------------------------------------ pixel borders
+// Unbiased estimator: material crossing the pixel borders. The border segments are the
+// (W+1) x H vertical and W x (H+1) horizontal unit segments of the pixel grid; segment q
+// contributes (dI[hi] - dI[lo]) . Int L v dl, L the radiance seen through the border
+// point and v the raster velocity of its primary vertex across the segment (material
+// flows into pixel hi and out of pixel lo; outside the image dI = 0). Segments are
+// importance-sampled by m_q = |dI[hi] - dI[lo]|_1 (zero where the term is zero) with
+// stratified inversion of the double-precision CDF: sample i of N takes
+// u = (i + xi) / N, its segment is the first with prefix > u * total and its position
+// along the segment the remainder, so every segment gets N m_q / total samples spread
+// evenly along it.
+PSDR_D void border_pixels(const DevView& V, long long q, bool& vert, int& k, int& j, int& lo, int& hi) {
+  const long long nv = (long long)(V.W + 1) * V.H;
+  vert = q < nv;
+  lo = hi = -1;
+  if (vert) {
+    k = (int)(q % (V.W + 1));
+    j = (int)(q / (V.W + 1));
+    if (k >= 1) lo = j * V.W + k - 1;
+    if (k < V.W) hi = j * V.W + k;
+  } else {
+    const long long r = q - nv;
+    k = (int)(r % V.W);
+    j = (int)(r / V.W);
+    if (j >= 1) lo = (j - 1) * V.W + k;
+    if (j < V.H) hi = j * V.W + k;
+  }
+}
+
+PSDR_D float3 dimage_at(const DevView& V, int p) {
+  if (p < 0) return f3(0.f, 0.f, 0.f);
+  const float* g = V.dimage + 3 * (size_t)p;
+  return f3(g[0], g[1], g[2]);
+}
+
+__global__ void k_border_mass(const DevView* __restrict__ views, int v, float* __restrict__ mass, long long S) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= S) return;
+  const DevView& V = views[v];
+  bool vert;
+  int k, j, lo, hi;
+  border_pixels(V, q, vert, k, j, lo, hi);
+  const float3 d = dimage_at(V, hi) - dimage_at(V, lo);
+  mass[q] = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+}
+
+// Segment and position of border sample i of N (explicitly rounded double arithmetic,
+// identical in the oracle).
+PSDR_D long long border_locate(const double* __restrict__ w, const double* __restrict__ pre, long long S,
+                               long long i, long long N, float xi, float& t, double& pmf) {
+  const double tot = pre[S - 1];
+  const double u = __ddiv_rn(__dadd_rn((double)i, (double)xi), (double)N);
+  const double tt = __dmul_rn(u, tot);
+  long long lo = 0, hi = S - 1;
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (pre[mid] > tt) hi = mid;
+    else lo = mid + 1;
+  }
+  const double base = lo > 0 ? pre[lo - 1] : 0.0;
+  double r = __ddiv_rn(__dsub_rn(tt, base), w[lo]);
+  r = r < 0.0 ? 0.0 : r;
+  t = fminf((float)r, 0.99999994f);
+  pmf = __ddiv_rn(w[lo], tot);
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_border_init(WF w, const DevScene* __restrict__ scenes,
+                                                     const DevView* __restrict__ views, int v, EdgeBuf eb,
+                                                     const double* __restrict__ mw, const double* __restrict__ mpre,
+                                                     long long S, long long begin, int n, long long N) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool alive = false;
+    if (s < n) {
+      const long long i = begin + s;
+      const DevView& V = views[v];
+      const DevScene& sc = scenes[V.scene];
+      Rng rng = make_rng((unsigned long long)i + w.seed);
+      const float xi = rng.next_float();
+      float t;
+      double pmf;
+      const long long q = border_locate(mw, mpre, S, i, N, xi, t, pmf);
+      bool vert;
+      int k, j, lo, hi;
+      border_pixels(V, q, vert, k, j, lo, hi);
+      const float3 fp = vert ? f3((float)k, t + (float)j, 1.0f) : f3(t + (float)k, (float)j, 1.0f);
+      float3 pc;
+      xform_pos(V.r2c, fp, pc);
+      const float3 d = normalize(xform_dir(V.c2w, pc));
+      const HitRec h = trace_closest(sc, V.pos, d, kTmin, INFINITY);
+      w.rs[s] = rng.state;
+      w.ri[s] = rng.inc;
+      w.view[s] = v;
+      w.pix[s] = -1;
+      w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
+      w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      w.cur[s] = hit4(h);
+      w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      eb.hb[s] = hit4(h);
+      eb.a[s] = make_float4(__int_as_float((int)q), t, (float)pmf, 0.f);
+      alive = h.tri >= 0 && pmf > 0.0;
+    }
+    const int k = warp_append(&w.cnt[0], alive);
+    if (alive) w.q0[k] = s;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_border_final(WF w, const DevScene* __restrict__ scenes,
+                                                      const DevView* __restrict__ views, int v, EdgeBuf eb, int n,
+                                                      long long N) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  float3 go = f3(0.f, 0.f, 0.f);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    if (s >= n || !V.dimage) continue;
+    const float4 h = eb.hb[s];
+    const int tri = __float_as_int(h.x);
+    if (tri < 0) continue;
+    const float4 a = eb.a[s];
+    if (!(a.z > 0.f)) continue;
+    bool vert;
+    int k, j, lo, hi;
+    border_pixels(V, __float_as_int(a.x), vert, k, j, lo, hi);
+    const float3 L = xyz(w.L[s]);
+    const float3 dg = dimage_at(V, hi) - dimage_at(V, lo);
+    const float wgt = dot(dg, L) / ((float)N * a.z);
+    if (!(wgt != 0.f) || !isfinite(wgt)) continue;
+    // raster coordinate c (x for vertical borders, y for horizontal) of the material
+    // point and its gradient w.r.t. the point
+    const Surf x = make_surf(sc, tri, h.y, h.z, V.pos);
+    float3 pc;
+    xform_pos(V.w2c, x.p, pc);
+    const float* m = V.c2r;
+    const int c = vert ? 0 : 1;
+    const float wden = m[12] * pc.x + m[13] * pc.y + m[14] * pc.z + m[15];
+    const float u = (m[4 * c] * pc.x + m[4 * c + 1] * pc.y + m[4 * c + 2] * pc.z + m[4 * c + 3]) / wden;
+    const float3 gpc = f3(m[4 * c] - u * m[12], m[4 * c + 1] - u * m[13], m[4 * c + 2] - u * m[14]) / wden;
+    const float* r = V.w2c;
+    const float3 gx = f3(r[0] * gpc.x + r[4] * gpc.y + r[8] * gpc.z, r[1] * gpc.x + r[5] * gpc.y + r[9] * gpc.z,
+                         r[2] * gpc.x + r[6] * gpc.y + r[10] * gpc.z);
+    const float3 ag = gx * wgt;
+    if (!finite3(ag)) continue;
+    if (sc.grad_verts) {
+      const int4 tv = __ldg(sc.tri_v + tri);
+      atomic_add3(sc.grad_verts + 3 * (size_t)tv.x, ag * (1.f - h.y - h.z));
+      atomic_add3(sc.grad_verts + 3 * (size_t)tv.y, ag * h.y);
+      atomic_add3(sc.grad_verts + 3 * (size_t)tv.z, ag * h.z);
+    }
+    go -= ag;
+  }
+  if (V.grad_pos) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      go.x += __shfl_xor_sync(0xffffffffu, go.x, o);
+      go.y += __shfl_xor_sync(0xffffffffu, go.y, o);
+      go.z += __shfl_xor_sync(0xffffffffu, go.z, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (go.x != 0.f || go.y != 0.f || go.z != 0.f)) atomic_add3(V.grad_pos, go);
+  }
+}
+
 // ------------------------------------------------------------------ direct edges
 // path_integrator.cc:274-353 and the boundary_term / hit_triangle adjoint (:11-78).
-template <bool PRE>
+// UNB (unbiased estimator, PRE=false): the same samples and visibility tests; the edge
+// point x_b, light point y and receiver x_d lie on one line and the shadow boundary
+// moves over the receiver at d_eff = dx_b - dx_d / lam - dy (1 - 1/lam),
+// lam = |x_d - y| / |x_b - y|. Per sample: -f_r L_e |n_y.w| / |x_b - y|^2 J_cam(x_d)
+// (d_eff . (w x e)) / (pdf_e pdf_y hc_density H W spp), e oriented by the edge's outward
+// vector so that the occluding faces lie on the -(w x e) side.
+template <bool PRE, bool UNB = false>
 __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict__ scenes,
                                                 const DevView* __restrict__ views, int v, long long n, HCube hc,
                                                 int round, float* mass, int spp) {
@@ -965,7 +1330,15 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     } else {
       rng = make_rng((unsigned long long)i + w.seed);
       s3[0] = rng.next_float(); s3[1] = rng.next_float(); s3[2] = rng.next_float();
-      const int cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s3[2], hpdf);
+      int cell;
+      if (UNB) {
+        double pm;
+        cell = hc_cell_unb(hc, s3[2], pm);
+        hpdf = (float)pm;
+        s3[2] = rng.next_float();
+      } else {
+        cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s3[2], hpdf);
+      }
       if (!(hpdf > 0.f)) continue;
       const int r12 = hc.res[1] * hc.res[2];
       const int c0 = cell / r12, rem = cell - c0 * r12;
@@ -1002,6 +1375,39 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     const HitRec h2 = trace_closest(sc, V.pos, cd, kTmin, INFINITY);
     const Surf i2 = make_surf(sc, h2.tri, h2.b1, h2.b2, V.pos);
     if (!(i2.valid && !i2.is_light && sqnorm(i2.p - d0.p) < kEps)) continue;
+    if (UNB && !PRE) {
+      if (!V.dimage || !sc.grad_verts) continue;
+      float3 ev = normalize(p1 - p0);
+      if (dot(cross(dir, ev), out) < 0.f) ev = -ev;
+      const float3 nsv = cross(dir, ev);
+      const float dby = norm(xb - ls.y), lam = norm(d0.p - ls.y) / dby;
+      const float cos_y = fabsf(dot(s0.n, dir));
+      const float3 rel = d0.p - V.pos;
+      const float z = dot(rel, view_look(V));
+      const float Jc = view_fxfy(V) * fabsf(dot(d0.n, rel)) / (z * z * z);
+      const float k = cos_y / (dby * dby) * Jc / (pdf_e * ls.pdf * (float)V.H * (float)V.W);
+      const DevLight& Lt = sc.lights[s0.light];
+      const DevObj& ob = sc.objs[d0.obj];
+      const float3 fr = tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi;
+      const float* gp = V.dimage + 3 * ((size_t)py * V.W + px);
+      const float phi = gp[0] * fr.x * Lt.emit[0] + gp[1] * fr.y * Lt.emit[1] + gp[2] * fr.z * Lt.emit[2];
+      const float3 a = nsv * (-phi * k / (hpdf * (float)hc.ncells * (float)spp));
+      if (!finite3(a)) continue;
+      const int2 evv = __ldg(sc.edge_v + e);
+      atomic_add3(sc.grad_verts + 3 * (size_t)evv.x, a * (1.f - sx));
+      atomic_add3(sc.grad_verts + 3 * (size_t)evv.y, a * sx);
+      const int4 td = __ldg(sc.tri_v + hd.tri);
+      const float3 ad = a * (-1.f / lam);
+      atomic_add3(sc.grad_verts + 3 * (size_t)td.x, ad * (1.f - hd.b1 - hd.b2));
+      atomic_add3(sc.grad_verts + 3 * (size_t)td.y, ad * hd.b1);
+      atomic_add3(sc.grad_verts + 3 * (size_t)td.z, ad * hd.b2);
+      const int4 tl = __ldg(sc.tri_v + ls.tri);
+      const float3 al = a * (1.f / lam - 1.f);
+      atomic_add3(sc.grad_verts + 3 * (size_t)tl.x, al * (1.f - ls.su - ls.sv));
+      atomic_add3(sc.grad_verts + 3 * (size_t)tl.y, al * ls.su);
+      atomic_add3(sc.grad_verts + 3 * (size_t)tl.z, al * ls.sv);
+      continue;
+    }
     const float pdf_xw = s0.sqd * pdf_e * ls.pdf / dot(s0.n, dir);
     // boundary_term (detached quantities)
     const float3 xs = s0.p, xd = d0.p, ns = s0.n, nd = d0.n;
@@ -1059,6 +1465,14 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
 __global__ void k_mass_cdf(const float* __restrict__ mass, int n, double* __restrict__ w) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) w[i] = (double)mass[i];
+}
+// Unbiased estimator: add a uniform share (5% of the mean mass) to every cell.
+__global__ void k_mass_floor(float* __restrict__ mass, const double* __restrict__ pre, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double tot = pre[n - 1];
+  const float f = tot > 0.0 ? (float)(0.05 * tot / (double)n) : 1.0f;
+  mass[i] = mass[i] + f;
 }
 __global__ void k_mass_finalize(const double* __restrict__ w, const double* __restrict__ pre, int n,
                                 float* __restrict__ pmf, float* __restrict__ cmf) {
@@ -1264,6 +1678,16 @@ int choose_cap(const psdr_config& cfg, const std::vector<DevView>& views, bool b
 
 }  // namespace psdr
 
+// Mass / prefix-sum buffers of the hypercube cells and pixel-border segments.
+void psdr_workspace::ensure_mass(long long n, cudaStream_t st) {
+  if (n <= mass_cap) return;
+  mass_cap = n;
+  mass.alloc(4 * (size_t)n, st);
+  mass_d.alloc(8 * (size_t)n, st);
+  mass_pre.alloc(8 * (size_t)n, st);
+  scan_tmp.alloc(8 * (psdr::scan_tmp_doubles((int)n) + 64), st);
+}
+
 void psdr_workspace::ensure(int c, int r, int d, int nv, int rec_needed, cudaStream_t st) {
   using namespace psdr;
   stream = st;
@@ -1278,10 +1702,9 @@ void psdr_workspace::ensure(int c, int r, int d, int nv, int rec_needed, cudaStr
     cnt.alloc(sizeof(int) * 2 * (kMaxDepth + 2), st);
     ro.alloc(16 * n * R, st); rd.alloc(16 * n * R, st); ra.alloc(16 * n * R, st); hit.alloc(16 * n * R, st);
     eb_a.alloc(16 * n, st); eb_n.alloc(16 * n, st); eb_hb.alloc(16 * n, st); eb_La.alloc(16 * n, st);
-    mass.alloc(4 * n, st); mass_d.alloc(8 * n, st); mass_pre.alloc(8 * n, st);
     hc_pmf.alloc(4 * n, st); hc_cmf.alloc(4 * n, st);
-    scan_tmp.alloc(8 * (scan_tmp_doubles((int)n) + 64), st);
   }
+  ensure_mass(cap, st);
   if (rec_needed) rec.alloc(16 * (size_t)cap * (1 + (size_t)D * R + 2 * (size_t)D), st);
   if (nv > nviews_cap) {
     nviews_cap = nv;
@@ -1310,7 +1733,9 @@ void set_wf(WF& w, const psdr_config& cfg, int nviews, int nB_override, int ligh
   w.R = w.nL + w.nB + 1;
   w.light_vis = light_vis;
   w.nviews = nviews;
-  w.seed = cfg.seed;
+  // seed s offsets every sample stream by s * 2654435761 (mod 2^32, the width of the
+  // stream index): jobs of different seeds draw from disjoint stream ranges
+  w.seed = cfg.seed * 2654435761ull;
   w.rec_stride = 1 + w.D * w.R + 2 * w.D;  // primary hit, hits per depth, (C, beta) per depth
 }
 
@@ -1345,8 +1770,8 @@ void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views
 static void edge_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb, long long begin,
                        int n, const HCube& hc, int round, bool pre, float* mass, int spp, cudaStream_t st) {
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
-  if (pre) k_edge_init<true><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round);
-  else k_edge_init<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round);
+  if (pre) k_edge_init<true><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round, 0);
+  else k_edge_init<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round, 0);
   PSDR_LAUNCHED(1);
   depth_loop(w, scenes, vd, MODE_FWD, st);
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
@@ -1359,9 +1784,49 @@ static void edge_phase(WF w, const DevScene* scenes, const DevView* vd, int v, c
   PSDR_CUDA(cudaGetLastError());
 }
 
-static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, cudaStream_t st) {
+// Unbiased silhouette samples: one path per sample (the background side).
+static void edge_phase_unb(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
+                           long long begin, int n, const HCube& hc, int spp, cudaStream_t st) {
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  k_edge_init<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, 0, 1);
+  PSDR_LAUNCHED(2);
+  depth_loop(w, scenes, vd, MODE_FWD, st);
+  k_edge_final_unb<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, n, (float)hc.ncells, spp);
+  PSDR_CUDA(cudaGetLastError());
+}
+
+// Pixel-border samples [begin, begin + n) of the N of view v (segment masses in w/pre).
+static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
+                         const double* mw, const double* mpre, long long S, long long begin, int n, long long N,
+                         cudaStream_t st) {
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  k_border_init<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, mw, mpre, S, begin, n, N);
+  PSDR_LAUNCHED(2);
+  depth_loop(w, scenes, vd, MODE_FWD, st);
+  k_border_final<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, n, N);
+  PSDR_CUDA(cudaGetLastError());
+}
+
+long long border_segments(const DevView& V) {
+  return (long long)(V.W + 1) * V.H + (long long)V.W * (V.H + 1);
+}
+
+void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector<DevView>& views, cudaStream_t st) {
+  if (cfg.estimator != PSDR_EST_UNBIASED) return;
+  long long s = 0;
+  for (const DevView& v : views) s = std::max(s, border_segments(v));
+  ws->ensure_mass(s, st);
+}
+
+static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, bool floor, cudaStream_t st) {
   HCube hc;
   const int b = (ncells + 255) / 256;
+  if (floor) {
+    k_mass_cdf<<<b, 256, 0, st>>>(ws->mass.as<float>(), ncells, ws->mass_d.as<double>());
+    PSDR_LAUNCHED(5);
+    inclusive_scan_double(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), ncells, ws->scan_tmp.as<double>(), st);
+    k_mass_floor<<<b, 256, 0, st>>>(ws->mass.as<float>(), ws->mass_pre.as<double>(), ncells);
+  }
   k_mass_cdf<<<b, 256, 0, st>>>(ws->mass.as<float>(), ncells, ws->mass_d.as<double>());
   PSDR_LAUNCHED(5);
   inclusive_scan_double(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), ncells, ws->scan_tmp.as<double>(), st);
@@ -1370,6 +1835,8 @@ static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, 
   PSDR_CUDA(cudaGetLastError());
   hc.pmf = ws->hc_pmf.as<float>();
   hc.cmf = ws->hc_cmf.as<float>();
+  hc.w = ws->mass_d.as<double>();
+  hc.pre = ws->mass_pre.as<double>();
   hc.ncells = ncells;
   for (int k = 0; k < 3; ++k) {
     hc.res[k] = k < N ? res[k] : 1;
@@ -1389,6 +1856,7 @@ void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& view
   const int cap = choose_cap(cfg, views, true);
   const int Rmax = cfg.mis_light_samples + std::max(cfg.mis_bsdf_samples, 1) + 1;
   ws->ensure(cap, Rmax, cfg.max_bounce, (int)views.size(), 1, st);
+  ensure_border(ws, cfg, views, st);
   upload_views(ws, views, st);
   backward_launch(scenes_dev, views, cfg, cap, ws, gi, st);
 }
@@ -1397,7 +1865,8 @@ void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& view
 void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg,
                      int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
   const DevView* vd = ws->views.as<DevView>();
-  const int terms = cfg.terms ? cfg.terms : 7;
+  const bool unb = cfg.estimator == PSDR_EST_UNBIASED;
+  const int terms = cfg.terms ? cfg.terms : (unb ? 15 : 7);
   // ---- interior
   if (terms & 1) {
     WF w = ws->wf;
@@ -1405,7 +1874,12 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
     set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
     for (const Tile& t : plan_tiles(views, cap)) {
       run_tile(w, scenes_dev, vd, t, MODE_REPLAY, st);
-      k_adjoint<<<grid_for(t.n, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+      if (cfg.estimator == PSDR_EST_UNBIASED)
+        k_adjoint<true><<<grid_for(t.n, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv,
+                                                                gi.emit_hot);
+      else
+        k_adjoint<false><<<grid_for(t.n, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv,
+                                                                 gi.emit_hot);
       PSDR_LAUNCHED(1);
     }
     PSDR_CUDA(cudaGetLastError());
@@ -1414,6 +1888,10 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
   WF w = ws->wf;
   w.cap = ws->cap;
   set_wf(w, cfg, (int)views.size(), 1, 0);
+  // paths of the unbiased boundary samples carry the interior estimator's radiance
+  WF wi = ws->wf;
+  wi.cap = ws->cap;
+  set_wf(wi, cfg, (int)views.size(), -1, cfg.enable_light_visable);
   EdgeBuf eb{ws->eb_a.as<float4>(), ws->eb_n.as<float4>(), ws->eb_hb.as<float4>(), ws->eb_La.as<float4>(), nullptr};
   for (int v = 0; v < (int)views.size(); ++v) {
     const DevView& V = views[v];
@@ -1426,11 +1904,13 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       for (int r = 0; r < cfg.primary_edge_preprocess_rounds; ++r)
         edge_phase(w, scenes_dev, vd, v, eb, 0, cells, none, r, true, ws->mass.as<float>(), 1, st);
       const int res[1] = {cells};
-      const HCube hc = build_hcube(ws, cells, res, 1, st);
+      const HCube hc = build_hcube(ws, cells, res, 1, unb, st);
       const long long N = (long long)V.H * V.W * cfg.spp_primary_edge;
-      for (long long b = 0; b < N; b += cap)
-        edge_phase(w, scenes_dev, vd, v, eb, b, (int)std::min<long long>(cap, N - b), hc, 0, false, nullptr,
-                   cfg.spp_primary_edge, st);
+      for (long long b = 0; b < N; b += cap) {
+        const int nb = (int)std::min<long long>(cap, N - b);
+        if (unb) edge_phase_unb(wi, scenes_dev, vd, v, eb, b, nb, hc, cfg.spp_primary_edge, st);
+        else edge_phase(w, scenes_dev, vd, v, eb, b, nb, hc, 0, false, nullptr, cfg.spp_primary_edge, st);
+      }
     }
     // direct edges
     if (terms & 4) {
@@ -1443,11 +1923,29 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r)
         k_direct<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
                                                                  ws->mass.as<float>(), 1);
-      const HCube hc = build_hcube(ws, cells, r3, 3, st);
+      const HCube hc = build_hcube(ws, cells, r3, 3, unb, st);
       const long long N = (long long)V.H * V.W * cfg.spp_secondary_edge;
-      k_direct<false><<<grid_for(N, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, N, hc, 0, nullptr,
-                                                            cfg.spp_secondary_edge);
+      if (unb)
+        k_direct<false, true><<<grid_for(N, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, N, hc, 0, nullptr,
+                                                                    cfg.spp_secondary_edge);
+      else
+        k_direct<false><<<grid_for(N, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, N, hc, 0, nullptr,
+                                                              cfg.spp_secondary_edge);
       PSDR_CUDA(cudaGetLastError());
+    }
+    // pixel borders (unbiased estimator): segment masses, their prefix sums, samples
+    if (unb && (terms & 8) && cfg.spp_pixel_boundary > 0 && V.dimage) {
+      const long long S = border_segments(V);
+      const long long N = S * cfg.spp_pixel_boundary;
+      const int b = (int)((S + 255) / 256);
+      k_border_mass<<<b, 256, 0, st>>>(vd, v, ws->mass.as<float>(), S);
+      k_mass_cdf<<<b, 256, 0, st>>>(ws->mass.as<float>(), (int)S, ws->mass_d.as<double>());
+      PSDR_LAUNCHED(2);
+      inclusive_scan_double(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), (int)S, ws->scan_tmp.as<double>(),
+                            st);
+      for (long long b0 = 0; b0 < N; b0 += cap)
+        border_phase(wi, scenes_dev, vd, v, eb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), S, b0,
+                     (int)std::min<long long>(cap, N - b0), N, st);
     }
   }
 }

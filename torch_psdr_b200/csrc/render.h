@@ -74,10 +74,12 @@ struct psdr_workspace {
   psdr::DBuf rs, ri, view, pix, T, L, cur, org, q0, q1, qs, cnt, ro, rd, ra, hit, rec;
   psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
   psdr::DBuf campos_acc;
+  long long mass_cap = 0;
   cudaStream_t stream = nullptr;
   std::vector<psdr::DevView> h_views;
   psdr::WF wf{};
   void ensure(int cap, int R, int D, int nviews, int rec_needed, cudaStream_t st);
+  void ensure_mass(long long n, cudaStream_t st);
 };
 
 namespace psdr {
@@ -121,4 +123,6 @@ void check_config(const psdr_config* c);
 void check_cameras(const psdr_camera_desc* cams, int n);
 void scene_build_geometry(psdr_scene* s, cudaStream_t st);
 std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap);
+long long border_segments(const DevView& V);
+void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector<DevView>& views, cudaStream_t st);
 }  // namespace psdr
