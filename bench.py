@@ -7,12 +7,20 @@ seed 0) on a 10x10 ground quad under a 1x1 area light (20,484 triangles in all);
 512x512, 32 spp interior, 4 spp primary-edge and 4 spp secondary-edge samples,
 max_bounce 3, one light and one BSDF MIS sample. One step = rebuild the scene from
 the (translated) vertices, renderD forward, L2 loss against a fixed target, and
-the full backward (interior path replay + both edge-sampling terms).
+the full backward (interior path replay + every boundary term of the estimator).
+The default estimator is the unbiased one (its gradient matches central finite
+differences; 4 pixel-border samples per border segment); --estimator reference
+reproduces the reference's renderD formulas.
 
 Metric: interior path samples (512*512*32 per view) per second of fwd+bwd.
-`value` is device time with inputs resident in HBM; `e2e` adds the host->device
-copies of the vertices and texture from pinned memory and the device->host read
-of the vertex gradient and the loss, through the public Python API.
+`value` is device time with inputs resident in HBM for the batched step (persistent
+scene, rebuild + forward + backward replayed from CUDA graphs); config.other_mode is
+the same step through a new Scene and per-view launch sequences. `e2e` adds the
+host->device copies of the vertices and texture from pinned memory and the
+device->host read of the vertex gradient and the loss, through the public Python
+API. `grad_check` compares the translation gradient of sum(w * image) for a smooth
+weight image w at the benchmark's sample counts with central differences
+(4096-spp renders, common random numbers), outside the timed region.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 Under torchrun every rank renders its own replica (weak scaling, replicas only).
@@ -41,7 +49,8 @@ SPP = 32
 CFG = dict(spp_interior=SPP, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=3, mis_light_samples=1,
            mis_bsdf_samples=1)
 WORKLOAD = ("geometry gradient: level-5 icosphere 20,480 tris (+ground, light = 20,484), 512x512, 32 spp interior "
-            "+ 4 spp primary edges + 4 spp secondary edges, depth 3, L2 loss, fwd+bwd incl. scene rebuild")
+            "+ 4 spp primary edges + 4 spp secondary edges (+ 4 per pixel-border segment, unbiased estimator), "
+            "depth 3, L2 loss, fwd+bwd incl. scene rebuild")
 TRACE_BYTES_PER_RAY = 40  # ray read 24 B + hit write 16 B (per-ray share of the trace kernel)
 STEP_BYTES_PER_SAMPLE = 2628  # fwd+bwd algorithmic bytes per path sample at depth 3
 
@@ -149,6 +158,43 @@ class Clocks:
                 "samples": len(sm)}
 
 
+# ---------------------------------------------------------------- gradient check
+def smooth_weights(torch, dev):
+    yy, xx = torch.meshgrid(torch.arange(H, device=dev) + 0.5, torch.arange(W, device=dev) + 0.5, indexing="ij")
+    return torch.stack([torch.sin(2 * math.pi * xx / W * 1.3 + c) * torch.cos(2 * math.pi * yy / H * 0.7) + 0.3
+                        for c in range(3)], -1).float().contiguous()
+
+
+def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=4096):
+    """Translation gradient of Phi = sum(w * image) for a smooth weight image w, from the
+    estimator at the benchmark's sample counts, against central differences of Phi from
+    fd_spp-spp renders (same sample streams at +-h). The benchmark's own L2 loss is not
+    used here: its image gradient is dominated by texel-scale residuals, which makes its
+    finite differences ill-conditioned (they move by tens of percent with h and spp)."""
+    from torch_psdr_b200 import _lib as L
+    w = smooth_weights(torch, dev)
+    t = torch.zeros(3, device=dev, requires_grad=True)
+    img = integ.renderD(build_scene(base + t, tex))[0]
+    img.backward(w)
+    ad = t.grad.double().cpu().numpy()
+    fd_integ = dr.PathIntegrator(**dict(CFG, spp_interior=fd_spp))
+    wd = w.double()
+    fd = []
+    with torch.no_grad():
+        for k in range(3):
+            e = torch.zeros(3, device=dev)
+            e[k] = h
+            lp = float((fd_integ.renderC(build_scene(base + e, tex))[0].double() * wd).sum())
+            lm = float((fd_integ.renderC(build_scene(base - e, tex))[0].double() * wd).sum())
+            fd.append((lp - lm) / (2 * h))
+    fd = np.array(fd)
+    return {"rel_l2_vs_fd": float(np.linalg.norm(ad - fd) / np.linalg.norm(fd)), "ad": ad.tolist(), "fd": fd.tolist(),
+            "functional": "sum(w * image), w = sin(2.6 pi x/W + c) cos(1.4 pi y/H) + 0.3 per channel c",
+            "parameter": "translation of the icosphere",
+            "estimator": "unbiased" if integ.cfg.estimator == L.EST_UNBIASED else "reference",
+            "fd_step": h, "fd_spp": fd_spp}
+
+
 # ---------------------------------------------------------------- B200 arm
 def run_b200(args):
     import torch
@@ -182,7 +228,7 @@ def run_b200(args):
     gV, gF, gT = tens(ground.vertices), tens(ground.faces, torch.int32), tens(ground.texture)
     lV, lF, lE = tens(light.vertices), tens(light.faces, torch.int32), tens(light.emit)
     cam = dr.PerspectiveCamera(tens(c.look_from), tens(c.look_at), tens(c.up), tens([c.vfov]), H, W)
-    integ = dr.PathIntegrator(**CFG)
+    integ = dr.PathIntegrator(estimator=args.estimator, **CFG)
 
     def build_scene(verts, texture):
         return dr.Scene([cam], [dr.Mesh(verts, uvs, faces, uvi, dr.DiffuseMaterial(texture)),
@@ -224,44 +270,49 @@ def run_b200(args):
         loss.backward()
         return loss
 
-    step = step_batched if args.mode == "batched" else step_plain
-
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    L.check(lib.psdr_profile_enable(1), "profile")  # before warm-up: graphs record their trace events
-    for _ in range(args.warmup):
-        step(base, tex)
-    torch.cuda.synchronize()
-
-    # ---------------- device-resident timing
     stream = torch.cuda.current_stream()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    L.check(lib.psdr_profile_reset(), "profile")
-    clocks = Clocks(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    for k in range(args.steps):
-        flush.fill_(float(k))  # evicts L2 between steps, outside the timed events
-        ev[k][0].record(stream)
-        step(base, tex)
-        ev[k][1].record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(step_ms)
-    prof = (ctypes.c_int64 * 3)()
-    trace_ms = ctypes.c_double()
-    L.check(lib.psdr_profile_read(prof, ctypes.byref(trace_ms)), "profile")
-    launches, trace_launches, rays = int(prof[0]), int(prof[1]), int(prof[2])
-    L.check(lib.psdr_profile_enable(0), "profile")
-    if dist:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+
+    def timed(stepfn, with_clocks):
+        """Device time (ms, summed over the timed steps, max over ranks) plus the
+        in-library profile of the timed region."""
+        L.check(lib.psdr_profile_enable(1), "profile")  # before warm-up: graphs record their trace events
+        for _ in range(args.warmup):
+            stepfn(base, tex)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        L.check(lib.psdr_profile_reset(), "profile")
+        clocks = Clocks(local) if with_clocks else None
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(float(k))  # evicts L2 between steps, outside the timed events
+            ev[k][0].record(stream)
+            stepfn(base, tex)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        clk = clocks.stop() if clocks else None
+        total = sum(a.elapsed_time(b) for a, b in ev)
+        prof = (ctypes.c_int64 * 3)()
+        tms = ctypes.c_double()
+        L.check(lib.psdr_profile_read(prof, ctypes.byref(tms)), "profile")
+        L.check(lib.psdr_profile_enable(0), "profile")
+        if dist:
+            tt = torch.tensor([total], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            total = float(tt.item())
+        return total, (int(prof[0]), int(prof[1]), int(prof[2])), tms.value, clk
+
     samples = H * W * SPP
+    step = step_batched if args.mode == "batched" else step_plain
+    other = step_plain if args.mode == "batched" else step_batched
+    total_ms, (launches, trace_launches, rays), trace_ms_v, clk = timed(step, True)
     value = world * samples * args.steps / (total_ms / 1e3)
+    other_ms, _, _, _ = timed(other, False)
+    other_value = world * samples * args.steps / (other_ms / 1e3)
 
     # ---------------- end-to-end through the public API with host buffers
     h_base = torch.tensor(sphere.vertices, dtype=torch.float32).pin_memory()
@@ -300,7 +351,7 @@ def run_b200(args):
     d2h = h_grad.numel() * 4 + 4
 
     peak, peak_kind = peaks()
-    trace_avg_ms = trace_ms.value / max(1, trace_launches)
+    trace_avg_ms = trace_ms_v / max(1, trace_launches)
     achieved = (rays / max(1, trace_launches)) * TRACE_BYTES_PER_RAY / (trace_avg_ms / 1e3) / 1e9
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -308,17 +359,22 @@ def run_b200(args):
             "config": {"workload": WORKLOAD,
                        "mode": ("batched (persistent scene, geometry rebuild + fwd and bwd replayed from CUDA graphs)"
                                 if args.mode == "batched" else "plain (new Scene per step, per-view launch sequences)"),
+                       "estimator": args.estimator,
+                       "other_mode": {"mode": "plain" if args.mode == "batched" else "batched",
+                                      "value": other_value, "ms_per_step": other_ms / args.steps},
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": "k_trace (LBVH closest hit)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": None,
                          "bytes_per_unit": f"{TRACE_BYTES_PER_RAY} B/ray", "rays_per_launch": rays / max(1, trace_launches),
-                         "trace_share_of_step": trace_ms.value / max(total_ms / world if world == 1 else total_ms, 1e-9),
+                         "trace_share_of_step": trace_ms_v / max(total_ms, 1e-9),
                          "step_algorithmic_gbs": samples * STEP_BYTES_PER_SAMPLE / (total_ms / args.steps / 1e3) / 1e9},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clk,
             "rays_per_s": rays / (total_ms / 1e3)}
+    if rank == 0 and world == 1 and not args.no_grad_check:
+        line["grad_check"] = grad_check(torch, dr, integ, build_scene, base, tex, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_rate(spec, seconds_budget=20.0)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
@@ -336,6 +392,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference", "ours"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad-check", action="store_true")
+    ap.add_argument("--estimator", default="unbiased", choices=["unbiased", "reference"])
     ap.add_argument("--mode", default="batched", choices=["batched", "plain"],
                     help="batched: persistent scene + graph replay; plain: new Scene + per-view launches each step")
     ap.add_argument("--size", type=int, default=512, help="image size (512 = the benchmark workload)")

@@ -231,6 +231,8 @@ inline V3<S> material_point(const Scene<S>& sc, const Its<T>& h) {
   return t.p0 + (t.p1 - t.p0) * S(h.b1) + (t.p2 - t.p0) * S(h.b2);
 }
 
+constexpr int kMaxChainOut = 16;  // camera connections of one shadow-boundary sample
+
 // True when triangle tri is one of the faces of edge E.
 template <class S, class T>
 inline bool tri_has_edge(const Scene<S>& sc, int tri, const Edge<T>& E) {
@@ -290,15 +292,30 @@ inline V3<S> eval_primary_unb(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx
   return value;
 }
 
-// Shadow-boundary term of direct light at the primary vertex. Sampling and visibility
-// tests are those of eval_direct; the edge point x_b, light point y and receiver x_d
-// lie on one line. The shadow boundary moves over the receiver's material at the
-// relative velocity d_eff = dx_b - dx_d/lam - dy (1 - 1/lam), lam = |x_d-y|/|x_b-y|;
-// the occluding faces lie on the side opposite the edge's outward vector.
+// Shadow-boundary term of direct light. Sampling and the edge/light visibility tests
+// are those of eval_direct; the edge point x_b, light point y and receiver x_d lie on
+// one line. The shadow boundary moves over the receiver's material at the relative
+// velocity d_eff = dx_b - dx_d/lam - dy (1 - 1/lam), lam = |x_d-y|/|x_b-y|; the
+// occluding faces lie on the side opposite the edge's outward vector. The change of
+// the radiance leaving x_d reaches the camera directly (x_d seen from the camera) and
+// through up to max_bounce-1 diffuse reflections: a chain of cosine-sampled bounces
+// from x_d connects each of its vertices to the camera; each bounce multiplies the
+// albedo (pi f_r against the cosine pdf), and the camera-visible end adds its camera
+// Jacobian. Returns the common derivative carrier d_eff . (w x e) and fills one
+// (pixel, RGB weight) pair per camera connection (in value mode too, for the guiding
+// masses: sum of |weight| |w x e| over the connections).
+struct DirectOut {
+  int n = 0;
+  int pix[kMaxChainOut];
+  V3<double> w[kMaxChainOut];
+  double nsn = 0;  // |w x e|
+};
+
 template <class S, bool AD>
-inline V3<S> eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], int& rx, int& ry, bool& valid) {
+inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32& rng, DirectOut& out) {
   using R = typename Traits<S>::R;
   const Scene<S>& sc = c.sc;
+  out.n = 0;
   R s = s3[0], pe;
   int ei = sc.edge_cdf.sample_reuse(s, pe);
   const Edge<S>& E = sc.edges[ei];
@@ -310,37 +327,57 @@ inline V3<S> eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], i
   V3<S> yl = light_sample_point(sc, l, sy, sz, pl);
   double pdf_l = double(pl) * double(pch);
   V3<S> dir = normalize(xb - yl);
-  valid = val(dot(E.nl, dir)) * val(dot(E.nr, dir)) < 0 && val(norm(E.nl - E.nr)) > 1e-5;
-  rx = ry = 0;
+  bool valid = val(dot(E.nl, dir)) * val(dot(E.nr, dir)) < 0 && val(norm(E.nl - E.nr)) > 1e-5;
   Its<S> is0 = scene_hit<S, AD>(sc, xb, -dir, valid);
   valid = valid && is0.valid && is0.is_light && val(sqnorm(is0.p - yl)) < double(R(1e-5));
   Its<S> id0 = scene_hit<S, AD>(sc, xb, dir, valid);
   valid = valid && id0.valid && !id0.is_light;
-  project(c.cam, id0.p, valid, rx, ry);
-  V3<S> cd = normalize(id0.p - c.cam_pos);
-  Its<S> i2 = scene_hit<S, AD>(sc, c.cam_pos, cd, valid);
-  valid = valid && i2.valid && !i2.is_light && val(sqnorm(i2.p - id0.p)) < double(R(1e-5));
-  V3<S> value;
-  if (!valid) return value;
-  if constexpr (AD) {
+  S dn = S(0);
+  if (!valid) return dn;
+  {
     V3<double> xbv = val3(xb), yv = val3(yl), xdv = val3(id0.p);
     V3<double> w = normalize(xbv - yv);
     V3<double> ev = normalize(val3(E.p1) - val3(E.p0));
     if (dot(cross(w, ev), val3(E.out)) < 0) ev = -ev;
     V3<double> ns = cross(w, ev);
+    out.nsn = norm(ns);
     double dby = norm(xbv - yv), lam = norm(xdv - yv) / dby;
-    V3<S> deff = (xb - detach(xb)) - (id0.p - detach(id0.p)) * S(1.0 / lam) - (yl - detach(yl)) * S(1.0 - 1.0 / lam);
-    S dn = dot(deff, V3<S>(S(ns.x), S(ns.y), S(ns.z)));
-    double cos_y = std::fabs(dot(val3(is0.n), w));
-    V3<double> o = val3(c.cam_pos);
-    double Jc = raster_fxfy(c.cam) * val(cam_jacobian(c.cam, xdv, val3(id0.n), o));
-    double k = cos_y / (dby * dby) * Jc / (pdf_e * pdf_l * c.cam.H * c.cam.W);
-    V3<S> fr = detach(tex_at(sc, id0.obj, id0.u, id0.v) * inv_pi<S>());
-    V3<S> Le = detach(sc.emit[is0.light]);
-    value = mul(fr, Le) * (dn * S(-k));
+    if constexpr (AD) {
+      V3<S> deff = (xb - detach(xb)) - (id0.p - detach(id0.p)) * S(1.0 / lam) - (yl - detach(yl)) * S(1.0 - 1.0 / lam);
+      dn = dot(deff, V3<S>(S(ns.x), S(ns.y), S(ns.z)));
+    }
+    const double cos_y = std::fabs(dot(val3(is0.n), w));
+    const double k0 = -cos_y / (dby * dby) / (pdf_e * pdf_l * c.cam.H * c.cam.W);
+    const double fxfy = raster_fxfy(c.cam);
+    const V3<double> o = val3(c.cam_pos);
+    V3<double> T = mul(val3(tex_at(sc, id0.obj, id0.u, id0.v)) * (1.0 / M_PI), val3(sc.emit[is0.light]));
+    // camera connection of a vertex whose reflection hemisphere (its normal) faces the camera
+    auto connect = [&](const Its<S>& v) {
+      if (val(dot(v.n, c.cam_pos - v.p)) <= 0) return;
+      bool vis = true;
+      int rx, ry;
+      project(c.cam, v.p, vis, rx, ry);
+      Its<S> iv = scene_hit<S, AD>(sc, c.cam_pos, normalize(v.p - c.cam_pos), vis);
+      vis = vis && iv.valid && !iv.is_light && val(sqnorm(iv.p - v.p)) < double(R(1e-5));
+      if (!vis || out.n >= kMaxChainOut) return;
+      const double Jc = fxfy * val(cam_jacobian(c.cam, val3(v.p), val3(v.n), o));
+      out.pix[out.n] = ry * c.cam.W + rx;
+      out.w[out.n] = T * (k0 * Jc);
+      ++out.n;
+    };
+    connect(id0);
+    Its<S> v = id0;
+    for (int j = 1; j < c.cfg.max_bounce; ++j) {
+      R ru = rng.next_float(), rv = rng.next_float(), ct;
+      V3<S> wo = diffuse_sample_dir(v, ru, rv, ct);
+      Its<S> nx = scene_hit<S, AD>(sc, v.p, wo, true);
+      if (!nx.valid || nx.is_light) break;
+      T = mul(T, val3(tex_at(sc, nx.obj, nx.u, nx.v)));
+      connect(nx);
+      v = nx;
+    }
   }
-  valid = valid && finite3(value);
-  return value;
+  return dn;
 }
 
 // Pixel-border term. Segment q of the (W+1) x H vertical and W x (H+1) horizontal unit
@@ -487,12 +524,13 @@ template <class R> struct HyperCube {
   }
 };
 
-// The unbiased estimator mixes a uniform share into the guiding masses so that no cell
-// whose preprocessing sample happened to be invalid is left unsampled.
+// The unbiased estimator mixes a uniform share into the guiding masses (a quarter of the
+// mean mass per cell, 20% of the samples): no cell whose preprocessing sample happened
+// to be invalid is left unsampled, and no sample weight exceeds 5x the uniform one.
 inline void mass_floor(std::vector<double>& m) {
   double tot = 0;
   for (double x : m) tot += x;
-  const double f = tot > 0 ? 0.05 * tot / double(m.size()) : 1.0;
+  const double f = tot > 0 ? 0.25 * tot / double(m.size()) : 1.0;
   for (double& x : m) x = double(float(float(x) + float(f)));
 }
 
@@ -545,6 +583,18 @@ inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
       for (int k = 0; k < 3; ++k) s3[k] = (R(cc[k]) + s3[k]) * hc.unit[k];
       int rx, ry;
       bool valid;
+      if (c.cfg.mode == 1) {
+        // unbiased estimator: the magnitude of its own per-sample weights (camera
+        // connections of the receiver and of its bounce chain, which uses a copy of the
+        // cell's sampler so that the rounds draw the same hypercube positions)
+        Pcg32 rc = rngs[i];
+        DirectOut o;
+        eval_direct_unb<R, false>(c, s3, rc, o);
+        double m = 0;
+        for (int q = 0; q < o.n; ++q) m += norm(o.w[q]);
+        add[i] = double(float(m * o.nsn));
+        continue;
+      }
       V3<R> v = eval_direct<R, false>(c, s3, rx, ry, valid);
       for (int k = 0; k < 3; ++k) if (v[k] < R(1e-5)) v[k] = R(1e-5);
       if (valid) add[i] = double(R(norm(v)));
@@ -636,11 +686,25 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
       R s3[3];
       for (int k = 0; k < 3; ++k) s3[k] = rng.next_float();
       const double hp = unb ? hc.sample_unb(s3, rng) : double(hc.sample_reuse(s3));
+      if (unb) {
+        if constexpr (KD > 0) {
+          DirectOut o;
+          const S dn = eval_direct_unb<S, AD>(c, s3, rng, o);
+          const double dens = hp * double(hc.cells) * spp;
+          for (int q = 0; q < o.n; ++q) {
+            double wg = 0;
+            for (int k = 0; k < 3; ++k) wg += dLdI[3 * o.pix[q] + k] * o.w[q][k];
+            if (!std::isfinite(wg)) continue;
+            for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += wg * dn.d[j] / dens;
+          }
+        }
+        continue;
+      }
       int rx, ry;
       bool valid;
-      V3<S> v = unb ? eval_direct_unb<S, AD>(c, s3, rx, ry, valid) : eval_direct<S, AD>(c, s3, rx, ry, valid);
+      V3<S> v = eval_direct<S, AD>(c, s3, rx, ry, valid);
       if (!valid) continue;
-      const double dens = double(hp) * (unb ? double(hc.cells) : 1.0);
+      const double dens = double(hp);
       if constexpr (KD > 0) {
         size_t pix = (size_t)ry * W + rx;
         for (int k = 0; k < 3; ++k)

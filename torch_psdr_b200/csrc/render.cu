@@ -1298,12 +1298,13 @@ __global__ void __launch_bounds__(256) k_border_final(WF w, const DevScene* __re
 
 // ------------------------------------------------------------------ direct edges
 // path_integrator.cc:274-353 and the boundary_term / hit_triangle adjoint (:11-78).
-// UNB (unbiased estimator, PRE=false): the same samples and visibility tests; the edge
-// point x_b, light point y and receiver x_d lie on one line and the shadow boundary
-// moves over the receiver at d_eff = dx_b - dx_d / lam - dy (1 - 1/lam),
-// lam = |x_d - y| / |x_b - y|. Per sample: -f_r L_e |n_y.w| / |x_b - y|^2 J_cam(x_d)
+// UNB (unbiased estimator, PRE=false): the same samples and edge/light visibility
+// tests; the edge point x_b, light point y and receiver x_d lie on one line and the
+// shadow boundary moves over the receiver at d_eff = dx_b - dx_d / lam - dy (1 - 1/lam),
+// lam = |x_d - y| / |x_b - y|. Per camera connection: -T |n_y.w| / |x_b - y|^2 J_cam
 // (d_eff . (w x e)) / (pdf_e pdf_y hc_density H W spp), e oriented by the edge's outward
-// vector so that the occluding faces lie on the -(w x e) side.
+// vector so that the occluding faces lie on the -(w x e) side, T = f_r(x_d) L_e times the
+// albedos of the diffuse bounces between x_d and the camera-visible vertex.
 template <bool PRE, bool UNB = false>
 __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict__ scenes,
                                                 const DevView* __restrict__ views, int v, long long n, HCube hc,
@@ -1369,30 +1370,64 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     const HitRec hd = trace_closest(sc, xb, dir, kTmin, INFINITY);
     const Surf d0 = make_surf(sc, hd.tri, hd.b1, hd.b2, xb);
     if (!(d0.valid && !d0.is_light)) continue;
-    int px, py;
-    if (!project(V, d0.p, px, py)) continue;
-    const float3 cd = normalize(d0.p - V.pos);
-    const HitRec h2 = trace_closest(sc, V.pos, cd, kTmin, INFINITY);
-    const Surf i2 = make_surf(sc, h2.tri, h2.b1, h2.b2, V.pos);
-    if (!(i2.valid && !i2.is_light && sqnorm(i2.p - d0.p) < kEps)) continue;
-    if (UNB && !PRE) {
-      if (!V.dimage || !sc.grad_verts) continue;
+    if (UNB) {
+      // PRE: the guiding mass is the sum over camera connections of |weight| |w x e|
+      // (the bounce chain draws from the sampler after its persisted state)
+      if (!PRE && (!V.dimage || !sc.grad_verts)) continue;
       float3 ev = normalize(p1 - p0);
       if (dot(cross(dir, ev), out) < 0.f) ev = -ev;
       const float3 nsv = cross(dir, ev);
       const float dby = norm(xb - ls.y), lam = norm(d0.p - ls.y) / dby;
       const float cos_y = fabsf(dot(s0.n, dir));
-      const float3 rel = d0.p - V.pos;
-      const float z = dot(rel, view_look(V));
-      const float Jc = view_fxfy(V) * fabsf(dot(d0.n, rel)) / (z * z * z);
-      const float k = cos_y / (dby * dby) * Jc / (pdf_e * ls.pdf * (float)V.H * (float)V.W);
+      const float k0 = -cos_y / (dby * dby) / (pdf_e * ls.pdf * (float)V.H * (float)V.W);
+      const float fxfy = view_fxfy(V);
+      const float3 look = view_look(V);
       const DevLight& Lt = sc.lights[s0.light];
       const DevObj& ob = sc.objs[d0.obj];
-      const float3 fr = tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi;
-      const float* gp = V.dimage + 3 * ((size_t)py * V.W + px);
-      const float phi = gp[0] * fr.x * Lt.emit[0] + gp[1] * fr.y * Lt.emit[1] + gp[2] * fr.z * Lt.emit[2];
-      const float3 a = nsv * (-phi * k / (hpdf * (float)hc.ncells * (float)spp));
-      if (!finite3(a)) continue;
+      float3 T = mul(tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi,
+                     f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]));
+      float wsum = 0.f, msum = 0.f;
+      // camera connection of a vertex whose reflection hemisphere faces the camera
+      auto connect = [&](const Surf& v) {
+        const float3 rel = v.p - V.pos;
+        if (dot(v.n, rel) >= 0.f) return;
+        int qx, qy;
+        if (!project(V, v.p, qx, qy)) return;
+        const HitRec hc2 = trace_closest(sc, V.pos, normalize(rel), kTmin, INFINITY);
+        const Surf iv = make_surf(sc, hc2.tri, hc2.b1, hc2.b2, V.pos);
+        if (!(iv.valid && !iv.is_light && sqnorm(iv.p - v.p) < kEps)) return;
+        const float z = dot(rel, look);
+        const float Jc = fxfy * fabsf(dot(v.n, rel)) / (z * z * z);
+        if (PRE) {
+          msum += norm(T) * fabsf(k0 * Jc);
+        } else {
+          const float* gp = V.dimage + 3 * ((size_t)qy * V.W + qx);
+          wsum += (gp[0] * T.x + gp[1] * T.y + gp[2] * T.z) * (k0 * Jc);
+        }
+      };
+      connect(d0);
+      // the change of the radiance leaving the receiver, carried to the camera through
+      // up to max_bounce - 1 cosine-sampled diffuse bounces (each multiplies the albedo)
+      Surf v = d0;
+      for (int j = 1; j < w.D; ++j) {
+        const float ru = rng.next_float(), rv = rng.next_float();
+        float ct, st, sp, cp;
+        const float3 wo = diffuse_dir(v.n, v.t, ru, rv, ct, st, sp, cp);
+        const HitRec hn = trace_closest(sc, v.p, wo, kTmin, INFINITY);
+        const Surf nx = make_surf(sc, hn.tri, hn.b1, hn.b2, v.p);
+        if (!nx.valid || nx.is_light) break;
+        const DevObj& on = sc.objs[nx.obj];
+        T = mul(T, tex_rgb(on.color, texel_offset(on.color, nx.u, nx.v)));
+        connect(nx);
+        v = nx;
+      }
+      if (PRE) {
+        const float m = msum * norm(nsv);
+        if (isfinite(m)) mass[i] = mass[i] + m;
+        continue;
+      }
+      const float3 a = nsv * (wsum / (hpdf * (float)hc.ncells * (float)spp));
+      if (!finite3(a) || wsum == 0.f) continue;
       const int2 evv = __ldg(sc.edge_v + e);
       atomic_add3(sc.grad_verts + 3 * (size_t)evv.x, a * (1.f - sx));
       atomic_add3(sc.grad_verts + 3 * (size_t)evv.y, a * sx);
@@ -1408,6 +1443,12 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
       atomic_add3(sc.grad_verts + 3 * (size_t)tl.z, al * ls.sv);
       continue;
     }
+    int px, py;
+    if (!project(V, d0.p, px, py)) continue;
+    const float3 cd = normalize(d0.p - V.pos);
+    const HitRec h2 = trace_closest(sc, V.pos, cd, kTmin, INFINITY);
+    const Surf i2 = make_surf(sc, h2.tri, h2.b1, h2.b2, V.pos);
+    if (!(i2.valid && !i2.is_light && sqnorm(i2.p - d0.p) < kEps)) continue;
     const float pdf_xw = s0.sqd * pdf_e * ls.pdf / dot(s0.n, dir);
     // boundary_term (detached quantities)
     const float3 xs = s0.p, xd = d0.p, ns = s0.n, nd = d0.n;
@@ -1466,12 +1507,13 @@ __global__ void k_mass_cdf(const float* __restrict__ mass, int n, double* __rest
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) w[i] = (double)mass[i];
 }
-// Unbiased estimator: add a uniform share (5% of the mean mass) to every cell.
+// Unbiased estimator: add a uniform share (a quarter of the mean mass, 20% of the
+// samples) to every cell, bounding sample weights at 5x the uniform one.
 __global__ void k_mass_floor(float* __restrict__ mass, const double* __restrict__ pre, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double tot = pre[n - 1];
-  const float f = tot > 0.0 ? (float)(0.05 * tot / (double)n) : 1.0f;
+  const float f = tot > 0.0 ? (float)(0.25 * tot / (double)n) : 1.0f;
   mass[i] = mass[i] + f;
 }
 __global__ void k_mass_finalize(const double* __restrict__ w, const double* __restrict__ pre, int n,
@@ -1920,9 +1962,14 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       HCube pre{};
       for (int k = 0; k < 3; ++k) { pre.res[k] = r3[k]; pre.unit[k] = 1.0f / (float)r3[k]; }
       PSDR_LAUNCHED(cfg.secondary_edge_preprocess_rounds + 1);
-      for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r)
-        k_direct<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
-                                                                 ws->mass.as<float>(), 1);
+      for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r) {
+        if (unb)
+          k_direct<true, true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
+                                                                         ws->mass.as<float>(), 1);
+        else
+          k_direct<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
+                                                                   ws->mass.as<float>(), 1);
+      }
       const HCube hc = build_hcube(ws, cells, r3, 3, unb, st);
       const long long N = (long long)V.H * V.W * cfg.spp_secondary_edge;
       if (unb)
