@@ -740,7 +740,7 @@ PSDR_D void cam_jacobian_adj(const DevView& V, const Surf& x, float phi, SurfAdj
 }
 
 template <bool UNB>
-__global__ void __launch_bounds__(128) k_adjoint(WF w, const DevScene* __restrict__ scenes,
+__global__ void __launch_bounds__(128, 3) k_adjoint(WF w, const DevScene* __restrict__ scenes,
                                                  const DevView* __restrict__ views, Tile tile, int hot_lv0,
                                                  int hot_nlv, int emit_hot) {
   const int stride = gridDim.x * blockDim.x;
