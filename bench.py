@@ -385,6 +385,100 @@ def run_b200(args):
     return 0
 
 
+# ---------------------------------------------------------------- multi-view workload
+MV_WORKLOAD = ("multi-view geometry + texture gradient: 64 views, H and W ~ U{128..512} (seed 3) on the radius-4 "
+               "sphere, over 3 scenes (geodesic spheres of 5,120 / 50,000 / 200,000 tris, noise 0.02, 256^2 texture, "
+               "ground, light), view v on scene v mod 3, 16 spp interior + 4 spp per edge kind, depth 4, L2 loss")
+
+
+def run_multiview(args):
+    """Batched (one work list and one graph each way for all 64 views) against plain
+    (per view: a new single-camera Scene, renderD, loss, backward), one GPU."""
+    import torch
+    import torch_psdr_b200 as dr
+    from torch_psdr_b200 import synth
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    cams = synth.orbit_cameras(64, 4.0, seed=3, size_lo=128, size_hi=512)
+    cfg = dict(spp_interior=16, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=4, estimator=args.estimator)
+    integ = dr.PathIntegrator(**cfg)
+
+    def tens(a, dt=torch.float32, rg=False):
+        return torch.tensor(np.asarray(a), dtype=dt, device=dev, requires_grad=rg)
+
+    scenes_data = []
+    for i, n in enumerate((16, 50, 100)):
+        spec = synth.sphere_scene(freq=n, tex_hw=256, tex_seed=i, noise_sigma=0.02, noise_seed=2)
+        sph, gr = spec.meshes
+        lt = spec.lights[0]
+        d = dict(v=tens(sph.vertices, rg=True), f=tens(sph.faces, torch.int32), uv=tens(sph.uvs),
+                 uvi=tens(sph.uv_indices, torch.int32), tex=tens(sph.texture, rg=True), gV=tens(gr.vertices),
+                 gF=tens(gr.faces, torch.int32), gT=tens(gr.texture), lV=tens(lt.vertices),
+                 lF=tens(lt.faces, torch.int32), lE=tens(lt.emit))
+        d["cams"] = [dr.PerspectiveCamera(tens(c.look_from), tens(c.look_at), tens(c.up), tens([c.vfov]), c.height,
+                                          c.width) for k, c in enumerate(cams) if k % 3 == i]
+        scenes_data.append(d)
+
+    def scene_of(d, cam_list, verts=None):
+        return dr.Scene(cam_list, [dr.Mesh(d["v"] if verts is None else verts, d["uv"], d["f"], d["uvi"],
+                                           dr.DiffuseMaterial(d["tex"])),
+                                   dr.Mesh(d["gV"], None, d["gF"], None, dr.DiffuseMaterial(d["gT"]))],
+                        [dr.AreaLight(d["lV"], d["lF"], d["lE"])])
+
+    with torch.no_grad():
+        targets = [[img.clone() for img in integ.renderC(scene_of(d, d["cams"], d["v"] + 0.03))] for d in scenes_data]
+    views = sum(len(d["cams"]) for d in scenes_data)
+    paths = sum(c.height * c.width for c in cams) * cfg["spp_interior"]
+
+    def step_plain():
+        for d, tg in zip(scenes_data, targets):
+            for cam, t in zip(d["cams"], tg):
+                img = integ.renderD(scene_of(d, [cam]))[0]
+                ((img - t) ** 2).sum().backward()
+
+    batch_scenes = [scene_of(d, d["cams"]) for d in scenes_data]
+    batch = dr.BatchRender(integ, batch_scenes)
+    flat_targets = [t for tg in targets for t in tg]
+
+    def step_batched():
+        imgs = batch.renderD()
+        sum(((a - b) ** 2).sum() for a, b in zip(imgs, flat_targets)).backward()
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, with_clocks):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        clocks = Clocks(dev.index) if with_clocks else None
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            fn()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks else None
+        return sum(a.elapsed_time(b) for a, b in ev), clk
+
+    b_ms, clk = timed(step_batched, True)
+    p_ms, _ = timed(step_plain, False)
+    value = paths * args.steps / (b_ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": b_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded geodesic-sphere scenes, orbit cameras)",
+            "config": {"workload": MV_WORKLOAD, "views": views, "paths_per_step": paths, "estimator": args.estimator,
+                       "mode": "batched (one work list, forward and backward graphs)",
+                       "other_mode": {"mode": "plain (per view: new Scene, renderD, backward)",
+                                      "value": paths * args.steps / (p_ms / 1e3), "ms_per_step": p_ms / args.steps},
+                       "batched_over_plain": p_ms / b_ms,
+                       "l2": "flushed between steps (256 MiB write outside the timed events)"},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -394,6 +488,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad-check", action="store_true")
     ap.add_argument("--estimator", default="unbiased", choices=["unbiased", "reference"])
+    ap.add_argument("--workload", default="geometry", choices=["geometry", "multiview"],
+                    help="geometry: the 512^2 fwd+bwd workload (default); multiview: 64 views over 3 scenes")
     ap.add_argument("--mode", default="batched", choices=["batched", "plain"],
                     help="batched: persistent scene + graph replay; plain: new Scene + per-view launches each step")
     ap.add_argument("--size", type=int, default=512, help="image size (512 = the benchmark workload)")
@@ -406,6 +502,8 @@ def main():
         CFG["spp_interior"] = SPP
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "multiview":
+        return run_multiview(args)
     return run_b200(args)
 
 
