@@ -230,11 +230,21 @@ def run_b200(args):
     cam = dr.PerspectiveCamera(tens(c.look_from), tens(c.look_at), tens(c.up), tens([c.vfov]), H, W)
     integ = dr.PathIntegrator(estimator=args.estimator, **CFG)
 
-    def build_scene(verts, texture):
-        return dr.Scene([cam], [dr.Mesh(verts, uvs, faces, uvi, dr.DiffuseMaterial(texture)),
-                                dr.Mesh(gV, None, gF, None, dr.DiffuseMaterial(gT))],
-                        [dr.AreaLight(lV, lF, lE)])
+    leaf = {"size": 1}
 
+    def build_scene(verts, texture):
+        sc = dr.Scene([cam], [dr.Mesh(verts, uvs, faces, uvi, dr.DiffuseMaterial(texture)),
+                              dr.Mesh(gV, None, gF, None, dr.DiffuseMaterial(gT))],
+                      [dr.AreaLight(lV, lF, lE)])
+        if leaf["size"] != 1:
+            L.check(lib.psdr_scene_set_leaf_size(sc.handle, leaf["size"],
+                                                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), "leaf")
+        return sc
+
+    # tile size (and leaf size, kept per scene) from the library's autotuner, untimed
+    tune = integ.autotune(build_scene(base, tex)) if not args.no_autotune else None
+    if tune:
+        leaf["size"] = tune["leaf_size"]
     with torch.no_grad():
         target = integ.renderC(build_scene(base + torch.tensor([0.05, 0.0, 0.0], device=dev), tex))[0].clone()
     t = torch.zeros(3, device=dev, requires_grad=True)
@@ -360,6 +370,7 @@ def run_b200(args):
                        "mode": ("batched (persistent scene, geometry rebuild + fwd and bwd replayed from CUDA graphs)"
                                 if args.mode == "batched" else "plain (new Scene per step, per-view launch sequences)"),
                        "estimator": args.estimator,
+                       "autotune": tune,
                        "other_mode": {"mode": "plain" if args.mode == "batched" else "batched",
                                       "value": other_value, "ms_per_step": other_ms / args.steps},
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
@@ -487,6 +498,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference", "ours"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad-check", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--estimator", default="unbiased", choices=["unbiased", "reference"])
     ap.add_argument("--workload", default="geometry", choices=["geometry", "multiview"],
                     help="geometry: the 512^2 fwd+bwd workload (default); multiview: 64 views over 3 scenes")

@@ -92,7 +92,8 @@ typedef struct {
 } psdr_camera_desc;
 
 /* PathIntegrator::Config (path_integrator.h:8-21; torch_psdr.py:478-536) plus the
- * B200 extensions: estimator, tile_paths (wavefront tile, 0 = autotuned), leaf_size
+ * B200 extensions: estimator, tile_paths (wavefront tile, 0 = 2^20 paths; see
+ * psdr_autotune), leaf_size
  * (BVH leaf collapse, 0 = default), terms, spp_pixel_boundary and seed (0 = the
  * reference's sample streams; seed s offsets every stream index by s * 2654435761
  * modulo 2^32).
@@ -149,6 +150,9 @@ PSDR_API psdr_status psdr_scene_destroy(psdr_scene* scene);
 /* Rebuild the acceleration structure, triangle attributes and edges after the
  * vertex buffers changed in place (same topology). */
 PSDR_API psdr_status psdr_scene_update(psdr_scene* scene, void* stream);
+/* BVH leaves of up to leaf_size (1..8) triangles; rebuilds the scene's geometry.
+ * Extension (the reference's OptiX build has no such knob); psdr_autotune picks it. */
+PSDR_API psdr_status psdr_scene_set_leaf_size(psdr_scene* scene, int32_t leaf_size, void* stream);
 /* Synchronous query: [0] triangles, [1] vertices, [2] edges, [3] bvh nodes,
  * [4] lights, [5] objects. */
 PSDR_API psdr_status psdr_scene_info(psdr_scene* scene, int64_t* info6);
@@ -190,9 +194,19 @@ PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const psdr_camer
  * values the film averages; used by the parity tests. */
 PSDR_API psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cam,
                                 const psdr_config* cfg, float* samples, void* stream);
+/* Autotuner (extension; the reference has no tuner): times forward renders of the
+ * given cameras for every wavefront tile size in {2^18, 2^19, 2^20, 2^21} paths and
+ * BVH leaf size in {1, 2, 4} triangles (the scene's BVH is rebuilt for each), keeps
+ * the fastest leaf size in the scene (later psdr_scene_update calls use it), writes
+ * the fastest tile size to cfg->tile_paths and, when non-null, the leaf size and the
+ * fastest render time to best_leaf / best_ms. Allocates and synchronises `stream`;
+ * results do not depend on either choice (hits and films are deterministic). */
+PSDR_API psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams,
+                                   int32_t n_cams, psdr_config* cfg, int32_t* best_leaf, float* best_ms,
+                                   void* stream);
 /* Path-replay adjoint of renderD (replaces Wrap2torch.backward + enoki's reverse
- * sweep, torch_psdr.py:48-72): interior term + primary-edge and direct-edge
- * boundary terms. d_images[c] is dLoss/dImage (H,W,3) per camera. */
+ * sweep, torch_psdr.py:48-72): interior term + the boundary terms of the selected
+ * estimator. d_images[c] is dLoss/dImage (H,W,3) per camera. */
 PSDR_API psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
                             const psdr_config* cfg, const float** d_images, const psdr_grad_targets* grads,
                             void* stream);

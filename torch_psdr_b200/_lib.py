@@ -75,6 +75,7 @@ SIGNATURES = {
     "psdr_scene_create": ([C.POINTER(SceneDesc), P, C.POINTER(P)], C.c_int),
     "psdr_scene_destroy": ([P], C.c_int),
     "psdr_scene_update": ([P, P], C.c_int),
+    "psdr_scene_set_leaf_size": ([P, C.c_int32, P], C.c_int),
     "psdr_scene_info": ([P, C.POINTER(C.c_int64)], C.c_int),
     "psdr_scene_edges": ([P, P, P, C.c_int64, C.POINTER(C.c_int64), P], C.c_int),
     "psdr_intersect": ([P, P, C.c_int64, P, P, P, C.c_int32, P], C.c_int),
@@ -82,6 +83,8 @@ SIGNATURES = {
     "psdr_workspace_destroy": ([P], C.c_int),
     "psdr_render_fwd": ([P, P, C.POINTER(CameraDesc), C.c_int32, C.POINTER(Config), C.POINTER(P), P], C.c_int),
     "psdr_render_samples": ([P, P, C.POINTER(CameraDesc), C.POINTER(Config), P, P], C.c_int),
+    "psdr_autotune": ([P, P, C.POINTER(CameraDesc), C.c_int32, C.POINTER(Config), C.POINTER(C.c_int32),
+                       C.POINTER(C.c_float), P], C.c_int),
     "psdr_render_fwd_noalloc": ([P, C.POINTER(CameraDesc), C.POINTER(Config), P, P], C.c_int),
     "psdr_render_bwd": ([P, P, C.POINTER(CameraDesc), C.c_int32, C.POINTER(Config), C.POINTER(P),
                          C.POINTER(GradTargets), P], C.c_int),

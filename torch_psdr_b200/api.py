@@ -415,6 +415,17 @@ class PathIntegrator:
                                           ptrs, _stream()), "psdr_render_fwd")
         return imgs
 
+    def autotune(self, scene: Scene) -> dict:
+        """Pick the wavefront tile size and the scene's BVH leaf size by timing forward
+        renders of the scene's cameras (psdr_autotune); the integrator keeps the tile
+        size, the scene keeps the leaf size. Extension: the reference has no tuner."""
+        leaf = C.c_int32()
+        ms = C.c_float()
+        cams = scene._camera_descs()
+        L.check(self._lib.psdr_autotune(scene.handle, self._workspace(), cams, len(cams), C.byref(self.cfg),
+                                        C.byref(leaf), C.byref(ms), _stream()), "psdr_autotune")
+        return {"tile_paths": int(self.cfg.tile_paths), "leaf_size": int(leaf.value), "forward_ms": float(ms.value)}
+
     def render_samples(self, scene: Scene, camera_index: int = 0) -> Tensor:
         """Per-sample interior radiance (H*W*spp, 3) of one camera (the values the film averages)."""
         c = scene.cameras[camera_index]

@@ -233,6 +233,15 @@ psdr_status psdr_scene_update(psdr_scene* scene, void* stream) {
   API_END
 }
 
+psdr_status psdr_scene_set_leaf_size(psdr_scene* scene, int32_t leaf_size, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene != nullptr, "null scene");
+  PSDR_CHECK(leaf_size >= 1 && leaf_size <= 8, "leaf_size must be in [1, 8]");
+  scene->leaf_size = leaf_size;
+  scene_build_geometry(scene, stream ? (cudaStream_t)stream : scene->stream);
+  API_END
+}
+
 psdr_status psdr_scene_info(psdr_scene* scene, int64_t* info) {
   API_BEGIN
   PSDR_CHECK(scene != nullptr && info != nullptr, "null argument");
@@ -316,6 +325,64 @@ psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psd
   std::vector<DevView> views(1);
   make_view(*cam, cfg->spp_interior, views[0]);
   render_forward_impl(dev_scene(scene), views, *cfg, ws, (cudaStream_t)stream, samples);
+  API_END
+}
+
+psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
+                          psdr_config* cfg, int32_t* best_leaf, float* best_ms, void* stream) {
+  struct Ev {
+    cudaEvent_t e = nullptr;
+    ~Ev() { if (e) cudaEventDestroy(e); }
+  };
+  API_BEGIN
+  PSDR_CHECK(scene && ws && cfg, "null argument");
+  check_cfg(cfg);
+  check_cams(cams, n_cams);
+  PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<DevView> views(n_cams);
+  size_t floats = 0;
+  for (int i = 0; i < n_cams; ++i) floats += 3 * (size_t)cams[i].height * cams[i].width;
+  DBuf img;
+  img.alloc(sizeof(float) * floats, st);
+  size_t off = 0;
+  for (int i = 0; i < n_cams; ++i) {
+    make_view(cams[i], cfg->spp_interior, views[i]);
+    views[i].image = img.as<float>() + off;
+    off += 3 * (size_t)cams[i].height * cams[i].width;
+  }
+  Ev ev0, ev1;
+  PSDR_CUDA(cudaEventCreate(&ev0.e));
+  PSDR_CUDA(cudaEventCreate(&ev1.e));
+  cudaEvent_t e0 = ev0.e, e1 = ev1.e;
+  const int leaves[3] = {1, 2, 4};
+  const int tiles[4] = {1 << 18, 1 << 19, 1 << 20, 1 << 21};
+  float best = INFINITY;
+  int bl = scene->leaf_size, bt = cfg->tile_paths;
+  for (int leaf : leaves) {
+    scene->leaf_size = leaf;
+    scene_build_geometry(scene, st);
+    for (int tile : tiles) {
+      psdr_config c = *cfg;
+      c.tile_paths = tile;
+      std::vector<DevView> v = views;
+      render_forward_impl(dev_scene(scene), v, c, ws, st, nullptr);  // warm-up, sizes the workspace
+      PSDR_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < 2; ++r) render_forward_impl(dev_scene(scene), v, c, ws, st, nullptr);
+      PSDR_CUDA(cudaEventRecord(e1, st));
+      PSDR_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      PSDR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      ms *= 0.5f;
+      if (ms < best) { best = ms; bl = leaf; bt = tile; }
+    }
+  }
+  scene->leaf_size = bl;
+  scene_build_geometry(scene, st);
+  PSDR_CUDA(cudaStreamSynchronize(st));
+  cfg->tile_paths = bt;
+  if (best_leaf) *best_leaf = bl;
+  if (best_ms) *best_ms = best;
   API_END
 }
 

@@ -1393,7 +1393,10 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
         if (dot(v.n, rel) >= 0.f) return;
         int qx, qy;
         if (!project(V, v.p, qx, qy)) return;
-        const HitRec hc2 = trace_closest(sc, V.pos, normalize(rel), kTmin, INFINITY);
+        // the closest hit must be v itself: stop at the first hit short of it (same
+        // outcome as a full closest-hit query followed by the distance test)
+        const float dist = norm(rel);
+        const HitRec hc2 = trace_closest(sc, V.pos, rel / dist, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
         const Surf iv = make_surf(sc, hc2.tri, hc2.b1, hc2.b2, V.pos);
         if (!(iv.valid && !iv.is_light && sqnorm(iv.p - v.p) < kEps)) return;
         const float z = dot(rel, look);

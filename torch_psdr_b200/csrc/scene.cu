@@ -488,12 +488,14 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
   if (n > 1) k_karras<<<nblk(n - 1), 256, 0, st>>>(n, keys, child, range, parent);
   k_bottom_up<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), child, parent, aabb, bflags);
   if (n > 1) {
-    // 4-wide nodes: flags (even depth), exclusive scan for their indices, layout
+    // 4-wide nodes: flags (even depth), exclusive scan for their indices, layout. The
+    // root (node 0) must stay an internal node: leaves hold fewer than n triangles.
+    const int leaf = std::min(s->leaf_size, n - 1);
     int* f4 = s->aux_i2.as<int>();
     int* idx4 = s->aux_i2.as<int>() + n;
-    k_depth_flags<<<nblk(n - 1), 256, 0, st>>>(n, parent, range, s->leaf_size, f4);
+    k_depth_flags<<<nblk(n - 1), 256, 0, st>>>(n, parent, range, leaf, f4);
     exclusive_scan_int(f4, idx4, n - 1, s->flags.as<int>() + 2 * (size_t)n, st);
-    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, s->leaf_size, child, range, aabb, cbox, f4, idx4, s->nodes.as<float4>());
+    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, leaf, child, range, aabb, cbox, f4, idx4, s->nodes.as<float4>());
   }
   k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), s->leaf.as<float4>());
   // records + lights + half-edge sort (2 x passes x 5) + edge build/CDF (8) + BVH (9 + morton sort)
