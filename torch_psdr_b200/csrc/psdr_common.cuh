@@ -342,6 +342,91 @@ PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, 
   return h;
 }
 
+// Resumable form of trace_closest for kernels that interleave many rays per thread
+// (dynamic ray fetch): the same visiting order, tests and tie rule, so the same hit.
+struct TraceState {
+  RayPre rp;
+  float3 inv, oi;
+  float tmin, t_occ;
+  HitRec h;
+  int node, sp;
+};
+
+PSDR_D void trace_begin(TraceState& s, float3 o, float3 d, float tmin, float tmax, float t_occ, int root) {
+  s.rp = ray_pre(o, d);
+  s.inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+  s.oi = f3(o.x * s.inv.x, o.y * s.inv.y, o.z * s.inv.z);
+  s.tmin = tmin;
+  s.t_occ = t_occ;
+  s.h.tri = -1; s.h.b1 = 0.f; s.h.b2 = 0.f; s.h.t = tmax;
+  s.node = root;
+  s.sp = 0;
+}
+
+// One node or leaf visit; returns true when the query is finished (s.h holds the hit).
+PSDR_D bool trace_step(const DevScene& sc, TraceState& s, int* stack) {
+  if (s.node >= 0) {
+    const float4* nd = sc.nodes + 7 * (size_t)s.node;
+    const float4 lx = __ldg(nd), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
+    const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5);
+    const int4 e = __ldg(reinterpret_cast<const int4*>(nd + 6));
+    const float cull = s.h.t * 1.00001f + 1e-12f;
+    const float3 inv = s.inv, oi = s.oi;
+    const float tmin = s.tmin;
+    auto slab = [&](float l_x, float h_x, float l_y, float h_y, float l_z, float h_z, int c) {
+      const float ax = fmaf(l_x, inv.x, -oi.x), bx = fmaf(h_x, inv.x, -oi.x);
+      const float ay = fmaf(l_y, inv.y, -oi.y), by = fmaf(h_y, inv.y, -oi.y);
+      const float az = fmaf(l_z, inv.z, -oi.z), bz = fmaf(h_z, inv.z, -oi.z);
+      const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), tmin));
+      const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), cull));
+      return (c != 0x7fffffff && tn <= tf * 1.0000005f) ? tn : INFINITY;
+    };
+    float k0 = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, e.x);
+    float k1 = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, e.y);
+    float k2 = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, e.z);
+    float k3 = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, e.w);
+    int c0 = e.x, c1 = e.y, c2 = e.z, c3 = e.w;
+    cswap(k0, c0, k1, c1);
+    cswap(k2, c2, k3, c3);
+    cswap(k0, c0, k2, c2);
+    cswap(k1, c1, k3, c3);
+    cswap(k1, c1, k2, c2);
+    if (k0 == INFINITY) {
+      if (s.sp == 0) return true;
+      s.node = stack[--s.sp];
+      return false;
+    }
+    s.node = c0;
+    if (s.sp + 3 <= kStack) {
+      if (k3 != INFINITY) stack[s.sp++] = c3;
+      if (k2 != INFINITY) stack[s.sp++] = c2;
+      if (k1 != INFINITY) stack[s.sp++] = c1;
+    } else {
+      atomicOr(sc.err, 1);
+    }
+    return false;
+  }
+  const int code = ~s.node;
+  const int first = code >> 3, cnt = (code & 7) + 1;
+  for (int k = 0; k < cnt; ++k) {
+    const float4* lt = sc.leaf + 3 * (size_t)(first + k);
+    const float4 q0 = __ldg(lt), q1 = __ldg(lt + 1), q2 = __ldg(lt + 2);
+    float tt, b1, b2;
+    if (tri_test(s.rp, xyz(q0), xyz(q1), xyz(q2), s.tmin, s.h.t, tt, b1, b2)) {
+      if (tt < s.t_occ) {
+        s.h.tri = -1;
+        s.h.t = tt;
+        return true;
+      }
+      const int id = __float_as_int(q0.w);
+      if (tt < s.h.t || s.h.tri < 0 || id < s.h.tri) { s.h.t = tt; s.h.tri = id; s.h.b1 = b1; s.h.b2 = b2; }
+    }
+  }
+  if (s.sp == 0) return true;
+  s.node = stack[--s.sp];
+  return false;
+}
+
 // ------------------------------------------------------------------ surface points
 // scene.cc:106-161 Scene::hit: the point is re-formed from the triangle and the
 // barycentrics; the normal and tangent face the incoming ray (is_front flip).

@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
   const int stride = gridDim.x * blockDim.x;
   const int n32 = (n + 31) & ~31;
   const bool last = d == w.D - 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.cnt[2 * w.D + 2] = 0;  // ray fetch counter of k_trace
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n32; q += stride) {
     bool go = false;
     int s = -1;
@@ -205,25 +206,64 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
 }
 
 // ------------------------------------------------------------------ trace kernel
+// Closest hit of every queued ray of a depth (light-sample rays r < nL stop at the first
+// hit short of the light). Persistent warps with dynamic ray fetch: a lane whose ray
+// has finished takes the next unclaimed ray of the queue after every 8 traversal steps,
+// so a warp keeps its lanes busy instead of waiting for its longest ray (the rays of a
+// warp differ in traversal length by an order of magnitude). The fetch counter is
+// w.cnt[2D+2], reset by k_shade.
+constexpr int kTraceSteps = 8;
 __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict__ scenes,
-                                               const DevView* __restrict__ views, int d,
-                                               unsigned long long* __restrict__ ray_count) {
+                                                   const DevView* __restrict__ views, int d,
+                                                   unsigned long long* __restrict__ ray_count) {
   const int nk = w.cnt[2 * d + 1];
   const int Rd = (d == w.D - 1) ? w.R - 1 : w.R;
   const long long total = (long long)nk * Rd;
   if (ray_count && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ray_count, (unsigned long long)total);
-  const int stride = gridDim.x * blockDim.x;
-  for (long long idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
-    const int r = (int)(idx / nk);
-    const int k = (int)(idx - (long long)r * nk);
-    const size_t slot = (size_t)r * w.cap + k;
-    const int s = w.qs[k];
-    const DevScene& sc = scenes[views[w.view[s]].scene];
-    const float4 o = w.ro[slot], dd = w.rd[slot];
-    // light-sample rays (r < nL) are occlusion tests below the target point
-    const float t_occ = r < w.nL ? (o.w - 4e-3f) / 1.0001f - 4e-3f : -INFINITY;
-    const HitRec h = trace_closest(sc, xyz(o), xyz(dd), kTmin, o.w, t_occ);
-    w.hit[slot] = hit4(h);
+  int* fetch = w.cnt + 2 * w.D + 2;
+  int stack[kStack];
+  TraceState s;
+  const DevScene* sc = nullptr;
+  size_t slot = 0;
+  bool live = false, done = false;
+  while (true) {
+    const unsigned want = __ballot_sync(0xffffffffu, !live && !done);
+    if (want) {
+      const int lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(fetch, __popc(want));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (!live && !done) {
+        const long long idx = (long long)base + __popc(want & lanemask_lt());
+        if (idx < total) {
+          const int r = (int)(idx / nk);
+          const int k = (int)(idx - (long long)r * nk);
+          slot = (size_t)r * w.cap + k;
+          sc = &scenes[views[w.view[w.qs[k]]].scene];
+          const float4 o = w.ro[slot], dd = w.rd[slot];
+          const float t_occ = r < w.nL ? (o.w - 4e-3f) / 1.0001f - 4e-3f : -INFINITY;
+          trace_begin(s, xyz(o), xyz(dd), kTmin, o.w, t_occ, sc->root);
+          live = sc->ntri > 0;
+          if (!live) w.hit[slot] = make_float4(__int_as_float(-1), 0.f, 0.f, o.w);
+        } else {
+          done = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, live)) {
+      if (__all_sync(0xffffffffu, done)) break;
+      continue;
+    }
+    if (live) {
+#pragma unroll 1
+      for (int it = 0; it < kTraceSteps; ++it) {
+        if (trace_step(*sc, s, stack)) {
+          w.hit[slot] = make_float4(__int_as_float(s.h.tri), s.h.b1, s.h.b2, s.h.t);
+          live = false;
+          break;
+        }
+      }
+    }
   }
 }
 
@@ -1684,7 +1724,7 @@ static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int 
     if (mode == MODE_REPLAY) k_shade<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
     else k_shade<MODE_FWD><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
     pf.begin_trace(st);
-    k_trace<<<grid_for((long long)cap * w.R, 128, 16), 128, 0, st>>>(w, scenes, views, d, pf.on ? pf.d_rays : nullptr);
+    k_trace<<<num_sms() * 8, 128, 0, st>>>(w, scenes, views, d, pf.on ? pf.d_rays : nullptr);
     pf.end_trace(st);
     PSDR_LAUNCHED(3);
     if (mode == MODE_REPLAY) k_accum<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
