@@ -338,6 +338,14 @@ class _RenderD(torch.autograd.Function):
         return (None, None) + tuple(out)
 
 
+def _grad_buf(param, internal):
+    """Zeroed gradient buffer shaped like `internal`, or None when `param` does not
+    require grad."""
+    if isinstance(param, Tensor) and param.requires_grad:
+        return torch.zeros_like(internal)
+    return None
+
+
 class PathIntegrator:
     def __init__(self, enable_light_visable: bool = False, n_pass: int = 1, spp_interior: int = 1,
                  max_bounce: int = 3, mis_light_samples: int = 1, mis_bsdf_samples: int = 1,
@@ -443,13 +451,16 @@ class PathIntegrator:
                 g = torch.zeros((c.height, c.width, 3), dtype=torch.float32, device=dev)
             dimgs.append(g.detach().float().contiguous())
         nm, nl = len(scene.meshes), len(scene.lights)
-        vert_g = [torch.zeros_like(m.v) for m in scene.meshes] + [torch.zeros_like(lt.v) for lt in scene.lights]
-        tex_g = [torch.zeros_like(m.material.texture.data) for m in scene.meshes]
+        # vertex gradients only for the meshes/lights whose vertices require grad (the
+        # library then skips the others' scatters)
+        vert_g = [_grad_buf(m.vertices, m.v) for m in scene.meshes] + [_grad_buf(lt.vertices, lt.v)
+                                                                        for lt in scene.lights]
+        tex_g = [_grad_buf(m.material.texture.tensor, m.material.texture.data) for m in scene.meshes]
         emit_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.lights]
         cam_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.cameras]
         P = C.c_void_p
-        vp = (P * (nm + nl))(*[t.data_ptr() for t in vert_g])
-        tp = (P * max(1, nm))(*[t.data_ptr() for t in tex_g])
+        vp = (P * (nm + nl))(*[None if t is None else t.data_ptr() for t in vert_g])
+        tp = (P * max(1, nm))(*[None if t is None else t.data_ptr() for t in tex_g])
         ep = (P * max(1, nl))(*[t.data_ptr() for t in emit_g])
         cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
         tg = L.GradTargets(vp, tp, ep, cp, 0)
@@ -499,9 +510,12 @@ class BatchRender:
 
     The forward graph rebuilds every scene's geometry from its meshes' vertex buffers
     (update them in place with `Mesh.set_vertices`) and renders every camera; the
-    backward graph runs the path-replay adjoint and both edge terms for all views.
-    Images, image gradients and gradient buffers are allocated once and bound to the
-    graphs. Extension: the reference has no batching.
+    backward graph runs the path-replay adjoint and every boundary term of the
+    integrator's estimator for all views. Images, image gradients and gradient buffers
+    are allocated once and bound to the graphs; vertex gradients are kept for the
+    meshes and lights whose vertices require grad when the batch is created (keep
+    that when swapping buffers with `Mesh.set_vertices`). Extension: the reference has
+    no batching.
     """
 
     def __init__(self, integrator: PathIntegrator, scenes: List[Scene], differentiable: bool = True):
@@ -526,12 +540,13 @@ class BatchRender:
         cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
         self.cam_grads = cam_g
         for sc in self.scenes:
-            vg = [torch.zeros_like(m.v) for m in sc.meshes] + [torch.zeros_like(lt.v) for lt in sc.lights]
-            tg = [torch.zeros_like(m.material.texture.data) for m in sc.meshes]
+            vg = [_grad_buf(m.vertices, m.v) for m in sc.meshes] + [_grad_buf(lt.vertices, lt.v)
+                                                                    for lt in sc.lights]
+            tg = [_grad_buf(m.material.texture.tensor, m.material.texture.data) for m in sc.meshes]
             eg = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in sc.lights]
             self.grads.append((vg, tg, eg))
-            vp = (P * max(1, len(vg)))(*[t.data_ptr() for t in vg])
-            tp = (P * max(1, len(tg)))(*[t.data_ptr() for t in tg])
+            vp = (P * max(1, len(vg)))(*[None if t is None else t.data_ptr() for t in vg])
+            tp = (P * max(1, len(tg)))(*[None if t is None else t.data_ptr() for t in tg])
             ep = (P * max(1, len(eg)))(*[t.data_ptr() for t in eg])
             self._keep += [vp, tp, ep]
             targets.append(L.GradTargets(vp, tp, ep, cp, 0))

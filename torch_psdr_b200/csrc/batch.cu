@@ -6,6 +6,7 @@
 // geometry rebuild) and the whole backward are each recorded once into a graph and
 // replayed with a single launch.
 #include <algorithm>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,8 @@ struct psdr_batch {
   std::vector<std::vector<float*>> gv, gt, ge;
   std::vector<float*> gc;
   std::vector<int> gacc;
+  std::vector<std::unique_ptr<psdr::DBuf>> vmasks;  // per-scene vertex-gradient masks of this batch's targets
+  std::vector<std::unique_ptr<psdr::DBuf>> objs;    // per-scene object tables (texture accumulators asked for)
   cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
   long long fwd_launches = 0, bwd_launches = 0;
   std::vector<psdr::Profiler::EvPair> fwd_ev, bwd_ev;  // trace timing events recorded in the graphs
@@ -122,6 +125,32 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     upload_views(&b->ws, b->views, st);
     std::vector<DevScene> ds(n_scenes);
     for (int i = 0; i < n_scenes; ++i) ds[i] = scenes[i]->dev;
+    if (b->backward) {
+      // only the vertices whose gradient the caller bound are accumulated
+      b->vmasks.resize(n_scenes);
+      b->objs.resize(n_scenes);
+      for (int i = 0; i < n_scenes; ++i) {
+        const psdr_scene* s = scenes[i];
+        std::vector<unsigned char> m(std::max(1, s->nvert), 0);
+        for (int o = 0; o < s->nobj; ++o)
+          if (grads[i].vertices && grads[i].vertices[o])
+            std::fill(m.begin() + s->obj_vert_off[o], m.begin() + s->obj_vert_off[o] + s->obj_nvert[o], 1);
+        b->vmasks[i].reset(new psdr::DBuf());
+        b->vmasks[i]->alloc(m.size(), st);
+        PSDR_CUDA(cudaMemcpyAsync(b->vmasks[i]->p, m.data(), m.size(), cudaMemcpyHostToDevice, st));
+        PSDR_CUDA(cudaStreamSynchronize(st));
+        ds[i].vmask = b->vmasks[i]->as<unsigned char>();
+        std::vector<DevObj> ob = s->h_objs;
+        for (int o = 0; o < (int)s->meshes.size(); ++o)
+          if (!(grads[i].textures && grads[i].textures[o])) ob[o].color.grad = nullptr;
+        b->objs[i].reset(new psdr::DBuf());
+        b->objs[i]->alloc(sizeof(DevObj) * std::max<size_t>(1, ob.size()), st);
+        PSDR_CUDA(cudaMemcpyAsync(b->objs[i]->p, ob.data(), sizeof(DevObj) * std::max<size_t>(1, ob.size()),
+                                  cudaMemcpyHostToDevice, st));
+        PSDR_CUDA(cudaStreamSynchronize(st));
+        ds[i].objs = b->objs[i]->as<DevObj>();
+      }
+    }
     b->scenes_dev.alloc(sizeof(DevScene) * n_scenes, st);
     PSDR_CUDA(cudaMemcpyAsync(b->scenes_dev.p, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice, st));
     if (n_scenes == 1) b->gi = grad_info(scenes[0]);

@@ -208,6 +208,9 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
     s->g_tex.alloc(sizeof(double) * std::max<size_t>(1, texoff), st);
     s->g_emit.alloc(sizeof(double) * 3 * std::max(1, nl), st);
     s->dev.grad_verts = s->g_verts.as<double>();
+    s->vmask.alloc(std::max<size_t>(1, s->nvert), st);
+    PSDR_CUDA(cudaMemsetAsync(s->vmask.p, 1, std::max<size_t>(1, s->nvert), st));
+    s->dev.vmask = s->vmask.as<unsigned char>();
     for (int o = 0; o < nm; ++o) s->h_objs[o].color.grad = s->g_tex.as<double>() + s->tex_grad_off[o];
     for (int l = 0; l < nl; ++l) s->h_lights[l].grad_emit = s->g_emit.as<double>() + 3 * l;
     s->upload_tables();
@@ -395,6 +398,20 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   check_cams(cams, n_cams);
   PSDR_CHECK(scene->nlight > 0, "scene has no light");
   cudaStream_t st = (cudaStream_t)stream;
+  // only the vertices whose gradient the caller asked for are accumulated
+  {
+    std::vector<unsigned char> m(std::max(1, scene->nvert), 0);
+    for (int o = 0; o < scene->nobj; ++o)
+      if (grads->vertices && grads->vertices[o])
+        std::fill(m.begin() + scene->obj_vert_off[o], m.begin() + scene->obj_vert_off[o] + scene->obj_nvert[o], 1);
+    PSDR_CUDA(cudaMemcpyAsync(scene->vmask.p, m.data(), m.size(), cudaMemcpyHostToDevice, st));
+    // and only the textures asked for: their accumulators stay in the object table
+    std::vector<DevObj> objs = scene->h_objs;
+    for (int o = 0; o < (int)scene->meshes.size(); ++o)
+      if (!(grads->textures && grads->textures[o])) objs[o].color.grad = nullptr;
+    PSDR_CUDA(cudaMemcpyAsync(scene->objs.p, objs.data(), sizeof(DevObj) * std::max<size_t>(1, objs.size()),
+                              cudaMemcpyHostToDevice, st));
+  }
   PSDR_CUDA(cudaMemsetAsync(scene->g_verts.p, 0, scene->g_verts.bytes, st));
   PSDR_CUDA(cudaMemsetAsync(scene->g_tex.p, 0, scene->g_tex.bytes, st));
   PSDR_CUDA(cudaMemsetAsync(scene->g_emit.p, 0, scene->g_emit.bytes, st));

@@ -141,6 +141,7 @@ struct DevScene {
   const float4* nodes;
   const float4* leaf;
   double* grad_verts;      // (nvert, 3) or null
+  const unsigned char* vmask;  // (nvert): 1 = the caller wants this vertex's gradient
   int* err;                // device error word (bit 0: traversal stack overflow)
 };
 

@@ -86,6 +86,7 @@ struct psdr_scene {
   psdr::SortTmp sort_tmp;
   // fp64 gradient accumulators (allocated on first backward)
   psdr::DBuf g_verts, g_tex, g_emit;
+  psdr::DBuf vmask;  // per-vertex gradient mask (set from the gradient targets of a backward)
   std::vector<size_t> tex_grad_off;  // per object offset into g_tex (doubles), SIZE_MAX if none
   bool grads_ready = false;
   psdr::DevScene dev{};

@@ -87,6 +87,12 @@ PSDR_D void atomic_add3(double* p, float3 v) {
   atomicAdd(p + 2, (double)v.z);
 }
 
+// Vertex gradients are accumulated only for the vertices the caller asked for.
+PSDR_D bool vert_wanted(const DevScene& sc, int v) { return sc.grad_verts && (!sc.vmask || sc.vmask[v]); }
+PSDR_D void vert_add(const DevScene& sc, int v, float3 a) {
+  if (vert_wanted(sc, v)) atomic_add3(sc.grad_verts + 3 * (size_t)v, a);
+}
+
 // ------------------------------------------------------------------ camera kernel
 template <int MODE>
 __global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict__ scenes,
@@ -435,7 +441,7 @@ PSDR_D void add_vertex(const DevScene& sc, HotAcc& hot, int v, float3 a) {
       if (k == rel) { hot.g[3 * k] += a.x; hot.g[3 * k + 1] += a.y; hot.g[3 * k + 2] += a.z; }
     return;
   }
-  atomic_add3(sc.grad_verts + 3 * (size_t)v, a);
+  vert_add(sc, v, a);
 }
 
 // Adjoint of Scene::hit's surface attributes (point, flipped normal and tangent,
@@ -472,9 +478,10 @@ PSDR_D void surf_vertex_adj(const DevScene& sc, int tri, float b1, float b2, boo
 PSDR_D void scatter_surf(const DevScene& sc, HotAcc& hot, int tri, float b1, float b2, bool front,
                          const SurfAdj& a) {
   if (!sc.grad_verts) return;
+  const int4 tv = __ldg(sc.tri_v + tri);
+  if (!vert_wanted(sc, tv.x) && !vert_wanted(sc, tv.y) && !vert_wanted(sc, tv.z)) return;
   float3 g0, g1, g2;
   surf_vertex_adj(sc, tri, b1, b2, front, a, g0, g1, g2);
-  const int4 tv = __ldg(sc.tri_v + tri);
   add_vertex(sc, hot, tv.x, g0);
   add_vertex(sc, hot, tv.y, g1);
   add_vertex(sc, hot, tv.z, g2);
@@ -676,6 +683,10 @@ PSDR_D void scatter_surf_warp(const DevScene* scp, HotAcc& hot, int tri, float b
     return;
   }
   if (!scp->grad_verts) return;
+  {
+    const int4 tv = __ldg(scp->tri_v + tri);
+    if (!vert_wanted(*scp, tv.x) && !vert_wanted(*scp, tv.y) && !vert_wanted(*scp, tv.z)) return;
+  }
   float3 g0, g1, g2;
   surf_vertex_adj(*scp, tri, b1, b2, front, a, g0, g1, g2);
   float v[9] = {g0.x, g0.y, g0.z, g1.x, g1.y, g1.z, g2.x, g2.y, g2.z};
@@ -899,7 +910,7 @@ __global__ void __launch_bounds__(128, 3) k_adjoint(WF w, const DevScene* __rest
   const unsigned long long addr = __shfl_sync(0xffffffffu, (unsigned long long)flush_sc, __ffs(have) - 1);
   const DevScene* fsc = reinterpret_cast<const DevScene*>(addr);
   if ((threadIdx.x & 31) == 0) {
-    if (hot_nlv > 0 && fsc->grad_verts)
+    if (hot_nlv > 0 && vert_wanted(*fsc, hot_lv0))
       for (int k = 0; k < hot_nlv * 3; ++k)
         if (hot.g[k] != 0.f) atomicAdd(fsc->grad_verts + 3 * (size_t)hot_lv0 + k, (double)hot.g[k]);
     if (emit_hot && fsc->nlight > 0 && fsc->lights[0].grad_emit)
@@ -1074,13 +1085,13 @@ __global__ void __launch_bounds__(256) k_edge_final_unb(WF w, const DevScene* __
     if (!finite3(av)) continue;
     if (sc.grad_verts) {
       const int2 ev = __ldg(sc.edge_v + e);
-      atomic_add3(sc.grad_verts + 3 * (size_t)ev.x, av * (1.f - ss));
-      atomic_add3(sc.grad_verts + 3 * (size_t)ev.y, av * ss);
+      vert_add(sc, ev.x, av * (1.f - ss));
+      vert_add(sc, ev.y, av * ss);
       const int4 tv = __ldg(sc.tri_v + tri);
       const float3 ag = av * (-ratio);
-      atomic_add3(sc.grad_verts + 3 * (size_t)tv.x, ag * (1.f - hg.y - hg.z));
-      atomic_add3(sc.grad_verts + 3 * (size_t)tv.y, ag * hg.y);
-      atomic_add3(sc.grad_verts + 3 * (size_t)tv.z, ag * hg.z);
+      vert_add(sc, tv.x, ag * (1.f - hg.y - hg.z));
+      vert_add(sc, tv.y, ag * hg.y);
+      vert_add(sc, tv.z, ag * hg.z);
     }
     go -= av * (1.f - ratio);
   }
@@ -1154,8 +1165,8 @@ __global__ void __launch_bounds__(256) k_edge_final(WF w, const DevScene* __rest
       const float ss = a.y;
       if (sc.grad_verts) {
         const int2 ev = __ldg(sc.edge_v + e);
-        atomic_add3(sc.grad_verts + 3 * (size_t)ev.x, ax * (1.f - ss));
-        atomic_add3(sc.grad_verts + 3 * (size_t)ev.y, ax * ss);
+        vert_add(sc, ev.x, ax * (1.f - ss));
+        vert_add(sc, ev.y, ax * ss);
       }
       go += f3(nrm.x, nrm.y, -nrm.z) * K;
     }
@@ -1319,9 +1330,9 @@ __global__ void __launch_bounds__(256) k_border_final(WF w, const DevScene* __re
     if (!finite3(ag)) continue;
     if (sc.grad_verts) {
       const int4 tv = __ldg(sc.tri_v + tri);
-      atomic_add3(sc.grad_verts + 3 * (size_t)tv.x, ag * (1.f - h.y - h.z));
-      atomic_add3(sc.grad_verts + 3 * (size_t)tv.y, ag * h.y);
-      atomic_add3(sc.grad_verts + 3 * (size_t)tv.z, ag * h.z);
+      vert_add(sc, tv.x, ag * (1.f - h.y - h.z));
+      vert_add(sc, tv.y, ag * h.y);
+      vert_add(sc, tv.z, ag * h.z);
     }
     go -= ag;
   }
@@ -1472,18 +1483,18 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
       const float3 a = nsv * (wsum / (hpdf * (float)hc.ncells * (float)spp));
       if (!finite3(a) || wsum == 0.f) continue;
       const int2 evv = __ldg(sc.edge_v + e);
-      atomic_add3(sc.grad_verts + 3 * (size_t)evv.x, a * (1.f - sx));
-      atomic_add3(sc.grad_verts + 3 * (size_t)evv.y, a * sx);
+      vert_add(sc, evv.x, a * (1.f - sx));
+      vert_add(sc, evv.y, a * sx);
       const int4 td = __ldg(sc.tri_v + hd.tri);
       const float3 ad = a * (-1.f / lam);
-      atomic_add3(sc.grad_verts + 3 * (size_t)td.x, ad * (1.f - hd.b1 - hd.b2));
-      atomic_add3(sc.grad_verts + 3 * (size_t)td.y, ad * hd.b1);
-      atomic_add3(sc.grad_verts + 3 * (size_t)td.z, ad * hd.b2);
+      vert_add(sc, td.x, ad * (1.f - hd.b1 - hd.b2));
+      vert_add(sc, td.y, ad * hd.b1);
+      vert_add(sc, td.z, ad * hd.b2);
       const int4 tl = __ldg(sc.tri_v + ls.tri);
       const float3 al = a * (1.f / lam - 1.f);
-      atomic_add3(sc.grad_verts + 3 * (size_t)tl.x, al * (1.f - ls.su - ls.sv));
-      atomic_add3(sc.grad_verts + 3 * (size_t)tl.y, al * ls.su);
-      atomic_add3(sc.grad_verts + 3 * (size_t)tl.z, al * ls.sv);
+      vert_add(sc, tl.x, al * (1.f - ls.su - ls.sv));
+      vert_add(sc, tl.y, al * ls.su);
+      vert_add(sc, tl.z, al * ls.sv);
       continue;
     }
     int px, py;
@@ -1539,8 +1550,8 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
       if (det > kEps && det < 1.f - kEps) ad += cross(e2, e1) * (-(au * u + avv * vv) * inv);
       const float3 axb = (ad - db * dot(db, ad)) / norm(rb);
       const int2 evv = __ldg(sc.edge_v + e);
-      atomic_add3(sc.grad_verts + 3 * (size_t)evv.x, axb * (1.f - sx));
-      atomic_add3(sc.grad_verts + 3 * (size_t)evv.y, axb * sx);
+      vert_add(sc, evv.x, axb * (1.f - sx));
+      vert_add(sc, evv.y, axb * sx);
     }
   }
 }

@@ -549,6 +549,7 @@ void psdr_scene_alloc(psdr_scene* s) {
   d.nodes = s->nodes.as<float4>(); d.leaf = s->leaf.as<float4>();
   d.root = s->ntri > 1 ? 0 : ~0;  // a single triangle makes the root a leaf
   d.grad_verts = nullptr;
+  d.vmask = nullptr;
   d.err = s->err.as<int>();
 }
 
