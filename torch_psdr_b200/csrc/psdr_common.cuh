@@ -268,8 +268,11 @@ PSDR_D void cswap(float& ka, int& va, float& kb, int& vb) {
   }
 }
 
-PSDR_D HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, float tmax,
-                            float t_occ = -INFINITY) {
+// Not inlined: kernels that trace from several places (shadow-boundary samples trace
+// up to seven times) then hold one copy of the traversal loop, which keeps their code
+// inside the instruction cache.
+static __device__ __noinline__ HitRec trace_closest(const DevScene& sc, float3 o, float3 d, float tmin, float tmax,
+                                                    float t_occ = -INFINITY) {
   const RayPre rp = ray_pre(o, d);
   const float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
   const float3 oi = f3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
