@@ -210,7 +210,7 @@ inline V3<S> eval_direct(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], int& 
   S pdf_xw = is0.sqd * pdf_e * S(pdf_l) / dot(is0.n, dir);
   V3<S> Tb = boundary_term<S, AD>(is0.p, id0.p, xb, is0.n, id0.n, E) / pdf_xw;
   V3<S> Ts = detach(sc.emit[is0.light]);
-  V3<S> Td = detach(tex_at(sc, id0.obj, id0.u, id0.v) * inv_pi<S>());
+  V3<S> Td = detach(bsdf_eval(sc, id0, -cd));
   value = mul(mul(Tb, Ts), Td);
   valid = valid && finite3(value);
   return value;
@@ -300,7 +300,8 @@ inline V3<S> eval_primary_unb(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx
 // the radiance leaving x_d reaches the camera directly (x_d seen from the camera) and
 // through up to max_bounce-1 diffuse reflections: a chain of cosine-sampled bounces
 // from x_d connects each of its vertices to the camera; each bounce multiplies the
-// albedo (pi f_r against the cosine pdf), and the camera-visible end adds its camera
+// albedo for diffuse surfaces (pi f_r against the cosine pdf about the geometric
+// normal), and the camera-visible end adds its BSDF toward the camera and its camera
 // Jacobian. Returns the common derivative carrier d_eff . (w x e) and fills one
 // (pixel, RGB weight) pair per camera connection (in value mode too, for the guiding
 // masses: sum of |weight| |w x e| over the connections).
@@ -350,8 +351,10 @@ inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32
     const double k0 = -cos_y / (dby * dby) / (pdf_e * pdf_l * c.cam.H * c.cam.W);
     const double fxfy = raster_fxfy(c.cam);
     const V3<double> o = val3(c.cam_pos);
-    V3<double> T = mul(val3(tex_at(sc, id0.obj, id0.u, id0.v)) * (1.0 / M_PI), val3(sc.emit[is0.light]));
-    // camera connection of a vertex whose reflection hemisphere (its normal) faces the camera
+    // running throughput: the emission, times pi f_r at every vertex the chain leaves
+    V3<double> T = val3(sc.emit[is0.light]);
+    // camera connection of a vertex whose reflection hemisphere (its normal) faces the
+    // camera: T times its BSDF toward the camera times its camera Jacobian
     auto connect = [&](const Its<S>& v) {
       if (val(dot(v.n, c.cam_pos - v.p)) <= 0) return;
       bool vis = true;
@@ -361,8 +364,9 @@ inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32
       vis = vis && iv.valid && !iv.is_light && val(sqnorm(iv.p - v.p)) < double(R(1e-5));
       if (!vis || out.n >= kMaxChainOut) return;
       const double Jc = fxfy * val(cam_jacobian(c.cam, val3(v.p), val3(v.n), o));
+      const V3<double> fr = val3(bsdf_eval(sc, v, normalize(c.cam_pos - v.p)));
       out.pix[out.n] = ry * c.cam.W + rx;
-      out.w[out.n] = T * (k0 * Jc);
+      out.w[out.n] = mul(T, fr) * (k0 * Jc);
       ++out.n;
     };
     connect(id0);
@@ -372,7 +376,7 @@ inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32
       V3<S> wo = diffuse_sample_dir(v, ru, rv, ct);
       Its<S> nx = scene_hit<S, AD>(sc, v.p, wo, true);
       if (!nx.valid || nx.is_light) break;
-      T = mul(T, val3(tex_at(sc, nx.obj, nx.u, nx.v)));
+      T = mul(T, val3(bsdf_eval(sc, v, wo))) * M_PI;  // cosine sampling around Ng: G / pdf = pi
       connect(nx);
       v = nx;
     }

@@ -26,7 +26,7 @@ class OrcTexture(C.Structure):
 class OrcMesh(C.Structure):
     _fields_ = [("V", C.c_void_p), ("nV", C.c_int), ("F", C.c_void_p), ("nF", C.c_int),
                 ("uv", C.c_void_p), ("nUV", C.c_int), ("uvi", C.c_void_p), ("mat", C.c_int),
-                ("color", OrcTexture)]
+                ("color", OrcTexture), ("rough", OrcTexture), ("normal", OrcTexture)]
 
 
 class OrcLight(C.Structure):
@@ -78,14 +78,14 @@ class Marshal:
             F = np.ascontiguousarray(m.faces, np.int32)
             uv = None if m.uvs is None else np.ascontiguousarray(m.uvs, np.float32)
             uvi = None if m.uv_indices is None else np.ascontiguousarray(m.uv_indices, np.int32)
-            tex = np.ascontiguousarray(m.texture, np.float32)
-            self.keep += [V, F, uv, uvi, tex]
-            if tex.ndim == 1:
-                t = OrcTexture(0, 1, 1, tex.shape[0], _ptr(tex))
-            else:
-                t = OrcTexture(1, tex.shape[0], tex.shape[1], tex.shape[2], _ptr(tex))
+            t = self._tex(m.texture)
+            self.keep += [V, F, uv, uvi]
+            rough = getattr(m, "roughness", None)
+            normal = getattr(m, "normal", None)
+            mat = 0 if rough is None else 1
             self.meshes[i] = OrcMesh(_ptr(V), V.shape[0], _ptr(F), F.shape[0], _ptr(uv),
-                                     0 if uv is None else uv.shape[0], _ptr(uvi), 0, t)
+                                     0 if uv is None else uv.shape[0], _ptr(uvi), mat, t, self._tex(rough),
+                                     self._tex(normal))
         self.lights = (OrcLight * max(1, len(spec.lights)))()
         for i, l in enumerate(spec.lights):
             V = np.ascontiguousarray(l.vertices, np.float32)
@@ -98,6 +98,17 @@ class Marshal:
             self.cams[i] = OrcCamera((C.c_float * 3)(*map(float, c.look_from)), (C.c_float * 3)(*map(float, c.look_at)),
                                      (C.c_float * 3)(*map(float, c.up)), float(c.vfov), int(c.height), int(c.width))
         self.nm, self.nl, self.nc = len(spec.meshes), len(spec.lights), len(spec.cameras)
+
+    def _tex(self, a):
+        """OrcTexture of a constant (1-D) or uv map ((H, W) or (H, W, C)); None -> absent."""
+        if a is None:
+            return OrcTexture(-1, 0, 0, 0, None)
+        a = np.ascontiguousarray(a, np.float32)
+        self.keep.append(a)
+        if a.ndim == 1:
+            return OrcTexture(0, 1, 1, a.shape[0], _ptr(a))
+        c = 1 if a.ndim == 2 else a.shape[2]
+        return OrcTexture(1, a.shape[0], a.shape[1], c, _ptr(a))
 
     def args(self):
         return (C.byref(self.meshes), self.nm, C.byref(self.lights), self.nl, C.byref(self.cams), self.nc)

@@ -267,8 +267,10 @@ struct OrcMesh {
   const int* F; int nF;
   const float* uv; int nUV;   // may be null
   const int* uvi;             // may be null
-  int mat;                    // 0 DiffuseMaterial
+  int mat;                    // 0 DiffuseMaterial, 1 DiffuseBsdfMaterial
   OrcTexture color;
+  OrcTexture rough;           // DiffuseBsdfMaterial: 1 channel
+  OrcTexture normal;          // DiffuseBsdfMaterial: 3 channels, kind -1 = none
 };
 struct OrcLight {
   const float* V; int nV;
@@ -399,6 +401,10 @@ template <class S> struct Scene {
   int n_obj = 0;
   std::vector<int> obj_light;        // light index or -1
   std::vector<int> obj_tex_kind, obj_tex_h, obj_tex_w, obj_tex_off;
+  // DiffuseBsdfMaterial: roughness (1 channel) and normal map (3 channels) in `tex`
+  struct TexRef { int kind = -1, h = 0, w = 0, c = 0, off = -1; };
+  std::vector<int> obj_mat;
+  std::vector<TexRef> obj_rough, obj_nrm;
   std::vector<S> tex;                // all textures concatenated (caller row order, 3 channels)
   std::vector<int> obj_vert_off;
   // lights
@@ -637,6 +643,23 @@ inline Scene<S> build_scene(const OrcMesh* meshes, int nm, const OrcLight* light
     const auto& M = meshes[m];
     add_mesh(M.V, M.nV, M.F, M.nF, M.uv, M.uvi, -1, &M.color);
   }
+  // roughness and normal maps of DiffuseBsdfMaterial meshes, after every color texture
+  // (their derivative seeds follow the colors' in the same order)
+  auto add_tex = [&](const OrcTexture& t, int ch) {
+    typename Scene<S>::TexRef r;
+    if (t.kind < 0 || !t.data) return r;
+    r.kind = t.kind; r.h = t.kind ? t.h : 1; r.w = t.kind ? t.w : 1; r.c = ch; r.off = texoff;
+    int cnt = r.h * r.w * ch;
+    for (int e = 0; e < cnt; ++e) sc.tex.push_back(Seeder<S>::make(t.data[t.kind ? e : (t.c == 1 ? 0 : e % t.c)], seeds.tex, tex_elem + e));
+    texoff += cnt; tex_elem += cnt;
+    return r;
+  };
+  for (int m = 0; m < nm; ++m) {
+    const auto& M = meshes[m];
+    sc.obj_mat.push_back(M.mat);
+    sc.obj_rough.push_back(M.mat == 1 ? add_tex(M.rough, 1) : typename Scene<S>::TexRef{});
+    sc.obj_nrm.push_back(M.mat == 1 ? add_tex(M.normal, 3) : typename Scene<S>::TexRef{});
+  }
   std::vector<double> powers;
   for (int l = 0; l < nl; ++l) {
     const auto& Lg = lights[l];
@@ -646,6 +669,9 @@ inline Scene<S> build_scene(const OrcMesh* meshes, int nm, const OrcLight* light
     sc.light_tri0.push_back((int)sc.tris.size());
     sc.light_ntri.push_back(Lg.nF);
     add_mesh(Lg.V, Lg.nV, Lg.F, Lg.nF, nullptr, nullptr, l, nullptr);
+    sc.obj_mat.push_back(0);
+    sc.obj_rough.push_back(typename Scene<S>::TexRef{});
+    sc.obj_nrm.push_back(typename Scene<S>::TexRef{});
     std::vector<double> areas;
     double tot = 0;
     for (int f = 0; f < Lg.nF; ++f) { double a = double(R(val(sc.tris[sc.light_tri0[l] + f].area))); areas.push_back(a); tot += a; }
@@ -758,6 +784,62 @@ inline V3<S> diffuse_sample_dir(const Its<S>& its, typename Traits<S>::R ru, typ
   return normalize(its.t * S(uu) + B * S(vv) + its.n * S(ct));
 }
 
+// texture.h:24-31, 65-74: nearest texel of a roughness / normal texture (c channels).
+template <class S>
+inline V3<S> tex_fetch(const Scene<S>& sc, const typename Scene<S>::TexRef& t, double u, double v) {
+  if (t.kind < 0) return V3<S>();
+  int e = t.off;
+  if (t.kind == 1) e += tex_index(1, t.h, t.w, u, v, std::is_same<typename Traits<S>::R, float>::value) / 3 * t.c;
+  if (t.c == 1) return V3<S>(sc.tex[e], S(0), S(0));
+  return V3<S>(sc.tex[e], sc.tex[e + 1], sc.tex[e + 2]);
+}
+
+// diffuse_bsdf.cc:10-20 shading normal: the normal map in the (T, Ng x T, Ng) frame,
+// or the (flipped) geometric normal.
+template <class S>
+inline V3<S> shading_normal(const Scene<S>& sc, const Its<S>& its) {
+  if (sc.obj_mat[its.obj] != 1 || sc.obj_nrm[its.obj].kind < 0) return its.n;
+  V3<S> m = tex_fetch(sc, sc.obj_nrm[its.obj], its.u, its.v);
+  V3<S> B = cross(its.n, its.t);
+  return normalize(its.t * (m.x * S(2) - S(1)) + B * (m.y * S(2) - S(1)) + its.n * (m.z * S(2) - S(1)));
+}
+
+// BSDF value for outgoing direction L (the incoming one is its.wi): DiffuseMaterial
+// color / pi (diffuse_material.cc:33-37); DiffuseBsdfMaterial's rough-diffuse model
+// (diffuse_bsdf.cc:56-88) with its sign rule on t.
+template <class S>
+inline V3<S> bsdf_eval(const Scene<S>& sc, const Its<S>& its, const V3<S>& L) {
+  using R = typename Traits<S>::R;
+  V3<S> color = tex_at(sc, its.obj, its.u, its.v);
+  if (sc.obj_mat[its.obj] != 1) return color * inv_pi<S>();
+  V3<S> N = shading_normal(sc, its);
+  S sigma = tex_fetch(sc, sc.obj_rough[its.obj], its.u, its.v).x;
+  S a = S(R(1)) / (S(R(M_PI)) + S(R((3 * M_PI - 4) / 6)) * sigma);
+  S b = sigma * a;
+  S nl = dot(N, L), nv = dot(N, its.wi);
+  if (val(nl) < 0) nl = S(0);
+  if (val(nv) < 0) nv = S(0);
+  S t = dot(its.wi, L) - nl * nv;
+  if (val(t) > 0) t = (val(nl) >= val(nv) ? nl : nv) + S(R(1e-5));
+  return color * (a + b * t);
+}
+
+// Material sampling (diffuse_material.cc:3-30, diffuse_bsdf.cc:3-53): cosine-weighted
+// around the shading normal in the (T, Ng x T, N) frame; pdf = cos_theta / pi.
+template <class S>
+inline V3<S> material_sample_dir(const Scene<S>& sc, const Its<S>& its, typename Traits<S>::R ru,
+                                 typename Traits<S>::R rv, typename Traits<S>::R& cos_theta) {
+  using R = typename Traits<S>::R;
+  V3<S> N = shading_normal(sc, its);
+  V3<S> B = cross(its.n, its.t);
+  R ct = ru > 0 ? std::sqrt(ru) : R(0);
+  R st = (R(1) - ru) > 0 ? std::sqrt(R(1) - ru) : R(0);
+  R phi = rv * R(2 * M_PI);
+  R sp = std::sin(phi), cp = std::cos(phi);
+  cos_theta = ct;
+  return normalize(its.t * S(cp * st) + B * S(sp * st) + N * S(ct));
+}
+
 // path_integrator.cc:3-9 (power heuristic, n1/n2 sample counts)
 template <class R> inline R mis_w(R w1, R w2, R n1, R n2) {
   R a = (n1 * w1) * (n1 * w1), b = (n2 * w2) * (n2 * w2);
@@ -809,7 +891,7 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
       bool is_hit = il.valid && il.is_light && val(sqnorm(il.p - y)) < double(eps);
       if (!is_hit) continue;
       V3<S> emit = sc.emit[l];
-      V3<S> bsdf = tex_at(sc, its.obj, its.u, its.v) * inv_pi<S>();
+      V3<S> bsdf = bsdf_eval(sc, its, dir);
       S tmp = dot(il.n, -dir) / il.sqd;
       S G = dot(its.n, dir) * tmp;
       V3<S> value = mul(emit, bsdf) * (G * il.jac / S(pdf_light));
@@ -824,18 +906,20 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
       R rx = rng.next_float(valid), ry = rng.next_float(valid);
       if (!valid) continue;
       R ct;
-      V3<S> wo = diffuse_sample_dir(its, rx, ry, ct);
+      V3<S> wo = material_sample_dir(sc, its, rx, ry, ct);
       Its<S> il = scene_hit<S, AD>(sc, its.p, wo, true);
       bool is_hit = il.valid && il.is_light;
       if (!is_hit) continue;
       V3<S> emit = sc.emit[il.light];
-      V3<S> bsdf = tex_at(sc, its.obj, its.u, its.v) * inv_pi<S>();
       S tmp = dot(il.n, -wo) / il.sqd;
       S G = dot(its.n, wo) * tmp;
+      V3<S> Lb = wo;
       if (geo_dirs) {
         const V3<S> wg = normalize(il.p - its.p);
         G = dot(its.n, wg) * (dot(il.n, -wg) / il.sqd);
+        Lb = wg;
       }
+      V3<S> bsdf = bsdf_eval(sc, its, Lb);
       R pdf_bsdf = R(ct) * R(1.0 / M_PI) * R(val(tmp));
       V3<S> value = mul(emit, bsdf) * (G * il.jac / S(pdf_bsdf));
       R weight = R(1) / R(nB);
@@ -851,17 +935,19 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
     if (depth + 1 == D) break;
     if (!valid) break;
     R ct;
-    V3<S> wo = diffuse_sample_dir(its, rx, ry, ct);
+    V3<S> wo = material_sample_dir(sc, its, rx, ry, ct);
     Its<S> nx = scene_hit<S, AD>(sc, its.p, wo, true);
     valid = valid && nx.valid;
     if (!valid) break;
-    V3<S> bsdf = tex_at(sc, its.obj, its.u, its.v) * inv_pi<S>();
     S tmp = dot(nx.n, -wo) / nx.sqd;
     S G = dot(its.n, wo) * tmp;
+    V3<S> Lb = wo;
     if (geo_dirs) {
       const V3<S> wg = normalize(nx.p - its.p);
       G = dot(its.n, wg) * (dot(nx.n, -wg) / nx.sqd);
+      Lb = wg;
     }
+    V3<S> bsdf = bsdf_eval(sc, its, Lb);
     R pdf = R(ct) * R(1.0 / M_PI) * R(val(tmp));
     T = mul(T, bsdf) * (nx.jac * G / S(pdf));
     its = nx;

@@ -134,6 +134,8 @@ class MeshSpec:
     uvs: np.ndarray | None = None   # (T,2) float32
     uv_indices: np.ndarray | None = None  # (F,3) int32
     texture: np.ndarray = None      # (3,) constant or (H,W,3)
+    roughness: np.ndarray | None = None  # DiffuseBsdfMaterial: (1,) or (H,W)
+    normal: np.ndarray | None = None     # DiffuseBsdfMaterial normal map: (3,) or (H,W,3)
 
 
 @dataclass
