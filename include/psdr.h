@@ -126,6 +126,8 @@ typedef struct {
  * vertices: one buffer per mesh followed by one per light, each (V,3), may be NULL.
  * textures: one per mesh (same shape as its color texture), may be NULL.
  * emit: one (3,) buffer per light, may be NULL. camera_origin: one (3,) per camera.
+ * roughness / normal: one per mesh (same shape as a DiffuseBsdfMaterial's roughness
+ * and normal textures; ignored for other meshes), may be NULL.
  * With accumulate = 0 the outputs are overwritten, otherwise added to. */
 typedef struct {
   float** vertices;
@@ -133,6 +135,8 @@ typedef struct {
   float** emit;
   float** camera_origin;
   int32_t accumulate;
+  float** roughness;
+  float** normal;
 } psdr_grad_targets;
 
 /* ---------------------------------------------------------------- general */

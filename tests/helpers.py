@@ -10,7 +10,8 @@ from torch_psdr_b200 import synth
 
 def to_torch_scene(spec, requires_grad=(), device="cuda"):
     """Build a dr.Scene from a synth.SceneSpec. requires_grad: subset of
-    {"verts", "tex", "light_verts", "emit", "cam"}; returns (scene, dict of tensors)."""
+    {"verts", "tex", "rough", "normal", "light_verts", "emit", "cam"}; returns (scene, dict
+    of tensors). Meshes with a roughness get a DiffuseBsdfMaterial."""
     T = {}
     meshes = []
     for i, m in enumerate(spec.meshes):
@@ -21,7 +22,20 @@ def to_torch_scene(spec, requires_grad=(), device="cuda"):
         tex = torch.tensor(m.texture, dtype=torch.float32, device=device, requires_grad="tex" in requires_grad)
         T[f"verts{i}"] = v
         T[f"tex{i}"] = tex
-        meshes.append(dr.Mesh(v, uv, f, uvi, dr.DiffuseMaterial(tex)))
+        if getattr(m, "roughness", None) is None:
+            mat = dr.DiffuseMaterial(tex)
+        else:
+            r = np.asarray(m.roughness, np.float32)
+            r = r if r.ndim == 1 else r.reshape(r.shape[0], r.shape[1], 1)
+            rough = torch.tensor(r, device=device, requires_grad="rough" in requires_grad)
+            nrm = None
+            if m.normal is not None:
+                nrm = torch.tensor(m.normal, dtype=torch.float32, device=device,
+                                   requires_grad="normal" in requires_grad)
+            T[f"rough{i}"] = rough
+            T[f"normal{i}"] = nrm
+            mat = dr.DiffuseBsdfMaterial(tex, rough, nrm)
+        meshes.append(dr.Mesh(v, uv, f, uvi, mat))
     lights = []
     for j, l in enumerate(spec.lights):
         v = torch.tensor(l.vertices, dtype=torch.float32, device=device, requires_grad="light_verts" in requires_grad)

@@ -1,0 +1,64 @@
+"""The oracle's DiffuseBsdfMaterial (diffuse_bsdf.cc:3-88), CPU only.
+
+* roughness 0 without a normal map is the Lambertian DiffuseMaterial, bit for bit;
+* the roughness derivative of the interior term (forward-mode duals) against central
+  finite differences with common random numbers (the roughness does not move the
+  sampled directions, so the estimate is smooth in it);
+* a normal map moves the image.
+"""
+import numpy as np
+
+import orc
+from torch_psdr_b200 import synth
+from helpers import rel_mse
+
+
+def _spec(rough, normal=None, hw=24):
+    spec = synth.sphere_scene(level=2, tex_hw=16, height=hw, width=hw)
+    spec.meshes[0].roughness = rough
+    spec.meshes[0].normal = normal
+    spec.meshes[1].roughness = np.array([0.0], np.float32)
+    return spec
+
+
+KW = dict(spp_interior=4, max_bounce=3)
+
+
+def test_zero_roughness_is_lambertian():
+    a = orc.render(_spec(np.zeros((5, 5), np.float32)), precision=1, **KW)[0]
+    b = orc.render(synth.sphere_scene(level=2, tex_hw=16, height=24, width=24), precision=1, **KW)[0]
+    np.testing.assert_array_equal(a, b)
+
+
+def test_roughness_derivative_vs_finite_differences():
+    rng = np.random.default_rng(1)
+    rough = rng.uniform(0.2, 0.9, size=(5, 5)).astype(np.float32)
+    spec = _spec(rough)
+    g = rng.normal(size=(24, 24, 3))
+    ncol = sum(m.texture.size for m in spec.meshes)
+    st = np.zeros((ncol + rough.size + 1, 8))
+    st[ncol:ncol + rough.size, 0] = rng.normal(size=rough.size)
+    ad = orc.grad_dir(spec, [g], which=1, seed_tex=st, **KW)[0]
+    d = st[ncol:ncol + rough.size, 0].reshape(rough.shape)
+    h = 1e-3
+    ph = []
+    for sgn in (1, -1):
+        spec.meshes[0].roughness = (rough + sgn * h * d).astype(np.float32)
+        ph.append(float((g * orc.render(spec, precision=1, **KW)[0]).sum()))
+    fd = (ph[0] - ph[1]) / (2 * h)
+    print("roughness derivative AD", ad, "FD", fd)
+    assert abs(ad) > 0
+    assert abs(ad - fd) <= 2e-2 * abs(fd)
+
+
+def test_normal_map_changes_the_image():
+    rough = np.full((5, 5), 0.5, np.float32)
+    flat = np.concatenate([np.full((4, 4, 2), 0.5), np.ones((4, 4, 1))], -1).astype(np.float32)
+    tilt = flat.copy()
+    tilt[..., 0] = 0.7
+    a = orc.render(_spec(rough), precision=1, **KW)[0]
+    b = orc.render(_spec(rough, flat), precision=1, **KW)[0]
+    c = orc.render(_spec(rough, tilt), precision=1, **KW)[0]
+    # (0.5, 0.5, 1) maps to the geometric normal: the same sampled directions and values
+    assert rel_mse(b, a) < 1e-10
+    assert rel_mse(c, a) > 1e-4

@@ -63,7 +63,8 @@ class Config(C.Structure):
 class GradTargets(C.Structure):
     _fields_ = [("vertices", C.POINTER(C.c_void_p)), ("textures", C.POINTER(C.c_void_p)),
                 ("emit", C.POINTER(C.c_void_p)), ("camera_origin", C.POINTER(C.c_void_p)),
-                ("accumulate", C.c_int32)]
+                ("accumulate", C.c_int32), ("roughness", C.POINTER(C.c_void_p)),
+                ("normal", C.POINTER(C.c_void_p))]
 
 
 # Every symbol include/psdr.h declares, with its ctypes signature.

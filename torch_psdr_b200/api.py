@@ -159,13 +159,18 @@ class DiffuseMaterial(Material):
             tex = Texture(tex)
         assert tex.tex_type == "Constant3f" or tex.tex_type == "UV3f"
         self.texture = tex
+        self.roughness = None
+        self.normal = None
         self.merge_variables(tex.get_variables())
         self.mat_type = L.MAT_DIFFUSE
 
 
 class DiffuseBsdfMaterial(Material):
     def __init__(self, color, roughness, normal=None):
-        """Oren-Nayar style diffuse BSDF (torch_psdr.py:298-335). Not built on this path yet."""
+        """Lambertian / Oren-Nayar diffuse reflection (torch_psdr.py:298-335;
+        diffuse_bsdf.cc:3-88): color (3,) or (H,W,3), roughness (1,) or (H,W,1) (0 is
+        Lambertian), normal (3,) or (H,W,3) shading normals in the (tangent,
+        normal x tangent, normal) frame, 0.5 + n/2 per channel; None = geometric normal."""
         super().__init__()
         if isinstance(color, Tensor):
             color = Texture(color)
@@ -176,7 +181,14 @@ class DiffuseBsdfMaterial(Material):
         assert color.tex_type == "Constant3f" or color.tex_type == "UV3f"
         assert roughness.tex_type == "Constant1f" or roughness.tex_type == "UV1f"
         assert normal is None or normal.tex_type == "Constant3f" or normal.tex_type == "UV3f"
-        raise NotImplementedError("DiffuseBsdfMaterial is not available in torch_psdr_b200 yet")
+        self.texture = color
+        self.roughness = roughness
+        self.normal = normal
+        self.merge_variables(color.get_variables())
+        self.merge_variables(roughness.get_variables())
+        if normal is not None:
+            self.merge_variables(normal.get_variables())
+        self.mat_type = L.MAT_DIFFUSE_BSDF
 
 
 class PrincipledMaterial(Material):
@@ -221,8 +233,9 @@ class Mesh(VarContex):
             d.uvs, d.num_uvs, d.uv_indices = self.uv.data_ptr(), int(self.uv.shape[0]), self.uvi.data_ptr()
         d.material = self.material.mat_type
         d.color = self.material.texture._desc()
-        d.roughness = L.TextureDesc(L.TEX_NONE, 0, 0, 0, None)
-        d.normal = L.TextureDesc(L.TEX_NONE, 0, 0, 0, None)
+        none = L.TextureDesc(L.TEX_NONE, 0, 0, 0, None)
+        d.roughness = self.material.roughness._desc() if self.material.roughness is not None else none
+        d.normal = self.material.normal._desc() if self.material.normal is not None else none
         return d
 
 
@@ -346,6 +359,17 @@ def _grad_buf(param, internal):
     return None
 
 
+def _tex_grad(tex):
+    """Gradient buffer of an optional Texture (None when absent or not requiring grad)."""
+    return None if tex is None else _grad_buf(tex.tensor, tex.data)
+
+
+def _ptrs(bufs):
+    """ctypes pointer array of optional tensors (at least one entry)."""
+    P = C.c_void_p
+    return (P * max(1, len(bufs)))(*[None if t is None else t.data_ptr() for t in bufs])
+
+
 class PathIntegrator:
     def __init__(self, enable_light_visable: bool = False, n_pass: int = 1, spp_interior: int = 1,
                  max_bounce: int = 3, mis_light_samples: int = 1, mis_bsdf_samples: int = 1,
@@ -456,6 +480,8 @@ class PathIntegrator:
         vert_g = [_grad_buf(m.vertices, m.v) for m in scene.meshes] + [_grad_buf(lt.vertices, lt.v)
                                                                         for lt in scene.lights]
         tex_g = [_grad_buf(m.material.texture.tensor, m.material.texture.data) for m in scene.meshes]
+        rough_g = [_tex_grad(m.material.roughness) for m in scene.meshes]
+        nrm_g = [_tex_grad(m.material.normal) for m in scene.meshes]
         emit_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.lights]
         cam_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.cameras]
         P = C.c_void_p
@@ -463,7 +489,7 @@ class PathIntegrator:
         tp = (P * max(1, nm))(*[None if t is None else t.data_ptr() for t in tex_g])
         ep = (P * max(1, nl))(*[t.data_ptr() for t in emit_g])
         cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
-        tg = L.GradTargets(vp, tp, ep, cp, 0)
+        tg = L.GradTargets(vp, tp, ep, cp, 0, _ptrs(rough_g), _ptrs(nrm_g))
         dp = (P * len(dimgs))(*[d.data_ptr() for d in dimgs])
         cams = scene._camera_descs()
         L.check(self._lib.psdr_render_bwd(scene.handle, self._workspace(), cams, len(dimgs), C.byref(self.cfg), dp,
@@ -481,6 +507,10 @@ class PathIntegrator:
         for i, m in enumerate(scene.meshes):
             add(m.vertices, vert_g[i])
             add(m.material.texture.tensor, tex_g[i])
+            if rough_g[i] is not None:
+                add(m.material.roughness.tensor, rough_g[i])
+            if nrm_g[i] is not None:
+                add(m.material.normal.tensor, nrm_g[i])
         for j, lt in enumerate(scene.lights):
             add(lt.vertices, vert_g[nm + j])
             add(lt.emit, emit_g[j])
@@ -544,12 +574,12 @@ class BatchRender:
                                                                     for lt in sc.lights]
             tg = [_grad_buf(m.material.texture.tensor, m.material.texture.data) for m in sc.meshes]
             eg = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in sc.lights]
-            self.grads.append((vg, tg, eg))
-            vp = (P * max(1, len(vg)))(*[None if t is None else t.data_ptr() for t in vg])
-            tp = (P * max(1, len(tg)))(*[None if t is None else t.data_ptr() for t in tg])
-            ep = (P * max(1, len(eg)))(*[t.data_ptr() for t in eg])
-            self._keep += [vp, tp, ep]
-            targets.append(L.GradTargets(vp, tp, ep, cp, 0))
+            rg = [_tex_grad(m.material.roughness) for m in sc.meshes]
+            ng = [_tex_grad(m.material.normal) for m in sc.meshes]
+            self.grads.append((vg, tg, eg, rg, ng))
+            vp, tp, ep, rp, npp = _ptrs(vg), _ptrs(tg), _ptrs(eg), _ptrs(rg), _ptrs(ng)
+            self._keep += [vp, tp, ep, rp, npp]
+            targets.append(L.GradTargets(vp, tp, ep, cp, 0, rp, npp))
         self._keep.append(cp)
         tgt = (L.GradTargets * len(targets))(*targets)
         sh = (P * len(self.scenes))(*[s.handle for s in self.scenes])
@@ -603,11 +633,15 @@ class BatchRender:
             acc[id(t)] = g if id(t) not in acc else acc[id(t)] + g
 
         k = 0
-        for sc, (vg, tg, eg) in zip(self.scenes, self.grads):
+        for sc, (vg, tg, eg, rg, ng) in zip(self.scenes, self.grads):
             nm = len(sc.meshes)
             for i, m in enumerate(sc.meshes):
                 add(m.vertices, vg[i])
                 add(m.material.texture.tensor, tg[i])
+                if rg[i] is not None:
+                    add(m.material.roughness.tensor, rg[i])
+                if ng[i] is not None:
+                    add(m.material.normal.tensor, ng[i])
             for j, lt in enumerate(sc.lights):
                 add(lt.vertices, vg[nm + j])
                 add(lt.emit, eg[j])

@@ -24,7 +24,7 @@ struct psdr_batch {
   bool rebuild = true;
   psdr::SceneGradInfo gi;
   // gradient targets, deep-copied pointer arrays per scene
-  std::vector<std::vector<float*>> gv, gt, ge;
+  std::vector<std::vector<float*>> gv, gt, ge, gr, gn;
   std::vector<float*> gc;
   std::vector<int> gacc;
   std::vector<std::unique_ptr<psdr::DBuf>> vmasks;  // per-scene vertex-gradient masks of this batch's targets
@@ -141,8 +141,11 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
         PSDR_CUDA(cudaStreamSynchronize(st));
         ds[i].vmask = b->vmasks[i]->as<unsigned char>();
         std::vector<DevObj> ob = s->h_objs;
-        for (int o = 0; o < (int)s->meshes.size(); ++o)
+        for (int o = 0; o < (int)s->meshes.size(); ++o) {
           if (!(grads[i].textures && grads[i].textures[o])) ob[o].color.grad = nullptr;
+          if (!(grads[i].roughness && grads[i].roughness[o])) ob[o].rough.grad = nullptr;
+          if (!(grads[i].normal && grads[i].normal[o])) ob[o].normal.grad = nullptr;
+        }
         b->objs[i].reset(new psdr::DBuf());
         b->objs[i]->alloc(sizeof(DevObj) * std::max<size_t>(1, ob.size()), st);
         PSDR_CUDA(cudaMemcpyAsync(b->objs[i]->p, ob.data(), sizeof(DevObj) * std::max<size_t>(1, ob.size()),
@@ -154,9 +157,13 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     b->scenes_dev.alloc(sizeof(DevScene) * n_scenes, st);
     PSDR_CUDA(cudaMemcpyAsync(b->scenes_dev.p, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice, st));
     if (n_scenes == 1) b->gi = grad_info(scenes[0]);
+    for (int i = 0; i < n_scenes; ++i)
+      if (scenes[i]->has_bsdf) b->gi.bsdf = 1;
     if (b->backward) {
       b->gv.resize(n_scenes);
       b->gt.resize(n_scenes);
+      b->gr.resize(n_scenes);
+      b->gn.resize(n_scenes);
       b->ge.resize(n_scenes);
       b->gacc.resize(n_scenes);
       for (int i = 0; i < n_scenes; ++i) {
@@ -164,7 +171,11 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
         const psdr_grad_targets& g = grads[i];
         const int nm = (int)s->meshes.size();
         for (int o = 0; o < s->nobj; ++o) b->gv[i].push_back(g.vertices ? g.vertices[o] : nullptr);
-        for (int m = 0; m < nm; ++m) b->gt[i].push_back(g.textures ? g.textures[m] : nullptr);
+        for (int m = 0; m < nm; ++m) {
+          b->gt[i].push_back(g.textures ? g.textures[m] : nullptr);
+          b->gr[i].push_back(g.roughness && s->rough_grad_off[m] != SIZE_MAX ? g.roughness[m] : nullptr);
+          b->gn[i].push_back(g.normal && s->nrm_grad_off[m] != SIZE_MAX ? g.normal[m] : nullptr);
+        }
         for (int l = 0; l < s->nlight; ++l) b->ge[i].push_back(g.emit ? g.emit[l] : nullptr);
         b->gacc[i] = g.accumulate;
       }
@@ -238,6 +249,12 @@ PSDR_API psdr_status psdr_batch_backward(psdr_batch* b, void* stream) {
             const DevObj& ob = s->h_objs[m];
             grad_out(s->g_tex.as<double>() + s->tex_grad_off[m], b->gt[i][m],
                      (long long)ob.color.h * ob.color.w * ob.color.ch, b->gacc[i], st);
+            if (b->gr[i][m])
+              grad_out(s->g_tex.as<double>() + s->rough_grad_off[m], b->gr[i][m], (long long)ob.rough.h * ob.rough.w,
+                       b->gacc[i], st);
+            if (b->gn[i][m])
+              grad_out(s->g_tex.as<double>() + s->nrm_grad_off[m], b->gn[i][m],
+                       (long long)ob.normal.h * ob.normal.w * 3, b->gacc[i], st);
           }
           for (int l = 0; l < s->nlight; ++l)
             grad_out(s->g_emit.as<double>() + 3 * l, b->ge[i][l], 3, b->gacc[i], st);

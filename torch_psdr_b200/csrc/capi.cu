@@ -94,6 +94,7 @@ DevScene* dev_scene(psdr_scene* s) { return s->d_dev.as<DevScene>(); }
 
 SceneGradInfo grad_info(const psdr_scene* s) {
   SceneGradInfo gi;
+  gi.bsdf = s->has_bsdf ? 1 : 0;
   const int nm = (int)s->meshes.size();
   if (s->nlight == 1) {
     gi.emit_hot = 1;
@@ -133,7 +134,7 @@ extern "C" {
 
 const char* psdr_last_error(void) { return psdr::g_err.c_str(); }
 const char* psdr_version(void) { return "torch_psdr_b200 0.1.0 (sm_100a)"; }
-int32_t psdr_abi_version(void) { return 2; }
+int32_t psdr_abi_version(void) { return 3; }
 
 psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_scene** out) {
   API_BEGIN
@@ -173,7 +174,7 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
       ob.normal.kind = -1;
       if (is_mesh) {
         const psdr_mesh_desc& m = s->meshes[o];
-        PSDR_CHECK(m.material == PSDR_MAT_DIFFUSE, "only DiffuseMaterial is supported by this build");
+        PSDR_CHECK(m.material == PSDR_MAT_DIFFUSE || m.material == PSDR_MAT_DIFFUSE_BSDF, "bad material");
         check_tex(m.color, "color", false);
         PSDR_CHECK(m.color.channels == 3, "color texture must have 3 channels");
         PSDR_CHECK((m.uvs == nullptr) == (m.uv_indices == nullptr) || m.uvs == nullptr || m.uv_indices == nullptr,
@@ -190,6 +191,34 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
       s->h_objs.push_back(ob);
       voff += nV;
       toff += nF;
+    }
+    // DiffuseBsdfMaterial: roughness (1 channel) and optional normal map (3 channels);
+    // their accumulators follow every color texture, roughness then normal per mesh
+    auto tex_of = [](const psdr_texture_desc& t) {
+      return DevTex{t.kind, t.channels, t.kind == PSDR_TEX_UV ? t.height : 1, t.kind == PSDR_TEX_UV ? t.width : 1,
+                    t.data, nullptr};
+    };
+    for (int o = 0; o < nm; ++o) {
+      const psdr_mesh_desc& m = s->meshes[o];
+      DevObj& ob = s->h_objs[o];
+      size_t ro = SIZE_MAX, no = SIZE_MAX;
+      if (m.material == PSDR_MAT_DIFFUSE_BSDF) {
+        s->has_bsdf = true;
+        check_tex(m.roughness, "roughness", false);
+        PSDR_CHECK(m.roughness.channels == 1, "roughness texture must have 1 channel");
+        check_tex(m.normal, "normal", true);
+        PSDR_CHECK(m.normal.kind == PSDR_TEX_NONE || m.normal.channels == 3, "normal texture must have 3 channels");
+        ob.rough = tex_of(m.roughness);
+        ro = texoff;
+        texoff += (size_t)ob.rough.h * ob.rough.w;
+        if (m.normal.kind != PSDR_TEX_NONE) {
+          ob.normal = tex_of(m.normal);
+          no = texoff;
+          texoff += (size_t)ob.normal.h * ob.normal.w * 3;
+        }
+      }
+      s->rough_grad_off.push_back(ro);
+      s->nrm_grad_off.push_back(no);
     }
     s->nvert = voff;
     s->ntri = toff;
@@ -211,7 +240,11 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
     s->vmask.alloc(std::max<size_t>(1, s->nvert), st);
     PSDR_CUDA(cudaMemsetAsync(s->vmask.p, 1, std::max<size_t>(1, s->nvert), st));
     s->dev.vmask = s->vmask.as<unsigned char>();
-    for (int o = 0; o < nm; ++o) s->h_objs[o].color.grad = s->g_tex.as<double>() + s->tex_grad_off[o];
+    for (int o = 0; o < nm; ++o) {
+      s->h_objs[o].color.grad = s->g_tex.as<double>() + s->tex_grad_off[o];
+      if (s->rough_grad_off[o] != SIZE_MAX) s->h_objs[o].rough.grad = s->g_tex.as<double>() + s->rough_grad_off[o];
+      if (s->nrm_grad_off[o] != SIZE_MAX) s->h_objs[o].normal.grad = s->g_tex.as<double>() + s->nrm_grad_off[o];
+    }
     for (int l = 0; l < nl; ++l) s->h_lights[l].grad_emit = s->g_emit.as<double>() + 3 * l;
     s->upload_tables();
     scene_build_geometry(s, s->stream);
@@ -407,8 +440,11 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
     PSDR_CUDA(cudaMemcpyAsync(scene->vmask.p, m.data(), m.size(), cudaMemcpyHostToDevice, st));
     // and only the textures asked for: their accumulators stay in the object table
     std::vector<DevObj> objs = scene->h_objs;
-    for (int o = 0; o < (int)scene->meshes.size(); ++o)
+    for (int o = 0; o < (int)scene->meshes.size(); ++o) {
       if (!(grads->textures && grads->textures[o])) objs[o].color.grad = nullptr;
+      if (!(grads->roughness && grads->roughness[o])) objs[o].rough.grad = nullptr;
+      if (!(grads->normal && grads->normal[o])) objs[o].normal.grad = nullptr;
+    }
     PSDR_CUDA(cudaMemcpyAsync(scene->objs.p, objs.data(), sizeof(DevObj) * std::max<size_t>(1, objs.size()),
                               cudaMemcpyHostToDevice, st));
   }
@@ -434,6 +470,16 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
       const DevObj& ob = scene->h_objs[o];
       grad_out(scene->g_tex.as<double>() + scene->tex_grad_off[o], grads->textures[o],
                (long long)ob.color.h * ob.color.w * ob.color.ch, grads->accumulate, st);
+    }
+    if (o < nm && grads->roughness && grads->roughness[o] && scene->rough_grad_off[o] != SIZE_MAX) {
+      const DevObj& ob = scene->h_objs[o];
+      grad_out(scene->g_tex.as<double>() + scene->rough_grad_off[o], grads->roughness[o],
+               (long long)ob.rough.h * ob.rough.w, grads->accumulate, st);
+    }
+    if (o < nm && grads->normal && grads->normal[o] && scene->nrm_grad_off[o] != SIZE_MAX) {
+      const DevObj& ob = scene->h_objs[o];
+      grad_out(scene->g_tex.as<double>() + scene->nrm_grad_off[o], grads->normal[o],
+               (long long)ob.normal.h * ob.normal.w * 3, grads->accumulate, st);
     }
   }
   for (int l = 0; l < scene->nlight; ++l)

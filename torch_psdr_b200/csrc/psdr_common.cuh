@@ -436,6 +436,7 @@ PSDR_D bool trace_step(const DevScene& sc, TraceState& s, int* stack) {
 // barycentrics; the normal and tangent face the incoming ray (is_front flip).
 struct Surf {
   float3 p, n, t;
+  float3 wi;     // unit direction toward the ray origin (the incoming direction V)
   float u, v;
   float area;
   float sqd;     // squared distance to the ray origin
@@ -462,6 +463,7 @@ PSDR_D Surf make_surf(const DevScene& sc, int tri, float b1, float b2, float3 or
   const float3 wun = s.p - org;
   s.sqd = sqnorm(wun);
   const float3 wi = -normalize(wun);
+  s.wi = wi;
   const float3 n = xyz(q3), t = xyz(q4);
   s.front = dot(wi, n) > 0.0f;
   s.n = s.front ? n : -n;
@@ -499,6 +501,63 @@ PSDR_D float3 diffuse_dir(float3 N, float3 T, float ru, float rv, float& cos_the
   sincosf(rv * k2Pi, &sphi, &cphi);
   const float uu = cphi * sin_theta, vv = sphi * sin_theta;
   return normalize(T * uu + B * vv + N * cos_theta);
+}
+
+// ------------------------------------------------------------------ materials
+constexpr int kMatDiffuseBsdf = 1;                      // PSDR_MAT_DIFFUSE_BSDF
+constexpr float kOrenC = (3.0f * kPi - 4.0f) / 6.0f;    // diffuse_bsdf.cc:36
+
+// Shading normal (diffuse_bsdf.cc:10-20): DiffuseBsdfMaterial's normal map in the
+// (T, Ng x T, Ng) frame, else the flipped geometric normal; m = 2 texel - 1.
+PSDR_D float3 shading_normal(const DevObj& ob, const Surf& x, float3& m, bool& mapped) {
+  mapped = ob.mat == kMatDiffuseBsdf && ob.normal.kind >= 0;
+  m = f3(0.f, 0.f, 1.f);
+  if (!mapped) return x.n;
+  const float3 tx = tex_rgb(ob.normal, texel_offset(ob.normal, x.u, x.v));
+  m = f3(tx.x * 2.f - 1.f, tx.y * 2.f - 1.f, tx.z * 2.f - 1.f);
+  const float3 B = cross(x.n, x.t);
+  return normalize(x.t * m.x + B * m.y + x.n * m.z);
+}
+
+// Roughness of a DiffuseBsdfMaterial point (1-channel texture).
+PSDR_D float material_sigma(const DevObj& ob, const Surf& x) {
+  if (ob.mat != kMatDiffuseBsdf) return 0.f;
+  return tex_rgb(ob.rough, texel_offset(ob.rough, x.u, x.v)).x;
+}
+
+// BSDF value toward L for the incoming direction V: DiffuseMaterial color / pi
+// (diffuse_material.cc:33-37); DiffuseBsdfMaterial's rough-diffuse model with its rule
+// on t (diffuse_bsdf.cc:56-88).
+PSDR_D float3 bsdf_value(const DevObj& ob, float3 color, float sigma, float3 N, float3 V, float3 L) {
+  if (ob.mat != kMatDiffuseBsdf) return color * kInvPi;
+  const float a = 1.0f / (kPi + kOrenC * sigma), b = sigma * a;
+  const float nl = fmaxf(dot(N, L), 0.f), nv = fmaxf(dot(N, V), 0.f);
+  float t = dot(V, L) - nl * nv;
+  if (t > 0.f) t = fmaxf(nl, nv) + kEps;
+  return color * (a + b * t);
+}
+
+// Material sampling (diffuse_material.cc:3-30, diffuse_bsdf.cc:3-53): cosine-weighted
+// about the shading normal N in the (T, Ng x T, N) frame; pdf = cos_theta / pi.
+PSDR_D float3 material_dir(const Surf& x, float3 N, float ru, float rv, float& cos_theta, float& sin_theta,
+                           float& sphi, float& cphi) {
+  const float3 B = cross(x.n, x.t);
+  cos_theta = ru > 0.f ? sqrtf(ru) : 0.f;
+  sin_theta = (1.0f - ru) > 0.f ? sqrtf(1.0f - ru) : 0.f;
+  sincosf(rv * k2Pi, &sphi, &cphi);
+  const float uu = cphi * sin_theta, vv = sphi * sin_theta;
+  return normalize(x.t * uu + B * vv + N * cos_theta);
+}
+
+// BSDF of surface point x toward L (incoming direction x.wi), any material.
+PSDR_D float3 surf_bsdf(const DevScene& sc, const Surf& x, float3 L) {
+  const DevObj& ob = sc.objs[x.obj];
+  const float3 color = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v));
+  if (ob.mat != kMatDiffuseBsdf) return color * kInvPi;
+  float3 m;
+  bool mapped;
+  const float3 N = shading_normal(ob, x, m, mapped);
+  return bsdf_value(ob, color, material_sigma(ob, x), N, x.wi, L);
 }
 
 PSDR_D float mis_power(float w1, float w2, float n1, float n2) {

@@ -88,6 +88,9 @@ struct psdr_scene {
   psdr::DBuf g_verts, g_tex, g_emit;
   psdr::DBuf vmask;  // per-vertex gradient mask (set from the gradient targets of a backward)
   std::vector<size_t> tex_grad_off;  // per object offset into g_tex (doubles), SIZE_MAX if none
+  // DiffuseBsdfMaterial roughness / normal-map accumulators (after every color texture)
+  std::vector<size_t> rough_grad_off, nrm_grad_off;
+  bool has_bsdf = false;
   bool grads_ready = false;
   psdr::DevScene dev{};
   psdr::DBuf d_dev;  // device copy of `dev`

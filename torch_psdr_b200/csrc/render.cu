@@ -173,6 +173,9 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
     if (!go) continue;
     w.qs[k] = s;
     Rng rng{w.rs[s], w.ri[s]};
+    float3 mm;
+    bool mapped;
+    const float3 Ns = shading_normal(sc->objs[x.obj], x, mm, mapped);
     // rays are stored type-major (slot r * cap + k): a warp of k_trace then traces
     // rays of one kind from neighbouring paths
     const size_t cs = (size_t)w.cap;
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
     for (int j = 0; j < w.nB; ++j) {
       const float rx = rng.next_float(), ry = rng.next_float();
       float ct, st, sp, cp;
-      const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+      const float3 wo = material_dir(x, Ns, rx, ry, ct, st, sp, cp);
       const size_t slot = (w.nL + j) * cs + k;
       w.ro[slot] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
       w.rd[slot] = make_float4(wo.x, wo.y, wo.z, 0.f);
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
       const float rx = rng.next_float(), ry = rng.next_float();
       if (!last) {
         float ct, st, sp, cp;
-        const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+        const float3 wo = material_dir(x, Ns, rx, ry, ct, st, sp, cp);
         const size_t slot = (w.nL + w.nB) * cs + k;
         w.ro[slot] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
         w.rd[slot] = make_float4(wo.x, wo.y, wo.z, 0.f);
@@ -297,7 +300,19 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
       const float4 c = w.cur[s];
       const Surf x = make_surf(sc, __float_as_int(c.x), c.y, c.z, xyz(w.org[s]));
       const DevObj& ob = sc.objs[x.obj];
-      const float3 bsdf = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v)) * kInvPi;
+      const float3 color = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v));
+      const float3 bsdf = color * kInvPi;
+      // DiffuseBsdfMaterial: the value depends on the outgoing direction
+      const bool rough = ob.mat == kMatDiffuseBsdf;
+      float3 Ns = x.n;
+      float sigma = 0.f;
+      if (rough) {
+        float3 mm;
+        bool mapped;
+        Ns = shading_normal(ob, x, mm, mapped);
+        sigma = material_sigma(ob, x);
+      }
+      auto fr = [&](float3 L) { return rough ? bsdf_value(ob, color, sigma, Ns, x.wi, L) : bsdf; };
       float3 C = f3(0.f, 0.f, 0.f), beta = f3(0.f, 0.f, 0.f);
       for (int i = 0; i < w.nL; ++i) {
         const float4 h = w.hit[i * cs + k];
@@ -313,7 +328,8 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
         const float pdf_l = aux.w;
         float wgt = 1.0f / fL;
         if (w.nB > 0) wgt *= mis_power(pdf_l, dot(x.n, dir) * kInvPi * tmp, fL, fB);
-        C += f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z) * (G / pdf_l * wgt);
+        const float3 f = fr(dir);
+        C += f3(Lt.emit[0] * f.x, Lt.emit[1] * f.y, Lt.emit[2] * f.z) * (G / pdf_l * wgt);
       }
       for (int j = 0; j < w.nB; ++j) {
         const size_t slot = (w.nL + j) * cs + k;
@@ -330,7 +346,8 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
         const float pdf_b = ct * kInvPi * tmp;
         float wgt = 1.0f / fB;
         if (w.nL > 0) wgt *= mis_power(pdf_b, __ldg(sc.light_pmf + q.light) * Lt.inv_area, fB, fL);
-        C += f3(Lt.emit[0] * bsdf.x, Lt.emit[1] * bsdf.y, Lt.emit[2] * bsdf.z) * (G / pdf_b * wgt);
+        const float3 f = fr(wo);
+        C += f3(Lt.emit[0] * f.x, Lt.emit[1] * f.y, Lt.emit[2] * f.z) * (G / pdf_b * wgt);
       }
       float4 hn = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f);
       if (!last) {
@@ -344,7 +361,7 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
           const float tmp = dot(nx.n, -wo) / nx.sqd;
           const float G = dot(x.n, wo) * tmp;
           const float pdf = ct * kInvPi * tmp;
-          beta = bsdf * (G / pdf);
+          beta = fr(wo) * (G / pdf);
           w.cur[s] = hn;
           w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
           cont = true;
@@ -516,6 +533,106 @@ PSDR_D void dir_adj(float3 adj_wo, float3 wo, float3 N, float3 T, float u, float
   ax.n += am * ct + cross(T, aB);
 }
 
+// ------------------------------------------------------------------ material adjoints
+// Material state of a shaded vertex (DiffuseBsdfMaterial, diffuse_bsdf.cc:3-88).
+struct MatPt {
+  float3 color;  // color texel
+  float3 N;      // shading normal
+  float3 m;      // normal-map vector 2 texel - 1
+  float sigma;   // roughness texel
+  bool rough, mapped;
+};
+PSDR_D MatPt mat_point(const DevObj& ob, const Surf& x) {
+  MatPt mp;
+  mp.color = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v));
+  mp.rough = ob.mat == kMatDiffuseBsdf;
+  mp.N = shading_normal(ob, x, mp.m, mp.mapped);
+  mp.sigma = material_sigma(ob, x);
+  return mp;
+}
+
+// Adjoints gathered at a vertex before they are folded into the surface and textures.
+struct MatAdj {
+  float3 color, N, V;
+  float sigma;
+};
+PSDR_D MatAdj zero_mat_adj() {
+  MatAdj a;
+  a.color = a.N = a.V = f3(0.f, 0.f, 0.f);
+  a.sigma = 0.f;
+  return a;
+}
+
+// f = bsdf_value(color, sigma, N, V, L): returns f and accumulates the adjoints of
+// color, sigma, N, V (ma) and L (adj_L) for the adjoint adj_f of f.
+PSDR_D float3 bsdf_adj(const MatPt& mp, float3 V, float3 L, float3 adj_f, MatAdj& ma, float3& adj_L) {
+  if (!mp.rough) {
+    ma.color += adj_f * kInvPi;
+    return mp.color * kInvPi;
+  }
+  const float a = 1.0f / (kPi + kOrenC * mp.sigma), b = mp.sigma * a;
+  const float nlr = dot(mp.N, L), nvr = dot(mp.N, V);
+  const float nl = fmaxf(nlr, 0.f), nv = fmaxf(nvr, 0.f);
+  const float t0 = dot(V, L) - nl * nv;
+  const float t = t0 > 0.f ? fmaxf(nl, nv) + kEps : t0;
+  const float g = a + b * t;
+  ma.color += adj_f * g;
+  const float adj_g = dot(adj_f, mp.color);
+  const float da = -kOrenC * a * a, db = a + mp.sigma * da;
+  ma.sigma += adj_g * (da + db * t);
+  const float adj_t = adj_g * b;
+  float adj_nl = 0.f, adj_nv = 0.f;
+  if (t0 > 0.f) {
+    if (nl >= nv) adj_nl = adj_t;
+    else adj_nv = adj_t;
+  } else {
+    adj_L += V * adj_t;
+    ma.V += L * adj_t;
+    adj_nl = -adj_t * nv;
+    adj_nv = -adj_t * nl;
+  }
+  if (nlr >= 0.f) { ma.N += L * adj_nl; adj_L += mp.N * adj_nl; }
+  if (nvr >= 0.f) { ma.N += V * adj_nv; ma.V += mp.N * adj_nv; }
+  return mp.color * g;
+}
+
+// Adjoint of a sampled direction wo = normalize(u T + v B + ct N), B = Ng x T, about
+// the shading normal N (its adjoint goes to adjN).
+PSDR_D void dir_adj_mat(float3 adj_wo, float3 wo, const Surf& x, float3 N, float u, float v, float ct, SurfAdj& ax,
+                        float3& adjN) {
+  const float3 B = cross(x.n, x.t);
+  const float3 m = x.t * u + B * v + N * ct;
+  const float3 am = (adj_wo - wo * dot(wo, adj_wo)) / norm(m);
+  const float3 aB = am * v;
+  ax.t += am * u + cross(aB, x.n);
+  ax.n += cross(x.t, aB);
+  adjN += am * ct;
+}
+
+// Folds a vertex's material adjoints into its surface adjoint (shading normal through
+// the normal map's frame, incoming direction into the point and the ray origin) and
+// scatters the roughness and normal-map texel adjoints. Returns the ray origin's adjoint.
+PSDR_D float3 mat_finalize(const DevObj& ob, const Surf& x, const MatPt& mp, const MatAdj& ma, SurfAdj& ax) {
+  if (mp.mapped) {
+    const float3 B = cross(x.n, x.t);
+    const float3 nn = x.t * mp.m.x + B * mp.m.y + x.n * mp.m.z;
+    const float3 am = (ma.N - mp.N * dot(mp.N, ma.N)) / norm(nn);
+    const float3 aB = am * mp.m.y;
+    ax.t += am * mp.m.x + cross(aB, x.n);
+    ax.n += am * mp.m.z + cross(x.t, aB);
+    if (ob.normal.grad)
+      atomic_add3(ob.normal.grad + texel_offset(ob.normal, x.u, x.v), f3(dot(am, x.t), dot(am, B), dot(am, x.n)) * 2.f);
+  } else {
+    ax.n += ma.N;
+  }
+  if (mp.rough && ob.rough.grad && ma.sigma != 0.f)
+    atomicAdd(ob.rough.grad + texel_offset(ob.rough, x.u, x.v), (double)ma.sigma);
+  // V = -normalize(x.p - o)
+  const float3 au = (ma.V - x.wi * dot(x.wi, ma.V)) * (-1.f / sqrtf(x.sqd));
+  ax.p += au;
+  return -au;
+}
+
 struct DepthVals {
   float3 C, beta;
   bool has_next;
@@ -524,13 +641,15 @@ struct DepthVals {
 // Adjoint of a BSDF-sampled segment's G in the unbiased estimator: the direction is
 // that of the segment's end points, w = normalize(q - x), so it back-propagates into
 // both points instead of the sampling frame.
-PSDR_D void geom_adj_points(float adjG, const Surf& x, const Surf& q, SurfAdj& ax, SurfAdj& aq) {
+PSDR_D void geom_adj_points(float adjG, const Surf& x, const Surf& q, SurfAdj& ax, SurfAdj& aq,
+                            float3 adj_w_extra = f3(0.f, 0.f, 0.f)) {
   const float3 rv = q.p - x.p;
   const float rn = norm(rv);
   const float3 wg = rv / rn;
   const float G = dot(x.n, wg) * (dot(q.n, -wg) / q.sqd);
   float3 adj_w;
   geom_adj(adjG, x.n, q.n, wg, x.p, q.p, q.sqd, G, ax, aq, adj_w);
+  adj_w += adj_w_extra;
   const float3 ar = (adj_w - wg * dot(wg, adj_w)) / rn;
   aq.p += ar;
   ax.p -= ar;
@@ -543,9 +662,13 @@ PSDR_D void geom_adj_points(float adjG, const Surf& x, const Surf& q, SurfAdj& a
 // UNB (unbiased estimator): BSDF-sampled segments differentiate G through their end
 // points (geom_adj_points); the reference differentiates it through the sampled
 // direction's frame.
-template <bool ADJ, bool UNB = false>
+// BSDF (DiffuseBsdfMaterial in the scene): the BSDF value depends on the shading normal
+// (mp), the incoming direction x.wi and the outgoing direction; their adjoints and the
+// color / roughness adjoints gather in ma (adj_tex is unused).
+template <bool ADJ, bool UNB = false, bool BSDF = false>
 PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng& rng, const float4* rec, bool last,
-                            float3 adjC, float3 adjB, SurfAdj& ax, SurfAdj& carry, HotAcc& hot, float3& adj_tex) {
+                            float3 adjC, float3 adjB, SurfAdj& ax, SurfAdj& carry, HotAcc& hot, float3& adj_tex,
+                            const MatPt* mp = nullptr, MatAdj* ma = nullptr) {
   DepthVals out;
   out.C = f3(0.f, 0.f, 0.f);
   out.beta = f3(0.f, 0.f, 0.f);
@@ -554,6 +677,8 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
   const DevObj& ob = sc.objs[x.obj];
   const float3 tex = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v));
   const float3 bsdf = tex * kInvPi;
+  // DiffuseBsdfMaterial (BSDF): sampling about the shading normal, the value per direction
+  const float3 Ns = BSDF ? mp->N : x.n;
   for (int i = 0; i < w.nL; ++i) {
     const float rx = rng.next_float(), ry = rng.next_float();
     const LightSample ls = sample_light(sc, rx, ry);
@@ -571,20 +696,25 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
     float wgt = 1.0f / fL;
     if (w.nB > 0) wgt *= mis_power(ls.pdf, dot(x.n, dir) * kInvPi * tmp, fL, fB);
     const float k = G / ls.pdf * wgt;
-    const float3 eb = mul(emit, bsdf);
     if (!ADJ) {
-      out.C += eb * k;
+      const float3 f = BSDF ? bsdf_value(ob, mp->color, mp->sigma, Ns, x.wi, dir) : bsdf;
+      out.C += mul(emit, f) * k;
     } else {
       const float3 av = adjC * wgt;
       const float s_ = G / ls.pdf;
-      const float3 ae = mul(av, bsdf) * s_;
+      float3 adjL = f3(0.f, 0.f, 0.f);
+      float3 f = bsdf;
+      if (BSDF) f = bsdf_adj(*mp, x.wi, dir, mul(av, emit) * s_, *ma, adjL);
+      else adj_tex += mul(av, emit) * (s_ * kInvPi);
+      const float3 eb = mul(emit, f);
+      const float3 ae = mul(av, f) * s_;
       add_emit(hot, sc.lights[ls.light].grad_emit, ae);
-      adj_tex += mul(av, emit) * (s_ * kInvPi);
       const float adj_gam = dot(av, eb) / ls.pdf;
       SurfAdj aq = zero_adj();
       aq.area = adj_gam * G / q.area;
       float3 adj_dir;
       geom_adj(adj_gam, x.n, q.n, dir, x.p, q.p, q.sqd, G, ax, aq, adj_dir);
+      if (BSDF) adj_dir += adjL;
       const float3 ar = (adj_dir - dir * dot(dir, adj_dir)) / norm(rv);
       ax.p -= ar;
       // light sample point y = p0 + (p1-p0) su + (p2-p0) sv
@@ -600,7 +730,7 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
   for (int j = 0; j < w.nB; ++j) {
     const float rx = rng.next_float(), ry = rng.next_float();
     float ct, st, sp, cp;
-    const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+    const float3 wo = BSDF ? material_dir(x, Ns, rx, ry, ct, st, sp, cp) : diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
     const float4 h = rec[w.nL + j];
     const int tri = __float_as_int(h.x);
     if (tri < 0) continue;
@@ -613,24 +743,30 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
     const float pdf_b = ct * kInvPi * tmp;
     float wgt = 1.0f / fB;
     if (w.nL > 0) wgt *= mis_power(pdf_b, __ldg(sc.light_pmf + q.light) * Lt.inv_area, fB, fL);
-    const float3 eb = mul(emit, bsdf);
     if (!ADJ) {
-      out.C += eb * (G / pdf_b * wgt);
+      const float3 f = BSDF ? bsdf_value(ob, mp->color, mp->sigma, Ns, x.wi, wo) : bsdf;
+      out.C += mul(emit, f) * (G / pdf_b * wgt);
     } else {
       const float3 av = adjC * wgt;
       const float s_ = G / pdf_b;
-      const float3 ae = mul(av, bsdf) * s_;
+      // the BSDF's outgoing direction: the sampled one, or the segment's (unbiased)
+      float3 adjL = f3(0.f, 0.f, 0.f);
+      float3 f = bsdf;
+      if (BSDF) f = bsdf_adj(*mp, x.wi, UNB ? normalize(q.p - x.p) : wo, mul(av, emit) * s_, *ma, adjL);
+      else adj_tex += mul(av, emit) * (s_ * kInvPi);
+      const float3 eb = mul(emit, f);
+      const float3 ae = mul(av, f) * s_;
       add_emit(hot, Lt.grad_emit, ae);
-      adj_tex += mul(av, emit) * (s_ * kInvPi);
       const float adj_gam = dot(av, eb) / pdf_b;
       SurfAdj aq = zero_adj();
       aq.area = adj_gam * G / q.area;
       if (UNB) {
-        geom_adj_points(adj_gam, x, q, ax, aq);
+        geom_adj_points(adj_gam, x, q, ax, aq, adjL);
       } else {
         float3 adj_wo;
         geom_adj(adj_gam, x.n, q.n, wo, x.p, q.p, q.sqd, G, ax, aq, adj_wo);
-        dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+        if (BSDF) dir_adj_mat(adj_wo + adjL, wo, x, Ns, cp * st, sp * st, ct, ax, ma->N);
+        else dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
       }
       scatter_surf(sc, hot, tri, h.y, h.z, q.front, aq);
     }
@@ -639,7 +775,8 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
     const float rx = rng.next_float(), ry = rng.next_float();
     if (!last) {
       float ct, st, sp, cp;
-      const float3 wo = diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
+      const float3 wo =
+          BSDF ? material_dir(x, Ns, rx, ry, ct, st, sp, cp) : diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
       const float4 h = rec[w.nL + w.nB];
       const int tri = __float_as_int(h.x);
       if (tri >= 0) {
@@ -650,18 +787,22 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
         const float pdf = ct * kInvPi * tmp;
         const float s_ = G / pdf;
         if (!ADJ) {
-          out.beta = bsdf * s_;
+          out.beta = (BSDF ? bsdf_value(ob, mp->color, mp->sigma, Ns, x.wi, wo) : bsdf) * s_;
         } else {
-          adj_tex += adjB * (s_ * kInvPi);
-          const float adj_gam = dot(adjB, bsdf) / pdf;
+          float3 adjL = f3(0.f, 0.f, 0.f);
+          float3 f = bsdf;
+          if (BSDF) f = bsdf_adj(*mp, x.wi, UNB ? normalize(nx.p - x.p) : wo, adjB * s_, *ma, adjL);
+          else adj_tex += adjB * (s_ * kInvPi);
+          const float adj_gam = dot(adjB, f) / pdf;
           carry = zero_adj();
           carry.area = adj_gam * G / nx.area;
           if (UNB) {
-            geom_adj_points(adj_gam, x, nx, ax, carry);
+            geom_adj_points(adj_gam, x, nx, ax, carry, adjL);
           } else {
             float3 adj_wo;
             geom_adj(adj_gam, x.n, nx.n, wo, x.p, nx.p, nx.sqd, G, ax, carry, adj_wo);
-            dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
+            if (BSDF) dir_adj_mat(adj_wo + adjL, wo, x, Ns, cp * st, sp * st, ct, ax, ma->N);
+            else dir_adj(adj_wo, wo, x.n, x.t, cp * st, sp * st, ct, ax);
           }
         }
       }
@@ -790,8 +931,11 @@ PSDR_D void cam_jacobian_adj(const DevView& V, const Surf& x, float phi, SurfAdj
   cam.add(&V, -ap);
 }
 
-template <bool UNB>
-__global__ void __launch_bounds__(128, 3) k_adjoint(WF w, const DevScene* __restrict__ scenes,
+// BSDF: DiffuseBsdfMaterial in the scene. The incoming direction of a vertex depends on
+// the previous vertex (or the camera origin), so a vertex's surface adjoint is scattered
+// one depth later.
+template <bool UNB, bool BSDF = false>
+__global__ void __launch_bounds__(128, BSDF ? 2 : 3) k_adjoint(WF w, const DevScene* __restrict__ scenes,
                                                  const DevView* __restrict__ views, Tile tile, int hot_lv0,
                                                  int hot_nlv, int emit_hot) {
   const int stride = gridDim.x * blockDim.x;
@@ -855,25 +999,59 @@ __global__ void __launch_bounds__(128, 3) k_adjoint(WF w, const DevScene* __rest
             int tric = tri0;
             float4 hc = h0;
             float3 T = f3(1.f, 1.f, 1.f);
+            // BSDF: the surface adjoint of depth d-1 >= 1, scattered after depth d
+            SurfAdj axq = zero_adj();
+            int triq = -1;
+            float4 hq = h0;
+            bool frontq = true;
             for (int d = 0; d < w.D; ++d) {
               const float3 adjC = mul(g, T);
               const float3 adjB = mul(adjC, suffix_radiance(cb, d + 1, w.D));
               SurfAdj nextc = zero_adj();
               float3 atx = f3(0.f, 0.f, 0.f);
-              const DepthVals dv = depth_eval<true, UNB>(w, sc, xc, rng, hits + (size_t)d * w.R, d == w.D - 1, adjC,
-                                                         adjB, ax, nextc, hot, atx);
               const DevObj& ob = sc.objs[xc.obj];
-              const int off = texel_offset(ob.color, xc.u, xc.v);
-              if (d == 0) {
-                ax0 = ax;
-                atex0 = atx;
-                tx0 = &ob.color;
-                toff0 = off;
+              if (BSDF) {
+                const MatPt mp = mat_point(ob, xc);
+                MatAdj ma = zero_mat_adj();
+                const DepthVals dv = depth_eval<true, UNB, true>(w, sc, xc, rng, hits + (size_t)d * w.R,
+                                                                 d == w.D - 1, adjC, adjB, ax, nextc, hot, atx, &mp,
+                                                                 &ma);
+                atx = ma.color;
+                const float3 aorg = mat_finalize(ob, xc, mp, ma, ax);
+                if (d == 0) cam.add(&V, aorg);
+                else if (d == 1) ax0.p += aorg;
+                else axq.p += aorg;
+                if (triq >= 0) scatter_surf(sc, hot, triq, hq.y, hq.z, frontq, axq);
+                triq = -1;
+                const int off = texel_offset(ob.color, xc.u, xc.v);
+                if (d == 0) {
+                  ax0 = ax;
+                  atex0 = atx;
+                  tx0 = &ob.color;
+                  toff0 = off;
+                } else {
+                  if (ob.color.grad) scatter_tex(ob.color, off, atx, false);
+                  axq = ax;
+                  triq = tric;
+                  hq = hc;
+                  frontq = xc.front;
+                }
+                if (!dv.has_next) break;
               } else {
-                if (ob.color.grad) scatter_tex(ob.color, off, atx, false);
-                scatter_surf(sc, hot, tric, hc.y, hc.z, xc.front, ax);
+                const DepthVals dv = depth_eval<true, UNB>(w, sc, xc, rng, hits + (size_t)d * w.R, d == w.D - 1,
+                                                           adjC, adjB, ax, nextc, hot, atx);
+                const int off = texel_offset(ob.color, xc.u, xc.v);
+                if (d == 0) {
+                  ax0 = ax;
+                  atex0 = atx;
+                  tx0 = &ob.color;
+                  toff0 = off;
+                } else {
+                  if (ob.color.grad) scatter_tex(ob.color, off, atx, false);
+                  scatter_surf(sc, hot, tric, hc.y, hc.z, xc.front, ax);
+                }
+                if (!dv.has_next) break;
               }
-              if (!dv.has_next) break;
               T = mul(T, xyz(cb[2 * d + 1]));
               hc = hits[(size_t)d * w.R + w.nL + w.nB];
               tric = __float_as_int(hc.x);
@@ -882,6 +1060,7 @@ __global__ void __launch_bounds__(128, 3) k_adjoint(WF w, const DevScene* __rest
               if (xc.is_light) break;  // the path ends on a light: nothing downstream
               ax = nextc;
             }
+            if (BSDF && triq >= 0) scatter_surf(sc, hot, triq, hq.y, hq.z, frontq, axq);
           }
         }
       }
@@ -889,7 +1068,7 @@ __global__ void __launch_bounds__(128, 3) k_adjoint(WF w, const DevScene* __rest
     scatter_surf_warp(scp, hot, tri0, b10, b20, front0, ax0, has0);
     scatter_tex_warp(tx0, toff0, atex0, has0);
   }
-  if (UNB) cam.flush_warp();
+  if (UNB || BSDF) cam.flush_warp();
   // flush register accumulators: warp reduce, one atomic per warp
 #pragma unroll
   for (int k = 0; k < kMaxLightVerts * 3; ++k) {
@@ -1434,11 +1613,11 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
       const float fxfy = view_fxfy(V);
       const float3 look = view_look(V);
       const DevLight& Lt = sc.lights[s0.light];
-      const DevObj& ob = sc.objs[d0.obj];
-      float3 T = mul(tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi,
-                     f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]));
+      // running throughput: the emission times pi f_r at every vertex the chain leaves
+      float3 T = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
       float wsum = 0.f, msum = 0.f;
-      // camera connection of a vertex whose reflection hemisphere faces the camera
+      // camera connection of a vertex whose reflection hemisphere faces the camera:
+      // T times its BSDF toward the camera times its camera Jacobian
       auto connect = [&](const Surf& v) {
         const float3 rel = v.p - V.pos;
         if (dot(v.n, rel) >= 0.f) return;
@@ -1452,16 +1631,18 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
         if (!(iv.valid && !iv.is_light && sqnorm(iv.p - v.p) < kEps)) return;
         const float z = dot(rel, look);
         const float Jc = fxfy * fabsf(dot(v.n, rel)) / (z * z * z);
+        const float3 Tf = mul(T, surf_bsdf(sc, v, -(rel / dist)));
         if (PRE) {
-          msum += norm(T) * fabsf(k0 * Jc);
+          msum += norm(Tf) * fabsf(k0 * Jc);
         } else {
           const float* gp = V.dimage + 3 * ((size_t)qy * V.W + qx);
-          wsum += (gp[0] * T.x + gp[1] * T.y + gp[2] * T.z) * (k0 * Jc);
+          wsum += (gp[0] * Tf.x + gp[1] * Tf.y + gp[2] * Tf.z) * (k0 * Jc);
         }
       };
       connect(d0);
       // the change of the radiance leaving the receiver, carried to the camera through
-      // up to max_bounce - 1 cosine-sampled diffuse bounces (each multiplies the albedo)
+      // up to max_bounce - 1 bounces cosine-sampled about the geometric normal (each
+      // multiplies pi f_r: G / pdf = pi)
       Surf v = d0;
       for (int j = 1; j < w.D; ++j) {
         const float ru = rng.next_float(), rv = rng.next_float();
@@ -1470,8 +1651,7 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
         const HitRec hn = trace_closest(sc, v.p, wo, kTmin, INFINITY);
         const Surf nx = make_surf(sc, hn.tri, hn.b1, hn.b2, v.p);
         if (!nx.valid || nx.is_light) break;
-        const DevObj& on = sc.objs[nx.obj];
-        T = mul(T, tex_rgb(on.color, texel_offset(on.color, nx.u, nx.v)));
+        T = mul(T, surf_bsdf(sc, v, wo)) * kPi;
         connect(nx);
         v = nx;
       }
@@ -1521,8 +1701,7 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     const float dG = cos_s * dot(nd, -db) / (len_sd * len_sd);
     const DevLight& Lt = sc.lights[s0.light];
     const float3 Ts = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
-    const DevObj& ob = sc.objs[d0.obj];
-    const float3 Td = tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi;
+    const float3 Td = surf_bsdf(sc, d0, -cd);
     if (PRE) {
       float3 val = mul(mul(f3(dG, dG, dG) * Jb / pdf_xw, Ts), Td);
       if (!finite3(val)) continue;
@@ -1970,12 +2149,14 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
     set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
     for (const Tile& t : plan_tiles(views, cap)) {
       run_tile(w, scenes_dev, vd, t, MODE_REPLAY, st);
-      if (cfg.estimator == PSDR_EST_UNBIASED)
-        k_adjoint<true><<<grid_for(t.n, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv,
-                                                                gi.emit_hot);
-      else
-        k_adjoint<false><<<grid_for(t.n, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv,
-                                                                 gi.emit_hot);
+      const int g = grid_for(t.n, 128, 16);
+      if (gi.bsdf) {
+        if (unb) k_adjoint<true, true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+        else k_adjoint<false, true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+      } else {
+        if (unb) k_adjoint<true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+        else k_adjoint<false><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+      }
       PSDR_LAUNCHED(1);
     }
     PSDR_CUDA(cudaGetLastError());

@@ -107,6 +107,7 @@ void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views
                          psdr_workspace* ws, cudaStream_t st, float* samples_out);
 struct SceneGradInfo {
   int hot_lv0 = 0, hot_nlv = 0, emit_hot = 0;
+  int bsdf = 0;  // a DiffuseBsdfMaterial mesh is present (material adjoint kernel)
 };
 void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
                           psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
