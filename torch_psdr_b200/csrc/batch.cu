@@ -157,8 +157,9 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     b->scenes_dev.alloc(sizeof(DevScene) * n_scenes, st);
     PSDR_CUDA(cudaMemcpyAsync(b->scenes_dev.p, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice, st));
     if (n_scenes == 1) b->gi = grad_info(scenes[0]);
+    b->ws.bsdf = 0;
     for (int i = 0; i < n_scenes; ++i)
-      if (scenes[i]->has_bsdf) b->gi.bsdf = 1;
+      if (scenes[i]->has_bsdf) b->gi.bsdf = b->ws.bsdf = 1;
     if (b->backward) {
       b->gv.resize(n_scenes);
       b->gt.resize(n_scenes);

@@ -338,6 +338,7 @@ psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
                             const psdr_config* cfg, float** images, void* stream) {
   API_BEGIN
   PSDR_CHECK(scene && ws && images, "null argument");
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cams, n_cams);
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
@@ -355,6 +356,7 @@ psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psd
                                 const psdr_config* cfg, float* samples, void* stream) {
   API_BEGIN
   PSDR_CHECK(scene && ws && samples, "null argument");
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cam, 1);
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
@@ -372,6 +374,7 @@ psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_came
   };
   API_BEGIN
   PSDR_CHECK(scene && ws && cfg, "null argument");
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cams, n_cams);
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
@@ -427,6 +430,7 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
                             void* stream) {
   API_BEGIN
   PSDR_CHECK(scene && ws && d_images && grads, "null argument");
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cams, n_cams);
   PSDR_CHECK(scene->nlight > 0, "scene has no light");

@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict
 
 // ------------------------------------------------------------------ shade kernel
 // Hit-light test and all samples of one depth; rays are written to the shaded slot.
-template <int MODE>
+template <int MODE, bool BSDF>
 __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict__ scenes,
                                                const DevView* __restrict__ views, int d) {
   const int* qin = (d & 1) ? w.q1 : w.q0;
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
     Rng rng{w.rs[s], w.ri[s]};
     float3 mm;
     bool mapped;
-    const float3 Ns = shading_normal(sc->objs[x.obj], x, mm, mapped);
+    const float3 Ns = BSDF ? shading_normal(sc->objs[x.obj], x, mm, mapped) : x.n;
     // rays are stored type-major (slot r * cap + k): a warp of k_trace then traces
     // rays of one kind from neighbouring paths
     const size_t cs = (size_t)w.cap;
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
     for (int j = 0; j < w.nB; ++j) {
       const float rx = rng.next_float(), ry = rng.next_float();
       float ct, st, sp, cp;
-      const float3 wo = material_dir(x, Ns, rx, ry, ct, st, sp, cp);
+      const float3 wo = BSDF ? material_dir(x, Ns, rx, ry, ct, st, sp, cp) : diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
       const size_t slot = (w.nL + j) * cs + k;
       w.ro[slot] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
       w.rd[slot] = make_float4(wo.x, wo.y, wo.z, 0.f);
@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
       const float rx = rng.next_float(), ry = rng.next_float();
       if (!last) {
         float ct, st, sp, cp;
-        const float3 wo = material_dir(x, Ns, rx, ry, ct, st, sp, cp);
+        const float3 wo =
+            BSDF ? material_dir(x, Ns, rx, ry, ct, st, sp, cp) : diffuse_dir(x.n, x.t, rx, ry, ct, st, sp, cp);
         const size_t slot = (w.nL + w.nB) * cs + k;
         w.ro[slot] = make_float4(x.p.x, x.p.y, x.p.z, INFINITY);
         w.rd[slot] = make_float4(wo.x, wo.y, wo.z, 0.f);
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict_
 // samples, path_integrator.cc:103-160) and throughput factor beta (indirect bounce,
 // :163-181). FWD folds them into L and T; REPLAY also stores the hit records and
 // (C, beta) of the depth, which is all the adjoint needs besides the sampler stream.
-template <int MODE>
+template <int MODE, bool BSDF>
 __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict__ scenes,
                                                const DevView* __restrict__ views, int d) {
   const int n = w.cnt[2 * d + 1];
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
       const float3 color = tex_rgb(ob.color, texel_offset(ob.color, x.u, x.v));
       const float3 bsdf = color * kInvPi;
       // DiffuseBsdfMaterial: the value depends on the outgoing direction
-      const bool rough = ob.mat == kMatDiffuseBsdf;
+      const bool rough = BSDF && ob.mat == kMatDiffuseBsdf;
       float3 Ns = x.n;
       float sigma = 0.f;
       if (rough) {
@@ -1535,7 +1536,9 @@ __global__ void __launch_bounds__(256) k_border_final(WF w, const DevScene* __re
 // (d_eff . (w x e)) / (pdf_e pdf_y hc_density H W spp), e oriented by the edge's outward
 // vector so that the occluding faces lie on the -(w x e) side, T = f_r(x_d) L_e times the
 // albedos of the diffuse bounces between x_d and the camera-visible vertex.
-template <bool PRE, bool UNB = false>
+// BSDF: the DiffuseBsdfMaterial instance (direction-dependent f at the receiver and
+// along the bounce chain); the other instance is the DiffuseMaterial one.
+template <bool PRE, bool UNB, bool BSDF>
 __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict__ scenes,
                                                 const DevView* __restrict__ views, int v, long long n, HCube hc,
                                                 int round, float* mass, int spp) {
@@ -1614,7 +1617,12 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
       const float3 look = view_look(V);
       const DevLight& Lt = sc.lights[s0.light];
       // running throughput: the emission times pi f_r at every vertex the chain leaves
+      // (DiffuseMaterial: f_r / pi of the receiver folded in up front, then the albedos)
       float3 T = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+      if (!BSDF) {
+        const DevObj& ob = sc.objs[d0.obj];
+        T = mul(tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi, T);
+      }
       float wsum = 0.f, msum = 0.f;
       // camera connection of a vertex whose reflection hemisphere faces the camera:
       // T times its BSDF toward the camera times its camera Jacobian
@@ -1631,7 +1639,7 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
         if (!(iv.valid && !iv.is_light && sqnorm(iv.p - v.p) < kEps)) return;
         const float z = dot(rel, look);
         const float Jc = fxfy * fabsf(dot(v.n, rel)) / (z * z * z);
-        const float3 Tf = mul(T, surf_bsdf(sc, v, -(rel / dist)));
+        const float3 Tf = BSDF ? mul(T, surf_bsdf(sc, v, -(rel / dist))) : T;
         if (PRE) {
           msum += norm(Tf) * fabsf(k0 * Jc);
         } else {
@@ -1651,7 +1659,12 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
         const HitRec hn = trace_closest(sc, v.p, wo, kTmin, INFINITY);
         const Surf nx = make_surf(sc, hn.tri, hn.b1, hn.b2, v.p);
         if (!nx.valid || nx.is_light) break;
-        T = mul(T, surf_bsdf(sc, v, wo)) * kPi;
+        if (BSDF) {
+          T = mul(T, surf_bsdf(sc, v, wo)) * kPi;
+        } else {
+          const DevObj& on = sc.objs[nx.obj];
+          T = mul(T, tex_rgb(on.color, texel_offset(on.color, nx.u, nx.v)));
+        }
         connect(nx);
         v = nx;
       }
@@ -1701,7 +1714,13 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     const float dG = cos_s * dot(nd, -db) / (len_sd * len_sd);
     const DevLight& Lt = sc.lights[s0.light];
     const float3 Ts = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
-    const float3 Td = surf_bsdf(sc, d0, -cd);
+    float3 Td;
+    if (BSDF) {
+      Td = surf_bsdf(sc, d0, -cd);
+    } else {
+      const DevObj& ob = sc.objs[d0.obj];
+      Td = tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi;
+    }
     if (PRE) {
       float3 val = mul(mul(f3(dG, dG, dG) * Jb / pdf_xw, Ts), Td);
       if (!finite3(val)) continue;
@@ -1907,18 +1926,37 @@ void Profiler::replayed(std::vector<EvPair>* graph_ev, long long n_trace) {
 #define PSDR_LAUNCHED(n) (profiler().launches += (n))
 void count_launches(int n) { profiler().launches += n; }
 
+// k_direct instance for the job's materials (w.bsdf).
+template <bool PRE, bool UNB>
+static void launch_direct(const WF& w, int grid, cudaStream_t st, const DevScene* scenes, const DevView* vd, int v,
+                          long long n, const HCube& hc, int round, float* mass, int spp) {
+  if (w.bsdf) k_direct<PRE, UNB, true><<<grid, 128, 0, st>>>(w, scenes, vd, v, n, hc, round, mass, spp);
+  else k_direct<PRE, UNB, false><<<grid, 128, 0, st>>>(w, scenes, vd, v, n, hc, round, mass, spp);
+}
+
 static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int mode, cudaStream_t st) {
   const int cap = w.cap;
   Profiler& pf = profiler();
   for (int d = 0; d < w.D; ++d) {
-    if (mode == MODE_REPLAY) k_shade<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
-    else k_shade<MODE_FWD><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
+    const int gs = grid_for(cap, 256, 8);
+    if (w.bsdf) {
+      if (mode == MODE_REPLAY) k_shade<MODE_REPLAY, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
+      else k_shade<MODE_FWD, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
+    } else {
+      if (mode == MODE_REPLAY) k_shade<MODE_REPLAY, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
+      else k_shade<MODE_FWD, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
+    }
     pf.begin_trace(st);
     k_trace<<<num_sms() * 8, 128, 0, st>>>(w, scenes, views, d, pf.on ? pf.d_rays : nullptr);
     pf.end_trace(st);
     PSDR_LAUNCHED(3);
-    if (mode == MODE_REPLAY) k_accum<MODE_REPLAY><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
-    else k_accum<MODE_FWD><<<grid_for(cap, 256, 8), 256, 0, st>>>(w, scenes, views, d);
+    if (w.bsdf) {
+      if (mode == MODE_REPLAY) k_accum<MODE_REPLAY, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
+      else k_accum<MODE_FWD, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
+    } else {
+      if (mode == MODE_REPLAY) k_accum<MODE_REPLAY, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
+      else k_accum<MODE_FWD, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
+    }
   }
   PSDR_CUDA(cudaGetLastError());
 }
@@ -2023,6 +2061,7 @@ void forward_launch(const DevScene* scenes_dev, const std::vector<DevView>& view
   WF w = ws->wf;
   w.cap = ws->cap;
   set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
+  w.bsdf = ws->bsdf;
   const DevView* vd = ws->views.as<DevView>();
   for (const Tile& t : plan_tiles(views, cap)) {
     run_tile(w, scenes_dev, vd, t, MODE_FWD, st);
@@ -2147,6 +2186,7 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
     WF w = ws->wf;
     w.cap = ws->cap;
     set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
+    w.bsdf = ws->bsdf;
     for (const Tile& t : plan_tiles(views, cap)) {
       run_tile(w, scenes_dev, vd, t, MODE_REPLAY, st);
       const int g = grid_for(t.n, 128, 16);
@@ -2165,10 +2205,12 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
   WF w = ws->wf;
   w.cap = ws->cap;
   set_wf(w, cfg, (int)views.size(), 1, 0);
+  w.bsdf = ws->bsdf;
   // paths of the unbiased boundary samples carry the interior estimator's radiance
   WF wi = ws->wf;
   wi.cap = ws->cap;
   set_wf(wi, cfg, (int)views.size(), -1, cfg.enable_light_visable);
+  wi.bsdf = ws->bsdf;
   EdgeBuf eb{ws->eb_a.as<float4>(), ws->eb_n.as<float4>(), ws->eb_hb.as<float4>(), ws->eb_La.as<float4>(), nullptr};
   for (int v = 0; v < (int)views.size(); ++v) {
     const DevView& V = views[v];
@@ -2199,20 +2241,20 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       PSDR_LAUNCHED(cfg.secondary_edge_preprocess_rounds + 1);
       for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r) {
         if (unb)
-          k_direct<true, true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
-                                                                         ws->mass.as<float>(), 1);
+          launch_direct<true, true>(w, grid_for(cells, 128, 16), st, scenes_dev, vd, v, cells, pre, r,
+                                    ws->mass.as<float>(), 1);
         else
-          k_direct<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, cells, pre, r,
-                                                                   ws->mass.as<float>(), 1);
+          launch_direct<true, false>(w, grid_for(cells, 128, 16), st, scenes_dev, vd, v, cells, pre, r,
+                                     ws->mass.as<float>(), 1);
       }
       const HCube hc = build_hcube(ws, cells, r3, 3, unb, st);
       const long long N = (long long)V.H * V.W * cfg.spp_secondary_edge;
       if (unb)
-        k_direct<false, true><<<grid_for(N, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, N, hc, 0, nullptr,
-                                                                    cfg.spp_secondary_edge);
+        launch_direct<false, true>(w, grid_for(N, 128, 16), st, scenes_dev, vd, v, N, hc, 0, nullptr,
+                                   cfg.spp_secondary_edge);
       else
-        k_direct<false><<<grid_for(N, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, N, hc, 0, nullptr,
-                                                              cfg.spp_secondary_edge);
+        launch_direct<false, false>(w, grid_for(N, 128, 16), st, scenes_dev, vd, v, N, hc, 0, nullptr,
+                                    cfg.spp_secondary_edge);
       PSDR_CUDA(cudaGetLastError());
     }
     // pixel borders (unbiased estimator): segment masses, their prefix sums, samples
@@ -2402,6 +2444,7 @@ extern "C" PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const
     w.hit = reinterpret_cast<float4*>(take(16 * cap * R));
     w.rec = nullptr;
     set_wf(w, *cfg, 1, -1, cfg->enable_light_visable);
+    w.bsdf = scene->has_bsdf ? 1 : 0;
     // the view record goes into the scratch too (the previous call's view is overwritten)
     DevView V;
     make_view(*cam, cfg->spp_interior, V);

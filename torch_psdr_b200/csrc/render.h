@@ -45,6 +45,7 @@ struct WF {
   float4* hit;   // tri(bits), b1, b2, t
   float4* rec;   // replay records: 1 + D*R per path
   int rec_stride;
+  int bsdf;      // host side: launch the DiffuseBsdfMaterial kernel instances
 };
 
 struct Tile {
@@ -75,6 +76,9 @@ struct psdr_workspace {
   psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
   psdr::DBuf campos_acc;
   long long mass_cap = 0;
+  // a DiffuseBsdfMaterial mesh is in the scenes of the current job (each entry point sets
+  // it; the material kernel instances also handle DiffuseMaterial, so 1 is always safe)
+  int bsdf = 1;
   cudaStream_t stream = nullptr;
   std::vector<psdr::DevView> h_views;
   psdr::WF wf{};
