@@ -338,9 +338,9 @@ psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
                             const psdr_config* cfg, float** images, void* stream) {
   API_BEGIN
   PSDR_CHECK(scene && ws && images, "null argument");
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cams, n_cams);
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
   std::vector<DevView> views(n_cams);
   for (int i = 0; i < n_cams; ++i) {
@@ -356,9 +356,9 @@ psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psd
                                 const psdr_config* cfg, float* samples, void* stream) {
   API_BEGIN
   PSDR_CHECK(scene && ws && samples, "null argument");
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cam, 1);
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
   std::vector<DevView> views(1);
   make_view(*cam, cfg->spp_interior, views[0]);
@@ -374,9 +374,9 @@ psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_came
   };
   API_BEGIN
   PSDR_CHECK(scene && ws && cfg, "null argument");
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cams, n_cams);
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
   cudaStream_t st = (cudaStream_t)stream;
   std::vector<DevView> views(n_cams);
@@ -430,9 +430,9 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
                             void* stream) {
   API_BEGIN
   PSDR_CHECK(scene && ws && d_images && grads, "null argument");
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   check_cfg(cfg);
   check_cams(cams, n_cams);
+  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   PSDR_CHECK(scene->nlight > 0, "scene has no light");
   cudaStream_t st = (cudaStream_t)stream;
   // only the vertices whose gradient the caller asked for are accumulated
