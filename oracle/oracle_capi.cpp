@@ -62,7 +62,24 @@ inline V3<S> raster_of(const Camera<R>& cam, const V3<S>& x, const V3<S>& o) {
   return Camera<R>::xpos(cam.c2r, pc);
 }
 
-// camera.h:235-258 PerspectiveCamera::gen_camera_ray_ for sample i.
+// camera.h:336-353 OrthographicCamera::gen_camera_ray_with_point_: the ray origin is x's
+// foot on the camera plane, c2w (w2c x).xy0, here with the camera translated to o (the
+// rotation fixed), so that it carries the derivatives of x and o.
+template <class S, class R>
+inline V3<S> ortho_origin(const Camera<R>& cam, const V3<S>& x, const V3<S>& o) {
+  V3<S> rel = x - o;
+  S px = S(cam.w2c[0][0]) * rel.x + S(cam.w2c[0][1]) * rel.y + S(cam.w2c[0][2]) * rel.z;
+  S py = S(cam.w2c[1][0]) * rel.x + S(cam.w2c[1][1]) * rel.y + S(cam.w2c[1][2]) * rel.z;
+  return o + V3<S>(S(cam.c2w[0][0]) * px + S(cam.c2w[0][1]) * py, S(cam.c2w[1][0]) * px + S(cam.c2w[1][1]) * py,
+                   S(cam.c2w[2][0]) * px + S(cam.c2w[2][1]) * py);
+}
+// camera.h:121 look direction: c2w (0, 0, -1).
+template <class S, class R> inline V3<S> look_dir(const Camera<R>& cam) {
+  return V3<S>(S(-cam.c2w[0][2]), S(-cam.c2w[1][2]), S(-cam.c2w[2][2]));
+}
+
+// camera.h:235-258 PerspectiveCamera::gen_camera_ray_ (camera.h:313-334 orthographic:
+// origin c2w (r2c film).xy0, direction the look direction) for sample i.
 template <class S, bool AD>
 inline V3<S> interior_sample(const Ctx<S, AD>& c, uint64_t i, int& pix, bool& valid) {
   using R = typename Traits<S>::R;
@@ -74,9 +91,17 @@ inline V3<S> interior_sample(const Ctx<S, AD>& c, uint64_t i, int& pix, bool& va
   int x = pix % W, y = pix / W;
   V3<R> fp(jx + R(x), jy + R(y), R(1));
   V3<R> pc = Camera<R>::xpos(c.cam.r2c, fp);
-  V3<R> d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
+  V3<S> org = c.cam_pos;
+  V3<R> d;
+  if (c.cam.ortho) {
+    V3<R> o = Camera<R>::xpos(c.cam.c2w, V3<R>(pc.x, pc.y, R(0)));
+    org = V3<S>(S(o.x), S(o.y), S(o.z)) + (c.cam_pos - detach(c.cam_pos));
+    d = look_dir<R>(c.cam);
+  } else {
+    d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
+  }
   V3<S> ds(S(d.x), S(d.y), S(d.z));
-  Its<S> its = scene_hit<S, AD>(c.sc, c.cam_pos, ds, true);
+  Its<S> its = scene_hit<S, AD>(c.sc, org, ds, true);
   valid = its.valid;
   const bool unb = c.cfg.mode == 1;
   V3<S> L = trace2light<S, AD>(c.sc, rng, its, its.valid, c.cfg.mis_light_samples, c.cfg.mis_bsdf_samples,
@@ -113,12 +138,19 @@ inline V3<S> eval_primary(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx, in
   float pdf_e = pe / E.len;
   valid = true;
   project(c.camf, xe, valid, rx, ry);
-  V3<float> rd = normalize(xe - c.posf);
+  V3<float> of = c.posf, rd;
+  if (c.camf.ortho) {
+    V3<float> pcf = Camera<float>::xpos(c.camf.w2c, xe);
+    of = Camera<float>::xpos(c.camf.c2w, V3<float>(pcf.x, pcf.y, 0.f));
+    rd = look_dir<float>(c.camf);
+  } else {
+    rd = normalize(xe - c.posf);
+  }
   V3<float> n = cross(rd, normalize(E.p1 - E.p0));
   const float eps = 1e-5f;
   V3<float> da = rd - n * eps, db = rd + n * eps;
-  Its<float> ia = scene_hit<float, false>(sf, c.posf, da, valid);
-  Its<float> ib = scene_hit<float, false>(sf, c.posf, db, valid);
+  Its<float> ia = scene_hit<float, false>(sf, of, da, valid);
+  Its<float> ib = scene_hit<float, false>(sf, of, db, valid);
   valid = valid && ia.valid && ib.valid && (norm(ia.p - xe) < 1e-4f || norm(ib.p - xe) < 1e-4f);
   V3<float> La = trace2light<float, false>(sf, rng, ia, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
   V3<float> Lb = trace2light<float, false>(sf, rng, ib, valid, c.cfg.mis_light_samples, 1, c.cfg.max_bounce, false);
@@ -129,7 +161,10 @@ inline V3<S> eval_primary(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx, in
     V3<S> xes = Es.p0 + (Es.p1 - Es.p0) * S(s);
     V3<S> ns(S(n.x), S(n.y), S(n.z));
     V3<S> nflip(S(n.x), S(n.y), S(-n.z));
-    S xdn = dot(xes - detach(xes), ns) + dot(c.cam_pos - detach(c.cam_pos), nflip);
+    // the ray origin: the camera position, or (orthographic) the edge point's foot on
+    // the camera plane, which moves with the edge point too
+    V3<S> org = c.cam.ortho ? ortho_origin(c.cam, xes, c.cam_pos) : c.cam_pos;
+    S xdn = dot(xes - detach(xes), ns) + dot(org - detach(org), nflip);
     V3<S> dLs(S(dL.x), S(dL.y), S(dL.z));
     value = dLs * (xdn / S(pdf_e));
   } else {
@@ -202,8 +237,14 @@ inline V3<S> eval_direct(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], int& 
   Its<S> id0 = scene_hit<S, AD>(sc, xb, dir, valid);
   valid = valid && id0.valid && !id0.is_light;
   project(c.cam, id0.p, valid, rx, ry);
-  V3<S> cd = normalize(id0.p - c.cam_pos);
-  Its<S> i2 = scene_hit<S, AD>(sc, c.cam_pos, cd, valid);
+  V3<S> corg = c.cam_pos, cd;
+  if (c.cam.ortho) {
+    corg = ortho_origin(c.cam, id0.p, c.cam_pos);
+    cd = look_dir<S>(c.cam);
+  } else {
+    cd = normalize(id0.p - c.cam_pos);
+  }
+  Its<S> i2 = scene_hit<S, AD>(sc, corg, cd, valid);
   valid = valid && i2.valid && !i2.is_light && val(sqnorm(i2.p - id0.p)) < double(R(1e-5));
   V3<S> value;
   if (!valid) return value;
@@ -742,6 +783,10 @@ template <class S, bool AD>
 static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
                        const OrcConfig* cfg, int which, double* images, const double* dLdI, double* dphi,
                        double* per_sample, const Seeds<S>& seeds) {
+  // the unbiased estimator's camera Jacobians are those of the perspective camera
+  if (cfg->mode == 1)
+    for (int ci = 0; ci < nc; ++ci)
+      if (cams[ci].type != 0) return 3;
   using R = typename Traits<S>::R;
   Scene<S> sc = mk_scene<S>(m, nm, l, nl, seeds);
   Seeds<R> none;

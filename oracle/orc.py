@@ -36,7 +36,7 @@ class OrcLight(C.Structure):
 
 class OrcCamera(C.Structure):
     _fields_ = [("look_from", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3),
-                ("fov", C.c_float), ("h", C.c_int), ("w", C.c_int)]
+                ("fov", C.c_float), ("h", C.c_int), ("w", C.c_int), ("type", C.c_int)]
 
 
 class OrcConfig(C.Structure):
@@ -96,7 +96,8 @@ class Marshal:
         self.cams = (OrcCamera * max(1, len(spec.cameras)))()
         for i, c in enumerate(spec.cameras):
             self.cams[i] = OrcCamera((C.c_float * 3)(*map(float, c.look_from)), (C.c_float * 3)(*map(float, c.look_at)),
-                                     (C.c_float * 3)(*map(float, c.up)), float(c.vfov), int(c.height), int(c.width))
+                                     (C.c_float * 3)(*map(float, c.up)), float(c.vfov), int(c.height), int(c.width),
+                                     int(getattr(c, "kind", 0)))
         self.nm, self.nl, self.nc = len(spec.meshes), len(spec.lights), len(spec.cameras)
 
     def _tex(self, a):
@@ -137,7 +138,9 @@ def render(spec, precision=1, per_sample=False, **cfg):
     total = sum(h * w for h, w in sizes)
     out = np.zeros(total * 3, np.float64)
     ps = np.zeros(total * 3 * c.spp_interior, np.float64) if per_sample else None
-    L.orc_render(*m.args(), C.byref(c), int(precision), _ptr(out), _ptr(ps))
+    rc = L.orc_render(*m.args(), C.byref(c), int(precision), _ptr(out), _ptr(ps))
+    if rc != 0:
+        raise ValueError(f"oracle render failed (code {rc})")
     imgs, off = [], 0
     for h, w in sizes:
         imgs.append(out[off * 3:(off + h * w) * 3].reshape(h, w, 3))
@@ -161,7 +164,10 @@ def grad_dir(spec, dLdI, which=1, seed_verts=None, seed_tex=None, seed_emit=None
     se = None if seed_emit is None else np.ascontiguousarray(seed_emit, np.float64)
     sc = None if seed_cam is None else np.ascontiguousarray(seed_cam, np.float64)
     out = np.zeros(8, np.float64)
-    L.orc_grad_dir(*m.args(), C.byref(c), int(which), _ptr(g), _ptr(sv), _ptr(st), _ptr(se), _ptr(sc), _ptr(out))
+    rc = L.orc_grad_dir(*m.args(), C.byref(c), int(which), _ptr(g), _ptr(sv), _ptr(st), _ptr(se), _ptr(sc),
+                        _ptr(out))
+    if rc != 0:
+        raise ValueError(f"oracle gradient failed (code {rc}; the unbiased estimator takes perspective cameras)")
     return out
 
 

@@ -279,8 +279,9 @@ struct OrcLight {
 };
 struct OrcCamera {
   float look_from[3], look_at[3], up[3];
-  float fov;
+  float fov;   // perspective: vertical field of view; orthographic: view width
   int h, w;
+  int type;    // 0 perspective, 1 orthographic
 };
 struct OrcConfig {
   int n_pass, spp_interior, enable_light_visable, spp_primary_edge, spp_secondary_edge;
@@ -324,10 +325,13 @@ inline M4 minv(const M4& a) {
   return r;
 }
 
-// camera.h:7-64 (perspective, look_at), :111-124 (BaseCamera), psdr.cc:24-29 (near -0.01, far -1000).
+// camera.h:7-64 (perspective, orthographic, look_at), :111-124 (BaseCamera), psdr.cc:24-37
+// (near -0.01, far -1000), camera.h:290-300 (orthographic view box: width view_width,
+// height view_width H / W).
 template <class R> struct Camera {
   R r2c[4][4], c2w[4][4], w2c[4][4], c2r[4][4];
   int H, W;
+  int ortho = 0;
   V3<double> pos_d;
   void setup(const OrcCamera& c) {
     H = c.h; W = c.w;
@@ -346,11 +350,22 @@ template <class R> struct Camera {
     for (int i = 0; i < 3; ++i) { cw.m[i][0] = right[i]; cw.m[i][1] = nup[i]; cw.m[i][2] = dir[i]; cw.m[i][3] = o[i]; }
     cw.m[3][3] = 1;
     double nearv = -0.01, farv = -1000.0;
-    double inv_nf = 1.0 / (nearv - farv);
-    double cot = 1.0 / std::tan(double(c.fov) * 0.5);
     M4 cs{};
-    cs.m[0][0] = -cot; cs.m[1][1] = -cot; cs.m[2][2] = (nearv + farv) * inv_nf;
-    cs.m[2][3] = -2 * farv * nearv * inv_nf; cs.m[3][2] = 1;
+    ortho = c.type == 1;
+    if (ortho) {
+      // orthographic(left, right, bottom, top, near, far) = scale * translate
+      double hw = double(c.fov) / 2, hh = double(H) * hw / double(W);
+      cs.m[0][0] = 2 / (2 * hw);
+      cs.m[1][1] = 2 / (2 * hh);
+      cs.m[2][2] = 2 / (nearv - farv);
+      cs.m[2][3] = cs.m[2][2] * (-(nearv + farv) / 2);
+      cs.m[3][3] = 1;
+    } else {
+      double inv_nf = 1.0 / (nearv - farv);
+      double cot = 1.0 / std::tan(double(c.fov) * 0.5);
+      cs.m[0][0] = -cot; cs.m[1][1] = -cot; cs.m[2][2] = (nearv + farv) * inv_nf;
+      cs.m[2][3] = -2 * farv * nearv * inv_nf; cs.m[3][2] = 1;
+    }
     M4 sr{};
     sr.m[0][0] = 0.5 * W; sr.m[1][1] = -0.5 * H; sr.m[2][2] = 1; sr.m[3][3] = 1;
     M4 tr{};

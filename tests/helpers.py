@@ -48,10 +48,10 @@ def to_torch_scene(spec, requires_grad=(), device="cuda"):
     for k, c in enumerate(spec.cameras):
         lf = torch.tensor(c.look_from, dtype=torch.float32, device=device, requires_grad="cam" in requires_grad)
         T[f"cam{k}"] = lf
-        cams.append(dr.PerspectiveCamera(lf, torch.tensor(c.look_at, dtype=torch.float32, device=device),
-                                         torch.tensor(c.up, dtype=torch.float32, device=device),
-                                         torch.tensor([c.vfov], dtype=torch.float32, device=device),
-                                         c.height, c.width))
+        cls = dr.OrthographicCamera if getattr(c, "kind", 0) == 1 else dr.PerspectiveCamera
+        cams.append(cls(lf, torch.tensor(c.look_at, dtype=torch.float32, device=device),
+                        torch.tensor(c.up, dtype=torch.float32, device=device),
+                        torch.tensor([c.vfov], dtype=torch.float32, device=device), c.height, c.width))
     return dr.Scene(cams, meshes, lights), T
 
 

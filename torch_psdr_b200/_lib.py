@@ -14,6 +14,7 @@ LIB_PATH = os.environ.get("PSDR_B200_LIB", os.path.join(HERE, "_lib", "libpsdr_b
 
 PSDR_OK = 0
 PSDR_ERR_INVALID_ARG = 1
+PSDR_ERR_UNSUPPORTED = 6
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "NUMERIC", 6: "UNSUPPORTED"}
 
 TEX_NONE, TEX_CONSTANT, TEX_UV = -1, 0, 1

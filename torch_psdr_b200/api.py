@@ -93,14 +93,32 @@ Camera = PerspectiveCamera  # example/optimize_texture.py:76 uses dr.Camera
 
 class OrthographicCamera(BaseCamera):
     def __init__(self, look_from, look_at, up, view_width, height: int, width: int):
-        """Orthographic camera (torch_psdr.py:161-206). Not built on this path yet."""
+        """Orthographic camera (torch_psdr.py:161-206; camera.h:279-353): parallel rays
+        along the view direction from a view box view_width wide and view_width * height /
+        width high. Renders with both estimators' forward pass; gradients with the
+        reference estimator (the unbiased one is built for perspective cameras)."""
         super().__init__()
         assert look_from.size() == (3,)
         assert look_at.size() == (3,)
         assert up.size() == (3,)
         assert view_width.size() == (1,)
         assert height > 0 and width > 0
-        raise NotImplementedError("OrthographicCamera is not available in torch_psdr_b200 yet")
+        self.look_from, self.look_at, self.up, self.view_width = look_from, look_at, up, view_width
+        self.vfov = view_width  # the lens parameter slot shared with PerspectiveCamera
+        for t in (look_from, look_at, up, view_width):
+            self.append_variable(t)
+        self.height = int(height)
+        self.width = int(width)
+
+    def _desc(self):
+        d = L.CameraDesc()
+        d.type = L.CAM_ORTHOGRAPHIC
+        d.look_from = _host3(self.look_from)
+        d.look_at = _host3(self.look_at)
+        d.up = _host3(self.up)
+        d.fov = float(self.view_width.detach().reshape(-1)[0].item())
+        d.height, d.width = self.height, self.width
+        return d
 
 
 class Texture(VarContex):

@@ -83,8 +83,9 @@ void check_cfg(const psdr_config* c) {
 void check_cams(const psdr_camera_desc* cams, int n) {
   PSDR_CHECK(cams != nullptr && n > 0, "no cameras");
   for (int i = 0; i < n; ++i) {
-    PSDR_CHECK(cams[i].type == PSDR_CAM_PERSPECTIVE, "only perspective cameras are supported");
+    PSDR_CHECK(cams[i].type == PSDR_CAM_PERSPECTIVE || cams[i].type == PSDR_CAM_ORTHOGRAPHIC, "bad camera type");
     PSDR_CHECK(cams[i].height > 0 && cams[i].width > 0, "camera height and width must be > 0");
+    PSDR_CHECK(cams[i].fov > 0.f, "camera fov / view width must be > 0");
   }
 }
 
@@ -108,6 +109,15 @@ SceneGradInfo grad_info(const psdr_scene* s) {
 
 void check_config(const psdr_config* c) { check_cfg(c); }
 void check_cameras(const psdr_camera_desc* cams, int n) { check_cams(cams, n); }
+
+// The unbiased estimator's camera Jacobians and raster velocities are those of the
+// perspective camera.
+void check_estimator_cameras(const psdr_config* cfg, const psdr_camera_desc* cams, int n) {
+  if (cfg->estimator != PSDR_EST_UNBIASED) return;
+  for (int i = 0; i < n; ++i)
+    PSDR_REQUIRE(cams[i].type == PSDR_CAM_PERSPECTIVE,
+                 "the unbiased estimator's gradients take perspective cameras (use the reference estimator)");
+}
 
 }  // namespace psdr
 
@@ -432,6 +442,7 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   PSDR_CHECK(scene && ws && d_images && grads, "null argument");
   check_cfg(cfg);
   check_cams(cams, n_cams);
+  check_estimator_cameras(cfg, cams, n_cams);
   ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
   PSDR_CHECK(scene->nlight > 0, "scene has no light");
   cudaStream_t st = (cudaStream_t)stream;

@@ -62,6 +62,24 @@ PSDR_D bool project(const DevView& V, float3 pt, int& px, int& py) {
   return pc.z < 0.f && p.x > 0.f && p.x < (float)V.W && p.y > 0.f && p.y < (float)V.H;
 }
 
+// camera.h:121 look direction c2w (0, 0, -1).
+PSDR_D float3 view_look_dir(const DevView& V) { return f3(-V.c2w[2], -V.c2w[6], -V.c2w[10]); }
+
+// camera.h:336-353 orthographic ray toward world point pt: origin c2w (w2c pt).xy0 (in
+// the same rounded operations as the float oracle), direction the look direction.
+PSDR_D float3 ortho_origin_rn(const DevView& V, float3 pt) {
+  const float3 pc = xform_pos_rn(V.w2c, pt);
+  return xform_pos_rn(V.c2w, f3(pc.x, pc.y, 0.f));
+}
+
+// Transposed Jacobian of that origin w.r.t. the point, applied to a: M^T a with
+// M = C diag(1, 1, 0) W (C, W the rotation parts of c2w, w2c).
+PSDR_D float3 ortho_origin_jt(const DevView& V, float3 a) {
+  const float ux = V.c2w[0] * a.x + V.c2w[4] * a.y + V.c2w[8] * a.z;
+  const float uy = V.c2w[1] * a.x + V.c2w[5] * a.y + V.c2w[9] * a.z;
+  return f3(V.w2c[0] * ux + V.w2c[4] * uy, V.w2c[1] * ux + V.w2c[5] * uy, V.w2c[2] * ux + V.w2c[6] * uy);
+}
+
 PSDR_D int find_view(const DevView* __restrict__ views, int nv, long long g) {
   int lo = 0, hi = nv - 1;
   while (lo < hi) {
@@ -113,8 +131,15 @@ __global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict
       const int x = pix % V.W, y = pix / V.W;
       float3 pc;
       xform_pos(V.r2c, f3(jx + (float)x, jy + (float)y, 1.0f), pc);
-      const float3 d = normalize(xform_dir(V.c2w, pc));
-      const HitRec h = trace_closest(sc, V.pos, d, kTmin, INFINITY);
+      float3 o = V.pos, d;
+      if (V.ortho) {
+        // camera.h:313-334: origin on the camera plane, direction the look direction
+        xform_pos(V.c2w, f3(pc.x, pc.y, 0.f), o);
+        d = view_look_dir(V);
+      } else {
+        d = normalize(xform_dir(V.c2w, pc));
+      }
+      const HitRec h = trace_closest(sc, o, d, kTmin, INFINITY);
       w.rs[s] = rng.state;
       w.ri[s] = rng.inc;
       w.view[s] = v;
@@ -122,7 +147,7 @@ __global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict
       w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
       w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       w.cur[s] = hit4(h);
-      w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      w.org[s] = make_float4(o.x, o.y, o.z, 0.f);
       if (MODE == MODE_REPLAY) {
         float4* rec = w.rec + (size_t)s * w.rec_stride;
         rec[0] = hit4(h);
@@ -971,7 +996,17 @@ __global__ void __launch_bounds__(128, BSDF ? 2 : 3) k_adjoint(WF w, const DevSc
         flush_sc = scp;
         const float* gp = V.dimage + 3 * (size_t)w.pix[s];
         const float3 g = f3(gp[0], gp[1], gp[2]) / (float)V.spp;
-        const Surf x0 = make_surf(sc, tri0, h0.y, h0.z, V.pos);
+        float3 o0 = V.pos;
+        if (V.ortho) {
+          // the camera ray's origin on the camera plane, as k_camera formed it
+          Rng r0 = make_rng((unsigned long long)(tile.begin + s - V.sample_off) + w.seed);
+          const float jx = r0.next_float(), jy = r0.next_float();
+          const int pix = w.pix[s];
+          float3 pc;
+          xform_pos(V.r2c, f3(jx + (float)(pix % V.W), jy + (float)(pix / V.W), 1.0f), pc);
+          xform_pos(V.c2w, f3(pc.x, pc.y, 0.f), o0);
+        }
+        const Surf x0 = make_surf(sc, tri0, h0.y, h0.z, o0);
         b10 = h0.y; b20 = h0.z; front0 = x0.front;
         const float4* hits = rec + 1;
         const float4* cb = rec + 1 + (size_t)w.D * w.R;
@@ -1186,14 +1221,17 @@ __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restr
       const float3 pr = xform_pos_rn(V.c2r, pc);
       const int px = (int)floorf(pr.x), py = (int)floorf(pr.y);
       bool valid = ok && pc.z < 0.f && pr.x > 0.f && pr.x < (float)V.W && pr.y > 0.f && pr.y < (float)V.H;
-      const float3 rd = normalize_rn(sub_rn(xe, V.pos));
+      // camera.h:260-276 / 336-353: the ray through the edge point
+      const bool ortho = V.ortho && !unb;
+      const float3 eo = ortho ? xform_pos_rn(V.c2w, f3(pc.x, pc.y, 0.f)) : V.pos;
+      const float3 rd = ortho ? view_look_dir(V) : normalize_rn(sub_rn(xe, V.pos));
       const float3 nrm = cross_rn(rd, normalize_rn(sub_rn(p1, p0)));
       HitRec ha, hb;
       ha.tri = hb.tri = -1;
       ha.b1 = ha.b2 = hb.b1 = hb.b2 = 0.f;
       if (valid) {
-        ha = trace_closest(sc, V.pos, sub_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
-        hb = trace_closest(sc, V.pos, add_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
+        ha = trace_closest(sc, eo, sub_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
+        hb = trace_closest(sc, eo, add_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
       }
       int flag;
       HitRec hcur = ha;
@@ -1206,8 +1244,8 @@ __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restr
         hcur = hg;
         eb.hb[s] = make_float4(__int_as_float(hg.tri), hg.b1, hg.b2, __int_as_float(flag));
       } else {
-        const Surf a = make_surf(sc, ha.tri, ha.b1, ha.b2, V.pos);
-        const Surf b = make_surf(sc, hb.tri, hb.b1, hb.b2, V.pos);
+        const Surf a = make_surf(sc, ha.tri, ha.b1, ha.b2, eo);
+        const Surf b = make_surf(sc, hb.tri, hb.b1, hb.b2, eo);
         valid = valid && a.valid && b.valid && (norm(a.p - xe) < 10.f * kEps || norm(b.p - xe) < 10.f * kEps);
         flag = valid ? 1 : 0;
         eb.hb[s] = make_float4(__int_as_float(hb.tri), hb.b1, hb.b2, __int_as_float(flag));
@@ -1220,7 +1258,8 @@ __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restr
       w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
       w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       w.cur[s] = hit4(hcur);
-      w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      w.org[s] = make_float4(eo.x, eo.y, eo.z, 0.f);
+      eb.La[s] = w.org[s];  // the ray origin, for the second path (k_edge_mid)
       alive = valid;
     }
     const int k = warp_append(&w.cnt[0], alive);
@@ -1297,12 +1336,12 @@ __global__ void __launch_bounds__(256) k_edge_mid(WF w, const DevView* __restric
       const float4 hb = eb.hb[s];
       alive = __float_as_int(hb.w) != 0;
       if (alive) {
-        const DevView& V = views[v];
+        const float4 eo = eb.La[s];  // the ray origin k_edge_init left there
         eb.La[s] = w.L[s];
         w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
         w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
         w.cur[s] = make_float4(hb.x, hb.y, hb.z, 0.f);
-        w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+        w.org[s] = eo;
       }
     }
     const int k = warp_append(&w.cnt[0], alive);
@@ -1340,7 +1379,11 @@ __global__ void __launch_bounds__(256) k_edge_final(WF w, const DevScene* __rest
       const float* gp = V.dimage + 3 * (size_t)pix;
       const float K = (gp[0] * dL.x + gp[1] * dL.y + gp[2] * dL.z) / (pdf_e * a.w * (float)spp);
       const float3 nrm = xyz(nn);
-      const float3 ax = nrm * K;
+      // x_dot_n = (x_e - detach(x_e)).n + (o - detach(o)).nflip; an orthographic ray's
+      // origin o is x_e's foot on the camera plane and moves with x_e as well
+      const float3 nflip = f3(nrm.x, nrm.y, -nrm.z);
+      const float3 jo = V.ortho ? ortho_origin_jt(V, nflip) : f3(0.f, 0.f, 0.f);
+      const float3 ax = (nrm + jo) * K;
       const int e = __float_as_int(a.x);
       const float ss = a.y;
       if (sc.grad_verts) {
@@ -1348,7 +1391,7 @@ __global__ void __launch_bounds__(256) k_edge_final(WF w, const DevScene* __rest
         vert_add(sc, ev.x, ax * (1.f - ss));
         vert_add(sc, ev.y, ax * ss);
       }
-      go += f3(nrm.x, nrm.y, -nrm.z) * K;
+      go += (nflip - jo) * K;
     }
   }
   if (!PRE && V.grad_pos) {
@@ -1692,9 +1735,15 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     }
     int px, py;
     if (!project(V, d0.p, px, py)) continue;
-    const float3 cd = normalize(d0.p - V.pos);
-    const HitRec h2 = trace_closest(sc, V.pos, cd, kTmin, INFINITY);
-    const Surf i2 = make_surf(sc, h2.tri, h2.b1, h2.b2, V.pos);
+    float3 co = V.pos, cd;
+    if (V.ortho) {
+      co = ortho_origin_rn(V, d0.p);
+      cd = view_look_dir(V);
+    } else {
+      cd = normalize(d0.p - V.pos);
+    }
+    const HitRec h2 = trace_closest(sc, co, cd, kTmin, INFINITY);
+    const Surf i2 = make_surf(sc, h2.tri, h2.b1, h2.b2, co);
     if (!(i2.valid && !i2.is_light && sqnorm(i2.p - d0.p) < kEps)) continue;
     const float pdf_xw = s0.sqd * pdf_e * ls.pdf / dot(s0.n, dir);
     // boundary_term (detached quantities)
@@ -1810,8 +1859,21 @@ void make_view(const psdr_camera_desc& c, int spp, DevView& v) {
   for (int i = 0; i < 3; ++i) { cw[i][0] = right[i]; cw[i][1] = nup[i]; cw[i][2] = dir[i]; cw[i][3] = o[i]; }
   cw[3][3] = 1;
   const double nearv = -0.01, farv = -1000.0, inv_nf = 1.0 / (nearv - farv);
-  const double cot = 1.0 / std::tan((double)c.fov * 0.5);
-  cs[0][0] = -cot; cs[1][1] = -cot; cs[2][2] = (nearv + farv) * inv_nf; cs[2][3] = -2 * farv * nearv * inv_nf; cs[3][2] = 1;
+  v.ortho = c.type == PSDR_CAM_ORTHOGRAPHIC;
+  if (v.ortho) {
+    // camera.h:19-31 orthographic(left, right, bottom, top, near, far) = scale * translate
+    // over the view box of camera.h:290-300 (width fov = view_width, height width H / W)
+    const double hw = (double)c.fov / 2, hh = (double)c.height * hw / (double)c.width;
+    cs[0][0] = 2 / (2 * hw);
+    cs[1][1] = 2 / (2 * hh);
+    cs[2][2] = 2 / (nearv - farv);
+    cs[2][3] = cs[2][2] * (-(nearv + farv) / 2);
+    cs[3][3] = 1;
+  } else {
+    const double cot = 1.0 / std::tan((double)c.fov * 0.5);
+    cs[0][0] = -cot; cs[1][1] = -cot; cs[2][2] = (nearv + farv) * inv_nf; cs[2][3] = -2 * farv * nearv * inv_nf;
+    cs[3][2] = 1;
+  }
   sr[0][0] = 0.5 * c.width; sr[1][1] = -0.5 * c.height; sr[2][2] = 1; sr[3][3] = 1;
   tr[0][0] = tr[1][1] = tr[2][2] = tr[3][3] = 1; tr[0][3] = 1; tr[1][3] = -1;
   auto mm = [](const double a[4][4], const double b[4][4], double r[4][4]) {

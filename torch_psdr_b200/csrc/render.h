@@ -16,6 +16,7 @@ struct DevView {
   float r2c[16], c2w[16], w2c[16], c2r[16];
   float3 pos;
   int H, W, spp, scene;
+  int ortho;             // orthographic camera (camera.h:279-353)
   long long sample_off;  // first sample of this view in the job's sample space
   long long pix_off;     // first pixel of this view in the job's pixel space
   float* image;          // (H,W,3) or null
@@ -126,6 +127,7 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
 SceneGradInfo grad_info(const psdr_scene* s);
 void check_config(const psdr_config* c);
 void check_cameras(const psdr_camera_desc* cams, int n);
+void check_estimator_cameras(const psdr_config* cfg, const psdr_camera_desc* cams, int n);
 void scene_build_geometry(psdr_scene* s, cudaStream_t st);
 std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap);
 long long border_segments(const DevView& V);

@@ -150,9 +150,10 @@ class CameraSpec:
     look_from: np.ndarray
     look_at: np.ndarray
     up: np.ndarray
-    vfov: float
+    vfov: float                     # perspective: vertical fov (radians); orthographic: view width
     height: int
     width: int
+    kind: int = 0                   # 0 perspective, 1 orthographic
 
 
 @dataclass
