@@ -250,7 +250,7 @@ inline V3<S> eval_direct(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], int& 
   if (!valid) return value;
   S pdf_xw = is0.sqd * pdf_e * S(pdf_l) / dot(is0.n, dir);
   V3<S> Tb = boundary_term<S, AD>(is0.p, id0.p, xb, is0.n, id0.n, E) / pdf_xw;
-  V3<S> Ts = detach(sc.emit[is0.light]);
+  V3<S> Ts = detach(light_emit(sc, is0));
   V3<S> Td = detach(bsdf_eval(sc, id0, -cd));
   value = mul(mul(Tb, Ts), Td);
   valid = valid && finite3(value);
@@ -393,7 +393,7 @@ inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32
     const double fxfy = raster_fxfy(c.cam);
     const V3<double> o = val3(c.cam_pos);
     // running throughput: the emission, times pi f_r at every vertex the chain leaves
-    V3<double> T = val3(sc.emit[is0.light]);
+    V3<double> T = val3(light_emit(sc, is0));
     // camera connection of a vertex whose reflection hemisphere (its normal) faces the
     // camera: T times its BSDF toward the camera times its camera Jacobian
     auto connect = [&](const Its<S>& v) {

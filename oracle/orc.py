@@ -31,7 +31,8 @@ class OrcMesh(C.Structure):
 
 class OrcLight(C.Structure):
     _fields_ = [("V", C.c_void_p), ("nV", C.c_int), ("F", C.c_void_p), ("nF", C.c_int),
-                ("emit", C.c_float * 3)]
+                ("emit", C.c_float * 3), ("type", C.c_int), ("cube_map", OrcTexture), ("sh9", C.c_float * 27),
+                ("box_min", C.c_float * 3), ("box_max", C.c_float * 3)]
 
 
 class OrcCamera(C.Structure):
@@ -87,12 +88,25 @@ class Marshal:
                                      0 if uv is None else uv.shape[0], _ptr(uvi), mat, t, self._tex(rough),
                                      self._tex(normal))
         self.lights = (OrcLight * max(1, len(spec.lights)))()
+        box = None
+        if any(getattr(l, "kind", 0) != 0 for l in spec.lights):
+            from torch_psdr_b200.synth import env_box
+            box = env_box([c.look_from for c in spec.cameras], [m.vertices for m in spec.meshes])
         for i, l in enumerate(spec.lights):
-            V = np.ascontiguousarray(l.vertices, np.float32)
-            F = np.ascontiguousarray(l.faces, np.int32)
+            kind = int(getattr(l, "kind", 0))
+            if kind == 0:
+                V = np.ascontiguousarray(l.vertices, np.float32)
+                F = np.ascontiguousarray(l.faces, np.int32)
+            else:
+                V = np.zeros((0, 3), np.float32)
+                F = np.zeros((0, 3), np.int32)
             self.keep += [V, F]
+            sh = np.zeros(27, np.float32) if kind != 2 else np.asarray(l.sh9, np.float32).reshape(27)
+            bmin, bmax = box if kind != 0 else (np.zeros(3, np.float32), np.zeros(3, np.float32))
             self.lights[i] = OrcLight(_ptr(V), V.shape[0], _ptr(F), F.shape[0],
-                                      (C.c_float * 3)(*[float(x) for x in l.emit]))
+                                      (C.c_float * 3)(*[float(x) for x in l.emit]), kind,
+                                      self._tex(l.cube_map if kind == 1 else None), (C.c_float * 27)(*map(float, sh)),
+                                      (C.c_float * 3)(*map(float, bmin)), (C.c_float * 3)(*map(float, bmax)))
         self.cams = (OrcCamera * max(1, len(spec.cameras)))()
         for i, c in enumerate(spec.cameras):
             self.cams[i] = OrcCamera((C.c_float * 3)(*map(float, c.look_from)), (C.c_float * 3)(*map(float, c.look_at)),

@@ -273,9 +273,13 @@ struct OrcMesh {
   OrcTexture normal;          // DiffuseBsdfMaterial: 3 channels, kind -1 = none
 };
 struct OrcLight {
-  const float* V; int nV;
+  const float* V; int nV;     // area light mesh (environment lights: ignored)
   const int* F; int nF;
   float emit[3];
+  int type;                   // 0 AreaLight, 1 EnvLight (cube map), 2 SH9Light
+  OrcTexture cube_map;        // EnvLight: UV3f texture
+  float sh9[27];              // SH9Light: 9 x 3 coefficients, row-major
+  float box_min[3], box_max[3];  // environment lights: the bounding box (scene.cc:31-49)
 };
 struct OrcCamera {
   float look_from[3], look_at[3], up[3];
@@ -424,6 +428,8 @@ template <class S> struct Scene {
   std::vector<int> obj_vert_off;
   // lights
   std::vector<V3<S>> emit;
+  std::vector<int> light_kind;          // 0 area, 1 env cube map, 2 SH9
+  std::vector<TexRef> light_tex;        // env: cube map; SH9: the 27 coefficients (c = 27)
   std::vector<int> light_tri0, light_ntri;
   std::vector<Discrete<R>> light_tri_cdf;
   std::vector<double> light_area, light_power;
@@ -610,6 +616,19 @@ template <int K> inline Dual<K> seeded_dual(double v, const double* seed) {
 template <class S> struct Seeder { static S make(double v, const double*, int) { return S(typename Traits<S>::R(v)); } };
 template <int K> struct Seeder<Dual<K>> { static Dual<K> make(double v, const double* s, int k) { return seeded_dual<K>(v, s ? s + (size_t)k * K : nullptr); } };
 
+// emitter.cc:103-119 bounding-box mesh of the environment lights: vertex v has
+// x = max if bit 2, y = max if bit 1, z = max if bit 0; faces and cube-map uvs (a 4 x 3
+// cross layout) as the reference lists them.
+static const int env_box_faces[36] = {
+    0, 1, 2, 3, 2, 1, 4, 5, 6, 7, 6, 5, 0, 4, 1, 5, 1, 4,
+    2, 6, 3, 7, 3, 6, 4, 0, 6, 2, 6, 0, 5, 1, 7, 3, 7, 1};
+static const float env_box_uvs[28] = {0.25f, 0.f, 0.5f, 0.f, 0.f, 1.f / 3, 0.25f, 1.f / 3, 0.5f, 1.f / 3,
+                                      0.75f, 1.f / 3, 1.f, 1.f / 3, 0.f, 2.f / 3, 0.25f, 2.f / 3, 0.5f, 2.f / 3,
+                                      0.75f, 2.f / 3, 1.f, 2.f / 3, 0.25f, 1.f, 0.5f, 1.f};
+static const int env_box_uv_indices[36] = {
+    2, 3, 7, 8, 7, 3, 5, 4, 10, 9, 10, 4, 0, 1, 3, 4, 3, 1,
+    12, 13, 8, 9, 8, 13, 5, 6, 10, 11, 10, 6, 4, 3, 9, 8, 9, 3};
+
 template <class S>
 inline Scene<S> build_scene(const OrcMesh* meshes, int nm, const OrcLight* lights, int nl, const Seeds<S>& seeds) {
   using R = typename Traits<S>::R;
@@ -617,7 +636,7 @@ inline Scene<S> build_scene(const OrcMesh* meshes, int nm, const OrcLight* light
   sc.n_obj = nm + nl;
   int vglob = 0, texoff = 0, tex_elem = 0;
   auto add_mesh = [&](const float* V, int nV, const int* F, int nF, const float* uv, const int* uvi,
-                      int light_id, const OrcTexture* tex) {
+                      int light_id, const OrcTexture* tex, bool edges = true) {
     int obj = (int)sc.obj_light.size();
     sc.obj_light.push_back(light_id);
     sc.obj_vert_off.push_back(vglob);
@@ -651,7 +670,7 @@ inline Scene<S> build_scene(const OrcMesh* meshes, int nm, const OrcLight* light
       tri_attrs(t);
       sc.tris.push_back(t);
     }
-    build_edges(sc, vglob, F, nF);
+    if (edges) build_edges(sc, vglob, F, nF);
     vglob += nV;
   };
   for (int m = 0; m < nm; ++m) {
@@ -681,20 +700,46 @@ inline Scene<S> build_scene(const OrcMesh* meshes, int nm, const OrcLight* light
     V3<S> e;
     for (int k = 0; k < 3; ++k) e[k] = Seeder<S>::make(Lg.emit[k], seeds.emit, 3 * l + k);
     sc.emit.push_back(e);
+    sc.light_kind.push_back(Lg.type);
     sc.light_tri0.push_back((int)sc.tris.size());
-    sc.light_ntri.push_back(Lg.nF);
-    add_mesh(Lg.V, Lg.nV, Lg.F, Lg.nF, nullptr, nullptr, l, nullptr);
+    if (Lg.type == 0) {
+      sc.light_tex.push_back(typename Scene<S>::TexRef{});
+      sc.light_ntri.push_back(Lg.nF);
+      add_mesh(Lg.V, Lg.nV, Lg.F, Lg.nF, nullptr, nullptr, l, nullptr);
+    } else {
+      // emitter.cc:97-131 / 221-244 set_aabb: the bounding box as a 12-triangle mesh
+      // (cube-map uvs for EnvLight), outside the edge list (scene.cc:59-62)
+      float bv[24];
+      for (int v = 0; v < 8; ++v) {
+        bv[3 * v] = (v & 4) ? Lg.box_max[0] : Lg.box_min[0];
+        bv[3 * v + 1] = (v & 2) ? Lg.box_max[1] : Lg.box_min[1];
+        bv[3 * v + 2] = (v & 1) ? Lg.box_max[2] : Lg.box_min[2];
+      }
+      if (Lg.type == 1) {
+        sc.light_tex.push_back(add_tex(Lg.cube_map, 3));
+      } else {
+        typename Scene<S>::TexRef r;
+        r.kind = 0; r.h = 1; r.w = 1; r.c = 27; r.off = texoff;
+        for (int k = 0; k < 27; ++k) sc.tex.push_back(Seeder<S>::make(Lg.sh9[k], seeds.tex, tex_elem + k));
+        texoff += 27; tex_elem += 27;
+        sc.light_tex.push_back(r);
+      }
+      sc.light_ntri.push_back(12);
+      add_mesh(bv, 8, env_box_faces, 12, Lg.type == 1 ? env_box_uvs : nullptr,
+               Lg.type == 1 ? env_box_uv_indices : nullptr, l, nullptr, false);
+    }
     sc.obj_mat.push_back(0);
     sc.obj_rough.push_back(typename Scene<S>::TexRef{});
     sc.obj_nrm.push_back(typename Scene<S>::TexRef{});
     std::vector<double> areas;
     double tot = 0;
-    for (int f = 0; f < Lg.nF; ++f) { double a = double(R(val(sc.tris[sc.light_tri0[l] + f].area))); areas.push_back(a); tot += a; }
+    for (int f = 0; f < sc.light_ntri[l]; ++f) { double a = double(R(val(sc.tris[sc.light_tri0[l] + f].area))); areas.push_back(a); tot += a; }
     Discrete<R> d; d.build(areas);
     sc.light_tri_cdf.push_back(d);
-    // emitter.cc:10-11 power = 2*pi*luminance(emit)*area
+    // emitter.cc:10-11 power = 2*pi*luminance(emit)*area; environment lights 4*pi
+    // (emitter.cc:130, 243)
     double lum = double(Lg.emit[0]) * 0.2126 + double(Lg.emit[1]) * 0.7152 + double(Lg.emit[2]) * 0.0722;
-    double pw = 2 * M_PI * lum * tot;
+    double pw = Lg.type == 0 ? 2 * M_PI * lum * tot : 4 * M_PI;
     sc.light_area.push_back(tot);
     sc.light_power.push_back(pw);
     powers.push_back(pw);
@@ -855,6 +900,28 @@ inline V3<S> material_sample_dir(const Scene<S>& sc, const Its<S>& its, typename
   return normalize(its.t * S(cp * st) + B * S(sp * st) + N * S(ct));
 }
 
+// Radiance of a light hit: AreaLight's constant (emitter.cc:17-28), EnvLight's cube map
+// at the box uv (emitter.cc:134-141; diffuse_material.h:53-58), SH9Light's second-order
+// real spherical harmonics at the hit's incoming direction (emitter.cc:246-283).
+template <class S>
+inline V3<S> light_emit(const Scene<S>& sc, const Its<S>& its) {
+  using R = typename Traits<S>::R;
+  const int l = its.light;
+  const int kind = sc.light_kind[l];
+  if (kind == 0) return sc.emit[l];
+  if (kind == 1) return tex_fetch(sc, sc.light_tex[l], its.u, its.v);
+  const S x = its.wi.x, y = its.wi.y, z = its.wi.z;
+  const R c0 = R(std::sqrt(1.0 / (4 * M_PI))), c1 = R(std::sqrt(0.75 / M_PI)), c2 = R(std::sqrt(3.75 / M_PI));
+  const R c3 = R(std::sqrt(5.0 / 16.0 / M_PI)), c4 = R(std::sqrt(15.0 / 16.0 / M_PI));
+  const S Y[9] = {S(c0), S(c1) * y, S(c1) * z, S(c1) * x, S(c2) * (x * y), S(c2) * (y * z),
+                  S(c3) * (S(R(2)) * (z * z) - x * x - y * y), S(c2) * (z * x), S(c4) * (x * x - y * y)};
+  const int off = sc.light_tex[l].off;
+  V3<S> e;
+  for (int k = 0; k < 9; ++k)
+    for (int ch = 0; ch < 3; ++ch) e[ch] = e[ch] + sc.tex[off + 3 * k + ch] * Y[k];
+  return e;
+}
+
 // path_integrator.cc:3-9 (power heuristic, n1/n2 sample counts)
 template <class R> inline R mis_w(R w1, R w2, R n1, R n2) {
   R a = (n1 * w1) * (n1 * w1), b = (n2 * w2) * (n2 * w2);
@@ -890,7 +957,7 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
   const R eps = R(1e-5);
   for (int depth = 0; depth < D; ++depth) {
     bool hit_light = valid && its.is_light;
-    if (light_vis && depth == 0 && hit_light) L = L + mul(T, sc.emit[its.light]);
+    if (light_vis && depth == 0 && hit_light) L = L + mul(T, light_emit(sc, its));
     valid = valid && !hit_light;
     for (int i = 0; i < nL; ++i) {
       R rx = rng.next_float(valid), ry = rng.next_float(valid);
@@ -905,7 +972,7 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
       Its<S> il = scene_hit<S, AD>(sc, its.p, dir, true);
       bool is_hit = il.valid && il.is_light && val(sqnorm(il.p - y)) < double(eps);
       if (!is_hit) continue;
-      V3<S> emit = sc.emit[l];
+      V3<S> emit = light_emit(sc, il);
       V3<S> bsdf = bsdf_eval(sc, its, dir);
       S tmp = dot(il.n, -dir) / il.sqd;
       S G = dot(its.n, dir) * tmp;
@@ -925,7 +992,7 @@ inline V3<S> trace2light(const Scene<S>& sc, Pcg32& rng, Its<S> its, bool valid,
       Its<S> il = scene_hit<S, AD>(sc, its.p, wo, true);
       bool is_hit = il.valid && il.is_light;
       if (!is_hit) continue;
-      V3<S> emit = sc.emit[il.light];
+      V3<S> emit = light_emit(sc, il);
       S tmp = dot(il.n, -wo) / il.sqd;
       S G = dot(its.n, wo) * tmp;
       V3<S> Lb = wo;

@@ -140,9 +140,12 @@ class MeshSpec:
 
 @dataclass
 class LightSpec:
-    vertices: np.ndarray
-    faces: np.ndarray
-    emit: np.ndarray
+    vertices: np.ndarray | None     # AreaLight mesh (environment lights: None)
+    faces: np.ndarray | None
+    emit: np.ndarray                # AreaLight radiance (environment lights: unused)
+    kind: int = 0                   # 0 AreaLight, 1 EnvLight, 2 SH9Light
+    cube_map: np.ndarray | None = None  # EnvLight: (H, W, 3) cube-map cross (4 x 3 faces)
+    sh9: np.ndarray | None = None       # SH9Light: (9, 3) coefficients
 
 
 @dataclass
@@ -211,3 +214,22 @@ def orbit_cameras(n, radius, seed, size_lo=128, size_hi=512):
         cams.append(CameraSpec((d * radius).astype(np.float32), np.zeros(3, np.float32), up,
                                math.pi / 4, int(hw[0]), int(hw[1])))
     return cams
+
+
+def env_box(cam_positions, mesh_vertices):
+    """Bounding box of the environment lights (scene.cc:31-49), in float32 like the
+    reference: the box of the camera positions and mesh vertices, its centre c and
+    d = 1000 * its largest extent; returns (c - d, c + d)."""
+    pmin = np.asarray(cam_positions[0], np.float32).copy()
+    pmax = pmin.copy()
+    for p in cam_positions:
+        p = np.asarray(p, np.float32)
+        pmin = np.minimum(pmin, p)
+        pmax = np.maximum(pmax, p)
+    for v in mesh_vertices:
+        v = np.asarray(v, np.float32).reshape(-1, 3)
+        pmin = np.minimum(pmin, v.min(0))
+        pmax = np.maximum(pmax, v.max(0))
+    d = np.float32(1000) * np.max(pmax - pmin)
+    c = (pmin + pmax) * np.float32(0.5)
+    return (c - d).astype(np.float32), (c + d).astype(np.float32)
