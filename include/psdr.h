@@ -44,6 +44,7 @@ typedef enum {
 enum { PSDR_TEX_NONE = -1, PSDR_TEX_CONSTANT = 0, PSDR_TEX_UV = 1 };
 enum { PSDR_MAT_DIFFUSE = 0, PSDR_MAT_DIFFUSE_BSDF = 1 };
 enum { PSDR_CAM_PERSPECTIVE = 0, PSDR_CAM_ORTHOGRAPHIC = 1 };
+enum { PSDR_LIGHT_AREA = 0, PSDR_LIGHT_ENV = 1, PSDR_LIGHT_SH9 = 2 };
 enum { PSDR_EST_REFERENCE = 0, PSDR_EST_UNBIASED = 1 };
 
 /* A texture (texture.h:16-111; torch_psdr.py:209-269 Texture).
@@ -70,11 +71,22 @@ typedef struct {
   psdr_texture_desc normal;                     /* DiffuseBsdf only, kind NONE if absent */
 } psdr_mesh_desc;
 
-/* An area light (emitter.cc:4-14 AreaLight; torch_psdr.py:388-414). emit is host data. */
+/* A light. AREA (emitter.cc:4-14 AreaLight; torch_psdr.py:388-414): a triangle mesh
+ * of constant radiance emit (host data). ENV / SH9 (emitter.cc:94-352 EnvLight,
+ * SH9Light; torch_psdr.py:417-452): the library builds the reference's 12-triangle box
+ * from box_min / box_max, which the caller computes as scene.cc:31-49 does (the box of
+ * the camera positions and mesh vertices around its centre, scaled to 1000 times its
+ * largest extent); vertices / faces / emit are ignored. ENV emits its cube map (UV3f,
+ * the 4 x 3 cross of the reference's box uvs); SH9 emits sum_k sh9[3k + c] Y_k(wi) of
+ * the hit's incoming direction wi. At most one ENV / SH9 light, the last of the array. */
 typedef struct {
   const float* vertices; int32_t num_vertices;
   const int32_t* faces;  int32_t num_faces;
   float emit[3];
+  int32_t type;                  /* PSDR_LIGHT_* */
+  psdr_texture_desc cube_map;    /* ENV */
+  float sh9[27];                 /* SH9: (9,3) row-major, host data */
+  float box_min[3], box_max[3];  /* ENV / SH9 */
 } psdr_area_light_desc;
 
 typedef struct {
@@ -128,6 +140,8 @@ typedef struct {
  * emit: one (3,) buffer per light, may be NULL. camera_origin: one (3,) per camera.
  * roughness / normal: one per mesh (same shape as a DiffuseBsdfMaterial's roughness
  * and normal textures; ignored for other meshes), may be NULL.
+ * light_params: one per light: an ENV light's cube-map gradient (its texture's shape),
+ * an SH9 light's (9,3) coefficient gradient; ignored for AREA lights; may be NULL.
  * With accumulate = 0 the outputs are overwritten, otherwise added to. */
 typedef struct {
   float** vertices;
@@ -137,6 +151,7 @@ typedef struct {
   int32_t accumulate;
   float** roughness;
   float** normal;
+  float** light_params;
 } psdr_grad_targets;
 
 /* ---------------------------------------------------------------- general */

@@ -10,8 +10,9 @@ from torch_psdr_b200 import synth
 
 def to_torch_scene(spec, requires_grad=(), device="cuda"):
     """Build a dr.Scene from a synth.SceneSpec. requires_grad: subset of
-    {"verts", "tex", "rough", "normal", "light_verts", "emit", "cam"}; returns (scene, dict
-    of tensors). Meshes with a roughness get a DiffuseBsdfMaterial."""
+    {"verts", "tex", "rough", "normal", "light_verts", "emit", "env", "cam"}; returns
+    (scene, dict of tensors). Meshes with a roughness get a DiffuseBsdfMaterial; lights of
+    kind 1 / 2 become EnvLight / SH9Light (their parameters under "env{j}")."""
     T = {}
     meshes = []
     for i, m in enumerate(spec.meshes):
@@ -38,6 +39,17 @@ def to_torch_scene(spec, requires_grad=(), device="cuda"):
         meshes.append(dr.Mesh(v, uv, f, uvi, mat))
     lights = []
     for j, l in enumerate(spec.lights):
+        kind = getattr(l, "kind", 0)
+        if kind == 1:
+            cube = torch.tensor(l.cube_map, dtype=torch.float32, device=device, requires_grad="env" in requires_grad)
+            T[f"env{j}"] = cube
+            lights.append(dr.EnvLight(dr.Texture(cube)))
+            continue
+        if kind == 2:
+            sh = torch.tensor(l.sh9, dtype=torch.float32, device=device, requires_grad="env" in requires_grad)
+            T[f"env{j}"] = sh
+            lights.append(dr.SH9Light(sh))
+            continue
         v = torch.tensor(l.vertices, dtype=torch.float32, device=device, requires_grad="light_verts" in requires_grad)
         f = torch.tensor(l.faces, dtype=torch.int32, device=device)
         e = torch.tensor(l.emit, dtype=torch.float32, device=device, requires_grad="emit" in requires_grad)

@@ -20,6 +20,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "TIMEOU
 TEX_NONE, TEX_CONSTANT, TEX_UV = -1, 0, 1
 MAT_DIFFUSE, MAT_DIFFUSE_BSDF = 0, 1
 CAM_PERSPECTIVE, CAM_ORTHOGRAPHIC = 0, 1
+LIGHT_AREA, LIGHT_ENV, LIGHT_SH9 = 0, 1, 2
 EST_REFERENCE, EST_UNBIASED = 0, 1
 
 
@@ -37,7 +38,9 @@ class MeshDesc(C.Structure):
 
 class AreaLightDesc(C.Structure):
     _fields_ = [("vertices", C.c_void_p), ("num_vertices", C.c_int32), ("faces", C.c_void_p),
-                ("num_faces", C.c_int32), ("emit", C.c_float * 3)]
+                ("num_faces", C.c_int32), ("emit", C.c_float * 3), ("type", C.c_int32),
+                ("cube_map", TextureDesc), ("sh9", C.c_float * 27), ("box_min", C.c_float * 3),
+                ("box_max", C.c_float * 3)]
 
 
 class SceneDesc(C.Structure):
@@ -65,7 +68,7 @@ class GradTargets(C.Structure):
     _fields_ = [("vertices", C.POINTER(C.c_void_p)), ("textures", C.POINTER(C.c_void_p)),
                 ("emit", C.POINTER(C.c_void_p)), ("camera_origin", C.POINTER(C.c_void_p)),
                 ("accumulate", C.c_int32), ("roughness", C.POINTER(C.c_void_p)),
-                ("normal", C.POINTER(C.c_void_p))]
+                ("normal", C.POINTER(C.c_void_p)), ("light_params", C.POINTER(C.c_void_p))]
 
 
 # Every symbol include/psdr.h declares, with its ctypes signature.

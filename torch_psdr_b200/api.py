@@ -15,6 +15,7 @@ import torch
 from torch import Tensor
 
 from . import _lib as L
+from . import synth
 
 
 def _dev_tensor(t: Tensor, dtype) -> Tensor:
@@ -284,18 +285,47 @@ class AreaLight(Light):
 
 class EnvLight(Light):
     def __init__(self, cube_map: Texture):
-        """Cube-map environment light (torch_psdr.py:417-430). Not built on this path."""
+        """Cube-map environment light (torch_psdr.py:417-430; emitter.cc:94-141): an
+        emissive box around the scene, 1000 times its size (scene.cc:31-49), showing the
+        cube map laid out as a 4 x 3 cross."""
         super().__init__()
         assert cube_map.tex_type == "UV3f"
-        raise NotImplementedError("EnvLight is not available in torch_psdr_b200")
+        self.cube_map = cube_map
+        self.merge_variables(cube_map.get_variables())
+        self.vertices = self.v = self.emit = None
+        self.params, self.params_data = cube_map.tensor, cube_map.data
+
+    def _desc(self, box):
+        d = L.AreaLightDesc()
+        d.type = L.LIGHT_ENV
+        d.cube_map = self.cube_map._desc()
+        d.box_min, d.box_max = (C.c_float * 3)(*map(float, box[0])), (C.c_float * 3)(*map(float, box[1]))
+        return d
 
 
 class SH9Light(Light):
     def __init__(self, sh9_coeff: Tensor):
-        """Spherical-harmonics light (torch_psdr.py:433-447). Not built on this path."""
+        """Second-order spherical-harmonics light (torch_psdr.py:433-447;
+        emitter.cc:206-283): the same box as EnvLight, emitting sum_k c_k Y_k(wi) of the
+        incoming direction wi at its hit point. sh9_coeff: (9, 3)."""
         super().__init__()
         assert sh9_coeff.size() == (9, 3)
-        raise NotImplementedError("SH9Light is not available in torch_psdr_b200")
+        self.sh9_coeff = sh9_coeff
+        self.append_variable(sh9_coeff)
+        self.vertices = self.v = self.emit = None
+        self.params = sh9_coeff
+        self.params_data = torch.zeros((9, 3), dtype=torch.float32, device="cuda")
+
+    def _desc(self, box):
+        d = L.AreaLightDesc()
+        d.type = L.LIGHT_SH9
+        d.sh9 = (C.c_float * 27)(*self.sh9_coeff.detach().reshape(-1).cpu().tolist())
+        d.box_min, d.box_max = (C.c_float * 3)(*map(float, box[0])), (C.c_float * 3)(*map(float, box[1]))
+        return d
+
+
+def _is_env(light):
+    return isinstance(light, (EnvLight, SH9Light))
 
 
 class Scene(VarContex):
@@ -305,10 +335,19 @@ class Scene(VarContex):
         super().__init__()
         self.cameras = list(cameras)
         self.meshes = list(meshes)
-        self.lights = list(lights)
+        # scene.cc:15-53: one environment light, appended after the other lights around the
+        # box of the camera positions and mesh vertices (self.lights keeps that order)
+        env = [lt for lt in lights if _is_env(lt)]
+        assert len(env) <= 1, "only support no more than one env_light"
+        self.lights = [lt for lt in lights if not _is_env(lt)] + env
+        box = None
+        if env:
+            box = synth.env_box([c.look_from.detach().cpu().numpy() for c in self.cameras],
+                                [m.v.detach().cpu().numpy() for m in self.meshes])
         lib = L.load()
         md = (L.MeshDesc * max(1, len(self.meshes)))(*[m._desc() for m in self.meshes])
-        ld = (L.AreaLightDesc * max(1, len(self.lights)))(*[lt._desc() for lt in self.lights])
+        ld = (L.AreaLightDesc * max(1, len(self.lights)))(*[lt._desc(box) if _is_env(lt) else lt._desc()
+                                                            for lt in self.lights])
         desc = L.SceneDesc(md, len(self.meshes), ld, len(self.lights))
         handle = C.c_void_p()
         L.check(lib.psdr_scene_create(C.byref(desc), _stream(), C.byref(handle)), "psdr_scene_create")
@@ -501,13 +540,14 @@ class PathIntegrator:
         rough_g = [_tex_grad(m.material.roughness) for m in scene.meshes]
         nrm_g = [_tex_grad(m.material.normal) for m in scene.meshes]
         emit_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.lights]
+        light_g = [_grad_buf(lt.params, lt.params_data) if _is_env(lt) else None for lt in scene.lights]
         cam_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.cameras]
         P = C.c_void_p
         vp = (P * (nm + nl))(*[None if t is None else t.data_ptr() for t in vert_g])
         tp = (P * max(1, nm))(*[None if t is None else t.data_ptr() for t in tex_g])
         ep = (P * max(1, nl))(*[t.data_ptr() for t in emit_g])
         cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
-        tg = L.GradTargets(vp, tp, ep, cp, 0, _ptrs(rough_g), _ptrs(nrm_g))
+        tg = L.GradTargets(vp, tp, ep, cp, 0, _ptrs(rough_g), _ptrs(nrm_g), _ptrs(light_g))
         dp = (P * len(dimgs))(*[d.data_ptr() for d in dimgs])
         cams = scene._camera_descs()
         L.check(self._lib.psdr_render_bwd(scene.handle, self._workspace(), cams, len(dimgs), C.byref(self.cfg), dp,
@@ -532,6 +572,8 @@ class PathIntegrator:
         for j, lt in enumerate(scene.lights):
             add(lt.vertices, vert_g[nm + j])
             add(lt.emit, emit_g[j])
+            if light_g[j] is not None:
+                add(lt.params, light_g[j])
         for k, c in enumerate(scene.cameras):
             add(c.look_from, cam_g[k])
             for t in (c.look_at, c.up, c.vfov):
@@ -594,10 +636,11 @@ class BatchRender:
             eg = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in sc.lights]
             rg = [_tex_grad(m.material.roughness) for m in sc.meshes]
             ng = [_tex_grad(m.material.normal) for m in sc.meshes]
-            self.grads.append((vg, tg, eg, rg, ng))
-            vp, tp, ep, rp, npp = _ptrs(vg), _ptrs(tg), _ptrs(eg), _ptrs(rg), _ptrs(ng)
-            self._keep += [vp, tp, ep, rp, npp]
-            targets.append(L.GradTargets(vp, tp, ep, cp, 0, rp, npp))
+            lg = [_grad_buf(lt.params, lt.params_data) if _is_env(lt) else None for lt in sc.lights]
+            self.grads.append((vg, tg, eg, rg, ng, lg))
+            vp, tp, ep, rp, npp, lp = _ptrs(vg), _ptrs(tg), _ptrs(eg), _ptrs(rg), _ptrs(ng), _ptrs(lg)
+            self._keep += [vp, tp, ep, rp, npp, lp]
+            targets.append(L.GradTargets(vp, tp, ep, cp, 0, rp, npp, lp))
         self._keep.append(cp)
         tgt = (L.GradTargets * len(targets))(*targets)
         sh = (P * len(self.scenes))(*[s.handle for s in self.scenes])
@@ -651,7 +694,7 @@ class BatchRender:
             acc[id(t)] = g if id(t) not in acc else acc[id(t)] + g
 
         k = 0
-        for sc, (vg, tg, eg, rg, ng) in zip(self.scenes, self.grads):
+        for sc, (vg, tg, eg, rg, ng, lg) in zip(self.scenes, self.grads):
             nm = len(sc.meshes)
             for i, m in enumerate(sc.meshes):
                 add(m.vertices, vg[i])
@@ -663,6 +706,8 @@ class BatchRender:
             for j, lt in enumerate(sc.lights):
                 add(lt.vertices, vg[nm + j])
                 add(lt.emit, eg[j])
+                if lg[j] is not None:
+                    add(lt.params, lg[j])
             for c in sc.cameras:
                 add(c.look_from, self.cam_grads[k])
                 for t in (c.look_at, c.up, c.vfov):

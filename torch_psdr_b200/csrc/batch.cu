@@ -24,7 +24,7 @@ struct psdr_batch {
   bool rebuild = true;
   psdr::SceneGradInfo gi;
   // gradient targets, deep-copied pointer arrays per scene
-  std::vector<std::vector<float*>> gv, gt, ge, gr, gn;
+  std::vector<std::vector<float*>> gv, gt, ge, gr, gn, gl;
   std::vector<float*> gc;
   std::vector<int> gacc;
   std::vector<std::unique_ptr<psdr::DBuf>> vmasks;  // per-scene vertex-gradient masks of this batch's targets
@@ -160,12 +160,13 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     if (n_scenes == 1) b->gi = grad_info(scenes[0]);
     b->ws.bsdf = 0;
     for (int i = 0; i < n_scenes; ++i)
-      if (scenes[i]->has_bsdf) b->gi.bsdf = b->ws.bsdf = 1;
+      if (scenes[i]->has_bsdf || scenes[i]->env_light >= 0) b->gi.bsdf = b->ws.bsdf = 1;
     if (b->backward) {
       b->gv.resize(n_scenes);
       b->gt.resize(n_scenes);
       b->gr.resize(n_scenes);
       b->gn.resize(n_scenes);
+      b->gl.resize(n_scenes);
       b->ge.resize(n_scenes);
       b->gacc.resize(n_scenes);
       for (int i = 0; i < n_scenes; ++i) {
@@ -178,7 +179,10 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
           b->gr[i].push_back(g.roughness && s->rough_grad_off[m] != SIZE_MAX ? g.roughness[m] : nullptr);
           b->gn[i].push_back(g.normal && s->nrm_grad_off[m] != SIZE_MAX ? g.normal[m] : nullptr);
         }
-        for (int l = 0; l < s->nlight; ++l) b->ge[i].push_back(g.emit ? g.emit[l] : nullptr);
+        for (int l = 0; l < s->nlight; ++l) {
+          b->ge[i].push_back(g.emit ? g.emit[l] : nullptr);
+          b->gl[i].push_back(g.light_params && s->light_grad_off[l] != SIZE_MAX ? g.light_params[l] : nullptr);
+        }
         b->gacc[i] = g.accumulate;
       }
       for (int c = 0; c < n_cams; ++c) {
@@ -258,8 +262,12 @@ PSDR_API psdr_status psdr_batch_backward(psdr_batch* b, void* stream) {
               grad_out(s->g_tex.as<double>() + s->nrm_grad_off[m], b->gn[i][m],
                        (long long)ob.normal.h * ob.normal.w * 3, b->gacc[i], st);
           }
-          for (int l = 0; l < s->nlight; ++l)
+          for (int l = 0; l < s->nlight; ++l) {
             grad_out(s->g_emit.as<double>() + 3 * l, b->ge[i][l], 3, b->gacc[i], st);
+            if (b->gl[i][l])
+              grad_out(s->g_tex.as<double>() + s->light_grad_off[l], b->gl[i][l], light_param_count(s, l), b->gacc[i],
+                       st);
+          }
         }
         for (size_t c = 0; c < b->views.size(); ++c)
           grad_out(b->campos.as<double>() + 3 * c, b->gc[c], 3, b->gacc[b->views[c].scene], st);

@@ -95,7 +95,7 @@ DevScene* dev_scene(psdr_scene* s) { return s->d_dev.as<DevScene>(); }
 
 SceneGradInfo grad_info(const psdr_scene* s) {
   SceneGradInfo gi;
-  gi.bsdf = s->has_bsdf ? 1 : 0;
+  gi.bsdf = s->has_bsdf || s->env_light >= 0 ? 1 : 0;
   const int nm = (int)s->meshes.size();
   if (s->nlight == 1) {
     gi.emit_hot = 1;
@@ -109,6 +109,13 @@ SceneGradInfo grad_info(const psdr_scene* s) {
 
 void check_config(const psdr_config* c) { check_cfg(c); }
 void check_cameras(const psdr_camera_desc* cams, int n) { check_cams(cams, n); }
+
+// Elements of an environment light's parameter gradient (cube map or SH coefficients).
+long long light_param_count(const psdr_scene* s, int l) {
+  const DevLight& L = s->h_lights[l];
+  if (L.kind == PSDR_LIGHT_ENV) return (long long)L.tex.h * L.tex.w * 3;
+  return L.kind == PSDR_LIGHT_SH9 ? 27 : 0;
+}
 
 // The unbiased estimator's camera Jacobians and raster velocities are those of the
 // perspective camera.
@@ -144,7 +151,18 @@ extern "C" {
 
 const char* psdr_last_error(void) { return psdr::g_err.c_str(); }
 const char* psdr_version(void) { return "torch_psdr_b200 0.1.0 (sm_100a)"; }
-int32_t psdr_abi_version(void) { return 3; }
+int32_t psdr_abi_version(void) { return 4; }
+
+// emitter.cc:103-119: the environment lights' bounding-box mesh. Vertex v has x = max if
+// bit 2, y = max if bit 1, z = max if bit 0; the faces and the cube-map uvs (a 4 x 3 cross)
+// are the reference's tables.
+const int kEnvFaces[36] = {0, 1, 2, 3, 2, 1, 4, 5, 6, 7, 6, 5, 0, 4, 1, 5, 1, 4,
+                           2, 6, 3, 7, 3, 6, 4, 0, 6, 2, 6, 0, 5, 1, 7, 3, 7, 1};
+const float kEnvUvs[28] = {0.25f, 0.f, 0.5f, 0.f, 0.f, 1.f / 3, 0.25f, 1.f / 3, 0.5f, 1.f / 3,
+                           0.75f, 1.f / 3, 1.f, 1.f / 3, 0.f, 2.f / 3, 0.25f, 2.f / 3, 0.5f, 2.f / 3,
+                           0.75f, 2.f / 3, 1.f, 2.f / 3, 0.25f, 1.f, 0.5f, 1.f};
+const int kEnvUvIndices[36] = {2, 3, 7, 8, 7, 3, 5, 4, 10, 9, 10, 4, 0, 1, 3, 4, 3, 1,
+                               12, 13, 8, 9, 8, 13, 5, 6, 10, 11, 10, 6, 4, 3, 9, 8, 9, 3};
 
 psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_scene** out) {
   API_BEGIN
@@ -162,6 +180,39 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
     s->lights.assign(desc->lights, desc->lights + nl);
     s->nobj = nm + nl;
     s->nlight = nl;
+    // environment light (scene.cc:15-53): at most one, appended after the other lights
+    for (int l = 0; l < nl; ++l) {
+      const psdr_area_light_desc& L = s->lights[l];
+      PSDR_CHECK(L.type == PSDR_LIGHT_AREA || L.type == PSDR_LIGHT_ENV || L.type == PSDR_LIGHT_SH9, "bad light type");
+      if (L.type == PSDR_LIGHT_AREA) continue;
+      PSDR_CHECK(l == nl - 1, "the environment light (EnvLight / SH9Light) must be the last light, and only one");
+      PSDR_CHECK(nm > 0, "an environment light needs a mesh in the scene");
+      for (int k = 0; k < 3; ++k) PSDR_CHECK(L.box_max[k] > L.box_min[k], "empty environment light box");
+      if (L.type == PSDR_LIGHT_ENV) {
+        check_tex(L.cube_map, "cube_map", false);
+        PSDR_CHECK(L.cube_map.kind == PSDR_TEX_UV && L.cube_map.channels == 3, "cube map must be a UV3f texture");
+      }
+      s->env_light = l;
+      cudaStream_t st = s->stream;
+      for (int v = 0; v < 8; ++v) {
+        s->env_host_v[3 * v] = (v & 4) ? L.box_max[0] : L.box_min[0];
+        s->env_host_v[3 * v + 1] = (v & 2) ? L.box_max[1] : L.box_min[1];
+        s->env_host_v[3 * v + 2] = (v & 1) ? L.box_max[2] : L.box_min[2];
+      }
+      s->env_v.alloc(sizeof(float) * 24, st);
+      s->env_f.alloc(sizeof(int) * 36, st);
+      s->env_uv.alloc(sizeof(float) * 28, st);
+      s->env_uvi.alloc(sizeof(int) * 36, st);
+      PSDR_CUDA(cudaMemcpyAsync(s->env_v.p, s->env_host_v, sizeof(float) * 24, cudaMemcpyHostToDevice, st));
+      PSDR_CUDA(cudaMemcpyAsync(s->env_f.p, kEnvFaces, sizeof(int) * 36, cudaMemcpyHostToDevice, st));
+      PSDR_CUDA(cudaMemcpyAsync(s->env_uv.p, kEnvUvs, sizeof(float) * 28, cudaMemcpyHostToDevice, st));
+      PSDR_CUDA(cudaMemcpyAsync(s->env_uvi.p, kEnvUvIndices, sizeof(int) * 36, cudaMemcpyHostToDevice, st));
+      PSDR_CUDA(cudaStreamSynchronize(st));
+      s->lights[l].vertices = s->env_v.as<float>();
+      s->lights[l].num_vertices = 8;
+      s->lights[l].faces = s->env_f.as<int>();
+      s->lights[l].num_faces = 12;
+    }
     int voff = 0, toff = 0;
     size_t texoff = 0;
     for (int o = 0; o < s->nobj; ++o) {
@@ -233,10 +284,24 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
     s->nvert = voff;
     s->ntri = toff;
     for (int l = 0; l < nl; ++l) {
+      const psdr_area_light_desc& D = s->lights[l];
       DevLight L{};
       L.tri0 = s->obj_tri_off[nm + l];
       L.ntri = s->obj_ntri[nm + l];
-      for (int k = 0; k < 3; ++k) L.emit[k] = s->lights[l].emit[k];
+      for (int k = 0; k < 3; ++k) L.emit[k] = D.emit[k];
+      L.kind = D.type;
+      L.tex.kind = -1;
+      size_t go = SIZE_MAX;
+      if (D.type == PSDR_LIGHT_ENV) {
+        L.tex = DevTex{PSDR_TEX_UV, 3, D.cube_map.height, D.cube_map.width, D.cube_map.data, nullptr};
+        go = texoff;
+        texoff += (size_t)D.cube_map.height * D.cube_map.width * 3;
+      } else if (D.type == PSDR_LIGHT_SH9) {
+        for (int k = 0; k < 27; ++k) L.sh[k] = D.sh9[k];
+        go = texoff;
+        texoff += 27;
+      }
+      s->light_grad_off.push_back(go);
       s->h_lights.push_back(L);
     }
     s->dev.ltri_base = nl > 0 ? s->obj_tri_off[nm] : 0;
@@ -255,7 +320,13 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
       if (s->rough_grad_off[o] != SIZE_MAX) s->h_objs[o].rough.grad = s->g_tex.as<double>() + s->rough_grad_off[o];
       if (s->nrm_grad_off[o] != SIZE_MAX) s->h_objs[o].normal.grad = s->g_tex.as<double>() + s->nrm_grad_off[o];
     }
-    for (int l = 0; l < nl; ++l) s->h_lights[l].grad_emit = s->g_emit.as<double>() + 3 * l;
+    for (int l = 0; l < nl; ++l) {
+      s->h_lights[l].grad_emit = s->g_emit.as<double>() + 3 * l;
+      if (s->light_grad_off[l] == SIZE_MAX) continue;
+      double* g = s->g_tex.as<double>() + s->light_grad_off[l];
+      if (s->h_lights[l].kind == PSDR_LIGHT_ENV) s->h_lights[l].tex.grad = g;
+      else s->h_lights[l].grad_sh = g;
+    }
     s->upload_tables();
     scene_build_geometry(s, s->stream);
   } catch (...) {
@@ -350,7 +421,7 @@ psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   PSDR_CHECK(scene && ws && images, "null argument");
   check_cfg(cfg);
   check_cams(cams, n_cams);
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
+  ws->bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;  // extended kernel instances
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
   std::vector<DevView> views(n_cams);
   for (int i = 0; i < n_cams; ++i) {
@@ -368,7 +439,7 @@ psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psd
   PSDR_CHECK(scene && ws && samples, "null argument");
   check_cfg(cfg);
   check_cams(cam, 1);
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
+  ws->bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;  // extended kernel instances
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
   std::vector<DevView> views(1);
   make_view(*cam, cfg->spp_interior, views[0]);
@@ -386,7 +457,7 @@ psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_came
   PSDR_CHECK(scene && ws && cfg, "null argument");
   check_cfg(cfg);
   check_cams(cams, n_cams);
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
+  ws->bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;  // extended kernel instances
   PSDR_CHECK(scene->nlight > 0 || cfg->mis_light_samples == 0, "scene has no light to sample");
   cudaStream_t st = (cudaStream_t)stream;
   std::vector<DevView> views(n_cams);
@@ -443,7 +514,7 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   check_cfg(cfg);
   check_cams(cams, n_cams);
   check_estimator_cameras(cfg, cams, n_cams);
-  ws->bsdf = scene->has_bsdf ? 1 : 0;  // material kernel instances
+  ws->bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;  // extended kernel instances
   PSDR_CHECK(scene->nlight > 0, "scene has no light");
   cudaStream_t st = (cudaStream_t)stream;
   // only the vertices whose gradient the caller asked for are accumulated
@@ -497,8 +568,12 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
                (long long)ob.normal.h * ob.normal.w * 3, grads->accumulate, st);
     }
   }
-  for (int l = 0; l < scene->nlight; ++l)
+  for (int l = 0; l < scene->nlight; ++l) {
     if (grads->emit && grads->emit[l]) grad_out(scene->g_emit.as<double>() + 3 * l, grads->emit[l], 3, grads->accumulate, st);
+    if (grads->light_params && grads->light_params[l] && scene->light_grad_off[l] != SIZE_MAX)
+      grad_out(scene->g_tex.as<double>() + scene->light_grad_off[l], grads->light_params[l],
+               light_param_count(scene, l), grads->accumulate, st);
+  }
   for (int i = 0; i < n_cams; ++i)
     if (grads->camera_origin && grads->camera_origin[i])
       grad_out(ws->campos_acc.as<double>() + 3 * i, grads->camera_origin[i], 3, grads->accumulate, st);

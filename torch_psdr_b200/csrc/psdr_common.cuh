@@ -110,6 +110,10 @@ struct DevLight {
   float emit[3];
   float area, inv_area, power;
   double* grad_emit;  // 3 doubles or null
+  int kind;           // PSDR_LIGHT_AREA, _ENV (cube map in tex), _SH9 (coefficients in sh)
+  DevTex tex;         // ENV cube map (tex.grad: its fp64 accumulator or null)
+  float sh[27];       // SH9 (9,3) coefficients
+  double* grad_sh;    // SH9: 27 doubles or null
 };
 
 // Per-triangle shading record, 6 x float4 (96 B) in original triangle order:
@@ -558,6 +562,48 @@ PSDR_D float3 surf_bsdf(const DevScene& sc, const Surf& x, float3 L) {
   bool mapped;
   const float3 N = shading_normal(ob, x, m, mapped);
   return bsdf_value(ob, color, material_sigma(ob, x), N, x.wi, L);
+}
+
+// ------------------------------------------------------------------ light emission
+constexpr int kLightArea = 0, kLightEnv = 1, kLightSh9 = 2;  // PSDR_LIGHT_*
+
+// Second-order real spherical harmonics (emitter.cc:246-266): Y(0,0), Y(1,-1..1), Y(2,-2..2).
+constexpr float kSh0 = 0.28209479177387814f;   // sqrt(1 / (4 pi))
+constexpr float kSh1 = 0.48860251190291992f;   // sqrt(3 / (4 pi))
+constexpr float kSh2 = 1.09254843059207907f;   // sqrt(15 / (4 pi))
+constexpr float kSh3 = 0.31539156525252005f;   // sqrt(5 / (16 pi))
+constexpr float kSh4 = 0.54627421529603953f;   // sqrt(15 / (16 pi))
+PSDR_D void sh9_basis(float3 d, float Y[9]) {
+  Y[0] = kSh0;
+  Y[1] = kSh1 * d.y;
+  Y[2] = kSh1 * d.z;
+  Y[3] = kSh1 * d.x;
+  Y[4] = kSh2 * (d.x * d.y);
+  Y[5] = kSh2 * (d.y * d.z);
+  Y[6] = kSh3 * (2.f * (d.z * d.z) - d.x * d.x - d.y * d.y);
+  Y[7] = kSh2 * (d.z * d.x);
+  Y[8] = kSh4 * (d.x * d.x - d.y * d.y);
+}
+
+// Radiance of an environment light hit at box uv (u, v) reached along incoming direction
+// wi: EnvLight's cube map (emitter.cc:134-141), SH9Light's harmonics of wi
+// (emitter.cc:268-275). Out of line: area-light kernels keep their register budgets.
+static __device__ __noinline__ float3 env_emit(const DevLight* L, float u, float v, float3 wi) {
+  if (L->kind == kLightEnv) return tex_rgb(L->tex, texel_offset(L->tex, u, v));
+  float Y[9];
+  sh9_basis(wi, Y);
+  float3 e = f3(0.f, 0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) e += f3(L->sh[3 * k], L->sh[3 * k + 1], L->sh[3 * k + 2]) * Y[k];
+  return e;
+}
+
+// Radiance of the light hit q (light L). EXT: the kernel instance for scenes with an
+// environment light (or a DiffuseBsdfMaterial); the other instance has area lights only.
+template <bool EXT>
+PSDR_D float3 light_emit(const DevLight& L, const Surf& q) {
+  if (!EXT || L.kind == kLightArea) return f3(L.emit[0], L.emit[1], L.emit[2]);
+  return env_emit(&L, q.u, q.v, q.wi);
 }
 
 PSDR_D float mis_power(float w1, float w2, float n1, float n2) {

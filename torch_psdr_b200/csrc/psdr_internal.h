@@ -93,6 +93,12 @@ struct psdr_scene {
   // DiffuseBsdfMaterial roughness / normal-map accumulators (after every color texture)
   std::vector<size_t> rough_grad_off, nrm_grad_off;
   bool has_bsdf = false;
+  // environment light (EnvLight / SH9Light): its index (the last light) or -1, the box
+  // mesh the library builds for it, and each light's parameter accumulator offset in g_tex
+  int env_light = -1;
+  float env_host_v[24];
+  psdr::DBuf env_v, env_f, env_uv, env_uvi;
+  std::vector<size_t> light_grad_off;
   bool grads_ready = false;
   psdr::DevScene dev{};
   psdr::DBuf d_dev;  // device copy of `dev`

@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
           const DevLight& Lt = sc->lights[x.light];
           float4 L = w.L[s];
           const float4 T = w.T[s];
-          L.x += T.x * Lt.emit[0]; L.y += T.y * Lt.emit[1]; L.z += T.z * Lt.emit[2];
+          const float3 e = light_emit<BSDF>(Lt, x);
+          L.x += T.x * e.x; L.y += T.y * e.y; L.z += T.z * e.z;
           w.L[s] = L;
         }
       } else {
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
         float wgt = 1.0f / fL;
         if (w.nB > 0) wgt *= mis_power(pdf_l, dot(x.n, dir) * kInvPi * tmp, fL, fB);
         const float3 f = fr(dir);
-        C += f3(Lt.emit[0] * f.x, Lt.emit[1] * f.y, Lt.emit[2] * f.z) * (G / pdf_l * wgt);
+        C += mul(light_emit<BSDF>(Lt, q), f) * (G / pdf_l * wgt);
       }
       for (int j = 0; j < w.nB; ++j) {
         const size_t slot = (w.nL + j) * cs + k;
@@ -373,7 +374,7 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
         float wgt = 1.0f / fB;
         if (w.nL > 0) wgt *= mis_power(pdf_b, __ldg(sc.light_pmf + q.light) * Lt.inv_area, fB, fL);
         const float3 f = fr(wo);
-        C += f3(Lt.emit[0] * f.x, Lt.emit[1] * f.y, Lt.emit[2] * f.z) * (G / pdf_b * wgt);
+        C += mul(light_emit<BSDF>(Lt, q), f) * (G / pdf_b * wgt);
       }
       float4 hn = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f);
       if (!last) {
@@ -469,10 +470,44 @@ struct HotAcc {
   float e[3];
 };
 
+// Adjoint ae of an environment light's radiance at box uv (u, v), incoming direction wi:
+// scatters into the cube-map texel or the SH coefficients and returns the adjoint of wi.
+static __device__ __noinline__ float3 env_emit_adj(const DevLight* L, float u, float v, float3 wi, float3 ae) {
+  if (L->kind == kLightEnv) {
+    if (L->tex.grad) atomic_add3(L->tex.grad + texel_offset(L->tex, u, v), ae);
+    return f3(0.f, 0.f, 0.f);
+  }
+  float Y[9];
+  sh9_basis(wi, Y);
+  float s[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    if (L->grad_sh) atomic_add3(L->grad_sh + 3 * k, ae * Y[k]);
+    s[k] = ae.x * L->sh[3 * k] + ae.y * L->sh[3 * k + 1] + ae.z * L->sh[3 * k + 2];
+  }
+  const float x = wi.x, y = wi.y, z = wi.z;
+  return f3(kSh1 * s[3] + kSh2 * (s[4] * y + s[7] * z) - 2.f * kSh3 * s[6] * x + 2.f * kSh4 * s[8] * x,
+            kSh1 * s[1] + kSh2 * (s[4] * x + s[5] * z) - 2.f * kSh3 * s[6] * y - 2.f * kSh4 * s[8] * y,
+            kSh1 * s[2] + kSh2 * (s[5] * y + s[7] * x) + 4.f * kSh3 * s[6] * z);
+}
+
+// Emission adjoint of light hit q reached from x: area lights into the emission
+// accumulator, environment lights into their parameters, and the SH9 direction's share
+// into the point x (wi = -normalize(q - x)).
 PSDR_D void add_emit(HotAcc& hot, double* grad_emit, float3 a) {
   if (!grad_emit) return;
   if (hot.emit_hot) { hot.e[0] += a.x; hot.e[1] += a.y; hot.e[2] += a.z; }
   else atomic_add3(grad_emit, a);
+}
+
+template <bool EXT>
+PSDR_D void add_light_emit(HotAcc& hot, const DevLight& Lt, const Surf& q, float3 ae, SurfAdj& ax) {
+  if (!EXT || Lt.kind == kLightArea) {
+    add_emit(hot, Lt.grad_emit, ae);
+    return;
+  }
+  const float3 aw = env_emit_adj(&Lt, q.u, q.v, q.wi, ae);
+  if (Lt.kind == kLightSh9) ax.p += (aw - q.wi * dot(q.wi, aw)) / sqrtf(q.sqd);
 }
 
 PSDR_D void add_vertex(const DevScene& sc, HotAcc& hot, int v, float3 a) {
@@ -716,7 +751,7 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
     const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
     if (!(q.is_light && sqnorm(q.p - ls.y) < kEps)) continue;
     const DevLight& Lt = sc.lights[ls.light];
-    const float3 emit = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+    const float3 emit = light_emit<BSDF>(Lt, q);
     const float tmp = dot(q.n, -dir) / q.sqd;
     const float G = dot(x.n, dir) * tmp;
     float wgt = 1.0f / fL;
@@ -734,7 +769,7 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
       else adj_tex += mul(av, emit) * (s_ * kInvPi);
       const float3 eb = mul(emit, f);
       const float3 ae = mul(av, f) * s_;
-      add_emit(hot, sc.lights[ls.light].grad_emit, ae);
+      add_light_emit<BSDF>(hot, Lt, q, ae, ax);
       const float adj_gam = dot(av, eb) / ls.pdf;
       SurfAdj aq = zero_adj();
       aq.area = adj_gam * G / q.area;
@@ -763,7 +798,7 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
     const Surf q = make_surf(sc, tri, h.y, h.z, x.p);
     if (!q.is_light) continue;
     const DevLight& Lt = sc.lights[q.light];
-    const float3 emit = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+    const float3 emit = light_emit<BSDF>(Lt, q);
     const float tmp = dot(q.n, -wo) / q.sqd;
     const float G = dot(x.n, wo) * tmp;
     const float pdf_b = ct * kInvPi * tmp;
@@ -782,7 +817,7 @@ PSDR_D DepthVals depth_eval(const WF& w, const DevScene& sc, const Surf& x, Rng&
       else adj_tex += mul(av, emit) * (s_ * kInvPi);
       const float3 eb = mul(emit, f);
       const float3 ae = mul(av, f) * s_;
-      add_emit(hot, Lt.grad_emit, ae);
+      add_light_emit<BSDF>(hot, Lt, q, ae, ax);
       const float adj_gam = dot(av, eb) / pdf_b;
       SurfAdj aq = zero_adj();
       aq.area = adj_gam * G / q.area;
@@ -1014,11 +1049,12 @@ __global__ void __launch_bounds__(128, BSDF ? 2 : 3) k_adjoint(WF w, const DevSc
           // camera ray on a light: L = emit at depth 0 when lights are visible
           if (w.light_vis) {
             const DevLight& Lt = sc.lights[x0.light];
-            const float3 L = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+            const float3 L = light_emit<BSDF>(Lt, x0);
             has0 = true;
             ax0.area = dot(g, L) / x0.area;
             if (UNB) cam_jacobian_adj(V, x0, dot(g, L), ax0, cam);
-            add_emit(hot, Lt.grad_emit, g);
+            if (!BSDF || Lt.kind == kLightArea) add_emit(hot, Lt.grad_emit, g);
+            else env_emit_adj(&Lt, x0.u, x0.v, x0.wi, g);  // the SH9 direction's share to the camera is not taken
           }
         } else {
           const float3 L = suffix_radiance(cb, 0, w.D);
@@ -1661,7 +1697,7 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
       const DevLight& Lt = sc.lights[s0.light];
       // running throughput: the emission times pi f_r at every vertex the chain leaves
       // (DiffuseMaterial: f_r / pi of the receiver folded in up front, then the albedos)
-      float3 T = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+      float3 T = light_emit<BSDF>(Lt, s0);
       if (!BSDF) {
         const DevObj& ob = sc.objs[d0.obj];
         T = mul(tex_rgb(ob.color, texel_offset(ob.color, d0.u, d0.v)) * kInvPi, T);
@@ -1762,7 +1798,7 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
     const float Jb = len_sd * len_sb * sin_b / (sin_d * cos_s);
     const float dG = cos_s * dot(nd, -db) / (len_sd * len_sd);
     const DevLight& Lt = sc.lights[s0.light];
-    const float3 Ts = f3(Lt.emit[0], Lt.emit[1], Lt.emit[2]);
+    const float3 Ts = light_emit<BSDF>(Lt, s0);
     float3 Td;
     if (BSDF) {
       Td = surf_bsdf(sc, d0, -cd);
@@ -2506,7 +2542,7 @@ extern "C" PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const
     w.hit = reinterpret_cast<float4*>(take(16 * cap * R));
     w.rec = nullptr;
     set_wf(w, *cfg, 1, -1, cfg->enable_light_visable);
-    w.bsdf = scene->has_bsdf ? 1 : 0;
+    w.bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;
     // the view record goes into the scratch too (the previous call's view is overwritten)
     DevView V;
     make_view(*cam, cfg->spp_interior, V);

@@ -46,7 +46,7 @@ struct WF {
   float4* hit;   // tri(bits), b1, b2, t
   float4* rec;   // replay records: 1 + D*R per path
   int rec_stride;
-  int bsdf;      // host side: launch the DiffuseBsdfMaterial kernel instances
+  int bsdf;      // host side: launch the extended kernel instances (DiffuseBsdfMaterial, environment light)
 };
 
 struct Tile {
@@ -77,8 +77,9 @@ struct psdr_workspace {
   psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
   psdr::DBuf campos_acc;
   long long mass_cap = 0;
-  // a DiffuseBsdfMaterial mesh is in the scenes of the current job (each entry point sets
-  // it; the material kernel instances also handle DiffuseMaterial, so 1 is always safe)
+  // a DiffuseBsdfMaterial mesh or an environment light is in the scenes of the current job
+  // (each entry point sets it; the extended kernel instances also handle the plain
+  // scenes, so 1 is always safe)
   int bsdf = 1;
   cudaStream_t stream = nullptr;
   std::vector<psdr::DevView> h_views;
@@ -112,7 +113,7 @@ void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views
                          psdr_workspace* ws, cudaStream_t st, float* samples_out);
 struct SceneGradInfo {
   int hot_lv0 = 0, hot_nlv = 0, emit_hot = 0;
-  int bsdf = 0;  // a DiffuseBsdfMaterial mesh is present (material adjoint kernel)
+  int bsdf = 0;  // a DiffuseBsdfMaterial mesh or an environment light (extended adjoint kernel)
 };
 void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
                           psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
@@ -128,6 +129,7 @@ SceneGradInfo grad_info(const psdr_scene* s);
 void check_config(const psdr_config* c);
 void check_cameras(const psdr_camera_desc* cams, int n);
 void check_estimator_cameras(const psdr_config* cfg, const psdr_camera_desc* cams, int n);
+long long light_param_count(const psdr_scene* s, int l);
 void scene_build_geometry(psdr_scene* s, cudaStream_t st);
 std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap);
 long long border_segments(const DevView& V);

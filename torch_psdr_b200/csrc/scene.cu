@@ -77,14 +77,17 @@ __global__ void k_light_setup(DevLight* lights, int nlight, const float4* __rest
     L.area = (float)tot;
     L.inv_area = 1.0f / (float)tot;
     const double lum = (double)L.emit[0] * 0.2126 + (double)L.emit[1] * 0.7152 + (double)L.emit[2] * 0.0722;
-    L.power = (float)(2.0 * 3.14159265358979323846 * lum * tot);
-    all_power += 2.0 * 3.14159265358979323846 * lum * tot;
+    // environment lights: 4 pi (emitter.cc:130, 243)
+    const double pw = L.kind == 0 ? 2.0 * 3.14159265358979323846 * lum * tot : 4.0 * 3.14159265358979323846;
+    L.power = (float)pw;
+    all_power += pw;
   }
   double acc = 0;
   for (int l = 0; l < nlight; ++l) {
     const double lum = (double)lights[l].emit[0] * 0.2126 + (double)lights[l].emit[1] * 0.7152 +
                        (double)lights[l].emit[2] * 0.0722;
-    const double p = 2.0 * 3.14159265358979323846 * lum * (double)lights[l].area;
+    const double p = lights[l].kind == 0 ? 2.0 * 3.14159265358979323846 * lum * (double)lights[l].area
+                                         : 4.0 * 3.14159265358979323846;
     acc += p;
     light_pmf[l] = (float)(p / all_power);
     light_cmf[l] = (float)(acc / all_power);
@@ -179,7 +182,9 @@ PSDR_D unsigned int f2ord(float f) {
 }
 PSDR_D float ord2f(unsigned int u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
 
-__global__ void k_centroid_box(int n, const float4* __restrict__ tri, unsigned int* __restrict__ cbox) {
+// n_core: triangles before the environment light's box (the box, 1000 times the scene,
+// would squeeze the scene into a few Morton cells); the geometry box covers all n.
+__global__ void k_centroid_box(int n, int n_core, const float4* __restrict__ tri, unsigned int* __restrict__ cbox) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   float3 lo = f3(INFINITY, INFINITY, INFINITY), hi = f3(-INFINITY, -INFINITY, -INFINITY);
   float3 glo = lo, ghi = hi;
@@ -189,7 +194,8 @@ __global__ void k_centroid_box(int n, const float4* __restrict__ tri, unsigned i
     const float3 bl = f3(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)), fminf(p0.z, fminf(p1.z, p2.z)));
     const float3 bh = f3(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)), fmaxf(p0.z, fmaxf(p1.z, p2.z)));
     const float3 c = (bl + bh) * 0.5f;
-    lo = c; hi = c; glo = bl; ghi = bh;
+    if (i < n_core) { lo = c; hi = c; }
+    glo = bl; ghi = bh;
   }
   for (int o = 16; o; o >>= 1) {
     lo.x = fminf(lo.x, __shfl_xor_sync(0xffffffffu, lo.x, o));
@@ -226,7 +232,7 @@ PSDR_D unsigned int expand_bits(unsigned int v) {
   return v;
 }
 
-__global__ void k_morton(int n, const float4* __restrict__ tri, const unsigned int* __restrict__ cbox,
+__global__ void k_morton(int n, int n_core, const float4* __restrict__ tri, const unsigned int* __restrict__ cbox,
                          uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -251,7 +257,7 @@ __global__ void k_morton(int n, const float4* __restrict__ tri, const unsigned i
   const float3 ghi = f3(ord2f(cbox[9]), ord2f(cbox[10]), ord2f(cbox[11]));
   const float sext = fmaxf(fmaxf(ghi.x - glo.x, ghi.y - glo.y), ghi.z - glo.z);
   const float text = fmaxf(fmaxf(bh.x - bl.x, bh.y - bl.y), bh.z - bl.z);
-  if (text > 0.25f * sext) m |= 1u << 30;
+  if (text > 0.25f * sext || i >= n_core) m |= 1u << 30;
   keys[i] = m;
   vals[i] = (uint32_t)i;
 }
@@ -439,6 +445,11 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
     const float* uvs = is_mesh ? s->meshes[o].uvs : nullptr;
     const int* uvi = is_mesh ? s->meshes[o].uv_indices : nullptr;
     if (is_mesh && (!uvs || !uvi)) { uvs = nullptr; uvi = nullptr; }
+    // the EnvLight box carries the cube-map uvs
+    if (!is_mesh && o - (int)s->meshes.size() == s->env_light && s->lights[s->env_light].type == PSDR_LIGHT_ENV) {
+      uvs = s->env_uv.as<float>();
+      uvi = s->env_uvi.as<int>();
+    }
     const int nF = s->obj_ntri[o];
     if (nF == 0) continue;
     k_tri_records<<<nblk(nF), 256, 0, st>>>(nF, faces, s->obj_vert_off[o], s->obj_tri_off[o], o, s->verts.as<float>(),
@@ -451,11 +462,13 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
                                    s->ltri_cmf.as<float>(), s->dev.ltri_base, s->light_pmf.as<float>(),
                                    s->light_cmf.as<float>());
   }
-  // edges: sort half-edges by (min,max) vertex id
-  const int nh = 3 * s->ntri;
+  // edges: sort half-edges by (min,max) vertex id; the environment light's box (the last
+  // triangles) has no edges (scene.cc:59-62 takes them from the other meshes only)
+  const int n_edge_tri = s->env_light >= 0 ? s->obj_tri_off[s->meshes.size() + s->env_light] : s->ntri;
+  const int nh = 3 * n_edge_tri;
   uint64_t* keys = s->keys.as<uint64_t>();
   uint32_t* vals = s->vals.as<uint32_t>();
-  k_halfedges<<<nblk(nh), 256, 0, st>>>(s->ntri, s->tri_v.as<int4>(), 0, s->ntri, keys, vals);
+  k_halfedges<<<nblk(std::max(1, nh)), 256, 0, st>>>(n_edge_tri, s->tri_v.as<int4>(), 0, n_edge_tri, keys, vals);
   int vbits = 1;
   while ((1ll << vbits) < (long long)s->nvert) ++vbits;
   radix_sort_pairs(keys, vals, nh, 32 + vbits, s->sort_tmp, st);
@@ -476,8 +489,8 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
   const int n = s->ntri;
   unsigned int* cbox = s->cbox.as<unsigned int>();
   k_cbox_init<<<1, 32, 0, st>>>(cbox);
-  k_centroid_box<<<nblk(n), 256, 0, st>>>(n, s->tri.as<float4>(), cbox);
-  k_morton<<<nblk(n), 256, 0, st>>>(n, s->tri.as<float4>(), cbox, keys, vals);
+  k_centroid_box<<<nblk(n), 256, 0, st>>>(n, n_edge_tri, s->tri.as<float4>(), cbox);
+  k_morton<<<nblk(n), 256, 0, st>>>(n, n_edge_tri, s->tri.as<float4>(), cbox, keys, vals);
   radix_sort_pairs(keys, vals, n, 31, s->sort_tmp, st);
   int2* child = s->aux_i.as<int2>();
   int2* range = s->range.as<int2>();
