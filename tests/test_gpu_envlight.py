@@ -132,6 +132,14 @@ def test_env_gradient_terms_match_oracle(cuda, kind, estimator, terms, kinds):
     unb = estimator == "unbiased"
     if unb:
         kw.update(spp_pixel_boundary=4)
+    if terms == 2 and not unb:
+        # The reference primary-edge term reuses the guiding CDF's uniforms, which makes it
+        # chaotic in the last bits of the guiding masses: in this scene a one-ulp change of
+        # the cube map or of the area light's emission moves the oracle's own estimate by
+        # 0.4-1.4 %. Without guiding the same change moves it by 1e-6, so the term's
+        # computation is compared without guiding (the guided path is compared in the
+        # DiffuseMaterial, DiffuseBsdfMaterial and orthographic suites).
+        kw.update(primary_edge_hypercube_resolution=1)
     gseeds, oseeds = _env_seeds(spec, kinds, np.random.default_rng(3))
     params = set()
     for k in kinds:
