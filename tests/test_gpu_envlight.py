@@ -107,7 +107,12 @@ def _env_seeds(spec, kinds, rng):
     if "env" in kinds:
         st[ntex:] = rng.normal(size=(npar, 8))
         gpu[f"env{len(spec.lights) - 1}"] = st[ntex:]
-    return gpu, dict(seed_verts=sv, seed_tex=st)
+    sc = None
+    if "cam" in kinds:
+        sc = rng.normal(size=(len(spec.cameras), 3, 8))
+        for k in range(len(spec.cameras)):
+            gpu[f"cam{k}"] = sc[k]
+    return gpu, dict(seed_verts=sv, seed_tex=st, seed_cam=sc)
 
 
 ENV_GRAD_CASES = [
@@ -121,6 +126,7 @@ ENV_GRAD_CASES = [
     (2, "unbiased", 2, ("verts",)),
     (1, "unbiased", 4, ("verts",)),
     (2, "unbiased", 8, ("verts",)),
+    (2, "reference_lv", 1, ("cam", "env")),  # the SH9 box seen directly (enable_light_visable)
 ]
 
 
@@ -129,6 +135,9 @@ def test_env_gradient_terms_match_oracle(cuda, kind, estimator, terms, kinds):
     spec = compact_env_spec(kind)
     kw = dict(spp_interior=4, max_bounce=3, spp_primary_edge=4, spp_secondary_edge=4,
               primary_edge_hypercube_resolution=500, secondary_edge_hypercube_resolution=[500, 3, 3])
+    if estimator == "reference_lv":
+        estimator = "reference"
+        kw.update(enable_light_visable=True)
     unb = estimator == "unbiased"
     if unb:
         kw.update(spp_pixel_boundary=4)
@@ -143,7 +152,7 @@ def test_env_gradient_terms_match_oracle(cuda, kind, estimator, terms, kinds):
     gseeds, oseeds = _env_seeds(spec, kinds, np.random.default_rng(3))
     params = set()
     for k in kinds:
-        params |= {"verts": {"verts", "light_verts"}, "env": {"env"}}[k]
+        params |= {"verts": {"verts", "light_verts"}, "env": {"env"}, "cam": {"cam"}}[k]
     scene, T = to_torch_scene(spec, requires_grad=params)
     integ = dr.PathIntegrator(gradient_terms=terms, estimator=estimator, **kw)
     img = integ.renderD(scene)[0]

@@ -1053,8 +1053,14 @@ __global__ void __launch_bounds__(128, BSDF ? 2 : 3) k_adjoint(WF w, const DevSc
             has0 = true;
             ax0.area = dot(g, L) / x0.area;
             if (UNB) cam_jacobian_adj(V, x0, dot(g, L), ax0, cam);
-            if (!BSDF || Lt.kind == kLightArea) add_emit(hot, Lt.grad_emit, g);
-            else env_emit_adj(&Lt, x0.u, x0.v, x0.wi, g);  // the SH9 direction's share to the camera is not taken
+            if (!BSDF || Lt.kind == kLightArea) {
+              add_emit(hot, Lt.grad_emit, g);
+            } else {
+              // an SH9 light's radiance depends on wi = -normalize(x0 - o): its share goes
+              // to the ray origin, which moves with the camera
+              const float3 aw = env_emit_adj(&Lt, x0.u, x0.v, x0.wi, g);
+              if (Lt.kind == kLightSh9) cam.add(&V, (aw - x0.wi * dot(x0.wi, aw)) / sqrtf(x0.sqd));
+            }
           }
         } else {
           const float3 L = suffix_radiance(cb, 0, w.D);
