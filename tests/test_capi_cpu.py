@@ -80,3 +80,45 @@ def test_api_asserts_mirror_reference():
 def test_cpu_tensors_are_rejected():
     with pytest.raises(ValueError):
         dr.Texture(torch.zeros(3))
+
+
+# ctypes mirror -> C struct of include/psdr.h, and the C field names where they differ
+_STRUCTS = {
+    "TextureDesc": ("psdr_texture_desc", {}),
+    "MeshDesc": ("psdr_mesh_desc", {}),
+    "AreaLightDesc": ("psdr_area_light_desc", {}),
+    "SceneDesc": ("psdr_scene_desc", {}),
+    "CameraDesc": ("psdr_camera_desc", {}),
+    "Config": ("psdr_config", {}),
+    "GradTargets": ("psdr_grad_targets", {}),
+}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every ctypes mirror in torch_psdr_b200/_lib.py has the size and field offsets of
+    its C struct (compiled here against include/psdr.h with gcc)."""
+    import os
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "psdr.h"', "int main(void) {"]
+    for py, (cname, rename) in _STRUCTS.items():
+        lines.append(f'  printf("{py} size %zu\\n", sizeof({cname}));')
+        for field, _ in getattr(L, py)._fields_:
+            lines.append(f'  printf("{py} {field} %zu\\n", offsetof({cname}, {rename.get(field, field)}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    seen = 0
+    for line in filter(None, out):
+        py, what, value = line.split()
+        cls = getattr(L, py)
+        want = C.sizeof(cls) if what == "size" else getattr(cls, what).offset
+        assert int(value) == want, (py, what, int(value), want)
+        seen += 1
+    assert seen > 40
