@@ -169,6 +169,13 @@ PSDR_API psdr_status psdr_scene_destroy(psdr_scene* scene);
 /* Rebuild the acceleration structure, triangle attributes and edges after the
  * vertex buffers changed in place (same topology). */
 PSDR_API psdr_status psdr_scene_update(psdr_scene* scene, void* stream);
+/* Like psdr_scene_update after vertex positions changed (same meshes, same faces), but
+ * the BVH keeps the tree of the last full build and only its node boxes are recomputed:
+ * cheaper, and the hits are the same; the tree's quality degrades as the geometry moves
+ * away from the state it was built for (psdr_scene_update rebuilds it). Replaces the
+ * per-iteration Scene reconstruction of the reference (scene.cc:3-104; its OptiX GAS
+ * build, scene_optix.cc:187-238) when only positions change. */
+PSDR_API psdr_status psdr_scene_refit(psdr_scene* scene, void* stream);
 /* BVH leaves of up to leaf_size (1..8) triangles; rebuilds the scene's geometry.
  * Extension (the reference's OptiX build has no such knob); psdr_autotune picks it. */
 PSDR_API psdr_status psdr_scene_set_leaf_size(psdr_scene* scene, int32_t leaf_size, void* stream);

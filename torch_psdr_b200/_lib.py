@@ -80,6 +80,7 @@ SIGNATURES = {
     "psdr_scene_create": ([C.POINTER(SceneDesc), P, C.POINTER(P)], C.c_int),
     "psdr_scene_destroy": ([P], C.c_int),
     "psdr_scene_update": ([P, P], C.c_int),
+    "psdr_scene_refit": ([P, P], C.c_int),
     "psdr_scene_set_leaf_size": ([P, C.c_int32, P], C.c_int),
     "psdr_scene_info": ([P, C.POINTER(C.c_int64)], C.c_int),
     "psdr_scene_edges": ([P, P, P, C.c_int64, C.POINTER(C.c_int64), P], C.c_int),

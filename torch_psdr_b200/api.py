@@ -370,9 +370,14 @@ class Scene(VarContex):
         L.check(self._lib.psdr_scene_info(self._handle, out), "psdr_scene_info")
         return dict(zip(["triangles", "vertices", "edges", "bvh_nodes", "lights", "objects"], list(out)))
 
-    def update(self):
-        """Rebuild triangle records, edges, CDFs and the BVH after Mesh.set_vertices."""
-        L.check(self._lib.psdr_scene_update(self._handle, _stream()), "psdr_scene_update")
+    def update(self, refit: bool = False):
+        """Rebuild triangle records, edges, CDFs and the BVH after Mesh.set_vertices.
+        refit=True keeps the BVH's tree and recomputes only its boxes (same hits; for small
+        vertex moves between full rebuilds)."""
+        if refit:
+            L.check(self._lib.psdr_scene_refit(self._handle, _stream()), "psdr_scene_refit")
+        else:
+            L.check(self._lib.psdr_scene_update(self._handle, _stream()), "psdr_scene_update")
 
     def _camera_descs(self):
         return (L.CameraDesc * len(self.cameras))(*[c._desc() for c in self.cameras])

@@ -350,6 +350,13 @@ psdr_status psdr_scene_update(psdr_scene* scene, void* stream) {
   API_END
 }
 
+psdr_status psdr_scene_refit(psdr_scene* scene, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(scene != nullptr, "null scene");
+  scene_refit_geometry(scene, stream ? (cudaStream_t)stream : scene->stream);
+  API_END
+}
+
 psdr_status psdr_scene_set_leaf_size(psdr_scene* scene, int32_t leaf_size, void* stream) {
   API_BEGIN
   PSDR_CHECK(scene != nullptr, "null scene");

@@ -83,6 +83,9 @@ struct psdr_scene {
   psdr::DBuf verts, tri, tri_v, objs, lights_buf, light_pmf, light_cmf, ltri_pmf, ltri_cmf;
   psdr::DBuf n_edges, edge, edge_v, edge_pmf, edge_cmf;
   psdr::DBuf nodes, leaf, err;
+  // tree topology of the last full build, kept for psdr_scene_refit: binary child links,
+  // leaf triangle order, 4-wide node flags and indices (the build's scratch is reused)
+  psdr::DBuf bvh_child, bvh_order, bvh_f4;
   // build scratch
   psdr::DBuf keys, vals, aux_i, aux_i2, aux_d, aux_d2, aabb, parent, range, flags, cbox;
   psdr::SortTmp sort_tmp;

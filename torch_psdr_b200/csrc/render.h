@@ -131,6 +131,7 @@ void check_cameras(const psdr_camera_desc* cams, int n);
 void check_estimator_cameras(const psdr_config* cfg, const psdr_camera_desc* cams, int n);
 long long light_param_count(const psdr_scene* s, int l);
 void scene_build_geometry(psdr_scene* s, cudaStream_t st);
+void scene_refit_geometry(psdr_scene* s, cudaStream_t st);
 std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap);
 long long border_segments(const DevView& V);
 void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector<DevView>& views, cudaStream_t st);

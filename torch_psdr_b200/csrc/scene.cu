@@ -432,7 +432,9 @@ int num_sms() {
 // Builds everything that depends on vertex positions (records, edges, CDFs, BVH) on
 // stream `st`. Device work only (after the first build sized the scratch), so it can
 // also be recorded into a graph.
-void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
+// Vertices, triangle records, light tables and the edge list (everything but the BVH).
+// Returns the number of triangles outside the environment light's box.
+static int build_records_and_edges(psdr_scene* s, cudaStream_t st, int& vbits_out) {
   // vertices
   for (int o = 0; o < s->nobj; ++o) {
     const float* src = o < (int)s->meshes.size() ? s->meshes[o].vertices : s->lights[o - s->meshes.size()].vertices;
@@ -485,6 +487,15 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
   k_cdf_finalize<<<nblk(nh), 256, 0, st>>>(s->aux_d.as<double>(), s->aux_d2.as<double>(), s->n_edges.as<int>(), nh,
                                            s->edge_pmf.as<float>(), s->edge_cmf.as<float>());
   PSDR_CUDA(cudaGetLastError());
+  vbits_out = vbits;
+  return n_edge_tri;
+}
+
+void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
+  int vbits = 1;
+  const int n_edge_tri = build_records_and_edges(s, st, vbits);
+  uint64_t* keys = s->keys.as<uint64_t>();
+  uint32_t* vals = s->vals.as<uint32_t>();
   // BVH
   const int n = s->ntri;
   unsigned int* cbox = s->cbox.as<unsigned int>();
@@ -509,10 +520,41 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
     k_depth_flags<<<nblk(n - 1), 256, 0, st>>>(n, parent, range, leaf, f4);
     exclusive_scan_int(f4, idx4, n - 1, s->flags.as<int>() + 2 * (size_t)n, st);
     k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, leaf, child, range, aabb, cbox, f4, idx4, s->nodes.as<float4>());
+    PSDR_CUDA(cudaMemcpyAsync(s->bvh_child.p, child, sizeof(int2) * (n - 1), cudaMemcpyDeviceToDevice, st));
+    PSDR_CUDA(cudaMemcpyAsync(s->bvh_f4.p, f4, sizeof(int) * 2 * (size_t)n, cudaMemcpyDeviceToDevice, st));
   }
   k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), s->leaf.as<float4>());
+  PSDR_CUDA(cudaMemcpyAsync(s->bvh_order.p, vals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
   // records + lights + half-edge sort (2 x passes x 5) + edge build/CDF (8) + BVH (9 + morton sort)
   count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 9 + 3 * 4);
+  PSDR_CUDA(cudaGetLastError());
+}
+
+// Same as scene_build_geometry for records, lights and edges, but the BVH keeps the tree
+// of the last full build and only its boxes are recomputed (bottom-up over the saved
+// child links and leaf order, then the 4-wide layout with the saved node indices). Any
+// tree whose boxes bound their triangles gives the same closest hits.
+void scene_refit_geometry(psdr_scene* s, cudaStream_t st) {
+  int vbits = 1;
+  const int n_edge_tri = build_records_and_edges(s, st, vbits);
+  const int n = s->ntri;
+  unsigned int* cbox = s->cbox.as<unsigned int>();
+  k_cbox_init<<<1, 32, 0, st>>>(cbox);  // the scene extent pads the node boxes
+  k_centroid_box<<<nblk(n), 256, 0, st>>>(n, n_edge_tri, s->tri.as<float4>(), cbox);
+  const int2* child = s->bvh_child.as<int2>();
+  const uint32_t* order = s->bvh_order.as<uint32_t>();
+  float* aabb = s->aabb.as<float>();
+  int* bflags = s->flags.as<int>();
+  PSDR_CUDA(cudaMemsetAsync(bflags, 0, sizeof(int) * std::max(1, n), st));
+  k_bottom_up<<<nblk(n), 256, 0, st>>>(n, order, s->tri.as<float4>(), child, s->parent.as<int>(), aabb, bflags);
+  if (n > 1) {
+    const int leaf = std::min(s->leaf_size, n - 1);
+    const int* f4 = s->bvh_f4.as<int>();
+    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, leaf, child, s->range.as<int2>(), aabb, cbox, f4, f4 + n,
+                                           s->nodes.as<float4>());
+  }
+  k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, order, s->tri.as<float4>(), s->leaf.as<float4>());
+  count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 6);
   PSDR_CUDA(cudaGetLastError());
 }
 
@@ -549,6 +591,9 @@ void psdr_scene_alloc(psdr_scene* s) {
   s->range.alloc(sizeof(int2) * n, st);
   s->flags.alloc(sizeof(int) * (2 * (size_t)n + std::max<size_t>(2 * (size_t)n, 2 * scan_tmp_ints(nh) + 64)), st);
   s->cbox.alloc(sizeof(unsigned int) * 12, st);
+  s->bvh_child.alloc(sizeof(int2) * n, st);
+  s->bvh_order.alloc(sizeof(uint32_t) * n, st);
+  s->bvh_f4.alloc(sizeof(int) * 2 * (size_t)n, st);
   s->d_dev.alloc(sizeof(DevScene), st);
   PSDR_CUDA(cudaMemsetAsync(s->err.p, 0, sizeof(int), st));
   DevScene& d = s->dev;
