@@ -67,3 +67,41 @@ def test_env_box_matches_scene_bounds_rule():
     # largest extent 20 -> half size 20000
     np.testing.assert_allclose(lo, [-20000.0, -19999.5, -20000.0])
     np.testing.assert_allclose(hi, [20000.0, 20000.5, 20000.0])
+
+
+def _fd_check(spec, attr, seed_slice_of, shape, kw, h=1e-2):
+    """Directional derivative of sum(g * image) along a random direction of a light
+    parameter (the tail of the oracle's texture seeds) against central differences."""
+    rng = np.random.default_rng(11)
+    H, W = spec.cameras[0].height, spec.cameras[0].width
+    g = rng.normal(size=(H, W, 3))
+    base = getattr(spec.lights[-1], attr).copy()
+    d = rng.normal(size=shape)
+    ntex = sum(m.texture.size for m in spec.meshes)
+    st = np.zeros((ntex + d.size, 8))
+    st[ntex:, 0] = d.reshape(-1)
+    ad = orc.grad_dir(spec, [g], which=1, seed_tex=st, **kw)[0]
+    ph = []
+    for sgn in (1, -1):
+        setattr(spec.lights[-1], attr, (base + sgn * h * d).astype(np.float32))
+        ph.append(float((g * orc.render(spec, precision=1, **kw)[0]).sum()))
+    setattr(spec.lights[-1], attr, base)
+    fd = (ph[0] - ph[1]) / (2 * h)
+    print(attr, "AD", ad, "FD", fd)
+    assert abs(ad) > 0
+    # the radiance is linear in the parameters; what remains is the float32 rounding of
+    # the perturbed parameters (about 1e-7 / h relative)
+    assert abs(ad - fd) <= 1e-4 * abs(fd)
+
+
+def test_cube_map_derivative_vs_finite_differences():
+    spec = env_spec(1, np.array([1.0, 0.8, 0.6]))
+    spec.lights[0].cube_map = np.random.default_rng(3).uniform(0.5, 1.5, size=(6, 8, 3)).astype(np.float32)
+    _fd_check(spec, "cube_map", None, (6, 8, 3), dict(spp_interior=4, max_bounce=2))
+
+
+def test_sh9_coefficient_derivative_vs_finite_differences():
+    spec = env_spec(2, np.array([2.0, 1.0, 0.5]))
+    spec.lights[0].sh9 = (np.random.default_rng(4).normal(scale=0.3, size=(9, 3)) +
+                          np.array([[2.0, 1.0, 0.5]] + [[0, 0, 0]] * 8)).astype(np.float32)
+    _fd_check(spec, "sh9", None, (9, 3), dict(spp_interior=4, max_bounce=2))
