@@ -195,6 +195,24 @@ def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=409
             "fd_step": h, "fd_spp": fd_spp}
 
 
+# ---------------------------------------------------------------- replicas
+def max_over_ranks(value, dist, device):
+    """The largest of the ranks' values (device times are taken as the max over ranks);
+    the value itself on one process (dist None)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank_step, steps, ms):
+    """Whole-job throughput of `world` replicas that each processed units_per_rank_step
+    units per step for `steps` steps in `ms` milliseconds (the max over ranks)."""
+    return world * units_per_rank_step * steps / (ms / 1e3)
+
+
 # ---------------------------------------------------------------- B200 arm
 def run_b200(args):
     import torch
@@ -310,19 +328,16 @@ def run_b200(args):
         tms = ctypes.c_double()
         L.check(lib.psdr_profile_read(prof, ctypes.byref(tms)), "profile")
         L.check(lib.psdr_profile_enable(0), "profile")
-        if dist:
-            tt = torch.tensor([total], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total = float(tt.item())
+        total = max_over_ranks(total, dist, dev)
         return total, (int(prof[0]), int(prof[1]), int(prof[2])), tms.value, clk
 
     samples = H * W * SPP
     step = step_batched if args.mode == "batched" else step_plain
     other = step_plain if args.mode == "batched" else step_batched
     total_ms, (launches, trace_launches, rays), trace_ms_v, clk = timed(step, True)
-    value = world * samples * args.steps / (total_ms / 1e3)
+    value = job_rate(world, samples, args.steps, total_ms)
     other_ms, _, _, _ = timed(other, False)
-    other_value = world * samples * args.steps / (other_ms / 1e3)
+    other_value = job_rate(world, samples, args.steps, other_ms)
 
     # ---------------- end-to-end through the public API with host buffers
     h_base = torch.tensor(sphere.vertices, dtype=torch.float32).pin_memory()
@@ -352,11 +367,8 @@ def run_b200(args):
         ee[k][1].record(stream)
     torch.cuda.synchronize()
     e2e_ms = sum(a.elapsed_time(b) for a, b in ee)
-    if dist:
-        tt = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e_value = world * samples * args.steps / (e2e_ms / 1e3)
+    e2e_ms = max_over_ranks(e2e_ms, dist, dev)
+    e2e_value = job_rate(world, samples, args.steps, e2e_ms)
     h2d = h_base.numel() * 4 + h_tex.numel() * 4
     d2h = h_grad.numel() * 4 + 4
 
