@@ -74,6 +74,16 @@ def test_api_asserts_mirror_reference():
         dr.PathIntegrator(secondary_edge_hypercube_resolution=[1, 2])
     with pytest.raises(AssertionError):
         dr.AreaLight(torch.zeros(4, 3), torch.zeros(2, 3, dtype=torch.int32), torch.zeros(4))
+    with pytest.raises(AssertionError):
+        dr.SH9Light(torch.zeros(8, 3))  # torch_psdr.py:445 (9, 3) coefficients
+    with pytest.raises(AssertionError):
+        dr.OrthographicCamera(t3, t3, t3, torch.zeros(2), 4, 4)  # view_width (1,)
+    with pytest.raises(AssertionError):
+        dr.OrthographicCamera(t3, t3, t3, torch.zeros(1), 4, 0)
+    cam = dr.OrthographicCamera(torch.tensor([0.0, 0.5, 4.0]), torch.zeros(3), torch.tensor([0.0, 1.0, 0.0]),
+                                torch.tensor([3.0]), 23, 25)
+    d = cam._desc()
+    assert (d.type, d.fov, d.height, d.width) == (L.CAM_ORTHOGRAPHIC, 3.0, 23, 25)
     assert dr.Camera is dr.PerspectiveCamera
 
 
