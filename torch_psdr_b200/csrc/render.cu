@@ -112,8 +112,11 @@ PSDR_D void vert_add(const DevScene& sc, int v, float3 a) {
 }
 
 // ------------------------------------------------------------------ camera kernel
-template <int MODE>
-__global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict__ scenes,
+// ORTHO: the instance for jobs with an orthographic view (it handles both camera types).
+// The replay instance is held to 4 blocks per SM (64 registers): its record writes
+// otherwise take it to 76 registers and 3 blocks.
+template <int MODE, bool ORTHO>
+__global__ void __launch_bounds__(256, MODE == MODE_REPLAY ? 4 : 1) k_camera(WF w, const DevScene* __restrict__ scenes,
                                                 const DevView* __restrict__ views, Tile tile) {
   const int stride = gridDim.x * blockDim.x;
   const int n32 = (tile.n + 31) & ~31;
@@ -132,13 +135,14 @@ __global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict
       float3 pc;
       xform_pos(V.r2c, f3(jx + (float)x, jy + (float)y, 1.0f), pc);
       float3 o = V.pos, d;
-      if (V.ortho) {
+      if (ORTHO && V.ortho) {
         // camera.h:313-334: origin on the camera plane, direction the look direction
         xform_pos(V.c2w, f3(pc.x, pc.y, 0.f), o);
         d = view_look_dir(V);
       } else {
         d = normalize(xform_dir(V.c2w, pc));
       }
+      w.org[s] = make_float4(o.x, o.y, o.z, 0.f);  // before the out-of-line trace: o dies there
       const HitRec h = trace_closest(sc, o, d, kTmin, INFINITY);
       w.rs[s] = rng.state;
       w.ri[s] = rng.inc;
@@ -147,7 +151,6 @@ __global__ void __launch_bounds__(256) k_camera(WF w, const DevScene* __restrict
       w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
       w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       w.cur[s] = hit4(h);
-      w.org[s] = make_float4(o.x, o.y, o.z, 0.f);
       if (MODE == MODE_REPLAY) {
         float4* rec = w.rec + (size_t)s * w.rec_stride;
         rec[0] = hit4(h);
@@ -2030,6 +2033,12 @@ void Profiler::replayed(std::vector<EvPair>* graph_ev, long long n_trace) {
 #define PSDR_LAUNCHED(n) (profiler().launches += (n))
 void count_launches(int n) { profiler().launches += n; }
 
+static int any_ortho(const std::vector<DevView>& views) {
+  for (const DevView& v : views)
+    if (v.ortho) return 1;
+  return 0;
+}
+
 // k_direct instance for the job's materials (w.bsdf).
 template <bool PRE, bool UNB>
 static void launch_direct(const WF& w, int grid, cudaStream_t st, const DevScene* scenes, const DevView* vd, int v,
@@ -2068,8 +2077,14 @@ static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int 
 static void run_tile(WF& w, const DevScene* scenes, const DevView* views, const Tile& tile, int mode,
                      cudaStream_t st) {
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
-  if (mode == MODE_REPLAY) k_camera<MODE_REPLAY><<<grid_for(tile.n, 256, 8), 256, 0, st>>>(w, scenes, views, tile);
-  else k_camera<MODE_FWD><<<grid_for(tile.n, 256, 8), 256, 0, st>>>(w, scenes, views, tile);
+  const int g = grid_for(tile.n, 256, 8);
+  if (w.ortho) {
+    if (mode == MODE_REPLAY) k_camera<MODE_REPLAY, true><<<g, 256, 0, st>>>(w, scenes, views, tile);
+    else k_camera<MODE_FWD, true><<<g, 256, 0, st>>>(w, scenes, views, tile);
+  } else {
+    if (mode == MODE_REPLAY) k_camera<MODE_REPLAY, false><<<g, 256, 0, st>>>(w, scenes, views, tile);
+    else k_camera<MODE_FWD, false><<<g, 256, 0, st>>>(w, scenes, views, tile);
+  }
   PSDR_LAUNCHED(1);
   depth_loop(w, scenes, views, mode, st);
 }
@@ -2166,6 +2181,7 @@ void forward_launch(const DevScene* scenes_dev, const std::vector<DevView>& view
   w.cap = ws->cap;
   set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
   w.bsdf = ws->bsdf;
+  w.ortho = any_ortho(views);
   const DevView* vd = ws->views.as<DevView>();
   for (const Tile& t : plan_tiles(views, cap)) {
     run_tile(w, scenes_dev, vd, t, MODE_FWD, st);
@@ -2291,6 +2307,7 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
     w.cap = ws->cap;
     set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
     w.bsdf = ws->bsdf;
+    w.ortho = any_ortho(views);
     for (const Tile& t : plan_tiles(views, cap)) {
       run_tile(w, scenes_dev, vd, t, MODE_REPLAY, st);
       const int g = grid_for(t.n, 128, 16);
@@ -2310,11 +2327,13 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
   w.cap = ws->cap;
   set_wf(w, cfg, (int)views.size(), 1, 0);
   w.bsdf = ws->bsdf;
+  w.ortho = any_ortho(views);
   // paths of the unbiased boundary samples carry the interior estimator's radiance
   WF wi = ws->wf;
   wi.cap = ws->cap;
   set_wf(wi, cfg, (int)views.size(), -1, cfg.enable_light_visable);
   wi.bsdf = ws->bsdf;
+  wi.ortho = any_ortho(views);
   EdgeBuf eb{ws->eb_a.as<float4>(), ws->eb_n.as<float4>(), ws->eb_hb.as<float4>(), ws->eb_La.as<float4>(), nullptr};
   for (int v = 0; v < (int)views.size(); ++v) {
     const DevView& V = views[v];
@@ -2549,6 +2568,7 @@ extern "C" PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const
     w.rec = nullptr;
     set_wf(w, *cfg, 1, -1, cfg->enable_light_visable);
     w.bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;
+    w.ortho = cam->type == PSDR_CAM_ORTHOGRAPHIC ? 1 : 0;
     // the view record goes into the scratch too (the previous call's view is overwritten)
     DevView V;
     make_view(*cam, cfg->spp_interior, V);

@@ -47,6 +47,7 @@ struct WF {
   float4* rec;   // replay records: 1 + D*R per path
   int rec_stride;
   int bsdf;      // host side: launch the extended kernel instances (DiffuseBsdfMaterial, environment light)
+  int ortho;     // host side: an orthographic view is in the job (camera kernel instance)
 };
 
 struct Tile {
