@@ -7,7 +7,10 @@ The reference publishes no golden vectors and cannot run here, so the fixtures a
   * sampler_streams.npz -- first draws of the reference's per-sample streams
                            (TEA-seeded PCG32, sampler.h:11-17), from the oracle;
   * oracle_tiny.npz     -- a 16x16, 4 spp FP64 oracle render of a level-1 sphere
-                           scene (regression pin of the oracle itself).
+                           scene (regression pin of the oracle itself);
+  * oracle_ext.npz      -- the same kind of pin for DiffuseBsdfMaterial (roughness and
+                           normal maps), an orthographic camera, and EnvLight / SH9Light
+                           (`python tests/golden/make_golden.py ext` writes only this one).
 """
 import json
 import os
@@ -28,6 +31,34 @@ def tiny_spec():
     return synth.sphere_scene(level=1, tex_hw=8, tex_seed=0, height=16, width=16)
 
 
+def ext_specs():
+    """Tiny scenes of the DiffuseBsdfMaterial, orthographic and environment-light pins."""
+    rng = np.random.default_rng(0)
+    bsdf = tiny_spec()
+    bsdf.meshes[0].roughness = rng.uniform(0.2, 0.9, size=(3, 5)).astype(np.float32)
+    bsdf.meshes[0].normal = np.stack([rng.uniform(0.4, 0.6, (4, 3)), rng.uniform(0.4, 0.6, (4, 3)),
+                                      np.ones((4, 3))], -1).astype(np.float32)
+    bsdf.meshes[1].roughness = np.array([0.5], np.float32)
+    ortho = tiny_spec()
+    c = ortho.cameras[0]
+    ortho.cameras[0] = synth.CameraSpec(c.look_from, c.look_at, c.up, 3.0, 16, 16, 1)
+    env = tiny_spec()
+    env.meshes[1].vertices = (env.meshes[1].vertices * np.array([0.2, 1.0, 0.2], np.float32)).astype(np.float32)
+    env.lights.append(synth.LightSpec(None, None, np.zeros(3, np.float32), 1,
+                                      cube_map=rng.uniform(0.5, 1.5, size=(3, 4, 3)).astype(np.float32)))
+    sh = tiny_spec()
+    sh.meshes[1].vertices = env.meshes[1].vertices.copy()
+    coeff = rng.normal(scale=0.3, size=(9, 3)).astype(np.float32)
+    coeff[0] = [2.0, 1.5, 1.0]
+    sh.lights.append(synth.LightSpec(None, None, np.zeros(3, np.float32), 2, sh9=coeff))
+    return {"bsdf": bsdf, "ortho": ortho, "env": env, "sh9": sh}
+
+
+def write_ext():
+    imgs = {k: orc.render(s, precision=1, spp_interior=4, max_bounce=3)[0] for k, s in ext_specs().items()}
+    np.savez(os.path.join(HERE, "oracle_ext.npz"), **imgs)
+
+
 def main():
     demo = [0xa15c02b7, 0x7b47f409, 0xba1d3330, 0x83d2f293, 0xbfa4784b, 0xcbed606e]
     got = [int(x) for x in orc.pcg32(42, 54, 6)]
@@ -44,4 +75,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["ext"]:
+        write_ext()
+    else:
+        main()
+        write_ext()

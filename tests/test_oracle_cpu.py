@@ -33,6 +33,21 @@ def test_oracle_tiny_golden():
     np.testing.assert_allclose(img, np.load(os.path.join(GOLDEN, "oracle_tiny.npz"))["image"], rtol=0, atol=1e-12)
 
 
+def test_oracle_ext_golden():
+    """DiffuseBsdfMaterial, orthographic camera, EnvLight and SH9Light renders of the
+    oracle against their fixtures (tests/golden/make_golden.py)."""
+    import importlib.util
+    spec_path = os.path.join(GOLDEN, "make_golden.py")
+    mod_spec = importlib.util.spec_from_file_location("make_golden", spec_path)
+    mg = importlib.util.module_from_spec(mod_spec)
+    mod_spec.loader.exec_module(mg)
+    want = np.load(os.path.join(GOLDEN, "oracle_ext.npz"))
+    for name, s in mg.ext_specs().items():
+        img = orc.render(s, precision=1, spp_interior=4, max_bounce=3)[0]
+        assert img.mean() > 0, name
+        np.testing.assert_allclose(img, want[name], rtol=0, atol=1e-12, err_msg=name)
+
+
 def _random_rays(spec, n, seed):
     rng = np.random.default_rng(seed)
     o = rng.uniform(-3, 3, size=(n, 3))
