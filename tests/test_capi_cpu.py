@@ -132,3 +132,45 @@ def test_struct_layouts_match_header(tmp_path):
         assert int(value) == want, (py, what, int(value), want)
         seen += 1
     assert seen > 40
+
+
+def test_environment_light_arguments_are_checked(lib):
+    """psdr_scene_create refuses malformed environment lights before any device work:
+    a bad light type, an environment light that is not the last light, an empty box,
+    a scene without meshes, a cube map that is not UV3f."""
+    V = (C.c_float * 9)(0, 0, 0, 1, 0, 0, 0, 1, 0)
+    F = (C.c_int32 * 3)(0, 1, 2)
+    mesh = L.MeshDesc()
+    mesh.vertices, mesh.num_vertices, mesh.faces, mesh.num_faces = C.cast(V, C.c_void_p), 3, C.cast(F, C.c_void_p), 1
+    mesh.color = L.TextureDesc(L.TEX_CONSTANT, 3, 1, 1, C.cast((C.c_float * 3)(0.5, 0.5, 0.5), C.c_void_p))
+    area = L.AreaLightDesc()
+    area.vertices, area.num_vertices, area.faces, area.num_faces = C.cast(V, C.c_void_p), 3, C.cast(F, C.c_void_p), 1
+
+    def sh9(lo=-1.0, hi=1.0):
+        d = L.AreaLightDesc()
+        d.type = L.LIGHT_SH9
+        d.box_min = (C.c_float * 3)(lo, lo, lo)
+        d.box_max = (C.c_float * 3)(hi, hi, hi)
+        return d
+
+    def create(meshes, lights):
+        md = (L.MeshDesc * max(1, len(meshes)))(*meshes)
+        ld = (L.AreaLightDesc * max(1, len(lights)))(*lights)
+        desc = L.SceneDesc(md, len(meshes), ld, len(lights))
+        out = C.c_void_p()
+        return lib.psdr_scene_create(C.byref(desc), None, C.byref(out)), lib.psdr_last_error()
+
+    bad = sh9()
+    bad.type = 7
+    assert create([mesh], [bad]) == (L.PSDR_ERR_INVALID_ARG, b"bad light type")
+    st, msg = create([mesh], [sh9(), area])
+    assert st == L.PSDR_ERR_INVALID_ARG and b"last light" in msg
+    st, msg = create([mesh], [area, sh9(1.0, 1.0)])
+    assert st == L.PSDR_ERR_INVALID_ARG and b"empty environment light box" in msg
+    st, msg = create([], [sh9()])
+    assert st == L.PSDR_ERR_INVALID_ARG and b"needs a mesh" in msg
+    env = sh9()
+    env.type = L.LIGHT_ENV
+    env.cube_map = L.TextureDesc(L.TEX_CONSTANT, 3, 1, 1, C.cast((C.c_float * 3)(1, 1, 1), C.c_void_p))
+    st, msg = create([mesh], [env])
+    assert st == L.PSDR_ERR_INVALID_ARG and b"UV3f" in msg
