@@ -174,3 +174,36 @@ def test_environment_light_arguments_are_checked(lib):
     env.cube_map = L.TextureDesc(L.TEX_CONSTANT, 3, 1, 1, C.cast((C.c_float * 3)(1, 1, 1), C.c_void_p))
     st, msg = create([mesh], [env])
     assert st == L.PSDR_ERR_INVALID_ARG and b"UV3f" in msg
+
+
+def test_material_and_camera_arguments_are_checked(lib):
+    """A DiffuseBsdfMaterial roughness of 3 channels and a camera with a non-positive
+    fov / view width are refused before device work."""
+    V = (C.c_float * 9)(0, 0, 0, 1, 0, 0, 0, 1, 0)
+    F = (C.c_int32 * 3)(0, 1, 2)
+    mesh = L.MeshDesc()
+    mesh.vertices, mesh.num_vertices, mesh.faces, mesh.num_faces = C.cast(V, C.c_void_p), 3, C.cast(F, C.c_void_p), 1
+    c3 = C.cast((C.c_float * 3)(0.5, 0.5, 0.5), C.c_void_p)
+    mesh.color = L.TextureDesc(L.TEX_CONSTANT, 3, 1, 1, c3)
+    mesh.material = L.MAT_DIFFUSE_BSDF
+    mesh.roughness = L.TextureDesc(L.TEX_CONSTANT, 3, 1, 1, c3)
+    mesh.normal = L.TextureDesc(L.TEX_NONE, 0, 0, 0, None)
+    md = (L.MeshDesc * 1)(mesh)
+    desc = L.SceneDesc(md, 1, None, 0)
+    out = C.c_void_p()
+    assert lib.psdr_scene_create(C.byref(desc), None, C.byref(out)) == L.PSDR_ERR_INVALID_ARG
+    assert b"roughness texture must have 1 channel" in lib.psdr_last_error()
+    ws = C.c_void_p()
+    assert lib.psdr_workspace_create(C.byref(ws)) == 0
+    cfg = L.Config()
+    for k, v in dict(n_pass=1, spp_interior=1, spp_primary_edge=1, spp_secondary_edge=1, max_bounce=1,
+                     mis_light_samples=1, mis_bsdf_samples=1, primary_edge_preprocess_rounds=1,
+                     secondary_edge_preprocess_rounds=1, primary_edge_hypercube_resolution=10).items():
+        setattr(cfg, k, v)
+    cfg.secondary_edge_hypercube_resolution[:] = [10, 1, 1]
+    cam = L.CameraDesc()
+    cam.type, cam.fov, cam.height, cam.width = L.CAM_ORTHOGRAPHIC, 0.0, 4, 4
+    img = (C.c_void_p * 1)(None)
+    st = lib.psdr_render_fwd(C.c_void_p(1), ws, C.byref(cam), 1, C.byref(cfg), img, None)
+    assert st == L.PSDR_ERR_INVALID_ARG and b"view width" in lib.psdr_last_error()
+    assert lib.psdr_workspace_destroy(ws) == 0
