@@ -65,7 +65,7 @@ def main():
     assert got == demo, (got, demo)
     with open(os.path.join(HERE, "pcg32_demo.json"), "w") as f:
         json.dump({"initstate": 42, "initseq": 54, "outputs": demo,
-                   "source": "pcg-basic pcg32-demo, round 1 (published PCG reference output)"}, f, indent=1)
+                   "source": "pcg-basic pcg32-demo, first block of printed outputs (published PCG reference output)"}, f, indent=1)
     idx = np.array([0, 1, 2, 3, 1000, 123456, 262143, 4194303], np.uint64)
     draws = np.stack([orc.sampler_floats(int(i), 8) for i in idx])
     np.savez(os.path.join(HERE, "sampler_streams.npz"), index=idx, draws=draws)
