@@ -62,3 +62,19 @@ def test_normal_map_changes_the_image():
     # (0.5, 0.5, 1) maps to the geometric normal: the same sampled directions and values
     assert rel_mse(b, a) < 1e-10
     assert rel_mse(c, a) > 1e-4
+
+
+def test_zero_roughness_derivatives_are_lambertian():
+    """With roughness 0 the rough-diffuse BRDF is color / pi (b = 0, no jump), so both
+    estimators' derivatives equal DiffuseMaterial's."""
+    from helpers import translation_seeds
+    rng = np.random.default_rng(2)
+    g = rng.normal(size=(24, 24, 3))
+    for mode in (0, 1):
+        kw = dict(KW, mode=mode, spp_primary_edge=2, spp_secondary_edge=2, spp_pixel_boundary=2,
+                  primary_edge_hypercube_resolution=200, secondary_edge_hypercube_resolution=(200, 3, 3))
+        a = orc.grad_dir(_spec(np.zeros((5, 5), np.float32)), [g], which=15 if mode else 7,
+                         seed_verts=translation_seeds(_spec(np.zeros((5, 5), np.float32)), 0), **kw)
+        lam = synth.sphere_scene(level=2, tex_hw=16, height=24, width=24)
+        b = orc.grad_dir(lam, [g], which=15 if mode else 7, seed_verts=translation_seeds(lam, 0), **kw)
+        np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
