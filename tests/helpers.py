@@ -144,7 +144,9 @@ def smooth_weights(h, w):
 
 def translation_seeds(spec, mesh):
     """Directional seeds (V_total, 3, 8): directions 0..2 translate mesh `mesh` along x, y, z."""
-    nvt = sum(m.vertices.shape[0] for m in spec.meshes) + sum(l.vertices.shape[0] for l in spec.lights)
+    # an environment light's box has 8 vertices in the scene's vertex list
+    nvt = sum(m.vertices.shape[0] for m in spec.meshes) + sum(
+        l.vertices.shape[0] if getattr(l, "kind", 0) == 0 else 8 for l in spec.lights)
     seeds = np.zeros((nvt, 3, 8))
     off = sum(m.vertices.shape[0] for m in spec.meshes[:mesh])
     n = spec.meshes[mesh].vertices.shape[0]

@@ -38,3 +38,26 @@ def test_reference_estimator_is_not_fd_consistent():
     ad = orc.grad_dir(spec, [g], which=7, seed_verts=translation_seeds(spec, mesh), **cfg)[:3]
     fd = fd_translation(lambda s: orc.render(s, precision=1, **cfg)[0], spec, mesh, g, 1e-2)
     assert rel_l2(ad, fd) > 1.0
+
+
+@pytest.mark.parametrize("kind", [2, 1])
+def test_unbiased_translation_matches_fd_under_environment_light(kind):
+    """The ball case with an SH9 light (direction-dependent radiance) or a cube-map
+    environment added to its area light."""
+    from torch_psdr_b200 import synth
+    spec, mesh = gradient_case("ball", 48, 48)
+    rng = np.random.default_rng(1)
+    if kind == 2:
+        sh = rng.normal(scale=0.2, size=(9, 3)).astype(np.float32)
+        sh[0] = [1.0, 0.8, 0.6]
+        spec.lights.append(synth.LightSpec(None, None, np.zeros(3, np.float32), 2, sh9=sh))
+    else:
+        spec.lights.append(synth.LightSpec(None, None, np.zeros(3, np.float32), 1,
+                                           cube_map=rng.uniform(0.3, 0.8, size=(6, 8, 3)).astype(np.float32)))
+    spp = 1024
+    cfg = dict(CFG, spp_interior=spp, spp_primary_edge=spp, spp_secondary_edge=spp, spp_pixel_boundary=spp,
+               secondary_edge_hypercube_resolution=(2000, 6, 6))
+    g = smooth_weights(48, 48)
+    ad = orc.grad_dir(spec, [g], which=15, seed_verts=translation_seeds(spec, mesh), **cfg)[:3]
+    fd = fd_translation(lambda s: orc.render(s, precision=1, **cfg)[0], spec, mesh, g, 1e-2)
+    assert rel_l2(ad, fd) < 0.06, (ad, fd)
