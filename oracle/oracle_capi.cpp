@@ -29,11 +29,13 @@ template <class S, bool AD> struct Ctx {
   double hc_cells = 1.0;  // hypercube cell count of the term being evaluated
 };
 
-// Raster area per unit surface area at x with normal n (up to fx*fy): |n.(x-o)|/z^3.
+// Raster area per unit surface area at x with normal n (up to fx*fy): |n.(x-o)|/z^3;
+// orthographic: |n.look| (parallel projection).
 template <class S, class R>
 inline S cam_jacobian(const Camera<R>& cam, const V3<S>& x, const V3<S>& n, const V3<S>& o) {
   V3<S> rel = x - o;
   V3<S> look(S(-cam.c2w[0][2]), S(-cam.c2w[1][2]), S(-cam.c2w[2][2]));
+  if (cam.ortho) return abs_(dot(n, look));
   S z = dot(rel, look);
   return abs_(dot(n, rel)) / (z * z * z);
 }
@@ -298,12 +300,19 @@ inline V3<S> eval_primary_unb(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx
   float pdf_e = pe / E.len;
   valid = true;
   project(c.camf, xe, valid, rx, ry);
-  V3<float> rd = normalize(xe - c.posf);
+  V3<float> of = c.posf, rd;
+  if (c.camf.ortho) {
+    V3<float> pcf = Camera<float>::xpos(c.camf.w2c, xe);
+    of = Camera<float>::xpos(c.camf.c2w, V3<float>(pcf.x, pcf.y, 0.f));
+    rd = look_dir<float>(c.camf);
+  } else {
+    rd = normalize(xe - c.posf);
+  }
   V3<float> n = cross(rd, normalize(E.p1 - E.p0));
   const float eps = 1e-5f;
   V3<float> da = rd - n * eps, db = rd + n * eps;
-  Its<float> ia = scene_hit<float, false>(sf, c.posf, da, valid);
-  Its<float> ib = scene_hit<float, false>(sf, c.posf, db, valid);
+  Its<float> ia = scene_hit<float, false>(sf, of, da, valid);
+  Its<float> ib = scene_hit<float, false>(sf, of, db, valid);
   const bool na = ia.valid && tri_has_edge(sf, ia.tri, E), nb = ib.valid && tri_has_edge(sf, ib.tri, E);
   valid = valid && na != nb;
   const Its<float>& ig = na ? ib : ia;
@@ -322,9 +331,14 @@ inline V3<S> eval_primary_unb(const Ctx<S, AD>& c, Pcg32& rng, float s1, int& rx
     double re = norm(rel_e), rg = norm(rel_g);
     V3<double> look(-double(c.camf.c2w[0][2]), -double(c.camf.c2w[1][2]), -double(c.camf.c2w[2][2]));
     double z = dot(rel_e, look);
-    double k = raster_fxfy(c.cam) * re / (z * z * z) / (double(pdf_e) * c.cam.H * c.cam.W);
+    // raster area swept per unit of (normal velocity x edge length): fx fy r_e / z^3, or
+    // fx fy for the parallel projection, where a translation of the camera moves the
+    // edge point and the background alike and depth does not scale velocities
+    const bool ortho = c.cam.ortho;
+    double k = raster_fxfy(c.cam) * (ortho ? 1.0 : re / (z * z * z)) / (double(pdf_e) * c.cam.H * c.cam.W);
     V3<S> dso = c.cam_pos - detach(c.cam_pos);
-    V3<S> vrel = (xes - detach(xes) - dso) - (xg - detach(xg) - dso) * S(re / rg);
+    V3<S> vrel = ortho ? (xes - detach(xes)) - (xg - detach(xg))
+                       : (xes - detach(xes) - dso) - (xg - detach(xg) - dso) * S(re / rg);
     V3<S> ns(S(n.x), S(n.y), S(n.z));
     S vn = dot(vrel, ns) * S(na ? 1.0 : -1.0);
     value = V3<S>(S(Lg.x), S(Lg.y), S(Lg.z)) * (vn * S(-k));
@@ -397,15 +411,19 @@ inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32
     // camera connection of a vertex whose reflection hemisphere (its normal) faces the
     // camera: T times its BSDF toward the camera times its camera Jacobian
     auto connect = [&](const Its<S>& v) {
-      if (val(dot(v.n, c.cam_pos - v.p)) <= 0) return;
+      // toward the camera: its position, or (orthographic) against the look direction
+      // from the point's foot on the camera plane
+      const V3<S> to_cam = c.cam.ortho ? -look_dir<S>(c.cam) : normalize(c.cam_pos - v.p);
+      if (val(dot(v.n, to_cam)) <= 0) return;
       bool vis = true;
       int rx, ry;
       project(c.cam, v.p, vis, rx, ry);
-      Its<S> iv = scene_hit<S, AD>(sc, c.cam_pos, normalize(v.p - c.cam_pos), vis);
+      const V3<S> co = c.cam.ortho ? ortho_origin(c.cam, v.p, c.cam_pos) : c.cam_pos;
+      Its<S> iv = scene_hit<S, AD>(sc, co, -to_cam, vis);
       vis = vis && iv.valid && !iv.is_light && val(sqnorm(iv.p - v.p)) < double(R(1e-5));
       if (!vis || out.n >= kMaxChainOut) return;
       const double Jc = fxfy * val(cam_jacobian(c.cam, val3(v.p), val3(v.n), o));
-      const V3<double> fr = val3(bsdf_eval(sc, v, normalize(c.cam_pos - v.p)));
+      const V3<double> fr = val3(bsdf_eval(sc, v, to_cam));
       out.pix[out.n] = ry * c.cam.W + rx;
       out.w[out.n] = mul(T, fr) * (k0 * Jc);
       ++out.n;
@@ -501,8 +519,13 @@ inline void pixel_border_sample(const Ctx<S, AD>& c, const Border& B, uint64_t i
     B.pixels(q, vert, k, j, lo, hi);
     V3<R> fp = vert ? V3<R>(R(float(k)), R(t + float(j)), R(1)) : V3<R>(R(t + float(k)), R(float(j)), R(1));
     V3<R> pc = Camera<R>::xpos(c.cam.r2c, fp);
-    V3<R> d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
-    V3<R> o(R(val(c.cam_pos.x)), R(val(c.cam_pos.y)), R(val(c.cam_pos.z)));
+    V3<R> o(R(val(c.cam_pos.x)), R(val(c.cam_pos.y)), R(val(c.cam_pos.z))), d;
+    if (c.cam.ortho) {
+      o = Camera<R>::xpos(c.cam.c2w, V3<R>(pc.x, pc.y, R(0)));
+      d = look_dir<R>(c.cam);
+    } else {
+      d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
+    }
     Its<R> its = scene_hit<R, false>(c.scv, o, d, true);
     if (!its.valid) return;
     V3<R> L = trace2light<R, false>(c.scv, rng, its, true, c.cfg.mis_light_samples, c.cfg.mis_bsdf_samples,
@@ -783,10 +806,7 @@ template <class S, bool AD>
 static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
                        const OrcConfig* cfg, int which, double* images, const double* dLdI, double* dphi,
                        double* per_sample, const Seeds<S>& seeds) {
-  // the unbiased estimator's camera Jacobians are those of the perspective camera
-  if (cfg->mode == 1)
-    for (int ci = 0; ci < nc; ++ci)
-      if (cams[ci].type != 0) return 3;
+
   using R = typename Traits<S>::R;
   Scene<S> sc = mk_scene<S>(m, nm, l, nl, seeds);
   Seeds<R> none;
