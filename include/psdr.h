@@ -38,7 +38,7 @@ typedef enum {
   PSDR_ERR_CUDA = 3,
   PSDR_ERR_TIMEOUT = 4,
   PSDR_ERR_NUMERIC = 5,
-  PSDR_ERR_UNSUPPORTED = 6
+  PSDR_ERR_UNSUPPORTED = 6 /* a feature combination the library does not implement */
 } psdr_status;
 
 enum { PSDR_TEX_NONE = -1, PSDR_TEX_CONSTANT = 0, PSDR_TEX_UV = 1 };

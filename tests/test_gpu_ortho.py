@@ -5,8 +5,9 @@ reference estimator's gradient terms against the oracle's forward-mode derivativ
 interior term, the primary-edge term (whose ray origin, the edge point's foot on the
 camera plane, moves with the edge point and the camera) and the direct-edge term (whose
 visibility ray runs along the view direction), for the vertices and the camera origin;
-also with a DiffuseBsdfMaterial, whose value depends on the incoming direction. The
-unbiased estimator refuses orthographic cameras.
+also with a DiffuseBsdfMaterial, whose value depends on the incoming direction; and the
+unbiased estimator's four terms (orthographic camera Jacobian, camera-plane border and
+silhouette rays, camera connections along the view direction).
 """
 import numpy as np
 import pytest
@@ -52,27 +53,35 @@ def test_ortho_image_matches_fp64_oracle(cuda):
 
 
 ORTHO_GRAD_CASES = [
-    # (material, terms bitmask, parameters)
-    ("diffuse", 1, ("verts",)),
-    ("diffuse", 2, ("verts",)),
-    ("diffuse", 2, ("cam",)),
-    ("diffuse", 4, ("verts",)),
-    ("bsdf", 1, ("verts", "cam")),
-    ("bsdf", 2, ("verts",)),
+    # (material, estimator, terms bitmask, parameters)
+    ("diffuse", "reference", 1, ("verts",)),
+    ("diffuse", "reference", 2, ("verts",)),
+    ("diffuse", "reference", 2, ("cam",)),
+    ("diffuse", "reference", 4, ("verts",)),
+    ("bsdf", "reference", 1, ("verts", "cam")),
+    ("bsdf", "reference", 2, ("verts",)),
+    ("diffuse", "unbiased", 1, ("verts", "cam")),
+    ("diffuse", "unbiased", 2, ("verts", "cam")),
+    ("diffuse", "unbiased", 4, ("verts",)),
+    ("diffuse", "unbiased", 8, ("verts", "cam")),
+    ("bsdf", "unbiased", 1, ("verts",)),
 ]
 
 
-@pytest.mark.parametrize("material,terms,kinds", ORTHO_GRAD_CASES)
-def test_ortho_gradient_terms_match_oracle(cuda, material, terms, kinds):
+@pytest.mark.parametrize("material,estimator,terms,kinds", ORTHO_GRAD_CASES)
+def test_ortho_gradient_terms_match_oracle(cuda, material, estimator, terms, kinds):
     spec = ortho_spec() if material == "diffuse" else _to_ortho(bsdf_spec())
     kw = dict(spp_interior=4, max_bounce=3, spp_primary_edge=4, spp_secondary_edge=4,
               primary_edge_hypercube_resolution=500, secondary_edge_hypercube_resolution=[500, 3, 3])
+    unb = estimator == "unbiased"
+    if unb:
+        kw.update(spp_pixel_boundary=4)
     gseeds, oseeds = _seeds(spec, kinds, np.random.default_rng(3))
     params = set()
     for k in kinds:
         params |= {"verts": {"verts", "light_verts"}, "cam": {"cam"}}[k]
     scene, T = to_torch_scene(spec, requires_grad=params)
-    integ = dr.PathIntegrator(gradient_terms=terms, **kw)
+    integ = dr.PathIntegrator(gradient_terms=terms, estimator=estimator, **kw)
     img = integ.renderD(scene)[0]
     dLdI = np.random.default_rng(5).normal(size=tuple(img.shape))
     img.backward(torch.tensor(dLdI, dtype=torch.float32, device="cuda"))
@@ -80,16 +89,8 @@ def test_ortho_gradient_terms_match_oracle(cuda, material, terms, kinds):
     for name, seed in gseeds.items():
         g = T[name].grad.detach().cpu().numpy().astype(np.float64).reshape(-1)
         got += g @ seed.reshape(g.shape[0], 8)
-    ref = orc.grad_dir(spec, [dLdI], which=terms, **oseeds, **kw)
+    ref = orc.grad_dir(spec, [dLdI], which=terms, mode=1 if unb else 0, **oseeds, **kw)
     err = np.abs(got - ref) / (np.abs(ref).max() + 1e-30)
-    print(f"ortho {material} terms={terms} {kinds}: gpu {got[:4]} oracle {ref[:4]} max rel {err.max():.2e}")
+    print(f"ortho {material} {estimator} terms={terms} {kinds}: gpu {got[:4]} oracle {ref[:4]} max rel {err.max():.2e}")
     assert np.abs(ref).max() > 0
     assert err.max() < (1e-2 if terms == 4 else 2e-3)
-
-
-def test_ortho_unbiased_gradients_are_refused(cuda):
-    spec = ortho_spec()
-    scene, T = to_torch_scene(spec, requires_grad={"verts"})
-    img = dr.PathIntegrator(estimator="unbiased").renderD(scene)[0]
-    with pytest.raises(Exception, match="perspective"):
-        img.sum().backward()

@@ -5,10 +5,7 @@
 * the oracle's unbiased estimator with an orthographic camera (camera Jacobian |n.look|,
   rays from the camera plane, silhouette velocities without the depth ratio, camera
   connections along the view direction) matches central differences;
-* the library's unbiased gradients still refuse orthographic cameras through the C ABI
-  (status PSDR_ERR_UNSUPPORTED before any device work).
 """
-import ctypes as C
 import math
 
 import numpy as np
@@ -16,7 +13,6 @@ import pytest
 
 import orc
 from torch_psdr_b200 import synth
-from torch_psdr_b200 import _lib as L
 from helpers import rel_mse
 
 
@@ -57,24 +53,3 @@ def test_oracle_unbiased_orthographic_matches_fd(name):
     ad = orc.grad_dir(spec, [g], which=15, seed_verts=translation_seeds(spec, mesh), **cfg)[:3]
     fd = fd_translation(lambda s: orc.render(s, precision=1, **cfg)[0], spec, mesh, g, 1e-2)
     assert rel_l2(ad, fd) < 0.05, (ad, fd)
-
-
-def test_unbiased_gradients_refuse_orthographic():
-    lib = L.load()
-    ws = C.c_void_p()
-    assert lib.psdr_workspace_create(C.byref(ws)) == 0
-    cfg = L.Config()
-    for k, v in dict(n_pass=1, spp_interior=1, spp_primary_edge=1, spp_secondary_edge=1, max_bounce=1,
-                     mis_light_samples=1, mis_bsdf_samples=1, primary_edge_preprocess_rounds=1,
-                     secondary_edge_preprocess_rounds=1, primary_edge_hypercube_resolution=10,
-                     estimator=L.EST_UNBIASED, spp_pixel_boundary=1).items():
-        setattr(cfg, k, v)
-    cfg.secondary_edge_hypercube_resolution[:] = [10, 1, 1]
-    cam = L.CameraDesc()
-    cam.type, cam.fov, cam.height, cam.width = L.CAM_ORTHOGRAPHIC, 2.0, 4, 4
-    d_img = (C.c_void_p * 1)(None)
-    grads = L.GradTargets()
-    # a non-null fake scene handle is never dereferenced: the camera check fails first
-    st = lib.psdr_render_bwd(C.c_void_p(1), ws, C.byref(cam), 1, C.byref(cfg), d_img, C.byref(grads), None)
-    assert st == L.PSDR_ERR_UNSUPPORTED and b"perspective" in lib.psdr_last_error()
-    assert lib.psdr_workspace_destroy(ws) == 0

@@ -96,8 +96,7 @@ class OrthographicCamera(BaseCamera):
     def __init__(self, look_from, look_at, up, view_width, height: int, width: int):
         """Orthographic camera (torch_psdr.py:161-206; camera.h:279-353): parallel rays
         along the view direction from a view box view_width wide and view_width * height /
-        width high. Renders with both estimators' forward pass; gradients with the
-        reference estimator (the unbiased one is built for perspective cameras)."""
+        width high."""
         super().__init__()
         assert look_from.size() == (3,)
         assert look_at.size() == (3,)

@@ -93,7 +93,6 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     *out = nullptr;
     check_config(cfg);
     check_cameras(cams, n_cams);
-    if (d_images) check_estimator_cameras(cfg, cams, n_cams);
     for (int i = 0; i < n_scenes; ++i) {
       PSDR_CHECK(scenes[i] != nullptr, "null scene");
       PSDR_CHECK(scenes[i]->nlight > 0 || cfg->mis_light_samples == 0, "a scene has no light to sample");

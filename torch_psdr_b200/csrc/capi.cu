@@ -117,14 +117,6 @@ long long light_param_count(const psdr_scene* s, int l) {
   return L.kind == PSDR_LIGHT_SH9 ? 27 : 0;
 }
 
-// The unbiased estimator's camera Jacobians and raster velocities are those of the
-// perspective camera.
-void check_estimator_cameras(const psdr_config* cfg, const psdr_camera_desc* cams, int n) {
-  if (cfg->estimator != PSDR_EST_UNBIASED) return;
-  for (int i = 0; i < n; ++i)
-    PSDR_REQUIRE(cams[i].type == PSDR_CAM_PERSPECTIVE,
-                 "the unbiased estimator's gradients take perspective cameras (use the reference estimator)");
-}
 
 }  // namespace psdr
 
@@ -520,7 +512,6 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   PSDR_CHECK(scene && ws && d_images && grads, "null argument");
   check_cfg(cfg);
   check_cams(cams, n_cams);
-  check_estimator_cameras(cfg, cams, n_cams);
   ws->bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;  // extended kernel instances
   PSDR_CHECK(scene->nlight > 0, "scene has no light");
   cudaStream_t st = (cudaStream_t)stream;

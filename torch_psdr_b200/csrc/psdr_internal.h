@@ -27,8 +27,6 @@ struct Error {
   } while (0)
 #define PSDR_CHECK(cond, msg) \
   do { if (!(cond)) throw ::psdr::Error{PSDR_ERR_INVALID_ARG, msg}; } while (0)
-#define PSDR_REQUIRE(cond, msg) \
-  do { if (!(cond)) throw ::psdr::Error{PSDR_ERR_UNSUPPORTED, msg}; } while (0)
 
 // Device allocation owned by the library (stream-ordered allocator).
 struct DBuf {

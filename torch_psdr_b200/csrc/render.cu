@@ -985,6 +985,12 @@ PSDR_D float view_fxfy(const DevView& V) {
 // Unbiased estimator, primary vertex: adjoint of the camera Jacobian ratio J/detach(J),
 // J = |n.(x-o)| / z^3, z = (x-o).look, scaled by phi = dot(dI, L).
 PSDR_D void cam_jacobian_adj(const DevView& V, const Surf& x, float phi, SurfAdj& ax, CamAcc& cam) {
+  if (V.ortho) {
+    // J = |n.look|: only the normal moves it
+    const float3 look = view_look(V);
+    ax.n += look * (phi / dot(x.n, look));
+    return;
+  }
   const float3 rel = x.p - V.pos;
   const float nr = dot(x.n, rel);
   const float3 look = view_look(V);
@@ -1267,7 +1273,7 @@ __global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restr
       const int px = (int)floorf(pr.x), py = (int)floorf(pr.y);
       bool valid = ok && pc.z < 0.f && pr.x > 0.f && pr.x < (float)V.W && pr.y > 0.f && pr.y < (float)V.H;
       // camera.h:260-276 / 336-353: the ray through the edge point
-      const bool ortho = V.ortho && !unb;
+      const bool ortho = V.ortho;
       const float3 eo = ortho ? xform_pos_rn(V.c2w, f3(pc.x, pc.y, 0.f)) : V.pos;
       const float3 rd = ortho ? view_look_dir(V) : normalize_rn(sub_rn(xe, V.pos));
       const float3 nrm = cross_rn(rd, normalize_rn(sub_rn(p1, p0)));
@@ -1343,8 +1349,10 @@ __global__ void __launch_bounds__(256) k_edge_final_unb(WF w, const DevScene* __
     const float re = norm(re3), z = dot(re3, look);
     const int tri = __float_as_int(hg.x);
     const Surf g = make_surf(sc, tri, hg.y, hg.z, V.pos);
-    const float ratio = re / sqrtf(g.sqd);
-    const float K = fxfy * re / (z * z * z) / (a.z * a.w * cells * (float)V.H * (float)V.W * (float)spp);
+    // orthographic: no depth scaling, and a camera translation moves both points alike
+    const float ratio = V.ortho ? 1.f : re / sqrtf(g.sqd);
+    const float K = fxfy * (V.ortho ? 1.f : re / (z * z * z)) / (a.z * a.w * cells * (float)V.H * (float)V.W *
+                                                                  (float)spp);
     const float3 av = xyz(nn) * (-(flag == 1 ? 1.f : -1.f) * phi * K);
     if (!finite3(av)) continue;
     if (sc.grad_verts) {
@@ -1540,8 +1548,14 @@ __global__ void __launch_bounds__(256) k_border_init(WF w, const DevScene* __res
       const float3 fp = vert ? f3((float)k, t + (float)j, 1.0f) : f3(t + (float)k, (float)j, 1.0f);
       float3 pc;
       xform_pos(V.r2c, fp, pc);
-      const float3 d = normalize(xform_dir(V.c2w, pc));
-      const HitRec h = trace_closest(sc, V.pos, d, kTmin, INFINITY);
+      float3 o = V.pos, d;
+      if (V.ortho) {
+        xform_pos(V.c2w, f3(pc.x, pc.y, 0.f), o);
+        d = view_look_dir(V);
+      } else {
+        d = normalize(xform_dir(V.c2w, pc));
+      }
+      const HitRec h = trace_closest(sc, o, d, kTmin, INFINITY);
       w.rs[s] = rng.state;
       w.ri[s] = rng.inc;
       w.view[s] = v;
@@ -1549,7 +1563,7 @@ __global__ void __launch_bounds__(256) k_border_init(WF w, const DevScene* __res
       w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
       w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       w.cur[s] = hit4(h);
-      w.org[s] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      w.org[s] = make_float4(o.x, o.y, o.z, 0.f);
       eb.hb[s] = hit4(h);
       eb.a[s] = make_float4(__int_as_float((int)q), t, (float)pmf, 0.f);
       alive = h.tri >= 0 && pmf > 0.0;
@@ -1715,19 +1729,23 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
       // camera connection of a vertex whose reflection hemisphere faces the camera:
       // T times its BSDF toward the camera times its camera Jacobian
       auto connect = [&](const Surf& v) {
-        const float3 rel = v.p - V.pos;
-        if (dot(v.n, rel) >= 0.f) return;
+        // from the camera position, or (orthographic) from v's foot on the camera plane
+        // along the look direction
+        const float3 co = V.ortho ? ortho_origin_rn(V, v.p) : V.pos;
+        const float3 rel = v.p - co;
+        const float dist = norm(rel);
+        const float3 dir = V.ortho ? look : rel / dist;
+        if (dot(v.n, dir) >= 0.f) return;
         int qx, qy;
         if (!project(V, v.p, qx, qy)) return;
         // the closest hit must be v itself: stop at the first hit short of it (same
         // outcome as a full closest-hit query followed by the distance test)
-        const float dist = norm(rel);
-        const HitRec hc2 = trace_closest(sc, V.pos, rel / dist, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
-        const Surf iv = make_surf(sc, hc2.tri, hc2.b1, hc2.b2, V.pos);
+        const HitRec hc2 = trace_closest(sc, co, dir, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
+        const Surf iv = make_surf(sc, hc2.tri, hc2.b1, hc2.b2, co);
         if (!(iv.valid && !iv.is_light && sqnorm(iv.p - v.p) < kEps)) return;
         const float z = dot(rel, look);
-        const float Jc = fxfy * fabsf(dot(v.n, rel)) / (z * z * z);
-        const float3 Tf = BSDF ? mul(T, surf_bsdf(sc, v, -(rel / dist))) : T;
+        const float Jc = V.ortho ? fxfy * fabsf(dot(v.n, look)) : fxfy * fabsf(dot(v.n, rel)) / (z * z * z);
+        const float3 Tf = BSDF ? mul(T, surf_bsdf(sc, v, -dir)) : T;
         if (PRE) {
           msum += norm(Tf) * fabsf(k0 * Jc);
         } else {

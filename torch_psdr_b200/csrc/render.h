@@ -129,7 +129,6 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
 SceneGradInfo grad_info(const psdr_scene* s);
 void check_config(const psdr_config* c);
 void check_cameras(const psdr_camera_desc* cams, int n);
-void check_estimator_cameras(const psdr_config* cfg, const psdr_camera_desc* cams, int n);
 long long light_param_count(const psdr_scene* s, int l);
 void scene_build_geometry(psdr_scene* s, cudaStream_t st);
 void scene_refit_geometry(psdr_scene* s, cudaStream_t st);
