@@ -209,7 +209,7 @@ PSDR_API psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, cons
  * __device__ array per GPU, held until the process exits; tiles shrink to fit it, so
  * any image size works, but spp_interior must not exceed the tile (about 100k paths
  * with one light and one BSDF sample; larger values return PSDR_ERR_INVALID_ARG).
- * The first call on a device resolves the array's address (cudaGetSymbolAddress), so
+ * It takes perspective cameras (others return PSDR_ERR_INVALID_ARG). The first call on a device resolves the array's address (cudaGetSymbolAddress), so
  * make that first call before any stream capture. All calls share the array and it
  * keeps the last call's contents: calls that overlap on the GPU (other streams,
  * other threads) race and must be serialised by the caller. The scene is an input

@@ -877,7 +877,8 @@ int orc_render(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCam
 }
 
 // Directional derivatives dPhi/dtheta . seed_k (k < 8) of Phi = sum dLdI * image, with the
-// reference's renderD semantics. which: bit0 interior, bit1 primary edges, bit2 direct edges.
+// reference's renderD semantics. which: bit0 interior, bit1 primary edges, bit2 direct edges,
+// bit3 pixel-border segments (unbiased estimator only).
 int orc_grad_dir(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
                  const OrcConfig* cfg, int which, const double* dLdI, const double* seed_verts,
                  const double* seed_tex, const double* seed_emit, const double* seed_cam, double* dphi_out) {

@@ -181,7 +181,7 @@ def grad_dir(spec, dLdI, which=1, seed_verts=None, seed_tex=None, seed_emit=None
     rc = L.orc_grad_dir(*m.args(), C.byref(c), int(which), _ptr(g), _ptr(sv), _ptr(st), _ptr(se), _ptr(sc),
                         _ptr(out))
     if rc != 0:
-        raise ValueError(f"oracle gradient failed (code {rc}; the unbiased estimator takes perspective cameras)")
+        raise ValueError(f"oracle gradient failed (code {rc})")
     return out
 
 
