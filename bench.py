@@ -502,6 +502,82 @@ def run_multiview(args):
     return 0
 
 
+# ---------------------------------------------------------------- large workload
+LG_WORKLOAD = ("large scene, full gradient with path replay: 16 noisy level-6 icospheres (1,310,720 tris) centred "
+               "uniformly in [-5,5]^3 (seed 4), a 512^2 texture each, ground, 4x4 light; 1024x1024, 64 spp interior "
+               "+ 4 spp per edge kind, depth 5, vertex + texture gradients of an L2 loss")
+
+
+def run_large(args):
+    """One persistent Scene of 16 level-6 spheres rendered and differentiated through
+    BatchRender (forward and backward replayed from graphs), one GPU."""
+    import torch
+    import torch_psdr_b200 as dr
+    from torch_psdr_b200 import synth
+    t0 = time.time()
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    spec = synth.large_scene()
+    cfg = dict(spp_interior=64, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=5, estimator=args.estimator)
+    integ = dr.PathIntegrator(**cfg)
+
+    def tens(a, dt=torch.float32, rg=False):
+        return torch.tensor(np.asarray(a), dtype=dt, device=dev, requires_grad=rg)
+
+    spheres, ground = spec.meshes[:-1], spec.meshes[-1]
+    sv = [tens(m.vertices, rg=True) for m in spheres]
+    st = [tens(m.texture, rg=True) for m in spheres]
+    f, uv, uvi = tens(spheres[0].faces, torch.int32), tens(spheres[0].uvs), tens(spheres[0].uv_indices, torch.int32)
+    gV, gF, gT = tens(ground.vertices), tens(ground.faces, torch.int32), tens(ground.texture)
+    lt, c = spec.lights[0], spec.cameras[0]
+    light = dr.AreaLight(tens(lt.vertices), tens(lt.faces, torch.int32), tens(lt.emit))
+    cam = dr.PerspectiveCamera(tens(c.look_from), tens(c.look_at), tens(c.up), tens([c.vfov]), c.height, c.width)
+
+    def scene_of(verts):
+        return dr.Scene([cam], [dr.Mesh(v, uv, f, uvi, dr.DiffuseMaterial(t)) for v, t in zip(verts, st)] +
+                        [dr.Mesh(gV, None, gF, None, dr.DiffuseMaterial(gT))], [light])
+
+    with torch.no_grad():
+        target = integ.renderC(scene_of([v + 0.03 for v in sv]))[0].clone()
+    batch = dr.BatchRender(integ, [scene_of(sv)])
+    print(f"large: setup {time.time() - t0:.1f} s", file=sys.stderr, flush=True)
+
+    def step():
+        img = batch.renderD()[0]
+        ((img - target) ** 2).sum().backward()
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    print(f"large: warm-up done {time.time() - t0:.1f} s", file=sys.stderr, flush=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(dev.index)
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    paths = c.height * c.width * cfg["spp_interior"]
+    g = sv[0].grad
+    line = {"metric": METRIC, "value": paths * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded icosphere scene)",
+            "config": {"workload": LG_WORKLOAD, "triangles": sum(len(m.faces) for m in spec.meshes) + len(lt.faces),
+                       "paths_per_step": paths, "estimator": args.estimator,
+                       "mode": "batched (persistent scene, forward and backward graphs)",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "grad_finite": bool(torch.isfinite(g).all().item()) and float(g.abs().sum()) > 0},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,8 +588,9 @@ def main():
     ap.add_argument("--no-grad-check", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--estimator", default="unbiased", choices=["unbiased", "reference"])
-    ap.add_argument("--workload", default="geometry", choices=["geometry", "multiview"],
-                    help="geometry: the 512^2 fwd+bwd workload (default); multiview: 64 views over 3 scenes")
+    ap.add_argument("--workload", default="geometry", choices=["geometry", "multiview", "large"],
+                    help="geometry: the 512^2 fwd+bwd workload (default); multiview: 64 views over 3 scenes; "
+                         "large: 16 level-6 spheres at 1024^2, 64 spp, depth 5")
     ap.add_argument("--mode", default="batched", choices=["batched", "plain"],
                     help="batched: persistent scene + graph replay; plain: new Scene + per-view launches each step")
     ap.add_argument("--size", type=int, default=512, help="image size (512 = the benchmark workload)")
@@ -528,6 +605,8 @@ def main():
         return run_reference(args)
     if args.workload == "multiview":
         return run_multiview(args)
+    if args.workload == "large":
+        return run_large(args)
     return run_b200(args)
 
 

@@ -199,6 +199,32 @@ def sphere_scene(level=3, tex_hw=256, tex_seed=0, noise_sigma=0.0, noise_seed=2,
     return SceneSpec([sphere, ground], [light], [default_camera(height, width)])
 
 
+def large_scene(n_spheres=16, level=6, tex_hw=512, seed=4, noise_sigma=0.02, height=1024,
+                width=1024) -> SceneSpec:
+    """Many-object workload: n_spheres noisy level-`level` icospheres (radius 1, radial
+    noise N(0, noise_sigma) seeded per sphere) centred uniformly in the box [-5, 5]^3
+    (seed `seed`), each with its own tex_hw^2 texture (seeds seed*100 + i); a 40x40
+    ground quad at y = -6.5 (albedo 0.5) and a 4x4 area light at y = 7 facing down
+    (radiance 20); the camera at (0, 4, 20) looks at the origin with a 45 degree field
+    of view, which frames the whole box. 16 level-6 spheres are 1,310,720 triangles."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(-5.0, 5.0, size=(n_spheres, 3))
+    V0, F = icosphere(level)
+    uvs, uvi = spherical_uv(V0, F)
+    meshes = []
+    for i in range(n_spheres):
+        V = radial_noise(V0, noise_sigma, seed * 100 + i) if noise_sigma > 0 else V0
+        meshes.append(MeshSpec((V + centres[i]).astype(np.float32), F, uvs, uvi,
+                               uniform_texture(tex_hw, tex_hw, seed * 100 + i)))
+    gV, gF = quad((0.0, 0.0), 40.0, -6.5, facing_down=False)
+    meshes.append(MeshSpec(gV, gF, None, None, np.array([0.5, 0.5, 0.5], np.float32)))
+    lV, lF = quad((0.0, 0.0), 4.0, 7.0, facing_down=True)
+    light = LightSpec(lV, lF, np.array([20.0, 20.0, 20.0], np.float32))
+    cam = CameraSpec(np.array([0, 4, 20], np.float32), np.array([0, 0, 0], np.float32),
+                     np.array([0, 1, 0], np.float32), math.pi / 4, height, width)
+    return SceneSpec(meshes, [light], [cam])
+
+
 def orbit_cameras(n, radius, seed, size_lo=128, size_hi=512):
     """n cameras uniform on a sphere of the given radius looking at the origin,
     image sizes uniform in [size_lo, size_hi] (independently for H and W)."""
