@@ -544,6 +544,108 @@ inline void pixel_border_sample(const Ctx<S, AD>& c, const Border& B, uint64_t i
   }
 }
 
+// Intersection record of a value-scene hit with the differentiated scene's frame (the
+// hit triangle's normal and tangent, flipped to the side the value hit faces).
+template <class S, class T>
+inline Its<S> material_its(const Scene<S>& sc, const Its<T>& h) {
+  Its<S> r;
+  const Tri<S>& tr = sc.tris[h.tri];
+  r.valid = true;
+  r.is_front = h.is_front;
+  r.p = material_point(sc, h);
+  r.n = h.is_front ? tr.n : -tr.n;
+  r.t = h.is_front ? tr.t : -tr.t;
+  r.u = h.u; r.v = h.v; r.b1 = h.b1; r.b2 = h.b2;
+  r.tri = h.tri; r.obj = h.obj; r.light = h.light; r.is_light = h.is_light;
+  return r;
+}
+
+// BSDF-jump term of DiffuseBsdfMaterial (diffuse_bsdf.cc:56-88). With N.L >= 0 and
+// N.V >= 0 the rule on t makes the value jump by color b (max(N.L, N.V) + 1e-5) where
+// t = V.L - (N.L)(N.V) = m.L crosses 0, m = V - (N.V) N: over the shading hemisphere, on
+// the half great circle through N perpendicular to m. In the material form the rendered
+// value at x_k changes at Int_arc dF L_i (Ng.L) d/dtheta[m . L_att] / |m| dl, where L_att is
+// the direction from the material point x_k to the material point x_{k+1} seen along L
+// (the arc's velocity relative to the surface it sweeps, per unit arc length). Sample i
+// follows one camera path of its pixel (the interior term's sampling); at each of its
+// vertices on a DiffuseBsdfMaterial with roughness > 0 it draws one arc direction
+// uniformly (pdf 1/pi), traces L_i with the path's remaining bounces and adds
+// dPhi/dtheta . seed_k to dphi through the zero-valued carrier m . L_att.
+template <class S, bool AD>
+inline void bsdf_jump_sample(const Ctx<S, AD>& c, uint64_t i, const double* dLdI, double* dphi) {
+  using R = typename Traits<S>::R;
+  if constexpr (AD) {
+    constexpr int KD = sizeof(S) / sizeof(double) - 1;
+    const int W = c.cam.W, spp = c.cfg.spp_interior, D = c.cfg.max_bounce;
+    const int nL = c.cfg.mis_light_samples, nB = c.cfg.mis_bsdf_samples;
+    Pcg32 rng = make_sampler(i);
+    R jx = rng.next_float(), jy = rng.next_float();
+    const int pix = spp > 1 ? int(i / (uint64_t)spp) : int(i);
+    V3<R> fp(jx + R(pix % W), jy + R(pix / W), R(1));
+    V3<R> pc = Camera<R>::xpos(c.cam.r2c, fp);
+    V3<R> o(R(val(c.cam_pos.x)), R(val(c.cam_pos.y)), R(val(c.cam_pos.z))), d;
+    if (c.cam.ortho) {
+      o = Camera<R>::xpos(c.cam.c2w, V3<R>(pc.x, pc.y, R(0)));
+      d = look_dir<R>(c.cam);
+    } else {
+      d = normalize(Camera<R>::xdir(c.cam.c2w, pc));
+    }
+    Its<R> its = scene_hit<R, false>(c.scv, o, d, true);
+    V3<R> T(R(1), R(1), R(1));
+    V3<S> xprev = c.cam_pos;  // previous material vertex (the camera for x_1)
+    for (int k = 1; k <= D; ++k) {
+      if (!its.valid || its.is_light) break;
+      const R sigma = c.scv.obj_mat[its.obj] == 1 ? R(tex_fetch(c.scv, c.scv.obj_rough[its.obj], its.u, its.v).x) : R(0);
+      const V3<R> N = shading_normal(c.scv, its);
+      const R nv = dot(N, its.wi);
+      const V3<R> m = its.wi - N * nv;
+      const R mlen = norm(m);
+      const R u_arc = rng.next_float();
+      if (sigma > 0 && nv >= 0 && mlen > R(1e-7)) {
+        const V3<R> w = normalize(cross(N, m));
+        const R psi = (u_arc - R(0.5)) * R(M_PI);
+        const V3<R> L = normalize(N * R(std::cos(psi)) + w * R(std::sin(psi)));
+        const R nl = std::max(dot(N, L), R(0));
+        const R a = R(1) / (R(M_PI) + R((3 * M_PI - 4) / 6) * sigma);
+        const R dF = sigma * a * (std::max(nl, nv) + R(1e-5));
+        Its<R> nx = scene_hit<R, false>(c.scv, its.p, L, true);
+        V3<R> Li;
+        if (nx.valid) {
+          if (nx.is_light) Li = light_emit(c.scv, nx);
+          else if (k < D) Li = trace2light<R, false>(c.scv, rng, nx, true, nL, nB, D - k, false);
+        }
+        const V3<R> wv = mul(mul(T, tex_at(c.scv, its.obj, its.u, its.v)), Li) *
+                         (dF * dot(its.n, L) * R(M_PI) / mlen / R(spp));
+        double wgt = 0;
+        for (int ch = 0; ch < 3; ++ch) wgt += dLdI[3 * pix + ch] * double(wv[ch]);
+        if (nx.valid && wgt != 0 && std::isfinite(wgt)) {
+          const Its<S> xk = material_its(c.sc, its);
+          const V3<S> xn = material_point(c.sc, nx);
+          V3<S> Vd = (k == 1 && c.cam.ortho) ? -V3<S>(S(d.x), S(d.y), S(d.z)) : normalize(xprev - xk.p);
+          const V3<S> Nd = shading_normal(c.sc, xk);
+          const V3<S> md = Vd - Nd * dot(Nd, Vd);
+          const S q = dot(md, normalize(xn - xk.p));
+          for (int qd = 0; qd < KD; ++qd) dphi[qd] += wgt * q.d[qd];
+        }
+      }
+      if (k == D) break;
+      // continue the camera path (cosine sampling about the shading normal)
+      const R rx = rng.next_float(), ry = rng.next_float();
+      R ct;
+      const V3<R> wo = material_sample_dir(c.scv, its, rx, ry, ct);
+      Its<R> nx = scene_hit<R, false>(c.scv, its.p, wo, true);
+      if (!nx.valid) break;
+      const R tmp = dot(nx.n, -wo) / nx.sqd;
+      const R G = dot(its.n, wo) * tmp;
+      const R pdf = ct * R(1.0 / M_PI) * tmp;
+      T = mul(T, bsdf_eval(c.scv, its, wo)) * (G / pdf);
+      if (!finite3(T)) break;
+      xprev = material_point(c.sc, its);
+      its = nx;
+    }
+  }
+}
+
 // sampler.h:201-247 HyperCubeSampler: cells in row-major order of the resolution.
 template <class R> struct HyperCube {
   int N = 1;
@@ -795,6 +897,17 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
       }
     }
   }
+  // ---- BSDF jumps of DiffuseBsdfMaterial (unbiased estimator only)
+  if ((which & 16) && unb &&
+      std::find(c.sc.obj_mat.begin(), c.sc.obj_mat.end(), 1) != c.sc.obj_mat.end()) {
+    if constexpr (KD > 0) {
+      const uint64_t N = (uint64_t)npix * c.cfg.spp_interior;
+      std::vector<double> phi_s(N * KD, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+      for (int64_t i = 0; i < (int64_t)N; ++i) bsdf_jump_sample<S, AD>(c, (uint64_t)i, dLdI, &phi_s[i * KD]);
+      for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+    }
+  }
 }
 
 template <class S>
@@ -878,7 +991,7 @@ int orc_render(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCam
 
 // Directional derivatives dPhi/dtheta . seed_k (k < 8) of Phi = sum dLdI * image, with the
 // reference's renderD semantics. which: bit0 interior, bit1 primary edges, bit2 direct edges,
-// bit3 pixel-border segments (unbiased estimator only).
+// bit3 pixel-border segments, bit4 DiffuseBsdfMaterial jumps (both unbiased estimator only).
 int orc_grad_dir(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
                  const OrcConfig* cfg, int which, const double* dLdI, const double* seed_verts,
                  const double* seed_tex, const double* seed_emit, const double* seed_cam, double* dphi_out) {
