@@ -92,6 +92,21 @@ def test_cpu_tensors_are_rejected():
         dr.Texture(torch.zeros(3))
 
 
+def test_index_buffers_are_range_checked():
+    """Mesh and AreaLight check face and uv indices against their vertex and uv counts
+    (the native gathers do not), on CPU tensors here."""
+    from torch_psdr_b200.api import check_indices
+    f = torch.tensor([[0, 1, 2], [0, 2, 3]], dtype=torch.int32)
+    check_indices(f, 4, "face_indices")
+    check_indices(torch.zeros((0, 3), dtype=torch.int32), 0, "face_indices")
+    with pytest.raises(ValueError, match=r"\[0, 3\): found values in \[0, 3\]"):
+        check_indices(f, 3, "face_indices")
+    with pytest.raises(ValueError, match="uv_indices"):
+        check_indices(f - 1, 4, "uv_indices")
+    with pytest.raises(AssertionError):  # one uv triangle per face
+        dr.Mesh(torch.zeros(4, 3), torch.zeros(4, 2), f, f[:1], None)
+
+
 # ctypes mirror -> C struct of include/psdr.h, and the C field names where they differ
 _STRUCTS = {
     "TextureDesc": ("psdr_texture_desc", {}),

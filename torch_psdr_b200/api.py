@@ -26,6 +26,18 @@ def _dev_tensor(t: Tensor, dtype) -> Tensor:
     return t.detach().to(dtype).contiguous().clone()
 
 
+def check_indices(idx: Tensor, n: int, what: str) -> None:
+    """Every entry of the index buffer idx must lie in [0, n): the native kernels gather
+    vertices and uvs through these buffers without bounds checks (as the reference's
+    gathers do), so an out-of-range index would read outside the buffer. One device
+    reduction and one host read; empty buffers are left to the library's own check."""
+    if idx.numel() == 0:
+        return
+    lo, hi = torch.stack([idx.min(), idx.max()]).tolist()
+    if lo < 0 or hi >= n:
+        raise ValueError(f"{what} must lie in [0, {n}): found values in [{lo}, {hi}]")
+
+
 def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -221,12 +233,16 @@ class Mesh(VarContex):
         assert uvs is None or (uvs.dim() == 2 and uvs.size(-1) == 2)
         assert face_indices.dim() == 2 and face_indices.size(-1) == 3
         assert uv_indices is None or (uv_indices.dim() == 2 and uv_indices.size(-1) == 3)
+        assert uvs is None or uv_indices is None or uv_indices.size(0) == face_indices.size(0)
         self.vertices = vertices
         self.v = _dev_tensor(vertices, torch.float32)
         self.f = _dev_tensor(face_indices, torch.int32)
+        check_indices(self.f, self.v.shape[0], "face_indices")
         no_uvs = uvs is None or uv_indices is None
         self.uv = None if no_uvs else _dev_tensor(uvs, torch.float32)
         self.uvi = None if no_uvs else _dev_tensor(uv_indices, torch.int32)
+        if self.uvi is not None:
+            check_indices(self.uvi, self.uv.shape[0], "uv_indices")
         self.material = material
         self.append_variable(vertices)
         self.merge_variables(material.get_variables())
@@ -271,6 +287,7 @@ class AreaLight(Light):
         self.vertices, self.emit = vertices, emit
         self.v = _dev_tensor(vertices, torch.float32)
         self.f = _dev_tensor(face_indices, torch.int32)
+        check_indices(self.f, self.v.shape[0], "face_indices")
         self.append_variable(vertices)
         self.append_variable(emit)
 
