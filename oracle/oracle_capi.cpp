@@ -570,7 +570,11 @@ inline Its<S> material_its(const Scene<S>& sc, const Its<T>& h) {
 // follows one camera path of its pixel (the interior term's sampling); at each of its
 // vertices on a DiffuseBsdfMaterial with roughness > 0 it draws one arc direction
 // uniformly (pdf 1/pi), traces L_i with the path's remaining bounces and adds
-// dPhi/dtheta . seed_k to dphi through the zero-valued carrier m . L_att.
+// dPhi/dtheta . seed_k to dphi through the zero-valued carrier m . L_att. The camera
+// path draws from stream i (2 jitter draws, then per vertex the arc draw and two
+// direction draws); the L_i of vertex k draws from its own stream 16 i + k, so that a
+// wavefront renderer can estimate each depth's L_i in a pass of its own.
+constexpr uint64_t kJumpStreams = 16;  // max_bounce <= 16
 template <class S, bool AD>
 inline void bsdf_jump_sample(const Ctx<S, AD>& c, uint64_t i, const double* dLdI, double* dphi) {
   using R = typename Traits<S>::R;
@@ -612,7 +616,10 @@ inline void bsdf_jump_sample(const Ctx<S, AD>& c, uint64_t i, const double* dLdI
         V3<R> Li;
         if (nx.valid) {
           if (nx.is_light) Li = light_emit(c.scv, nx);
-          else if (k < D) Li = trace2light<R, false>(c.scv, rng, nx, true, nL, nB, D - k, false);
+          else if (k < D) {
+            Pcg32 rli = make_sampler(i * kJumpStreams + (uint64_t)k);
+            Li = trace2light<R, false>(c.scv, rli, nx, true, nL, nB, D - k, false);
+          }
         }
         const V3<R> wv = mul(mul(T, tex_at(c.scv, its.obj, its.u, its.v)), Li) *
                          (dF * dot(its.n, L) * R(M_PI) / mlen / R(spp));
