@@ -129,7 +129,8 @@ typedef struct {
   int32_t leaf_size;
   int32_t terms;  /* gradient terms of psdr_render_bwd: bit 0 interior, bit 1 primary
                      edges, bit 2 direct edges, bit 3 pixel borders (UNBIASED only);
-                     0 = all */
+                     0 = those four. Bit 4: BRDF jumps of DiffuseBsdfMaterial
+                     (UNBIASED only, on request: not part of 0) */
   int32_t spp_pixel_boundary; /* UNBIASED: samples per unit pixel-border segment */
   uint64_t seed;
 } psdr_config;

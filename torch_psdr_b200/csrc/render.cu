@@ -1629,6 +1629,188 @@ __global__ void __launch_bounds__(256) k_border_final(WF w, const DevScene* __re
   }
 }
 
+// ------------------------------------------------------------------ BSDF jumps
+// Unbiased estimator, DiffuseBsdfMaterial with roughness > 0 (diffuse_bsdf.cc:56-88).
+// With N.L >= 0 and N.V >= 0 the rough-diffuse value jumps by color b (max(N.L, N.V) +
+// 1e-5) where t = m.L crosses 0, m = V - (N.V) N: over the shading hemisphere, the half
+// great circle through N perpendicular to m. The rendered value at x_k changes at
+// Int_arc dF L_i (Ng.L) d/dtheta[m . L_att] / |m| dl, L_att the direction from the material
+// point x_k to the material point x_{k+1} seen along L. One pass per depth k:
+// k_jump_init replays camera sample i to its k-th vertex (stream i: 2 jitter draws, then
+// per vertex the arc draw and two direction draws), draws the arc direction there
+// (uniform, pdf 1/pi) and starts a path along it on stream 16 i + k; the path kernels
+// estimate L_i with D - k bounces; k_jump_final scatters the adjoint of the carrier
+// m . normalize(x_{k+1} - x_k). Side buffers: a = weight (prefix throughput x color x dF x
+// (Ng.L) pi / (|m| spp)) and pixel; n = x_k's hit (w: 1 when the sample is live);
+// hb = x_{k+1}'s hit; La = x_{k-1}'s hit (tri -1: the camera).
+constexpr unsigned long long kJumpStreams = 16;  // max_bounce <= 16
+
+__global__ void __launch_bounds__(256) k_jump_init(WF w, const DevScene* __restrict__ scenes,
+                                                   const DevView* __restrict__ views, int v, EdgeBuf eb,
+                                                   long long begin, int n, int k, int D) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool alive = false;
+    if (s < n) {
+      const long long i = begin + s;
+      const DevView& V = views[v];
+      const DevScene& sc = scenes[V.scene];
+      Rng rng = make_rng((unsigned long long)i + w.seed);
+      const float jx = rng.next_float(), jy = rng.next_float();
+      const int pix = V.spp > 1 ? (int)(i / V.spp) : (int)i;
+      float3 pc;
+      xform_pos(V.r2c, f3(jx + (float)(pix % V.W), jy + (float)(pix / V.W), 1.0f), pc);
+      float3 o = V.pos, d;
+      if (V.ortho) {
+        xform_pos(V.c2w, f3(pc.x, pc.y, 0.f), o);
+        d = view_look_dir(V);
+      } else {
+        d = normalize(xform_dir(V.c2w, pc));
+      }
+      HitRec h = trace_closest(sc, o, d, kTmin, INFINITY);
+      Surf x = make_surf(sc, h.tri, h.b1, h.b2, o);
+      HitRec hp;
+      hp.tri = -1; hp.b1 = hp.b2 = hp.t = 0.f;
+      float3 T = f3(1.f, 1.f, 1.f);
+      eb.n[s] = make_float4(__int_as_float(-1), 0.f, 0.f, __int_as_float(0));
+      w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int kk = 1; kk <= k; ++kk) {
+        if (!x.valid || x.is_light) break;
+        const float u_arc = rng.next_float();
+        const DevObj& ob = sc.objs[x.obj];
+        const MatPt mp = mat_point(ob, x);
+        if (kk == k) {
+          const float nv = dot(mp.N, x.wi);
+          const float3 m = x.wi - mp.N * nv;
+          const float mlen = norm(m);
+          if (!(mp.rough && mp.sigma > 0.f && nv >= 0.f && mlen > 1e-7f)) break;
+          const float3 wa = normalize(cross(mp.N, m));
+          float sp, cp;
+          sincosf((u_arc - 0.5f) * kPi, &sp, &cp);
+          const float3 L = normalize(mp.N * cp + wa * sp);
+          const float nl = fmaxf(dot(mp.N, L), 0.f);
+          const float a = 1.0f / (kPi + kOrenC * mp.sigma);
+          const float dF = mp.sigma * a * (fmaxf(nl, nv) + kEps);
+          const float3 wv = mul(T, mp.color) * (dF * dot(x.n, L) * kPi / (mlen * (float)V.spp));
+          const HitRec ha = trace_closest(sc, x.p, L, kTmin, INFINITY);
+          if (ha.tri < 0 || !finite3(wv)) break;
+          eb.a[s] = make_float4(wv.x, wv.y, wv.z, __int_as_float(pix));
+          eb.n[s] = make_float4(__int_as_float(h.tri), h.b1, h.b2, __int_as_float(1));
+          eb.hb[s] = hit4(ha);
+          eb.La[s] = hit4(hp);
+          const Surf xa = make_surf(sc, ha.tri, ha.b1, ha.b2, x.p);
+          if (k < D && !xa.is_light) {
+            const Rng rl = make_rng((unsigned long long)i * kJumpStreams + (unsigned long long)k + w.seed);
+            w.rs[s] = rl.state;
+            w.ri[s] = rl.inc;
+            w.view[s] = v;
+            w.pix[s] = -1;
+            w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
+            w.cur[s] = hit4(ha);
+            w.org[s] = make_float4(x.p.x, x.p.y, x.p.z, 0.f);
+            alive = true;
+          }
+          break;
+        }
+        // continue the camera path: cosine sampling about the shading normal
+        const float rx = rng.next_float(), ry = rng.next_float();
+        float ct, st, sphi, cphi;
+        const float3 wo = material_dir(x, mp.N, rx, ry, ct, st, sphi, cphi);
+        const HitRec hn = trace_closest(sc, x.p, wo, kTmin, INFINITY);
+        const Surf nx = make_surf(sc, hn.tri, hn.b1, hn.b2, x.p);
+        if (!nx.valid) break;
+        const float tmp = dot(nx.n, -wo) / nx.sqd;
+        const float G = dot(x.n, wo) * tmp;
+        const float pdf = ct * kInvPi * tmp;
+        T = mul(T, surf_bsdf(sc, x, wo)) * (G / pdf);
+        if (!finite3(T)) break;
+        hp = h;
+        h = hn;
+        x = nx;
+      }
+    }
+    const int kq = warp_append(&w.cnt[0], alive);
+    if (alive) w.q0[kq] = s;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_jump_final(WF w, const DevScene* __restrict__ scenes,
+                                                    const DevView* __restrict__ views, int v, EdgeBuf eb, int n,
+                                                    int k) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  HotAcc hot;
+  hot.lv0 = 0;
+  hot.nlv = 0;
+  hot.emit_hot = false;
+  float3 go = f3(0.f, 0.f, 0.f);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    if (s >= n || !V.dimage) continue;
+    const float4 hk = eb.n[s];
+    if (__float_as_int(hk.w) != 1) continue;
+    const float4 a = eb.a[s], hn = eb.hb[s], hp = eb.La[s];
+    const int pix = __float_as_int(a.w);
+    const int tp = __float_as_int(hp.x);
+    // the vertex before x_k: the camera (k = 1) or the material point of the last hit
+    float3 op = V.pos;
+    if (tp >= 0) op = make_surf(sc, tp, hp.y, hp.z, V.pos).p;
+    const int tk = __float_as_int(hk.x);
+    float3 ok = op;
+    if (tp < 0 && V.ortho) {
+      const Surf x0 = make_surf(sc, tk, hk.y, hk.z, V.pos);
+      ok = ortho_origin_rn(V, x0.p);
+    }
+    const Surf x = make_surf(sc, tk, hk.y, hk.z, ok);
+    const int ta = __float_as_int(hn.x);
+    const Surf xa = make_surf(sc, ta, hn.y, hn.z, x.p);
+    if (!x.valid || !xa.valid) continue;
+    const float3 Li = xa.is_light ? light_emit<true>(sc.lights[xa.light], xa) : xyz(w.L[s]);
+    const float* gp = V.dimage + 3 * (size_t)pix;
+    const float wgt = gp[0] * a.x * Li.x + gp[1] * a.y * Li.y + gp[2] * a.z * Li.z;
+    if (!(wgt != 0.f) || !isfinite(wgt)) continue;
+    // q = m . l, m = V - (N.V) N, l = normalize(x_{k+1} - x_k)
+    const DevObj& ob = sc.objs[x.obj];
+    const MatPt mp = mat_point(ob, x);
+    const bool fixed_v = tp < 0 && V.ortho;  // orthographic primary vertex: V = -look
+    const float3 Vd = fixed_v ? -view_look_dir(V) : x.wi;
+    const float3 u = xa.p - x.p;
+    const float r = norm(u);
+    const float3 l = u / r;
+    const float nv = dot(mp.N, Vd), nl = dot(mp.N, l);
+    const float3 m = Vd - mp.N * nv;
+    const float3 du = (m - l * dot(m, l)) * (wgt / r);
+    MatAdj ma = zero_mat_adj();
+    ma.N = (Vd * nl + l * nv) * (-wgt);
+    if (!fixed_v) ma.V = (l - mp.N * nl) * wgt;
+    if (!finite3(du) || !finite3(ma.N) || !finite3(ma.V)) continue;
+    SurfAdj ax = zero_adj(), aa = zero_adj();
+    aa.p = du;
+    ax.p = -du;
+    const float3 ao = mat_finalize(ob, x, mp, ma, ax);
+    scatter_surf(sc, hot, tk, hk.y, hk.z, x.front, ax);
+    scatter_surf(sc, hot, ta, hn.y, hn.z, xa.front, aa);
+    if (tp >= 0) {
+      SurfAdj ap = zero_adj();
+      ap.p = ao;
+      scatter_surf(sc, hot, tp, hp.y, hp.z, true, ap);
+    } else if (!fixed_v) {
+      go += ao;
+    }
+  }
+  if (V.grad_pos) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      go.x += __shfl_xor_sync(0xffffffffu, go.x, o);
+      go.y += __shfl_xor_sync(0xffffffffu, go.y, o);
+      go.z += __shfl_xor_sync(0xffffffffu, go.z, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (go.x != 0.f || go.y != 0.f || go.z != 0.f)) atomic_add3(V.grad_pos, go);
+  }
+}
+
 // ------------------------------------------------------------------ direct edges
 // path_integrator.cc:274-353 and the boundary_term / hit_triangle adjoint (:11-78).
 // UNB (unbiased estimator, PRE=false): the same samples and edge/light visibility
@@ -2259,6 +2441,25 @@ static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v,
   PSDR_CUDA(cudaGetLastError());
 }
 
+// BSDF-jump samples [begin, begin + n) of view v at depth k (1 <= k <= D): the arc
+// paths run D - k bounces (none at k = D, where only a light seen along the arc counts).
+static void jump_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb, long long begin,
+                       int n, int k, cudaStream_t st) {
+  const int D = w.D;
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (D + 1), st));
+  k_jump_init<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, k, D);
+  PSDR_LAUNCHED(1);
+  if (k < D) {
+    WF wk = w;
+    wk.D = D - k;
+    wk.light_vis = 0;
+    depth_loop(wk, scenes, vd, MODE_FWD, st);
+  }
+  k_jump_final<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, n, k);
+  PSDR_LAUNCHED(1);
+  PSDR_CUDA(cudaGetLastError());
+}
+
 long long border_segments(const DevView& V) {
   return (long long)(V.W + 1) * V.H + (long long)V.W * (V.H + 1);
 }
@@ -2411,6 +2612,13 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       for (long long b0 = 0; b0 < N; b0 += cap)
         border_phase(wi, scenes_dev, vd, v, eb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), S, b0,
                      (int)std::min<long long>(cap, N - b0), N, st);
+    }
+    // BSDF jumps (unbiased estimator, DiffuseBsdfMaterial scenes; on request only)
+    if (unb && (terms & 16) && gi.bsdf && V.dimage) {
+      const long long N = (long long)V.H * V.W * V.spp;
+      for (int k = 1; k <= cfg.max_bounce; ++k)
+        for (long long b0 = 0; b0 < N; b0 += cap)
+          jump_phase(wi, scenes_dev, vd, v, eb, b0, (int)std::min<long long>(cap, N - b0), k, st);
     }
   }
 }
