@@ -10,7 +10,12 @@ The reference publishes no golden vectors and cannot run here, so the fixtures a
                            scene (regression pin of the oracle itself);
   * oracle_ext.npz      -- the same kind of pin for DiffuseBsdfMaterial (roughness and
                            normal maps), an orthographic camera, and EnvLight / SH9Light
-                           (`python tests/golden/make_golden.py ext` writes only this one).
+                           (`python tests/golden/make_golden.py ext` writes only this one);
+  * oracle_grad.npz     -- regression pins of the oracle's gradient terms: directional
+                           derivatives (8 random directions over vertices, texels, light
+                           parameters, emission and camera origin) of every term of both
+                           estimators on the same tiny scenes
+                           (`python tests/golden/make_golden.py grad` writes only this one).
 """
 import json
 import os
@@ -54,6 +59,47 @@ def ext_specs():
     return {"bsdf": bsdf, "ortho": ortho, "env": env, "sh9": sh}
 
 
+GRAD_CFG = dict(spp_interior=4, max_bounce=3, spp_primary_edge=2, spp_secondary_edge=2, spp_pixel_boundary=2,
+                primary_edge_hypercube_resolution=100, secondary_edge_hypercube_resolution=(100, 3, 3))
+
+
+def grad_cases():
+    """(name, scene, estimator mode, terms) of the gradient pins: every term of both
+    estimators on the DiffuseBsdfMaterial scene (the unbiased one's BRDF jumps included),
+    and all unbiased terms together on the other scenes."""
+    out = [(f"bsdf_m{mode}_t{terms}", "bsdf", mode, terms)
+           for mode, terms in ((0, 1), (0, 2), (0, 4), (1, 1), (1, 2), (1, 4), (1, 8), (1, 16))]
+    out += [(f"{key}_m1_t15", key, 1, 15) for key in ("tiny", "ortho", "env", "sh9")]
+    return out
+
+
+def grad_seeds(spec, seed=7):
+    """Random directions over every parameter: vertices (an environment light's box counts
+    8), texture elements in the oracle's order (color, roughness, normal map per mesh,
+    then cube maps and SH coefficients), emission and camera origin."""
+    rng = np.random.default_rng(seed)
+    nvt = sum(m.vertices.shape[0] for m in spec.meshes) + sum(
+        l.vertices.shape[0] if getattr(l, "kind", 0) == 0 else 8 for l in spec.lights)
+    ntex = sum(np.size(a) for m in spec.meshes for a in (m.texture, m.roughness, m.normal) if a is not None)
+    ntex += sum(np.size(l.cube_map) if l.kind == 1 else 27 if l.kind == 2 else 0 for l in spec.lights)
+    return dict(seed_verts=rng.normal(size=(nvt, 3, 8)), seed_tex=rng.normal(size=(ntex, 8)),
+                seed_emit=rng.normal(size=(len(spec.lights), 3, 8)), seed_cam=rng.normal(size=(len(spec.cameras), 3, 8)))
+
+
+def grad_pins():
+    specs = dict(ext_specs(), tiny=tiny_spec())
+    out = {}
+    for name, key, mode, terms in grad_cases():
+        s = specs[key]
+        g = np.random.default_rng(5).normal(size=(s.cameras[0].height, s.cameras[0].width, 3))
+        out[name] = orc.grad_dir(s, [g], which=terms, mode=mode, **grad_seeds(s), **GRAD_CFG)
+    return out
+
+
+def write_grad():
+    np.savez(os.path.join(HERE, "oracle_grad.npz"), **grad_pins())
+
+
 def write_ext():
     imgs = {k: orc.render(s, precision=1, spp_interior=4, max_bounce=3)[0] for k, s in ext_specs().items()}
     np.savez(os.path.join(HERE, "oracle_ext.npz"), **imgs)
@@ -77,6 +123,9 @@ def main():
 if __name__ == "__main__":
     if sys.argv[1:] == ["ext"]:
         write_ext()
+    elif sys.argv[1:] == ["grad"]:
+        write_grad()
     else:
         main()
         write_ext()
+        write_grad()

@@ -48,6 +48,25 @@ def test_oracle_ext_golden():
         np.testing.assert_allclose(img, want[name], rtol=0, atol=1e-12, err_msg=name)
 
 
+def test_oracle_gradient_golden():
+    """Every gradient term of both estimators (the unbiased one's BRDF jumps included) on
+    the tiny scenes, as directional derivatives, against their fixtures
+    (tests/golden/make_golden.py grad). Per-sample contributions are summed in sample
+    order, so the values do not depend on the thread count."""
+    import importlib.util
+    spec_path = os.path.join(GOLDEN, "make_golden.py")
+    mod_spec = importlib.util.spec_from_file_location("make_golden", spec_path)
+    mg = importlib.util.module_from_spec(mod_spec)
+    mod_spec.loader.exec_module(mg)
+    want = np.load(os.path.join(GOLDEN, "oracle_grad.npz"))
+    got = mg.grad_pins()
+    assert sorted(got) == sorted(want.files)
+    for name in want.files:
+        assert np.abs(want[name]).max() > 0, name
+        np.testing.assert_allclose(got[name], want[name], rtol=1e-12, atol=1e-12 * np.abs(want[name]).max(),
+                                   err_msg=name)
+
+
 def _random_rays(spec, n, seed):
     rng = np.random.default_rng(seed)
     o = rng.uniform(-3, 3, size=(n, 3))
