@@ -989,6 +989,20 @@ void orc_sampler_floats(uint64_t i, int n, float* out) {
 }
 void orc_set_threads(int n) { omp_set_num_threads(n); }
 
+// sampler.h:86-117 DiscreteSampler over the weights w[0..n) (float instance): for each of
+// the m uniforms u, the sampled index, the rescaled uniform and the index's pmf.
+int orc_discrete_sample(const double* w, int n, const float* u, int m, int* idx, float* u_out, float* pmf) {
+  Discrete<float> d;
+  d.build(std::vector<double>(w, w + n));
+  for (int i = 0; i < m; ++i) {
+    float s = u[i], p;
+    idx[i] = d.sample_reuse(s, p);
+    u_out[i] = s;
+    pmf[i] = p;
+  }
+  return 0;
+}
+
 // Image render (interior term). precision 0 = float, 1 = double.
 int orc_render(const OrcMesh* m, int nm, const OrcLight* l, int nl, const OrcCamera* cams, int nc,
                const OrcConfig* cfg, int precision, double* images, double* per_sample) {

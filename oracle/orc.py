@@ -61,6 +61,7 @@ def lib():
         _lib.orc_set_threads.argtypes = [C.c_int]
         _lib.orc_pcg32.argtypes = [C.c_uint64, C.c_uint64, C.c_int, P]
         _lib.orc_sampler_floats.argtypes = [C.c_uint64, C.c_int, P]
+        _lib.orc_discrete_sample.argtypes = [P, C.c_int, P, C.c_int, P, P, P]
     return _lib
 
 
@@ -213,6 +214,18 @@ def pcg32(initstate, initseq, n):
     out = np.zeros(n, np.uint32)
     lib().orc_pcg32(initstate, initseq, n, _ptr(out))
     return out
+
+
+def discrete_sample(weights, u):
+    """DiscreteSampler::sample_reuse (float instance) of the uniforms u over the weights:
+    (indices, rescaled uniforms, pmf of each index)."""
+    w = np.ascontiguousarray(weights, np.float64)
+    uu = np.ascontiguousarray(u, np.float32)
+    idx = np.zeros(uu.shape[0], np.int32)
+    uo = np.zeros(uu.shape[0], np.float32)
+    pm = np.zeros(uu.shape[0], np.float32)
+    lib().orc_discrete_sample(_ptr(w), w.shape[0], _ptr(uu), uu.shape[0], _ptr(idx), _ptr(uo), _ptr(pm))
+    return idx, uo, pm
 
 
 def sampler_floats(i, n):
