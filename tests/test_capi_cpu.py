@@ -1,6 +1,7 @@
 """The C-ABI library builds, loads and exports every symbol include/psdr.h declares;
 host-side argument checks and the Python API asserts (no GPU needed)."""
 import ctypes as C
+import json
 import os
 import re
 
@@ -222,3 +223,35 @@ def test_material_and_camera_arguments_are_checked(lib):
     st = lib.psdr_render_fwd(C.c_void_p(1), ws, C.byref(cam), 1, C.byref(cfg), img, None)
     assert st == L.PSDR_ERR_INVALID_ARG and b"view width" in lib.psdr_last_error()
     assert lib.psdr_workspace_destroy(ws) == 0
+
+
+def test_autotune_cache_keys_and_reuse(tmp_path, monkeypatch):
+    """PathIntegrator.autotune(scene, cache=path): a miss tunes (the native call, faked
+    here) and records the result under a key of the GPU and the job's shape; a hit
+    applies the stored sizes without tuning; another shape or GPU misses."""
+    from types import SimpleNamespace as NS
+    integ = dr.PathIntegrator(spp_interior=8, max_bounce=3)
+    calls, applied = [], []
+    monkeypatch.setattr(integ, "_autotune_native",
+                        lambda scene: calls.append(scene) or {"tile_paths": 1 << 19, "leaf_size": 2, "forward_ms": 1.5})
+    monkeypatch.setattr(integ, "_apply_tuning", lambda scene, entry: applied.append(dict(entry)))
+    gpu = {"gpu": "B200", "sms": 148}
+    monkeypatch.setattr(dr.PathIntegrator, "_gpu_id", staticmethod(lambda: dict(gpu)))
+    mesh = NS(f=torch.zeros((20, 3), dtype=torch.int32))
+    light = NS(f=torch.zeros((2, 3), dtype=torch.int32))
+    scene = NS(meshes=[mesh], lights=[light], cameras=[NS(height=64, width=48)])
+    path = str(tmp_path / "tune.json")
+    first = integ.autotune(scene, cache=path)
+    assert len(calls) == 1 and "cached" not in first
+    again = integ.autotune(scene, cache=path)
+    assert len(calls) == 1 and again["cached"] and applied == [first]
+    key = json.loads(next(iter(json.load(open(path)))))
+    assert key == {"gpu": "B200", "sms": 148, "tris": 22, "views": [[64, 48]], "spp": 8, "depth": 3, "nl": 1,
+                   "nb": 1, "estimator": int(integ.cfg.estimator)}
+    scene.cameras[0].width = 49          # another view size misses
+    integ.autotune(scene, cache=path)
+    gpu["sms"] = 132                      # another GPU misses
+    integ.autotune(scene, cache=path)
+    assert len(calls) == 3 and len(json.load(open(path))) == 3
+    integ.autotune(scene)                 # no cache: always tunes
+    assert len(calls) == 4

@@ -9,6 +9,8 @@ calls psdr_render_bwd (the path-replay adjoint).
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 from typing import List, Optional, Union
 
 import torch
@@ -526,16 +528,61 @@ class PathIntegrator:
                                           ptrs, _stream()), "psdr_render_fwd")
         return imgs
 
-    def autotune(self, scene: Scene) -> dict:
+    def autotune(self, scene: Scene, cache: Optional[str] = None) -> dict:
         """Pick the wavefront tile size and the scene's BVH leaf size by timing forward
         renders of the scene's cameras (psdr_autotune); the integrator keeps the tile
-        size, the scene keeps the leaf size. Extension: the reference has no tuner."""
+        size, the scene keeps the leaf size. Extension: the reference has no tuner.
+
+        cache: path of a JSON file of earlier results, keyed by the GPU (name, SM count)
+        and the job's shape (triangles, view sizes, spp, depth, light and BSDF samples,
+        estimator). A hit applies the stored sizes without timing (and returns them with
+        "cached": True); a miss tunes and adds its result to the file."""
+        key = self._tune_key(scene) if cache else None
+        if key is not None and os.path.exists(cache):
+            with open(cache) as f:
+                entry = json.load(f).get(key)
+            if entry is not None:
+                self._apply_tuning(scene, entry)
+                return dict(entry, cached=True)
+        entry = self._autotune_native(scene)
+        if key is not None:
+            table = {}
+            if os.path.exists(cache):
+                with open(cache) as f:
+                    table = json.load(f)
+            table[key] = entry
+            tmp = cache + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(table, f, indent=1, sort_keys=True)
+            os.replace(tmp, cache)
+        return entry
+
+    def _autotune_native(self, scene: Scene) -> dict:
         leaf = C.c_int32()
         ms = C.c_float()
         cams = scene._camera_descs()
         L.check(self._lib.psdr_autotune(scene.handle, self._workspace(), cams, len(cams), C.byref(self.cfg),
                                         C.byref(leaf), C.byref(ms), _stream()), "psdr_autotune")
         return {"tile_paths": int(self.cfg.tile_paths), "leaf_size": int(leaf.value), "forward_ms": float(ms.value)}
+
+    def _apply_tuning(self, scene: Scene, entry: dict) -> None:
+        self.cfg.tile_paths = int(entry["tile_paths"])
+        L.check(self._lib.psdr_scene_set_leaf_size(scene.handle, int(entry["leaf_size"]), _stream()),
+                "psdr_scene_set_leaf_size")
+
+    @staticmethod
+    def _gpu_id() -> dict:
+        p = torch.cuda.get_device_properties(torch.cuda.current_device())
+        return {"gpu": p.name, "sms": int(p.multi_processor_count)}
+
+    def _tune_key(self, scene: Scene) -> str:
+        c = self.cfg
+        tris = sum(int(m.f.shape[0]) for m in scene.meshes) + sum(
+            int(lt.f.shape[0]) for lt in scene.lights if getattr(lt, "f", None) is not None)
+        shape = dict(self._gpu_id(), tris=tris, views=[[int(v.height), int(v.width)] for v in scene.cameras],
+                     spp=int(c.spp_interior), depth=int(c.max_bounce), nl=int(c.mis_light_samples),
+                     nb=int(c.mis_bsdf_samples), estimator=int(c.estimator))
+        return json.dumps(shape, sort_keys=True)
 
     def render_samples(self, scene: Scene, camera_index: int = 0) -> Tensor:
         """Per-sample interior radiance (H*W*spp, 3) of one camera (the values the film averages)."""
