@@ -165,34 +165,45 @@ def smooth_weights(torch, dev):
                         for c in range(3)], -1).float().contiguous()
 
 
-def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=4096):
+def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=4096, replicas=4):
     """Translation gradient of Phi = sum(w * image) for a smooth weight image w, from the
     estimator at the benchmark's sample counts, against central differences of Phi from
-    fd_spp-spp renders (same sample streams at +-h). The benchmark's own L2 loss is not
-    used here: its image gradient is dominated by texel-scale residuals, which makes its
-    finite differences ill-conditioned (they move by tens of percent with h and spp)."""
+    fd_spp-spp renders (same sample streams at +-h). Both sides are averaged over
+    `replicas` independent sample streams (seeds 1..replicas), whose spread gives the
+    standard error of each mean. The benchmark's own L2 loss is not used here: its image
+    gradient is dominated by texel-scale residuals, which makes its finite differences
+    ill-conditioned (they move by tens of percent with h and spp)."""
     from torch_psdr_b200 import _lib as L
     w = smooth_weights(torch, dev)
-    t = torch.zeros(3, device=dev, requires_grad=True)
-    img = integ.renderD(build_scene(base + t, tex))[0]
-    img.backward(w)
-    ad = t.grad.double().cpu().numpy()
-    fd_integ = dr.PathIntegrator(**dict(CFG, spp_interior=fd_spp))
     wd = w.double()
-    fd = []
-    with torch.no_grad():
-        for k in range(3):
-            e = torch.zeros(3, device=dev)
-            e[k] = h
-            lp = float((fd_integ.renderC(build_scene(base + e, tex))[0].double() * wd).sum())
-            lm = float((fd_integ.renderC(build_scene(base - e, tex))[0].double() * wd).sum())
-            fd.append((lp - lm) / (2 * h))
-    fd = np.array(fd)
+    kw = {k: getattr(integ.cfg, k) for k in ("spp_interior", "spp_primary_edge", "spp_secondary_edge",
+                                              "spp_pixel_boundary", "max_bounce")}
+    est = "unbiased" if integ.cfg.estimator == L.EST_UNBIASED else "reference"
+    ads, fds = [], []
+    for r in range(1, replicas + 1):
+        ad_integ = dr.PathIntegrator(estimator=est, seed=r, **kw)
+        t = torch.zeros(3, device=dev, requires_grad=True)
+        ad_integ.renderD(build_scene(base + t, tex))[0].backward(w)
+        ads.append(t.grad.double().cpu().numpy())
+        fd_integ = dr.PathIntegrator(**dict(CFG, spp_interior=fd_spp, seed=r))
+        fd = []
+        with torch.no_grad():
+            for k in range(3):
+                e = torch.zeros(3, device=dev)
+                e[k] = h
+                lp = float((fd_integ.renderC(build_scene(base + e, tex))[0].double() * wd).sum())
+                lm = float((fd_integ.renderC(build_scene(base - e, tex))[0].double() * wd).sum())
+                fd.append((lp - lm) / (2 * h))
+        fds.append(np.array(fd))
+    ads, fds = np.array(ads), np.array(fds)
+    ad, fd = ads.mean(0), fds.mean(0)
+    se = lambda a: a.std(0, ddof=1) / np.sqrt(len(a)) if len(a) > 1 else np.zeros(3)
     return {"rel_l2_vs_fd": float(np.linalg.norm(ad - fd) / np.linalg.norm(fd)), "ad": ad.tolist(), "fd": fd.tolist(),
+            "ad_stderr": se(ads).tolist(), "fd_stderr": se(fds).tolist(),
+            "rel_l2_fd_stderr": float(np.linalg.norm(se(fds)) / np.linalg.norm(fd)),
             "functional": "sum(w * image), w = sin(2.6 pi x/W + c) cos(1.4 pi y/H) + 0.3 per channel c",
-            "parameter": "translation of the icosphere",
-            "estimator": "unbiased" if integ.cfg.estimator == L.EST_UNBIASED else "reference",
-            "fd_step": h, "fd_spp": fd_spp}
+            "parameter": "translation of the icosphere", "estimator": est,
+            "fd_step": h, "fd_spp": fd_spp, "replicas": replicas, "seeds": list(range(1, replicas + 1))}
 
 
 # ---------------------------------------------------------------- replicas
@@ -397,7 +408,10 @@ def run_b200(args):
             "gpu_launches": launches, "clocks": clk,
             "rays_per_s": rays / (total_ms / 1e3)}
     if rank == 0 and world == 1 and not args.no_grad_check:
-        line["grad_check"] = grad_check(torch, dr, integ, build_scene, base, tex, dev)
+        try:
+            line["grad_check"] = grad_check(torch, dr, integ, build_scene, base, tex, dev)
+        except Exception as exc:  # the measured line is printed either way
+            line["grad_check"] = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_rate(spec, seconds_budget=20.0)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
