@@ -166,6 +166,12 @@ PSDR_API int32_t psdr_abi_version(void);
  * flattens the meshes, builds the edge list and the sampling CDFs and an LBVH,
  * all on `stream`. Texture data pointers are borrowed and must outlive the scene. */
 PSDR_API psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_scene** out);
+/* Checks the index buffers of a scene description before psdr_scene_create (extension;
+ * the reference does not check them): every face index must lie in [0, num_vertices) of
+ * its mesh or area light, every uv index in [0, num_uvs). One device reduction per
+ * buffer on `stream` and one host read; PSDR_ERR_INVALID_ARG names the first buffer out
+ * of range. psdr_scene_create itself trusts the indices. */
+PSDR_API psdr_status psdr_scene_validate(const psdr_scene_desc* desc, void* stream);
 PSDR_API psdr_status psdr_scene_destroy(psdr_scene* scene);
 /* Rebuild the acceleration structure, triangle attributes and edges after the
  * vertex buffers changed in place (same topology). */

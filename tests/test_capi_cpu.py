@@ -255,3 +255,24 @@ def test_autotune_cache_keys_and_reuse(tmp_path, monkeypatch):
     assert len(calls) == 3 and len(json.load(open(path))) == 3
     integ.autotune(scene)                 # no cache: always tunes
     assert len(calls) == 4
+
+
+def test_scene_validate_argument_checks(lib):
+    """psdr_scene_validate (the opt-in index-range check before psdr_scene_create): its
+    host-side argument checks, which return before any device work."""
+    assert lib.psdr_scene_validate(None, None) == L.PSDR_ERR_INVALID_ARG
+    assert b"null" in lib.psdr_last_error()
+    desc = L.SceneDesc(None, 1, None, 0)
+    assert lib.psdr_scene_validate(C.byref(desc), None) == L.PSDR_ERR_INVALID_ARG
+    assert b"null mesh array" in lib.psdr_last_error()
+    m = L.MeshDesc()
+    m.num_vertices, m.num_faces = 3, -1
+    meshes = (L.MeshDesc * 1)(m)
+    desc = L.SceneDesc(meshes, 1, None, 0)
+    assert lib.psdr_scene_validate(C.byref(desc), None) == L.PSDR_ERR_INVALID_ARG
+    assert b"negative counts" in lib.psdr_last_error()
+    meshes[0].num_faces = 1  # faces null
+    assert lib.psdr_scene_validate(C.byref(desc), None) == L.PSDR_ERR_INVALID_ARG
+    assert b"null face buffer" in lib.psdr_last_error()
+    empty = L.SceneDesc(None, 0, None, 0)
+    assert lib.psdr_scene_validate(C.byref(empty), None) == L.PSDR_OK  # nothing to check

@@ -78,6 +78,7 @@ SIGNATURES = {
     "psdr_version": ([], C.c_char_p),
     "psdr_abi_version": ([], C.c_int32),
     "psdr_scene_create": ([C.POINTER(SceneDesc), P, C.POINTER(P)], C.c_int),
+    "psdr_scene_validate": ([C.POINTER(SceneDesc), P], C.c_int),
     "psdr_scene_destroy": ([P], C.c_int),
     "psdr_scene_update": ([P, P], C.c_int),
     "psdr_scene_refit": ([P, P], C.c_int),

@@ -1,5 +1,6 @@
 // capi.cu -- the extern "C" entry points declared in include/psdr.h.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -117,6 +118,26 @@ long long light_param_count(const psdr_scene* s, int l) {
   return L.kind == PSDR_LIGHT_SH9 ? 27 : 0;
 }
 
+
+// Min and max of n indices into out[0] / out[1] (initialised to INT_MAX / INT_MIN):
+// grid-stride loads, warp reduction, one atomic pair per warp.
+__global__ void k_index_range(const int* __restrict__ idx, long long n, int* __restrict__ out) {
+  int lo = INT_MAX, hi = INT_MIN;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int v = __ldg(idx + i);
+    lo = min(lo, v);
+    hi = max(hi, v);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(out, lo);
+    atomicMax(out + 1, hi);
+  }
+}
 
 }  // namespace psdr
 
@@ -326,6 +347,56 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
     throw;
   }
   *out = s;
+  API_END
+}
+
+psdr_status psdr_scene_validate(const psdr_scene_desc* desc, void* stream) {
+  API_BEGIN
+  PSDR_CHECK(desc != nullptr, "null argument");
+  PSDR_CHECK(desc->num_meshes >= 0 && desc->num_lights >= 0, "negative counts");
+  PSDR_CHECK(desc->num_meshes == 0 || desc->meshes != nullptr, "null mesh array");
+  PSDR_CHECK(desc->num_lights == 0 || desc->lights != nullptr, "null light array");
+  // (index buffer, entries, bound, what) of every mesh's faces and uv indices and every
+  // area light's faces; environment lights have no caller index buffers
+  struct Job { const int* p; long long n; int bound; std::string what; };
+  std::vector<Job> jobs;
+  for (int i = 0; i < desc->num_meshes; ++i) {
+    const psdr_mesh_desc& m = desc->meshes[i];
+    PSDR_CHECK(m.num_faces >= 0 && m.num_vertices >= 0 && m.num_uvs >= 0, "negative counts");
+    PSDR_CHECK(m.num_faces == 0 || m.faces != nullptr, "null face buffer");
+    jobs.push_back({m.faces, 3LL * m.num_faces, m.num_vertices, "mesh " + std::to_string(i) + " face"});
+    if (m.uvs != nullptr && m.uv_indices != nullptr)
+      jobs.push_back({m.uv_indices, 3LL * m.num_faces, m.num_uvs, "mesh " + std::to_string(i) + " uv"});
+  }
+  for (int l = 0; l < desc->num_lights; ++l) {
+    const psdr_area_light_desc& L = desc->lights[l];
+    if (L.type != PSDR_LIGHT_AREA) continue;
+    PSDR_CHECK(L.num_faces >= 0 && L.num_vertices >= 0, "negative counts");
+    PSDR_CHECK(L.num_faces == 0 || L.faces != nullptr, "null face buffer");
+    jobs.push_back({L.faces, 3LL * L.num_faces, L.num_vertices, "light " + std::to_string(l) + " face"});
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int k = (int)jobs.size();
+  if (k == 0) return PSDR_OK;
+  DBuf range;
+  range.alloc(sizeof(int) * 2 * k, st);
+  std::vector<int> h(2 * k);
+  for (int j = 0; j < k; ++j) { h[2 * j] = INT_MAX; h[2 * j + 1] = INT_MIN; }
+  PSDR_CUDA(cudaMemcpyAsync(range.p, h.data(), sizeof(int) * 2 * k, cudaMemcpyHostToDevice, st));
+  for (int j = 0; j < k; ++j) {
+    if (jobs[j].n == 0) continue;
+    const int blocks = (int)std::min<long long>((jobs[j].n + 255) / 256, 148LL * 8);
+    k_index_range<<<blocks, 256, 0, st>>>(jobs[j].p, jobs[j].n, range.as<int>() + 2 * j);
+  }
+  PSDR_CUDA(cudaGetLastError());
+  PSDR_CUDA(cudaMemcpyAsync(h.data(), range.p, sizeof(int) * 2 * k, cudaMemcpyDeviceToHost, st));
+  PSDR_CUDA(cudaStreamSynchronize(st));
+  for (int j = 0; j < k; ++j) {
+    if (jobs[j].n == 0) continue;
+    PSDR_CHECK(h[2 * j] >= 0 && h[2 * j + 1] < jobs[j].bound,
+               jobs[j].what + " indices must lie in [0, " + std::to_string(jobs[j].bound) + "): found [" +
+                   std::to_string(h[2 * j]) + ", " + std::to_string(h[2 * j + 1]) + "]");
+  }
   API_END
 }
 
