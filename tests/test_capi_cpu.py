@@ -276,3 +276,18 @@ def test_scene_validate_argument_checks(lib):
     assert b"null face buffer" in lib.psdr_last_error()
     empty = L.SceneDesc(None, 0, None, 0)
     assert lib.psdr_scene_validate(C.byref(empty), None) == L.PSDR_OK  # nothing to check
+
+
+def test_header_is_strict_c99_and_cxx17(tmp_path):
+    """include/psdr.h compiles warning-free as ISO C99 and as C++17 (the bindings a C,
+    C++ or FFI host writes against it)."""
+    import shutil
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "hdr.c"
+    src.write_text('#include "psdr.h"\nint main(void) { return (int)sizeof(psdr_config) == 0; }\n')
+    for cc, flags in (("gcc", ["-std=c99"]), ("g++", ["-std=c++17", "-x", "c++"])):
+        if shutil.which(cc) is None:
+            pytest.skip(f"{cc} not available")
+        subprocess.run([cc, *flags, "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(root, "include"),
+                        str(src), "-o", str(tmp_path / f"hdr_{cc}")], check=True)
