@@ -143,6 +143,16 @@ typedef struct {
  * and normal textures; ignored for other meshes), may be NULL.
  * light_params: one per light: an ENV light's cube-map gradient (its texture's shape),
  * an SH9 light's (9,3) coefficient gradient; ignored for AREA lights; may be NULL.
+ * camera_lens (ABI 5): one (10,) buffer per camera, may be NULL: the derivative with
+ * respect to the camera parameters as they enter its basis and projection -- look_from
+ * through the view direction [0..2], look_at [3..5], up [6..8], fov [9] (camera.h:7-64,
+ * 111-124, 235-258; torch_psdr.py:145-152 makes all four differentiable). camera_origin
+ * is the derivative with the basis held fixed, so d/dlook_from = camera_origin +
+ * camera_lens[0..2]. UNBIASED estimator: the image derivative (the camera basis and fov
+ * move the image content over the pixel grid). REFERENCE estimator: zeros, as the
+ * reference's tape has no path from these inputs to the image (the camera ray's direction
+ * is not used after the hit, scene.cc:130-137). Perspective cameras only
+ * (PSDR_ERR_UNSUPPORTED for an orthographic camera).
  * With accumulate = 0 the outputs are overwritten, otherwise added to. */
 typedef struct {
   float** vertices;
@@ -153,6 +163,7 @@ typedef struct {
   float** roughness;
   float** normal;
   float** light_params;
+  float** camera_lens;
 } psdr_grad_targets;
 
 /* ---------------------------------------------------------------- general */
@@ -200,6 +211,14 @@ PSDR_API psdr_status psdr_scene_edges(psdr_scene* scene, int32_t* v01, float* ge
 PSDR_API psdr_status psdr_intersect(psdr_scene* scene, const float* rays, int64_t n, int32_t* tri, float* bary,
                            float* t, int32_t brute_force, void* stream);
 
+/* Synchronous host query (extension, no device work): the raster-to-direction map of a
+ * perspective camera that the camera_lens gradient differentiates, M (3x3 row-major,
+ * raster coordinates taken from the image centre: the world direction seen at raster
+ * point u is proportional to M [u_x - W/2, u_y - H/2, 1]), and P_j = M^-1 dM/dtheta_j for
+ * the ten parameters theta = (look_from, look_at, up, fov) (10 x 9 doubles), built as
+ * camera.h:7-64 builds the camera basis. Either output may be NULL. */
+PSDR_API psdr_status psdr_camera_lens_jacobian(const psdr_camera_desc* cam, double* m9, double* p90);
+
 /* ---------------------------------------------------------------- rendering
  * psdr_render_fwd replaces PathIntegrator::renderC / the forward of renderD
  * (path_integrator.cc:381-414; torch_psdr.py:538-556). images[c] is a device
@@ -211,16 +230,18 @@ PSDR_API psdr_status psdr_render_fwd(psdr_scene* scene, psdr_workspace* ws, cons
 /* Allocation-free variant of psdr_render_fwd for one camera; no counterpart in the
  * reference. For callers that cannot allocate device memory at render time (a host
  * that gives the library a fixed budget up front, a loop that cannot afford
- * cudaMalloc's implicit device synchronisation, code that must not add allocation
- * nodes to a stream being recorded). The wavefront tiles use one file-scope 32 MiB
- * __device__ array per GPU, held until the process exits; tiles shrink to fit it, so
- * any image size works, but spp_interior must not exceed the tile (about 100k paths
- * with one light and one BSDF sample; larger values return PSDR_ERR_INVALID_ARG).
- * It takes perspective cameras (others return PSDR_ERR_INVALID_ARG). The first call on a device resolves the array's address (cudaGetSymbolAddress), so
- * make that first call before any stream capture. All calls share the array and it
- * keeps the last call's contents: calls that overlap on the GPU (other streams,
- * other threads) race and must be serialised by the caller. The scene is an input
- * created earlier by psdr_scene_create; image is the (H,W,3) output. */
+ * cudaMalloc's implicit device synchronisation). The wavefront tiles use one
+ * file-scope 32 MiB __device__ array per GPU, held until the process exits; tiles
+ * shrink to fit it, so any image size works, but spp_interior must not exceed the
+ * tile (about 100k paths with one light and one BSDF sample; larger values return
+ * PSDR_ERR_INVALID_ARG). It takes perspective cameras (others return
+ * PSDR_ERR_INVALID_ARG), and the device current at the call must be the one the scene
+ * was created on (else PSDR_ERR_INVALID_ARG). The first call on a device resolves the
+ * array's address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture. All calls share the array and it keeps the last call's contents: calls
+ * that overlap on the GPU (other streams, other threads) race and must be serialised
+ * by the caller. The scene is an input created earlier by psdr_scene_create; image is
+ * the (H,W,3) output. */
 PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const psdr_camera_desc* cam, const psdr_config* cfg,
                                              float* image, void* stream);
 /* Per-sample interior radiance of one camera ((H*W*spp, 3) device buffer), the

@@ -12,7 +12,12 @@ def to_torch_scene(spec, requires_grad=(), device="cuda"):
     """Build a dr.Scene from a synth.SceneSpec. requires_grad: subset of
     {"verts", "tex", "rough", "normal", "light_verts", "emit", "env", "cam"}; returns
     (scene, dict of tensors). Meshes with a roughness get a DiffuseBsdfMaterial; lights of
-    kind 1 / 2 become EnvLight / SH9Light (their parameters under "env{j}")."""
+    kind 1 / 2 become EnvLight / SH9Light (their parameters under "env{j}").
+
+    "cam" makes T["cam{k}"] a translation of camera k: a perspective camera's look_at is
+    look_from plus a constant, so the gradient of T["cam{k}"] is the derivative with the
+    camera's basis held fixed (the oracle's camera derivative). An orthographic camera's
+    look_at stays constant (its look_from gradient is already the translation)."""
     T = {}
     meshes = []
     for i, m in enumerate(spec.meshes):
@@ -60,9 +65,12 @@ def to_torch_scene(spec, requires_grad=(), device="cuda"):
     for k, c in enumerate(spec.cameras):
         lf = torch.tensor(c.look_from, dtype=torch.float32, device=device, requires_grad="cam" in requires_grad)
         T[f"cam{k}"] = lf
-        cls = dr.OrthographicCamera if getattr(c, "kind", 0) == 1 else dr.PerspectiveCamera
-        cams.append(cls(lf, torch.tensor(c.look_at, dtype=torch.float32, device=device),
-                        torch.tensor(c.up, dtype=torch.float32, device=device),
+        ortho = getattr(c, "kind", 0) == 1
+        cls = dr.OrthographicCamera if ortho else dr.PerspectiveCamera
+        at = torch.tensor(c.look_at, dtype=torch.float32, device=device)
+        if "cam" in requires_grad and not ortho:
+            at = lf + (at - lf.detach())
+        cams.append(cls(lf, at, torch.tensor(c.up, dtype=torch.float32, device=device),
                         torch.tensor([c.vfov], dtype=torch.float32, device=device), c.height, c.width))
     return dr.Scene(cams, meshes, lights), T
 

@@ -5,6 +5,7 @@ import json
 import os
 import re
 
+import numpy as np
 import pytest
 import torch
 
@@ -36,7 +37,7 @@ def test_header_symbols_exported(lib):
 
 def test_version_and_errors(lib):
     assert b"sm_100a" in lib.psdr_version()
-    assert lib.psdr_abi_version() == 4
+    assert lib.psdr_abi_version() == 5
     out = C.c_void_p()
     st = lib.psdr_scene_create(None, None, C.byref(out))
     assert st == L.PSDR_ERR_INVALID_ARG
@@ -291,3 +292,44 @@ def test_header_is_strict_c99_and_cxx17(tmp_path):
             pytest.skip(f"{cc} not available")
         subprocess.run([cc, *flags, "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(root, "include"),
                         str(src), "-o", str(tmp_path / f"hdr_{cc}")], check=True)
+
+
+def _lens_map(p):
+    """The raster-to-direction map of a perspective camera from (look_from, look_at, up,
+    fov) = p[0:3], p[3:6], p[6:9], p[9], restated from camera.h:7-64 (numpy, float64):
+    M = C diag(2 tan(fov/2) / W, -2 tan(fov/2) / H, -1), C = (right, up', dir)."""
+    W, H = 40.0, 30.0
+    frm, at, up, fov = p[0:3], p[3:6], p[6:9], p[9]
+    d = (frm - at) / np.linalg.norm(frm - at)
+    r = np.cross(up / np.linalg.norm(up), d)
+    u2 = np.cross(d, r)
+    t = np.tan(fov / 2)
+    return np.stack([r * 2 * t / W, u2 * -2 * t / H, -d], axis=1)
+
+
+def test_camera_lens_jacobian_matches_finite_differences():
+    """psdr_camera_lens_jacobian (host code behind the camera_lens gradient): M equals the
+    restated map and P_j = M^-1 dM/dtheta_j equals central differences of it."""
+    lib = L.load()
+    p = np.array([0.3, 0.5, 4.0, 0.1, -0.2, 0.05, 0.1, 1.0, 0.2, 0.8])
+    d = L.CameraDesc()
+    d.type = L.CAM_PERSPECTIVE
+    d.look_from = (C.c_float * 3)(*p[0:3])
+    d.look_at = (C.c_float * 3)(*p[3:6])
+    d.up = (C.c_float * 3)(*p[6:9])
+    d.fov = float(p[9])
+    d.height, d.width = 30, 40
+    pf = np.array(list(d.look_from) + list(d.look_at) + list(d.up) + [d.fov], np.float64)  # the float inputs
+    m = (C.c_double * 9)()
+    P = (C.c_double * 90)()
+    assert lib.psdr_camera_lens_jacobian(C.byref(d), m, P) == L.PSDR_OK
+    M = _lens_map(pf)
+    np.testing.assert_allclose(np.array(m).reshape(3, 3), M, rtol=1e-12, atol=1e-14)
+    Minv = np.linalg.inv(M)
+    for j in range(10):
+        e = np.zeros(10)
+        e[j] = 1e-6
+        dM = (_lens_map(pf + e) - _lens_map(pf - e)) / 2e-6
+        np.testing.assert_allclose(np.array(P[9 * j:9 * j + 9]).reshape(3, 3), Minv @ dM, rtol=1e-6, atol=1e-8)
+    d.type = L.CAM_ORTHOGRAPHIC
+    assert lib.psdr_camera_lens_jacobian(C.byref(d), m, P) == L.PSDR_ERR_INVALID_ARG

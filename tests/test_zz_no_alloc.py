@@ -1,12 +1,13 @@
 """The allocation-free forward entry point (psdr_render_fwd_noalloc).
 
 Some callers cannot allocate device memory when they render: a host that hands the
-library a fixed memory budget up front, a loop that cannot pay for cudaMalloc's
-implicit device synchronisation, or code that must not add allocation nodes to a
-stream being recorded. For them the library renders one camera out of a fixed
-32 MiB scratch array compiled into the library. These tests call that entry point
-through the C ABI twice in a row and compare each image with the regular
-psdr_render_fwd output. This file is collected last on purpose.
+library a fixed memory budget up front, or a loop that cannot pay for cudaMalloc's
+implicit device synchronisation. For them the library renders one camera out of a
+fixed 32 MiB scratch array compiled into the library. These tests call that entry
+point through the C ABI twice in a row, compare each image with the regular
+psdr_render_fwd output, and check that the second call changes neither torch's
+allocator counters nor the device's free memory. This file is collected last on
+purpose.
 """
 import ctypes as C
 
@@ -34,12 +35,24 @@ def test_noalloc_matches_render_fwd_twice(cuda, h, w, spp, nl, nb):
     ref = integ.renderC(scene)[0]
     lib = L.load()
     cams = scene._camera_descs()
-    for _ in range(2):
-        out = torch.full_like(ref, float("nan"))
+    outs = [torch.full_like(ref, float("nan")) for _ in range(2)]
+    torch.cuda.synchronize()
+    for k, out in enumerate(outs):
+        if k == 1:  # the first call resolved the scratch address; the second must allocate nothing
+            stats0 = _alloc_counters()
+            free0 = torch.cuda.mem_get_info()[0]
         L.check(lib.psdr_render_fwd_noalloc(scene.handle, C.byref(cams[0]), C.byref(integ.cfg), out.data_ptr(),
                                             _stream()), "psdr_render_fwd_noalloc")
         torch.cuda.synchronize()
+        if k == 1:
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert _alloc_counters() == stats0
         np.testing.assert_allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=1e-6, atol=1e-7)
+
+
+def _alloc_counters():
+    s = torch.cuda.memory_stats()
+    return {k: s.get(k) for k in ("allocation.all.allocated", "segment.all.allocated", "reserved_bytes.all.current")}
 
 
 def test_noalloc_rejects_oversized_tiles(cuda):

@@ -68,7 +68,8 @@ class GradTargets(C.Structure):
     _fields_ = [("vertices", C.POINTER(C.c_void_p)), ("textures", C.POINTER(C.c_void_p)),
                 ("emit", C.POINTER(C.c_void_p)), ("camera_origin", C.POINTER(C.c_void_p)),
                 ("accumulate", C.c_int32), ("roughness", C.POINTER(C.c_void_p)),
-                ("normal", C.POINTER(C.c_void_p)), ("light_params", C.POINTER(C.c_void_p))]
+                ("normal", C.POINTER(C.c_void_p)), ("light_params", C.POINTER(C.c_void_p)),
+                ("camera_lens", C.POINTER(C.c_void_p))]
 
 
 # Every symbol include/psdr.h declares, with its ctypes signature.
@@ -86,6 +87,7 @@ SIGNATURES = {
     "psdr_scene_info": ([P, C.POINTER(C.c_int64)], C.c_int),
     "psdr_scene_edges": ([P, P, P, C.c_int64, C.POINTER(C.c_int64), P], C.c_int),
     "psdr_intersect": ([P, P, C.c_int64, P, P, P, C.c_int32, P], C.c_int),
+    "psdr_camera_lens_jacobian": ([P, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "psdr_workspace_create": ([C.POINTER(P)], C.c_int),
     "psdr_workspace_destroy": ([P], C.c_int),
     "psdr_render_fwd": ([P, P, C.POINTER(CameraDesc), C.c_int32, C.POINTER(Config), C.POINTER(P), P], C.c_int),

@@ -450,6 +450,38 @@ def _ptrs(bufs):
     return (P * max(1, len(bufs)))(*[None if t is None else t.data_ptr() for t in bufs])
 
 
+def _wants(t) -> bool:
+    return isinstance(t, Tensor) and t.requires_grad
+
+
+def _lens_buf(cam, unbiased: bool):
+    """(10,) camera-lens gradient buffer (look_from through the basis, look_at, up, fov), or
+    None when no camera parameter that enters the basis or the projection requires grad.
+    With the unbiased estimator look_from needs it too: moving look_from with look_at fixed
+    turns the camera. Orthographic cameras have no lens gradient: their look_at, up and
+    view_width gradients are refused rather than returned as zeros."""
+    lens_params = (cam.look_at, cam.up, cam.vfov)
+    if isinstance(cam, OrthographicCamera):
+        if any(_wants(t) for t in lens_params):
+            raise NotImplementedError("gradients of an OrthographicCamera's look_at, up and view_width are not "
+                                      "implemented; only look_from (with the camera's basis held fixed)")
+        return None
+    if any(_wants(t) for t in lens_params) or (unbiased and _wants(cam.look_from)):
+        return torch.zeros(10, dtype=torch.float32, device="cuda")
+    return None
+
+
+def _add_camera_grads(add, cam, origin_g, lens_g):
+    """Map a camera's origin gradient (basis fixed) and its lens gradient onto its tensors."""
+    if lens_g is None:
+        add(cam.look_from, origin_g)
+        return
+    add(cam.look_from, origin_g + lens_g[0:3])
+    add(cam.look_at, lens_g[3:6])
+    add(cam.up, lens_g[6:9])
+    add(cam.vfov, lens_g[9:10])
+
+
 class PathIntegrator:
     def __init__(self, enable_light_visable: bool = False, n_pass: int = 1, spp_interior: int = 1,
                  max_bounce: int = 3, mis_light_samples: int = 1, mis_bsdf_samples: int = 1,
@@ -611,12 +643,14 @@ class PathIntegrator:
         emit_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.lights]
         light_g = [_grad_buf(lt.params, lt.params_data) if _is_env(lt) else None for lt in scene.lights]
         cam_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in scene.cameras]
+        unb = self.cfg.estimator == L.EST_UNBIASED
+        lens_g = [_lens_buf(c, unb) for c in scene.cameras]
         P = C.c_void_p
         vp = (P * (nm + nl))(*[None if t is None else t.data_ptr() for t in vert_g])
         tp = (P * max(1, nm))(*[None if t is None else t.data_ptr() for t in tex_g])
         ep = (P * max(1, nl))(*[t.data_ptr() for t in emit_g])
         cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
-        tg = L.GradTargets(vp, tp, ep, cp, 0, _ptrs(rough_g), _ptrs(nrm_g), _ptrs(light_g))
+        tg = L.GradTargets(vp, tp, ep, cp, 0, _ptrs(rough_g), _ptrs(nrm_g), _ptrs(light_g), _ptrs(lens_g))
         dp = (P * len(dimgs))(*[d.data_ptr() for d in dimgs])
         cams = scene._camera_descs()
         L.check(self._lib.psdr_render_bwd(scene.handle, self._workspace(), cams, len(dimgs), C.byref(self.cfg), dp,
@@ -644,9 +678,7 @@ class PathIntegrator:
             if light_g[j] is not None:
                 add(lt.params, light_g[j])
         for k, c in enumerate(scene.cameras):
-            add(c.look_from, cam_g[k])
-            for t in (c.look_at, c.up, c.vfov):
-                add(t, torch.zeros_like(t, dtype=torch.float32))
+            _add_camera_grads(add, c, cam_g[k], lens_g[k])
         return [acc.get(id(t), torch.zeros_like(t)) for t in torch_vars]
 
     def renderC(self, scene: Scene) -> List[Tensor]:
@@ -660,6 +692,8 @@ class PathIntegrator:
         torch_vars = scene.get_variables()
         if not torch_vars:
             return self._render(scene)
+        for c in scene.cameras:  # refuse unsupported camera gradients before rendering
+            _lens_buf(c, self.cfg.estimator == L.EST_UNBIASED)
         imgs = _RenderD.apply(self, scene, *torch_vars)
         return list(imgs)
 
@@ -698,6 +732,9 @@ class BatchRender:
         cam_g = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in cams]
         cp = (P * len(cam_g))(*[t.data_ptr() for t in cam_g])
         self.cam_grads = cam_g
+        unb = integrator.cfg.estimator == L.EST_UNBIASED
+        self.lens_grads = [_lens_buf(c, unb) for c in cams] if differentiable else [None] * len(cams)
+        lp_cam = _ptrs(self.lens_grads)
         for sc in self.scenes:
             vg = [_grad_buf(m.vertices, m.v) for m in sc.meshes] + [_grad_buf(lt.vertices, lt.v)
                                                                     for lt in sc.lights]
@@ -709,8 +746,8 @@ class BatchRender:
             self.grads.append((vg, tg, eg, rg, ng, lg))
             vp, tp, ep, rp, npp, lp = _ptrs(vg), _ptrs(tg), _ptrs(eg), _ptrs(rg), _ptrs(ng), _ptrs(lg)
             self._keep += [vp, tp, ep, rp, npp, lp]
-            targets.append(L.GradTargets(vp, tp, ep, cp, 0, rp, npp, lp))
-        self._keep.append(cp)
+            targets.append(L.GradTargets(vp, tp, ep, cp, 0, rp, npp, lp, lp_cam))
+        self._keep += [cp, lp_cam]
         tgt = (L.GradTargets * len(targets))(*targets)
         sh = (P * len(self.scenes))(*[s.handle for s in self.scenes])
         cd = (L.CameraDesc * len(cams))(*[c._desc() for c in cams])
@@ -778,9 +815,7 @@ class BatchRender:
                 if lg[j] is not None:
                     add(lt.params, lg[j])
             for c in sc.cameras:
-                add(c.look_from, self.cam_grads[k])
-                for t in (c.look_at, c.up, c.vfov):
-                    add(t, torch.zeros_like(t, dtype=torch.float32))
+                _add_camera_grads(add, c, self.cam_grads[k], self.lens_grads[k])
                 k += 1
         return [acc.get(id(t), torch.zeros_like(t)) for t in torch_vars]
 

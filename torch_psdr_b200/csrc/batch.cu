@@ -19,13 +19,15 @@ struct psdr_batch {
   psdr_workspace ws;
   psdr::DBuf scenes_dev;  // DevScene array, one entry per scene
   psdr::DBuf campos;      // fp64 camera-origin accumulators, 3 per view
+  psdr::DBuf lens;        // fp64 camera-lens accumulators, kLensAcc per view
   int cap = 0;
   bool backward = false;
   bool rebuild = true;
   psdr::SceneGradInfo gi;
   // gradient targets, deep-copied pointer arrays per scene
   std::vector<std::vector<float*>> gv, gt, ge, gr, gn, gl;
-  std::vector<float*> gc;
+  std::vector<float*> gc, glens;
+  std::vector<psdr::LensChain> lens_chain;
   std::vector<int> gacc;
   std::vector<std::unique_ptr<psdr::DBuf>> vmasks;  // per-scene vertex-gradient masks of this batch's targets
   std::vector<std::unique_ptr<psdr::DBuf>> objs;    // per-scene object tables (texture accumulators asked for)
@@ -105,7 +107,20 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
       PSDR_CHECK(grads != nullptr, "d_images given without gradient targets");
     }
     cudaStream_t st = nullptr;
-    b->campos.alloc(sizeof(double) * 3 * n_cams, st);
+    const bool unb = cfg->estimator == PSDR_EST_UNBIASED;
+    b->lens_chain.resize(n_cams);
+    b->glens.assign(n_cams, nullptr);
+    for (int i = 0; b->backward && i < n_cams; ++i) {
+      PSDR_CHECK(cam_scene[i] >= 0 && cam_scene[i] < n_scenes, "camera scene index out of range");
+      const psdr_grad_targets& g = grads[cam_scene[i]];
+      if (!(g.camera_lens && g.camera_lens[i])) continue;
+      if (cams[i].type != PSDR_CAM_PERSPECTIVE)
+        throw Error{PSDR_ERR_UNSUPPORTED, "camera_lens gradients are implemented for perspective cameras only"};
+      b->glens[i] = g.camera_lens[i];
+      if (unb) lens_chain(cams[i], b->lens_chain[i]);
+    }
+    b->campos.alloc(sizeof(GradAcc) * 3 * n_cams, st);
+    b->lens.alloc(sizeof(GradAcc) * kLensAcc * n_cams, st);
     b->views.resize(n_cams);
     for (int i = 0; i < n_cams; ++i) {
       PSDR_CHECK(cam_scene[i] >= 0 && cam_scene[i] < n_scenes, "camera scene index out of range");
@@ -114,7 +129,8 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
       b->views[i].scene = cam_scene[i];
       b->views[i].image = images[i];
       b->views[i].dimage = b->backward ? d_images[i] : nullptr;
-      b->views[i].grad_pos = b->campos.as<double>() + 3 * i;
+      b->views[i].grad_pos = b->campos.as<GradAcc>() + 3 * i;
+      if (b->glens[i] && unb) b->views[i].grad_lens = b->lens.as<GradAcc>() + kLensAcc * i;
       if (b->backward) PSDR_CHECK(d_images[i] != nullptr, "null image gradient");
     }
     assign_offsets(b->views);
@@ -242,34 +258,41 @@ PSDR_API psdr_status psdr_batch_backward(psdr_batch* b, void* stream) {
           PSDR_CUDA(cudaMemsetAsync(s->g_tex.p, 0, s->g_tex.bytes, st));
           PSDR_CUDA(cudaMemsetAsync(s->g_emit.p, 0, s->g_emit.bytes, st));
         }
-        PSDR_CUDA(cudaMemsetAsync(b->campos.p, 0, sizeof(double) * 3 * b->views.size(), st));
+        PSDR_CUDA(cudaMemsetAsync(b->campos.p, 0, sizeof(GradAcc) * 3 * b->views.size(), st));
+        PSDR_CUDA(cudaMemsetAsync(b->lens.p, 0, sizeof(GradAcc) * kLensAcc * b->views.size(), st));
         backward_launch(b->scenes_dev.as<DevScene>(), b->views, b->cfg, b->cap, &b->ws, b->gi, st);
         for (size_t i = 0; i < b->scenes.size(); ++i) {
           psdr_scene* s = b->scenes[i];
           const int nm = (int)s->meshes.size();
           for (int o = 0; o < s->nobj; ++o)
-            grad_out(s->g_verts.as<double>() + 3 * (size_t)s->obj_vert_off[o], b->gv[i][o],
+            grad_out(s->g_verts.as<GradAcc>() + 3 * (size_t)s->obj_vert_off[o], b->gv[i][o],
                      3 * (long long)s->obj_nvert[o], b->gacc[i], st);
           for (int m = 0; m < nm; ++m) {
             const DevObj& ob = s->h_objs[m];
-            grad_out(s->g_tex.as<double>() + s->tex_grad_off[m], b->gt[i][m],
+            grad_out(s->g_tex.as<GradAcc>() + s->tex_grad_off[m], b->gt[i][m],
                      (long long)ob.color.h * ob.color.w * ob.color.ch, b->gacc[i], st);
             if (b->gr[i][m])
-              grad_out(s->g_tex.as<double>() + s->rough_grad_off[m], b->gr[i][m], (long long)ob.rough.h * ob.rough.w,
+              grad_out(s->g_tex.as<GradAcc>() + s->rough_grad_off[m], b->gr[i][m], (long long)ob.rough.h * ob.rough.w,
                        b->gacc[i], st);
             if (b->gn[i][m])
-              grad_out(s->g_tex.as<double>() + s->nrm_grad_off[m], b->gn[i][m],
+              grad_out(s->g_tex.as<GradAcc>() + s->nrm_grad_off[m], b->gn[i][m],
                        (long long)ob.normal.h * ob.normal.w * 3, b->gacc[i], st);
           }
           for (int l = 0; l < s->nlight; ++l) {
-            grad_out(s->g_emit.as<double>() + 3 * l, b->ge[i][l], 3, b->gacc[i], st);
+            grad_out(s->g_emit.as<GradAcc>() + 3 * l, b->ge[i][l], 3, b->gacc[i], st);
             if (b->gl[i][l])
-              grad_out(s->g_tex.as<double>() + s->light_grad_off[l], b->gl[i][l], light_param_count(s, l), b->gacc[i],
+              grad_out(s->g_tex.as<GradAcc>() + s->light_grad_off[l], b->gl[i][l], light_param_count(s, l), b->gacc[i],
                        st);
           }
         }
-        for (size_t c = 0; c < b->views.size(); ++c)
-          grad_out(b->campos.as<double>() + 3 * c, b->gc[c], 3, b->gacc[b->views[c].scene], st);
+        for (size_t c = 0; c < b->views.size(); ++c) {
+          grad_out(b->campos.as<GradAcc>() + 3 * c, b->gc[c], 3, b->gacc[b->views[c].scene], st);
+          if (!b->glens[c]) continue;
+          if (b->views[c].grad_lens)
+            lens_out(b->views[c].grad_lens, b->lens_chain[c], b->glens[c], b->gacc[b->views[c].scene], st);
+          else if (!b->gacc[b->views[c].scene])
+            PSDR_CUDA(cudaMemsetAsync(b->glens[c], 0, sizeof(float) * 10, st));
+        }
       }, b->bwd_launches, &b->bwd_ev);
     }
     PSDR_CUDA(cudaGraphLaunch(b->bwd_exec, st));

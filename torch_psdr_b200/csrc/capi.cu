@@ -164,7 +164,7 @@ extern "C" {
 
 const char* psdr_last_error(void) { return psdr::g_err.c_str(); }
 const char* psdr_version(void) { return "torch_psdr_b200 0.1.0 (sm_100a)"; }
-int32_t psdr_abi_version(void) { return 4; }
+int32_t psdr_abi_version(void) { return 5; }
 
 // emitter.cc:103-119: the environment lights' bounding-box mesh. Vertex v has x = max if
 // bit 2, y = max if bit 1, z = max if bit 0; the faces and the cube-map uvs (a 4 x 3 cross)
@@ -188,6 +188,12 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
   psdr_scene* s = new psdr_scene();
   s->stream = (cudaStream_t)stream;
   try {
+    // the device that will hold the scene (argument errors below are reported first on a
+    // machine without one; its first allocation reports a missing device)
+    if (cudaGetDevice(&s->device) != cudaSuccess) {
+      s->device = -1;
+      cudaGetLastError();
+    }
     const int nm = desc->num_meshes, nl = desc->num_lights;
     s->meshes.assign(desc->meshes, desc->meshes + nm);
     s->lights.assign(desc->lights, desc->lights + nl);
@@ -321,22 +327,22 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
     psdr_scene_alloc(s);
     // fp64 gradient accumulators live with the scene
     cudaStream_t st = s->stream;
-    s->g_verts.alloc(sizeof(double) * 3 * s->nvert, st);
-    s->g_tex.alloc(sizeof(double) * std::max<size_t>(1, texoff), st);
-    s->g_emit.alloc(sizeof(double) * 3 * std::max(1, nl), st);
-    s->dev.grad_verts = s->g_verts.as<double>();
+    s->g_verts.alloc(sizeof(GradAcc) * 3 * s->nvert, st);
+    s->g_tex.alloc(sizeof(GradAcc) * std::max<size_t>(1, texoff), st);
+    s->g_emit.alloc(sizeof(GradAcc) * 3 * std::max(1, nl), st);
+    s->dev.grad_verts = s->g_verts.as<GradAcc>();
     s->vmask.alloc(std::max<size_t>(1, s->nvert), st);
     PSDR_CUDA(cudaMemsetAsync(s->vmask.p, 1, std::max<size_t>(1, s->nvert), st));
     s->dev.vmask = s->vmask.as<unsigned char>();
     for (int o = 0; o < nm; ++o) {
-      s->h_objs[o].color.grad = s->g_tex.as<double>() + s->tex_grad_off[o];
-      if (s->rough_grad_off[o] != SIZE_MAX) s->h_objs[o].rough.grad = s->g_tex.as<double>() + s->rough_grad_off[o];
-      if (s->nrm_grad_off[o] != SIZE_MAX) s->h_objs[o].normal.grad = s->g_tex.as<double>() + s->nrm_grad_off[o];
+      s->h_objs[o].color.grad = s->g_tex.as<GradAcc>() + s->tex_grad_off[o];
+      if (s->rough_grad_off[o] != SIZE_MAX) s->h_objs[o].rough.grad = s->g_tex.as<GradAcc>() + s->rough_grad_off[o];
+      if (s->nrm_grad_off[o] != SIZE_MAX) s->h_objs[o].normal.grad = s->g_tex.as<GradAcc>() + s->nrm_grad_off[o];
     }
     for (int l = 0; l < nl; ++l) {
-      s->h_lights[l].grad_emit = s->g_emit.as<double>() + 3 * l;
+      s->h_lights[l].grad_emit = s->g_emit.as<GradAcc>() + 3 * l;
       if (s->light_grad_off[l] == SIZE_MAX) continue;
-      double* g = s->g_tex.as<double>() + s->light_grad_off[l];
+      GradAcc* g = s->g_tex.as<GradAcc>() + s->light_grad_off[l];
       if (s->h_lights[l].kind == PSDR_LIGHT_ENV) s->h_lights[l].tex.grad = g;
       else s->h_lights[l].grad_sh = g;
     }
@@ -576,6 +582,19 @@ psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_came
   API_END
 }
 
+psdr_status psdr_camera_lens_jacobian(const psdr_camera_desc* cam, double* m9, double* p90) {
+  API_BEGIN
+  PSDR_CHECK(cam != nullptr, "null argument");
+  check_cams(cam, 1);
+  PSDR_CHECK(cam->type == PSDR_CAM_PERSPECTIVE, "the lens map is defined for perspective cameras");
+  LensChain ch;
+  double m[9];
+  lens_chain(*cam, ch, m);
+  if (m9) std::copy(m, m + 9, m9);
+  if (p90) std::copy(&ch.P[0][0], &ch.P[0][0] + 90, p90);
+  API_END
+}
+
 psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams, int32_t n_cams,
                             const psdr_config* cfg, const float** d_images, const psdr_grad_targets* grads,
                             void* stream) {
@@ -585,6 +604,14 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   check_cams(cams, n_cams);
   ws->bsdf = scene->has_bsdf || scene->env_light >= 0 ? 1 : 0;  // extended kernel instances
   PSDR_CHECK(scene->nlight > 0, "scene has no light");
+  const bool unb = cfg->estimator == PSDR_EST_UNBIASED;
+  std::vector<LensChain> chains(n_cams);
+  for (int i = 0; grads->camera_lens && i < n_cams; ++i) {
+    if (!grads->camera_lens[i]) continue;
+    if (cams[i].type != PSDR_CAM_PERSPECTIVE)
+      throw Error{PSDR_ERR_UNSUPPORTED, "camera_lens gradients are implemented for perspective cameras only"};
+    if (unb) lens_chain(cams[i], chains[i]);
+  }
   cudaStream_t st = (cudaStream_t)stream;
   // only the vertices whose gradient the caller asked for are accumulated
   {
@@ -606,46 +633,54 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
   PSDR_CUDA(cudaMemsetAsync(scene->g_verts.p, 0, scene->g_verts.bytes, st));
   PSDR_CUDA(cudaMemsetAsync(scene->g_tex.p, 0, scene->g_tex.bytes, st));
   PSDR_CUDA(cudaMemsetAsync(scene->g_emit.p, 0, scene->g_emit.bytes, st));
-  ws->campos_acc.alloc(sizeof(double) * 3 * n_cams, st);
-  PSDR_CUDA(cudaMemsetAsync(ws->campos_acc.p, 0, sizeof(double) * 3 * n_cams, st));
+  ws->campos_acc.alloc(sizeof(GradAcc) * 3 * n_cams, st);
+  PSDR_CUDA(cudaMemsetAsync(ws->campos_acc.p, 0, sizeof(GradAcc) * 3 * n_cams, st));
+  ws->lens_acc.alloc(sizeof(GradAcc) * kLensAcc * n_cams, st);
+  PSDR_CUDA(cudaMemsetAsync(ws->lens_acc.p, 0, sizeof(GradAcc) * kLensAcc * n_cams, st));
   std::vector<DevView> views(n_cams);
   for (int i = 0; i < n_cams; ++i) {
     PSDR_CHECK(d_images[i] != nullptr, "null image gradient");
     make_view(cams[i], cfg->spp_interior, views[i]);
     views[i].dimage = d_images[i];
-    views[i].grad_pos = ws->campos_acc.as<double>() + 3 * i;
+    views[i].grad_pos = ws->campos_acc.as<GradAcc>() + 3 * i;
+    if (grads->camera_lens && grads->camera_lens[i] && unb) views[i].grad_lens = ws->lens_acc.as<GradAcc>() + kLensAcc * i;
   }
   render_backward_impl(dev_scene(scene), views, *cfg, ws, grad_info(scene), st);
   const int nm = (int)scene->meshes.size();
   for (int o = 0; o < scene->nobj; ++o) {
     if (grads->vertices && grads->vertices[o])
-      grad_out(scene->g_verts.as<double>() + 3 * (size_t)scene->obj_vert_off[o], grads->vertices[o],
+      grad_out(scene->g_verts.as<GradAcc>() + 3 * (size_t)scene->obj_vert_off[o], grads->vertices[o],
                3 * (long long)scene->obj_nvert[o], grads->accumulate, st);
     if (o < nm && grads->textures && grads->textures[o]) {
       const DevObj& ob = scene->h_objs[o];
-      grad_out(scene->g_tex.as<double>() + scene->tex_grad_off[o], grads->textures[o],
+      grad_out(scene->g_tex.as<GradAcc>() + scene->tex_grad_off[o], grads->textures[o],
                (long long)ob.color.h * ob.color.w * ob.color.ch, grads->accumulate, st);
     }
     if (o < nm && grads->roughness && grads->roughness[o] && scene->rough_grad_off[o] != SIZE_MAX) {
       const DevObj& ob = scene->h_objs[o];
-      grad_out(scene->g_tex.as<double>() + scene->rough_grad_off[o], grads->roughness[o],
+      grad_out(scene->g_tex.as<GradAcc>() + scene->rough_grad_off[o], grads->roughness[o],
                (long long)ob.rough.h * ob.rough.w, grads->accumulate, st);
     }
     if (o < nm && grads->normal && grads->normal[o] && scene->nrm_grad_off[o] != SIZE_MAX) {
       const DevObj& ob = scene->h_objs[o];
-      grad_out(scene->g_tex.as<double>() + scene->nrm_grad_off[o], grads->normal[o],
+      grad_out(scene->g_tex.as<GradAcc>() + scene->nrm_grad_off[o], grads->normal[o],
                (long long)ob.normal.h * ob.normal.w * 3, grads->accumulate, st);
     }
   }
   for (int l = 0; l < scene->nlight; ++l) {
-    if (grads->emit && grads->emit[l]) grad_out(scene->g_emit.as<double>() + 3 * l, grads->emit[l], 3, grads->accumulate, st);
+    if (grads->emit && grads->emit[l]) grad_out(scene->g_emit.as<GradAcc>() + 3 * l, grads->emit[l], 3, grads->accumulate, st);
     if (grads->light_params && grads->light_params[l] && scene->light_grad_off[l] != SIZE_MAX)
-      grad_out(scene->g_tex.as<double>() + scene->light_grad_off[l], grads->light_params[l],
+      grad_out(scene->g_tex.as<GradAcc>() + scene->light_grad_off[l], grads->light_params[l],
                light_param_count(scene, l), grads->accumulate, st);
   }
-  for (int i = 0; i < n_cams; ++i)
+  for (int i = 0; i < n_cams; ++i) {
     if (grads->camera_origin && grads->camera_origin[i])
-      grad_out(ws->campos_acc.as<double>() + 3 * i, grads->camera_origin[i], 3, grads->accumulate, st);
+      grad_out(ws->campos_acc.as<GradAcc>() + 3 * i, grads->camera_origin[i], 3, grads->accumulate, st);
+    if (grads->camera_lens && grads->camera_lens[i]) {
+      if (unb) lens_out(ws->lens_acc.as<GradAcc>() + kLensAcc * i, chains[i], grads->camera_lens[i], grads->accumulate, st);
+      else if (!grads->accumulate) PSDR_CUDA(cudaMemsetAsync(grads->camera_lens[i], 0, sizeof(float) * 10, st));
+    }
+  }
   PSDR_CUDA(cudaGetLastError());
   API_END
 }

@@ -92,13 +92,40 @@ PSDR_HD Rng make_rng(uint64_t i) {
   return r;
 }
 
+// ------------------------------------------------------------------ gradient accumulators
+// Exact, order-independent gradient sum: a fixed-point value in two int64 limbs,
+// value = hi 2^-20 + lo 2^-52. A contribution v adds sign(v) floor(|v| 2^20) to hi and
+// sign(v) round(frac(|v| 2^20) 2^32) to lo with integer atomics (fire-and-forget
+// reductions). Integer additions commute, so the sum does not depend on the order in
+// which threads reach it: backward passes are bitwise reproducible for any tile size and
+// scheduling. Each contribution is rounded once, to 2^-52 (2.2e-16); the only other
+// rounding is the final conversion. Limits: a contribution's magnitude saturates at 2^42,
+// the hi limb holds totals below 2^43, the lo limb absorbs 2^31 contributions per entry;
+// non-finite contributions are dropped.
+struct GradAcc {
+  long long hi, lo;
+};
+PSDR_D void acc_add(GradAcc* a, float v) {
+  if (!(v != 0.f) || !isfinite(v)) return;
+  const double q = fmin(fabs((double)v) * 1048576.0, 4398046511104.0 * 1048576.0);  // |v| 2^20, at most 2^62
+  const double fh = floor(q);
+  const long long dh = (long long)fh;
+  const long long dl = __double2ll_rn((q - fh) * 4294967296.0);  // in [0, 2^32]
+  const bool neg = v < 0.f;
+  if (dh) atomicAdd(reinterpret_cast<unsigned long long*>(&a->hi), (unsigned long long)(neg ? -dh : dh));
+  if (dl) atomicAdd(reinterpret_cast<unsigned long long*>(&a->lo), (unsigned long long)(neg ? -dl : dl));
+}
+PSDR_HD double acc_value(long long hi, long long lo) {
+  return (double)hi * 9.5367431640625e-07 + (double)lo * 2.220446049250313e-16;  // 2^-20, 2^-52
+}
+
 // ------------------------------------------------------------------ scene records
 struct DevTex {
   int kind;  // -1 none, 0 constant, 1 uv
   int ch;
   int h, w;
   const float* data;
-  double* grad;  // fp64 accumulator with the same layout, or null
+  GradAcc* grad;  // accumulator with the same layout, or null
 };
 struct DevObj {
   int mat;
@@ -109,11 +136,11 @@ struct DevLight {
   int tri0, ntri;
   float emit[3];
   float area, inv_area, power;
-  double* grad_emit;  // 3 doubles or null
+  GradAcc* grad_emit;  // 3 accumulators or null
   int kind;           // PSDR_LIGHT_AREA, _ENV (cube map in tex), _SH9 (coefficients in sh)
-  DevTex tex;         // ENV cube map (tex.grad: its fp64 accumulator or null)
+  DevTex tex;         // ENV cube map (tex.grad: its accumulator or null)
   float sh[27];       // SH9 (9,3) coefficients
-  double* grad_sh;    // SH9: 27 doubles or null
+  GradAcc* grad_sh;   // SH9: 27 accumulators or null
 };
 
 // Per-triangle shading record, 6 x float4 (96 B) in original triangle order:
@@ -144,7 +171,7 @@ struct DevScene {
   int root;
   const float4* nodes;
   const float4* leaf;
-  double* grad_verts;      // (nvert, 3) or null
+  GradAcc* grad_verts;     // (nvert, 3) or null
   const unsigned char* vmask;  // (nvert): 1 = the caller wants this vertex's gradient
   int* err;                // device error word (bit 0: traversal stack overflow)
 };

@@ -71,6 +71,7 @@ void radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int bits, SortTmp& 
 
 struct psdr_scene {
   cudaStream_t stream = nullptr;
+  int device = 0;  // the CUDA device current at psdr_scene_create (holds every buffer below)
   std::vector<psdr_mesh_desc> meshes;
   std::vector<psdr_area_light_desc> lights;
   int ntri = 0, nvert = 0, nobj = 0, nlight = 0, nnode = 0, leaf_size = 1;

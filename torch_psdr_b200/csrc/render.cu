@@ -99,10 +99,10 @@ PSDR_D int find_view_pix(const DevView* __restrict__ views, int nv, long long g)
 
 PSDR_D float4 hit4(const HitRec& h) { return make_float4(__int_as_float(h.tri), h.b1, h.b2, h.t); }
 
-PSDR_D void atomic_add3(double* p, float3 v) {
-  atomicAdd(p, (double)v.x);
-  atomicAdd(p + 1, (double)v.y);
-  atomicAdd(p + 2, (double)v.z);
+PSDR_D void atomic_add3(GradAcc* p, float3 v) {
+  acc_add(p, v.x);
+  acc_add(p + 1, v.y);
+  acc_add(p + 2, v.z);
 }
 
 // Vertex gradients are accumulated only for the vertices the caller asked for.
@@ -497,7 +497,7 @@ static __device__ __noinline__ float3 env_emit_adj(const DevLight* L, float u, f
 // Emission adjoint of light hit q reached from x: area lights into the emission
 // accumulator, environment lights into their parameters, and the SH9 direction's share
 // into the point x (wi = -normalize(q - x)).
-PSDR_D void add_emit(HotAcc& hot, double* grad_emit, float3 a) {
+PSDR_D void add_emit(HotAcc& hot, GradAcc* grad_emit, float3 a) {
   if (!grad_emit) return;
   if (hot.emit_hot) { hot.e[0] += a.x; hot.e[1] += a.y; hot.e[2] += a.z; }
   else atomic_add3(grad_emit, a);
@@ -570,7 +570,7 @@ PSDR_D void scatter_surf(const DevScene& sc, HotAcc& hot, int tri, float b1, flo
 
 PSDR_D void scatter_tex(const DevTex& tx, int off, float3 a, bool /*unused*/) {
   if (!tx.grad) return;
-  if (tx.ch == 1) atomicAdd(tx.grad + off, (double)(a.x + a.y + a.z));
+  if (tx.ch == 1) acc_add(tx.grad + off, a.x + a.y + a.z);
   else atomic_add3(tx.grad + off, a);
 }
 
@@ -690,7 +690,7 @@ PSDR_D float3 mat_finalize(const DevObj& ob, const Surf& x, const MatPt& mp, con
     ax.n += ma.N;
   }
   if (mp.rough && ob.rough.grad && ma.sigma != 0.f)
-    atomicAdd(ob.rough.grad + texel_offset(ob.rough, x.u, x.v), (double)ma.sigma);
+    acc_add(ob.rough.grad + texel_offset(ob.rough, x.u, x.v), ma.sigma);
   // V = -normalize(x.p - o)
   const float3 au = (ma.V - x.wi * dot(x.wi, ma.V)) * (-1.f / sqrtf(x.sqd));
   ax.p += au;
@@ -1178,10 +1178,10 @@ __global__ void __launch_bounds__(128, BSDF ? 2 : 3) k_adjoint(WF w, const DevSc
   if ((threadIdx.x & 31) == 0) {
     if (hot_nlv > 0 && vert_wanted(*fsc, hot_lv0))
       for (int k = 0; k < hot_nlv * 3; ++k)
-        if (hot.g[k] != 0.f) atomicAdd(fsc->grad_verts + 3 * (size_t)hot_lv0 + k, (double)hot.g[k]);
+        if (hot.g[k] != 0.f) acc_add(fsc->grad_verts + 3 * (size_t)hot_lv0 + k, hot.g[k]);
     if (emit_hot && fsc->nlight > 0 && fsc->lights[0].grad_emit)
       for (int k = 0; k < 3; ++k)
-        if (hot.e[k] != 0.f) atomicAdd(fsc->lights[0].grad_emit + k, (double)hot.e[k]);
+        if (hot.e[k] != 0.f) acc_add(fsc->lights[0].grad_emit + k, hot.e[k]);
   }
 }
 
@@ -1629,6 +1629,152 @@ __global__ void __launch_bounds__(256) k_border_final(WF w, const DevScene* __re
   }
 }
 
+// ------------------------------------------------------------------ camera lens
+// Unbiased estimator, perspective views: derivative of the image with respect to the
+// camera's basis and field of view (look_at, up, fov, and look_from through the basis).
+// With the camera origin fixed, the world direction seen at raster point u (taken from
+// the image centre) is M [u; 1], M = C diag(2 tan(fov/2) / W, -2 tan(fov/2) / H, -1), C the
+// camera basis (right, up, dir) of camera.h:35-52. A change dM moves the image content
+// with the raster velocity V(u) = (h_3 u_x - h_1, h_3 u_y - h_2), h = G [u; 1],
+// G = M^-1 dM. A box-filtered pixel then changes by the content flowing in across its
+// borders (the integral the pixel-border samples estimate, with V in place of the
+// material point's raster velocity) plus Int_P L div V du, where
+// div V = 3 (G_31 u_x + G_32 u_y) + 2 G_33 - G_11 - G_22.
+// Per view: grad_lens[0..2] = sum over camera samples of g.L {1, u_x, u_y} / spp (g the
+// pixel's dPhi/dI), grad_lens[3..11] = dPhi/dG of the border part (row-major 3x3).
+struct LensAcc {
+  const DevView* v = nullptr;
+  float s0 = 0.f, sx = 0.f, sy = 0.f;
+  PSDR_D void add(const DevView* view, float gl, float ux, float uy) {
+    if (view != v) {
+      flush();
+      v = view;
+      s0 = sx = sy = 0.f;
+    }
+    s0 += gl;
+    sx += gl * ux;
+    sy += gl * uy;
+  }
+  PSDR_D void flush() {
+    if (v && v->grad_lens && (s0 != 0.f || sx != 0.f || sy != 0.f)) {
+      acc_add(v->grad_lens, s0);
+      acc_add(v->grad_lens + 1, sx);
+      acc_add(v->grad_lens + 2, sy);
+    }
+    v = nullptr;
+  }
+  PSDR_D void flush_warp() {
+    const unsigned long long key = (unsigned long long)v;
+    const unsigned long long k0 = __shfl_sync(0xffffffffu, key, 0);
+    if (!__all_sync(0xffffffffu, key == k0) || !v) { flush(); return; }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      sx += __shfl_xor_sync(0xffffffffu, sx, o);
+      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if ((threadIdx.x & 31) == 0) flush();
+    v = nullptr;
+  }
+};
+
+// Interior moments from the replay records of a tile (after its adjoint): the sample's
+// radiance is the film's value (the emission of a visible light, or the path's suffix
+// radiance from depth 0); its raster position replays the two jitter draws of k_camera.
+template <bool BSDF>
+__global__ void __launch_bounds__(256) k_lens_interior(WF w, const DevScene* __restrict__ scenes,
+                                                       const DevView* __restrict__ views, Tile tile) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (tile.n + 31) & ~31;
+  LensAcc acc;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    if (s >= tile.n) continue;
+    const DevView& V = views[w.view[s]];
+    if (!V.grad_lens || !V.dimage) continue;
+    const float4* rec = w.rec + (size_t)s * w.rec_stride;
+    const float4 h0 = rec[0];
+    const int tri0 = __float_as_int(h0.x);
+    if (tri0 < 0) continue;
+    const DevScene& sc = scenes[V.scene];
+    const Surf x0 = make_surf(sc, tri0, h0.y, h0.z, V.pos);
+    float3 L;
+    if (x0.is_light) {
+      if (!w.light_vis) continue;
+      L = light_emit<BSDF>(sc.lights[x0.light], x0);
+    } else {
+      L = suffix_radiance(rec + 1 + (size_t)w.D * w.R, 0, w.D);
+    }
+    if (!finite3(L)) continue;
+    const int pix = w.pix[s];
+    const float* gp = V.dimage + 3 * (size_t)pix;
+    const float gl = (gp[0] * L.x + gp[1] * L.y + gp[2] * L.z) / (float)V.spp;
+    Rng rng = make_rng((unsigned long long)(tile.begin + s - V.sample_off) + w.seed);
+    const float jx = rng.next_float(), jy = rng.next_float();
+    acc.add(&V, gl, jx + (float)(pix % V.W) - 0.5f * (float)V.W, jy + (float)(pix / V.W) - 0.5f * (float)V.H);
+  }
+  acc.flush_warp();
+}
+
+// Border part from the pixel-border samples of view v (after k_border_final): the
+// sample's weight times dV_c/dG at its raster point, c the coordinate across the border.
+__global__ void __launch_bounds__(256) k_lens_border(WF w, const DevView* __restrict__ views, int v, EdgeBuf eb,
+                                                     int n, long long N) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const DevView& V = views[v];
+  float b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f, b4 = 0.f, b5 = 0.f, b6 = 0.f, b7 = 0.f, b8 = 0.f;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    if (s >= n || !V.dimage || !V.grad_lens) continue;
+    if (__float_as_int(eb.hb[s].x) < 0) continue;  // the border ray left the scene: no radiance
+    const float4 a = eb.a[s];
+    if (!(a.z > 0.f)) continue;
+    bool vert;
+    int k, j, lo, hi;
+    border_pixels(V, __float_as_int(a.x), vert, k, j, lo, hi);
+    const float3 L = xyz(w.L[s]);
+    const float3 dg = dimage_at(V, hi) - dimage_at(V, lo);
+    const float wgt = dot(dg, L) / ((float)N * a.z);
+    if (!(wgt != 0.f) || !isfinite(wgt)) continue;
+    const float ux = (vert ? (float)k : a.y + (float)k) - 0.5f * (float)V.W;
+    const float uy = (vert ? a.y + (float)j : (float)j) - 0.5f * (float)V.H;
+    const float wc = wgt * (vert ? ux : uy);
+    if (vert) { b0 -= wgt * ux; b1 -= wgt * uy; b2 -= wgt; }
+    else { b3 -= wgt * ux; b4 -= wgt * uy; b5 -= wgt; }
+    b6 += wc * ux;
+    b7 += wc * uy;
+    b8 += wc;
+  }
+  float b[9] = {b0, b1, b2, b3, b4, b5, b6, b7, b8};
+#pragma unroll
+  for (int o = 16; o; o >>= 1)
+#pragma unroll
+    for (int m = 0; m < 9; ++m) b[m] += __shfl_xor_sync(0xffffffffu, b[m], o);
+  if ((threadIdx.x & 31) == 0 && V.grad_lens) {
+#pragma unroll
+    for (int m = 0; m < 9; ++m)
+      if (b[m] != 0.f) acc_add(V.grad_lens + 3 + m, b[m]);
+  }
+}
+
+// dPhi/dtheta_j = <Gamma, P_j>, Gamma = B + the interior part of dPhi/dG.
+__global__ void k_lens_out(const GradAcc* __restrict__ acc, LensChain ch, float* __restrict__ out, int accumulate) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double G[9];
+  for (int m = 0; m < 9; ++m) G[m] = acc_value(acc[3 + m].hi, acc[3 + m].lo);
+  const double s0 = acc_value(acc[0].hi, acc[0].lo), sx = acc_value(acc[1].hi, acc[1].lo),
+               sy = acc_value(acc[2].hi, acc[2].lo);
+  G[0] -= s0;
+  G[4] -= s0;
+  G[6] += 3.0 * sx;
+  G[7] += 3.0 * sy;
+  G[8] += 2.0 * s0;
+  for (int j = 0; j < 10; ++j) {
+    double d = 0.0;
+    for (int m = 0; m < 9; ++m) d += G[m] * ch.P[j][m];
+    out[j] = accumulate ? out[j] + (float)d : (float)d;
+  }
+}
+
 // ------------------------------------------------------------------ BSDF jumps
 // Unbiased estimator, DiffuseBsdfMaterial with roughness > 0 (diffuse_bsdf.cc:56-88).
 // With N.L >= 0 and N.V >= 0 the rough-diffuse value jumps by color b (max(N.L, N.V) +
@@ -2071,10 +2217,11 @@ __global__ void k_mass_finalize(const double* __restrict__ w, const double* __re
   pmf[i] = (float)(w[i] / tot);
   cmf[i] = (float)(pre[i] / tot);
 }
-__global__ void k_grad_out(const double* __restrict__ acc, float* __restrict__ out, long long n, int accumulate) {
+__global__ void k_grad_out(const GradAcc* __restrict__ acc, float* __restrict__ out, long long n, int accumulate) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  out[i] = (accumulate ? out[i] : 0.f) + (float)acc[i];
+  const longlong2 a = __ldg(reinterpret_cast<const longlong2*>(acc) + i);
+  out[i] = (accumulate ? out[i] : 0.f) + (float)acc_value(a.x, a.y);
 }
 
 
@@ -2156,6 +2303,92 @@ void make_view(const psdr_camera_desc& c, int spp, DevView& v) {
   v.image = nullptr;
   v.dimage = nullptr;
   v.grad_pos = nullptr;
+  v.grad_lens = nullptr;
+}
+
+// Forward-mode derivative of the raster-to-direction map M = C diag(2 t / W, -2 t / H, -1),
+// t = tan(fov / 2), C = (right, up, dir) built as camera.h:35-52 does (dir = normalize(from -
+// at), right = cross(normalize(up), dir) unnormalised, up' = cross(dir, right)), with
+// respect to the ten camera parameters (from, at, up, fov); P_j = M^-1 dM/dtheta_j.
+namespace {
+struct Dual10 {
+  double v;
+  double d[10];
+};
+Dual10 dconst(double v) { Dual10 r{v, {0}}; return r; }
+Dual10 dvar(double v, int j) { Dual10 r = dconst(v); r.d[j] = 1.0; return r; }
+Dual10 operator+(const Dual10& a, const Dual10& b) { Dual10 r{a.v + b.v, {0}}; for (int j = 0; j < 10; ++j) r.d[j] = a.d[j] + b.d[j]; return r; }
+Dual10 operator-(const Dual10& a, const Dual10& b) { Dual10 r{a.v - b.v, {0}}; for (int j = 0; j < 10; ++j) r.d[j] = a.d[j] - b.d[j]; return r; }
+Dual10 operator*(const Dual10& a, const Dual10& b) { Dual10 r{a.v * b.v, {0}}; for (int j = 0; j < 10; ++j) r.d[j] = a.d[j] * b.v + a.v * b.d[j]; return r; }
+Dual10 operator*(const Dual10& a, double k) { Dual10 r{a.v * k, {0}}; for (int j = 0; j < 10; ++j) r.d[j] = a.d[j] * k; return r; }
+Dual10 dinv(const Dual10& a) { Dual10 r{1.0 / a.v, {0}}; for (int j = 0; j < 10; ++j) r.d[j] = -a.d[j] / (a.v * a.v); return r; }
+Dual10 dsqrt(const Dual10& a) { Dual10 r{std::sqrt(a.v), {0}}; for (int j = 0; j < 10; ++j) r.d[j] = a.d[j] / (2.0 * r.v); return r; }
+Dual10 dtan(const Dual10& a) {
+  const double t = std::tan(a.v);
+  Dual10 r{t, {0}};
+  for (int j = 0; j < 10; ++j) r.d[j] = a.d[j] * (1.0 + t * t);
+  return r;
+}
+void dnormalize(Dual10* a) {
+  const Dual10 n = dinv(dsqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+  for (int k = 0; k < 3; ++k) a[k] = a[k] * n;
+}
+void dcross(const Dual10* a, const Dual10* b, Dual10* r) {
+  r[0] = a[1] * b[2] - a[2] * b[1];
+  r[1] = a[2] * b[0] - a[0] * b[2];
+  r[2] = a[0] * b[1] - a[1] * b[0];
+}
+bool inv3(const double* m, double* r) {
+  const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[5] * m[6] - m[3] * m[8], c02 = m[3] * m[7] - m[4] * m[6];
+  const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
+  if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) return false;
+  const double id = 1.0 / det;
+  r[0] = c00 * id; r[1] = (m[2] * m[7] - m[1] * m[8]) * id; r[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+  r[3] = c01 * id; r[4] = (m[0] * m[8] - m[2] * m[6]) * id; r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+  r[6] = c02 * id; r[7] = (m[1] * m[6] - m[0] * m[7]) * id; r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+  return true;
+}
+}  // namespace
+
+void lens_chain(const psdr_camera_desc& c, LensChain& out, double* m9) {
+  Dual10 from[3], at[3], up[3];
+  for (int k = 0; k < 3; ++k) {
+    from[k] = dvar(c.look_from[k], k);
+    at[k] = dvar(c.look_at[k], 3 + k);
+    up[k] = dvar(c.up[k], 6 + k);
+  }
+  const Dual10 fov = dvar(c.fov, 9);
+  Dual10 dir[3] = {from[0] - at[0], from[1] - at[1], from[2] - at[2]};
+  dnormalize(dir);
+  dnormalize(up);
+  Dual10 right[3], nup[3];
+  dcross(up, dir, right);
+  dcross(dir, right, nup);
+  const Dual10 t = dtan(fov * 0.5);
+  const Dual10 sx = t * (2.0 / c.width), sy = t * (-2.0 / c.height);
+  Dual10 M[9];
+  for (int i = 0; i < 3; ++i) {
+    M[3 * i] = right[i] * sx;
+    M[3 * i + 1] = nup[i] * sy;
+    M[3 * i + 2] = dir[i] * -1.0;
+  }
+  double m[9], mi[9];
+  for (int q = 0; q < 9; ++q) m[q] = M[q].v;
+  if (m9) std::copy(m, m + 9, m9);
+  PSDR_CHECK(inv3(m, mi), "degenerate camera basis (look_at equals look_from, or up parallel to the view)");
+  for (int j = 0; j < 10; ++j)
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q) {
+        double acc = 0.0;
+        for (int k = 0; k < 3; ++k) acc += mi[3 * r + k] * M[3 * k + q].d[j];
+        out.P[j][3 * r + q] = acc;
+      }
+}
+
+void lens_out(const GradAcc* acc, const LensChain& ch, float* out, int accumulate, cudaStream_t st) {
+  k_lens_out<<<1, 32, 0, st>>>(acc, ch, out, accumulate);
+  profiler().launches += 1;
+  PSDR_CUDA(cudaGetLastError());
 }
 
 std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap) {
@@ -2432,12 +2665,16 @@ static void edge_phase_unb(WF w, const DevScene* scenes, const DevView* vd, int 
 // Pixel-border samples [begin, begin + n) of the N of view v (segment masses in w/pre).
 static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
                          const double* mw, const double* mpre, long long S, long long begin, int n, long long N,
-                         cudaStream_t st) {
+                         bool lens, cudaStream_t st) {
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
   k_border_init<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, mw, mpre, S, begin, n, N);
   PSDR_LAUNCHED(2);
   depth_loop(w, scenes, vd, MODE_FWD, st);
   k_border_final<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, n, N);
+  if (lens) {
+    k_lens_border<<<grid_for(n, 256, 8), 256, 0, st>>>(w, vd, v, eb, n, N);
+    PSDR_LAUNCHED(1);
+  }
   PSDR_CUDA(cudaGetLastError());
 }
 
@@ -2520,6 +2757,8 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
   const DevView* vd = ws->views.as<DevView>();
   const bool unb = cfg.estimator == PSDR_EST_UNBIASED;
   const int terms = cfg.terms ? cfg.terms : (unb ? 15 : 7);
+  bool lens = false;  // a view wants the camera-lens gradient
+  for (const DevView& V : views) lens = lens || V.grad_lens != nullptr;
   // ---- interior
   if (terms & 1) {
     WF w = ws->wf;
@@ -2538,6 +2777,11 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
         else k_adjoint<false><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
       }
       PSDR_LAUNCHED(1);
+      if (lens) {
+        if (gi.bsdf) k_lens_interior<true><<<grid_for(t.n, 256, 8), 256, 0, st>>>(w, scenes_dev, vd, t);
+        else k_lens_interior<false><<<grid_for(t.n, 256, 8), 256, 0, st>>>(w, scenes_dev, vd, t);
+        PSDR_LAUNCHED(1);
+      }
     }
     PSDR_CUDA(cudaGetLastError());
   }
@@ -2611,7 +2855,7 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
                             st);
       for (long long b0 = 0; b0 < N; b0 += cap)
         border_phase(wi, scenes_dev, vd, v, eb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), S, b0,
-                     (int)std::min<long long>(cap, N - b0), N, st);
+                     (int)std::min<long long>(cap, N - b0), N, V.grad_lens != nullptr, st);
     }
     // BSDF jumps (unbiased estimator, DiffuseBsdfMaterial scenes; on request only)
     if (unb && (terms & 16) && gi.bsdf && V.dimage) {
@@ -2623,7 +2867,7 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
   }
 }
 
-void grad_out(const double* acc, float* out, long long n, int accumulate, cudaStream_t st) {
+void grad_out(const GradAcc* acc, float* out, long long n, int accumulate, cudaStream_t st) {
   if (!out || n <= 0) return;
   k_grad_out<<<(int)((n + 255) / 256), 256, 0, st>>>(acc, out, n, accumulate);
   PSDR_LAUNCHED(1);
@@ -2699,11 +2943,16 @@ PSDR_API psdr_status psdr_profile_read(int64_t* out3, double* trace_ms) {
 // wavefront buffers of each tile live in one file-scope __device__ array that every
 // GPU loading this library holds until the process exits. It exists for callers that
 // cannot call cudaMalloc at render time -- hosts that hand the library a fixed memory
-// budget up front (plugin hosts, engines with their own pools), latency-critical loops
-// where cudaMalloc's implicit device synchronisation is not acceptable, and code that
-// must not add allocation nodes while a stream is being recorded.
+// budget up front (plugin hosts, engines with their own pools), and latency-critical
+// loops where cudaMalloc's implicit device synchronisation is not acceptable.
 namespace psdr {
 namespace {
+
+// Writes the view record into the scratch from a kernel argument, so the call issues no
+// host-to-device copy from host memory.
+__global__ void k_put_view(DevView* dst, DevView v) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dst = v;
+}
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -2768,6 +3017,13 @@ extern "C" PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const
                 " exceeds the allocation-free tile of " + std::to_string(cap) + " paths (32 MiB scratch)");
       return PSDR_ERR_INVALID_ARG;
     }
+    int cur_dev = 0;
+    PSDR_CUDA(cudaGetDevice(&cur_dev));
+    if (cur_dev != scene->device) {
+      set_error("psdr_render_fwd_noalloc: the scene was created on device " + std::to_string(scene->device) +
+                " but device " + std::to_string(cur_dev) + " is current");
+      return PSDR_ERR_INVALID_ARG;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     unsigned char* base = noalloc_scratch();
     size_t off = 0;
@@ -2801,7 +3057,8 @@ extern "C" PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const
     V.sample_off = 0;
     V.pix_off = 0;
     V.image = image;
-    PSDR_CUDA(cudaMemcpyAsync(vd, &V, sizeof(DevView), cudaMemcpyHostToDevice, st));
+    k_put_view<<<1, 32, 0, st>>>(vd, V);
+    count_launches(1);
     // tiles of whole pixels, walked without building a host-side list
     const long long npix = (long long)cam->height * cam->width;
     const long long pix_per_tile = (long long)cap / cfg->spp_interior;

@@ -21,7 +21,8 @@ struct DevView {
   long long pix_off;     // first pixel of this view in the job's pixel space
   float* image;          // (H,W,3) or null
   const float* dimage;   // (H,W,3) or null
-  double* grad_pos;      // 3 doubles or null
+  GradAcc* grad_pos;     // 3 accumulators or null
+  GradAcc* grad_lens;    // 12 accumulators or null: the camera-lens sums (k_lens_interior, k_lens_border)
 };
 
 // Path states and ray queues of one tile (structure of arrays, capacity `cap`).
@@ -76,7 +77,7 @@ struct psdr_workspace {
   int cap = 0, R = 0, D = 0, nviews_cap = 0;
   psdr::DBuf rs, ri, view, pix, T, L, cur, org, q0, q1, qs, cnt, ro, rd, ra, hit, rec;
   psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
-  psdr::DBuf campos_acc;
+  psdr::DBuf campos_acc, lens_acc;
   long long mass_cap = 0;
   // a DiffuseBsdfMaterial mesh or an environment light is in the scenes of the current job
   // (each entry point sets it; the extended kernel instances also handle the plain
@@ -118,7 +119,7 @@ struct SceneGradInfo {
 };
 void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
                           psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
-void grad_out(const double* acc, float* out, long long n, int accumulate, cudaStream_t st);
+void grad_out(const GradAcc* acc, float* out, long long n, int accumulate, cudaStream_t st);
 void assign_offsets(std::vector<DevView>& views);
 int choose_cap(const psdr_config& cfg, const std::vector<DevView>& views, bool backward);
 void upload_views(psdr_workspace* ws, const std::vector<DevView>& views, cudaStream_t st);
@@ -133,6 +134,16 @@ long long light_param_count(const psdr_scene* s, int l);
 void scene_build_geometry(psdr_scene* s, cudaStream_t st);
 void scene_refit_geometry(psdr_scene* s, cudaStream_t st);
 std::vector<Tile> plan_tiles(const std::vector<DevView>& views, int cap);
+// Camera-lens gradient (unbiased estimator, perspective cameras): P[j] = M^-1 dM/dtheta_j
+// for the raster-to-direction map M of camera c and its parameters theta = (look_from,
+// look_at, up, fov) as they enter the camera's basis and projection (row-major 3x3 each).
+struct LensChain {
+  double P[10][9];
+};
+void lens_chain(const psdr_camera_desc& c, LensChain& out, double* m9 = nullptr);
+constexpr int kLensAcc = 12;  // accumulators per view: S0, Sx, Sy, B (3x3)
+// out[10] (fp32, overwritten or accumulated) from a view's accumulators.
+void lens_out(const GradAcc* acc, const LensChain& ch, float* out, int accumulate, cudaStream_t st);
 long long border_segments(const DevView& V);
 void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector<DevView>& views, cudaStream_t st);
 }  // namespace psdr
