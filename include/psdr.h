@@ -133,6 +133,9 @@ typedef struct {
                      (UNBIASED only, on request: not part of 0) */
   int32_t spp_pixel_boundary; /* UNBIASED: samples per unit pixel-border segment */
   uint64_t seed;
+  int32_t trace_queue; /* ABI 5: rays each SM traverses concurrently in the wavefront
+                          closest-hit kernel, in units of 128 (the traversal queue depth;
+                          1..8, 0 = 8); psdr_autotune picks it. Results do not depend on it. */
 } psdr_config;
 
 /* Gradient outputs of psdr_render_bwd (caller-owned device buffers, fp32).
@@ -174,14 +177,15 @@ PSDR_API int32_t psdr_abi_version(void);
 /* ---------------------------------------------------------------- scene
  * Replaces Scene::Scene (scene.cc:3-104) + SceneOptix ctor / build_accel
  * (scene_optix.cc:10-46, 187-238) + TriangleMesh edge build (mesh.cc:97-204):
- * flattens the meshes, builds the edge list and the sampling CDFs and an LBVH,
- * all on `stream`. Texture data pointers are borrowed and must outlive the scene. */
+ * checks the index buffers (psdr_scene_validate), then flattens the meshes, builds the
+ * edge list and the sampling CDFs and an LBVH, all on `stream`. Texture data pointers
+ * are borrowed and must outlive the scene. */
 PSDR_API psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_scene** out);
-/* Checks the index buffers of a scene description before psdr_scene_create (extension;
- * the reference does not check them): every face index must lie in [0, num_vertices) of
- * its mesh or area light, every uv index in [0, num_uvs). One device reduction per
- * buffer on `stream` and one host read; PSDR_ERR_INVALID_ARG names the first buffer out
- * of range. psdr_scene_create itself trusts the indices. */
+/* Checks the index buffers of a scene description (extension; the reference does not
+ * check them): every face index must lie in [0, num_vertices) of its mesh or area light,
+ * every uv index in [0, num_uvs). One device reduction per buffer on `stream` and one
+ * host read; PSDR_ERR_INVALID_ARG names the first buffer out of range. psdr_scene_create
+ * runs the same check before its build gathers through the indices. */
 PSDR_API psdr_status psdr_scene_validate(const psdr_scene_desc* desc, void* stream);
 PSDR_API psdr_status psdr_scene_destroy(psdr_scene* scene);
 /* Rebuild the acceleration structure, triangle attributes and edges after the
@@ -249,12 +253,13 @@ PSDR_API psdr_status psdr_render_fwd_noalloc(psdr_scene* scene, const psdr_camer
 PSDR_API psdr_status psdr_render_samples(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cam,
                                 const psdr_config* cfg, float* samples, void* stream);
 /* Autotuner (extension; the reference has no tuner): times forward renders of the
- * given cameras for every wavefront tile size in {2^18, 2^19, 2^20, 2^21} paths and
- * BVH leaf size in {1, 2, 4} triangles (the scene's BVH is rebuilt for each), keeps
- * the fastest leaf size in the scene (later psdr_scene_update calls use it), writes
- * the fastest tile size to cfg->tile_paths and, when non-null, the leaf size and the
- * fastest render time to best_leaf / best_ms. Allocates and synchronises `stream`;
- * results do not depend on either choice (hits and films are deterministic). */
+ * given cameras for every wavefront tile size in {2^18, 2^19, 2^20, 2^21} paths, BVH
+ * leaf size in {1, 2, 4} triangles (the scene's BVH is rebuilt for each) and traversal
+ * queue depth in {4, 6, 8} x 128 rays per SM, keeps the fastest leaf size in the scene
+ * (later psdr_scene_update calls use it), writes the fastest tile size and queue depth to
+ * cfg->tile_paths / cfg->trace_queue and, when non-null, the leaf size and the fastest
+ * render time to best_leaf / best_ms. Allocates and synchronises `stream`; results do
+ * not depend on any of the choices (hits and films are deterministic). */
 PSDR_API psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_camera_desc* cams,
                                    int32_t n_cams, psdr_config* cfg, int32_t* best_leaf, float* best_ms,
                                    void* stream);

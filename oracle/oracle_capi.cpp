@@ -808,6 +808,12 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
     std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < (int64_t)N; ++i) {
+      if constexpr (KD > 0) {
+        // derivatives only: a sample of a pixel with zero weight adds nothing to dphi (the
+        // image buffer is not an output of the derivative queries)
+        const int64_t p = i / spp;
+        if (!per_sample && dLdI[3 * p] == 0.0 && dLdI[3 * p + 1] == 0.0 && dLdI[3 * p + 2] == 0.0) continue;
+      }
       int pix;
       bool valid;
       V3<S> L = interior_sample<S, AD>(c, (uint64_t)i, pix, valid);

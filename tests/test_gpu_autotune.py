@@ -52,6 +52,7 @@ def test_autotune_keeps_images(cuda):
     print("autotune", info)
     assert info["tile_paths"] in (1 << 18, 1 << 19, 1 << 20, 1 << 21)
     assert info["leaf_size"] in (1, 2, 4)
+    assert info["trace_queue"] in (4, 6, 8)
     assert info["forward_ms"] > 0
     after = integ.renderC(scene)[0]
     torch.cuda.synchronize()

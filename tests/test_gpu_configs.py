@@ -1,0 +1,153 @@
+"""Parity at the reference workloads' own sizes (the scenes of torch_psdr_b200.synth):
+
+* the plain forward render (level-3 icosphere, 128x128, 16 spp, depth 3) against the FP64
+  oracle, and the same scene at 4096 spp (64x64) against the FP64 oracle at 4096 spp;
+* the texture-gradient workload (256x256, 64 spp, L2 loss against the render with the
+  seed-1 texture) against central differences on 64 texels drawn with seed 0 from all
+  256*256*3, step 1e-3, common random numbers;
+* the geometry-gradient workload's scene (level-5 icosphere with radial noise 0.02, seed 2)
+  at 64x64: every gradient term of both estimators against the oracle's forward-mode
+  derivatives along random vertex directions;
+* the large scene (16 noisy level-6 icospheres, 1.31 M triangles, 1024x1024, depth 5):
+  vertex and texture directional derivatives of a loss on a 64x64 window against the FP64
+  oracle (interior term; 4 spp so that the oracle's share stays in seconds).
+"""
+import numpy as np
+import pytest
+import torch
+
+import orc
+import torch_psdr_b200 as dr
+from torch_psdr_b200 import synth
+from helpers import rel_l2, rel_mse, to_torch_scene
+
+pytestmark = pytest.mark.gpu
+
+
+def test_plain_forward_workload_matches_fp64_oracle(cuda):
+    spec = synth.sphere_scene(level=3, tex_hw=256, tex_seed=0, height=128, width=128)
+    kw = dict(spp_interior=16, max_bounce=3)
+    scene, _ = to_torch_scene(spec)
+    img = dr.PathIntegrator(**kw).renderC(scene)[0].cpu().numpy().astype(np.float64)
+    ref = orc.render(spec, precision=1, **kw)[0]
+    e = rel_mse(img, ref)
+    print(f"128x128, 16 spp: rel MSE vs FP64 {e:.3e}")
+    assert ref.mean() > 0 and e < 1e-3
+
+
+def test_plain_forward_at_4096_spp_matches_fp64_oracle(cuda):
+    spec = synth.sphere_scene(level=3, tex_hw=256, tex_seed=0, height=64, width=64)
+    kw = dict(spp_interior=4096, max_bounce=3)
+    scene, _ = to_torch_scene(spec)
+    img = dr.PathIntegrator(**kw).renderC(scene)[0].cpu().numpy().astype(np.float64)
+    ref = orc.render(spec, precision=1, **kw)[0]
+    e = rel_mse(img, ref)
+    print(f"64x64, 4096 spp: rel MSE vs FP64 {e:.3e}")
+    assert ref.mean() > 0 and e < 1e-3
+
+
+def test_texture_gradient_workload_vs_finite_differences(cuda):
+    H = W = 256
+    kw = dict(spp_interior=64, max_bounce=3)
+    spec = synth.sphere_scene(level=3, tex_hw=256, tex_seed=0, height=H, width=W)
+    tgt_spec = synth.sphere_scene(level=3, tex_hw=256, tex_seed=1, height=H, width=W)
+    integ = dr.PathIntegrator(gradient_terms=1, **kw)
+    target = integ.renderC(to_torch_scene(tgt_spec)[0])[0].double()
+    scene, T = to_torch_scene(spec, requires_grad={"tex"})
+    img = integ.renderD(scene)[0]
+    ((img - target.float()) ** 2).sum().backward()
+    grad = T["tex0"].grad.detach().double().cpu().numpy().reshape(-1)
+    pick = np.random.default_rng(0).choice(grad.size, size=64, replace=False)
+    scene_fd, _ = to_torch_scene(spec)
+    flat = scene_fd.meshes[0].material.texture.data.view(-1)  # the texture the native scene reads
+    base = flat.clone()
+
+    def loss():
+        return float(((integ.renderC(scene_fd)[0].double() - target) ** 2).sum())
+
+    h = 1e-3
+    fd = []
+    for k in pick:
+        flat.copy_(base)
+        flat[k] += h
+        lp = loss()
+        flat.copy_(base)
+        flat[k] -= h
+        lm = loss()
+        fd.append((lp - lm) / (2 * h))
+    flat.copy_(base)
+    fd = np.array(fd)
+    e = rel_l2(grad[pick], fd)
+    print(f"texture gradient, 64 texels (seed 0), {np.count_nonzero(fd)} seen: rel L2 vs FD {e:.2e}")
+    assert np.count_nonzero(fd) >= 8
+    assert e < 0.01
+
+
+def _vertex_seeds(spec, rng, meshes):
+    nv = [m.vertices.shape[0] for m in spec.meshes] + [l.vertices.shape[0] for l in spec.lights]
+    sv = np.zeros((sum(nv), 3, 8))
+    gpu = {}
+    off = 0
+    for i, n in enumerate(nv[:len(spec.meshes)]):
+        if i in meshes:
+            sv[off:off + n] = rng.normal(size=(n, 3, 8))
+            gpu[f"verts{i}"] = sv[off:off + n]
+        off += n
+    return gpu, sv
+
+
+@pytest.mark.parametrize("estimator,terms", [("unbiased", 1), ("unbiased", 2), ("unbiased", 4), ("unbiased", 8),
+                                             ("reference", 1), ("reference", 2), ("reference", 4)])
+def test_geometry_workload_terms_match_oracle(cuda, estimator, terms):
+    spec = synth.sphere_scene(level=5, tex_hw=256, tex_seed=0, noise_sigma=0.02, noise_seed=2, height=64, width=64)
+    unb = estimator == "unbiased"
+    kw = dict(spp_interior=4, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=3,
+              primary_edge_hypercube_resolution=2000, secondary_edge_hypercube_resolution=[2000, 6, 6])
+    if unb:
+        kw.update(spp_pixel_boundary=4)
+    gseeds, sv = _vertex_seeds(spec, np.random.default_rng(3), meshes={0, 1})
+    scene, T = to_torch_scene(spec, requires_grad={"verts"})
+    img = dr.PathIntegrator(gradient_terms=terms, estimator=estimator, **kw).renderD(scene)[0]
+    dLdI = np.random.default_rng(5).normal(size=tuple(img.shape))
+    img.backward(torch.tensor(dLdI, dtype=torch.float32, device="cuda"))
+    got = np.zeros(8)
+    for name, seed in gseeds.items():
+        g = T[name].grad.detach().cpu().numpy().astype(np.float64).reshape(-1)
+        got += g @ seed.reshape(g.shape[0], 8)
+    ref = orc.grad_dir(spec, [dLdI], which=terms, mode=1 if unb else 0, seed_verts=sv, **kw)
+    err = np.abs(got - ref) / (np.abs(ref).max() + 1e-30)
+    print(f"level-5 noisy sphere, {estimator} terms={terms}: gpu {got[:3]} oracle {ref[:3]} max rel {err.max():.2e}")
+    assert np.abs(ref).max() > 0
+    assert err.max() < (1e-2 if terms == 4 else 2e-3)
+
+
+def test_large_scene_window_gradients_match_fp64_oracle(cuda):
+    spec = synth.large_scene()  # 1024 x 1024
+    H, W = spec.cameras[0].height, spec.cameras[0].width
+    kw = dict(spp_interior=4, max_bounce=5)
+    rng = np.random.default_rng(4)
+    dLdI = np.zeros((H, W, 3))
+    y0, x0 = 448, 448  # a 64 x 64 window at the centre of the view
+    dLdI[y0:y0 + 64, x0:x0 + 64] = rng.normal(size=(64, 64, 3))
+    n_sph = len(spec.meshes) - 1
+    gseeds, sv = _vertex_seeds(spec, rng, meshes=set(range(n_sph)))
+    ntex = [m.texture.size for m in spec.meshes]
+    st = np.zeros((sum(ntex), 8))
+    st[:sum(ntex[:n_sph])] = rng.normal(size=(sum(ntex[:n_sph]), 8))
+    scene, T = to_torch_scene(spec, requires_grad={"verts", "tex"})
+    img = dr.PathIntegrator(gradient_terms=1, **kw).renderD(scene)[0]
+    img.backward(torch.tensor(dLdI, dtype=torch.float32, device="cuda"))
+    got = np.zeros(8)
+    for name, seed in gseeds.items():
+        g = T[name].grad.detach().cpu().numpy().astype(np.float64).reshape(-1)
+        got += g @ seed.reshape(g.shape[0], 8)
+    toff = 0
+    for i in range(n_sph):
+        g = T[f"tex{i}"].grad.detach().cpu().numpy().astype(np.float64).reshape(-1)
+        got += g @ st[toff:toff + ntex[i]]
+        toff += ntex[i]
+    ref = orc.grad_dir(spec, [dLdI], which=1, mode=0, seed_verts=sv, seed_tex=st, **kw)
+    err = np.abs(got - ref) / (np.abs(ref).max() + 1e-30)
+    print(f"large scene, 64x64 window: gpu {got[:3]} FP64 oracle {ref[:3]} max rel {err.max():.2e}")
+    assert np.abs(ref).max() > 0
+    assert err.max() < 1e-2

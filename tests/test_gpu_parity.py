@@ -249,3 +249,27 @@ def test_texture_gradient_vs_finite_differences(cuda):
     e = rel_l2(grad[pick], np.array(fd))
     print("texture grad rel L2 vs FD", e)
     assert e < 0.05
+
+
+def test_scene_validate_accepts_valid_and_names_bad_index(cuda):
+    """psdr_scene_validate, and psdr_scene_create, which runs the same check: a valid
+    description passes; one face index out of range is refused and named."""
+    spec = synth.sphere_scene(level=2, tex_hw=16, height=16, width=16)
+    scene, _ = to_torch_scene(spec)
+    lib = L.load()
+    sphere = scene.meshes[0]
+    md = (L.MeshDesc * 2)(*[m._desc() for m in scene.meshes])
+    ld = (L.AreaLightDesc * 1)(*[lt._desc() for lt in scene.lights])
+    desc = L.SceneDesc(md, 2, ld, 1)
+    assert lib.psdr_scene_validate(C.byref(desc), _stream()) == L.PSDR_OK
+    bad_faces = sphere.f.clone()
+    bad_faces.view(-1)[17] = sphere.v.shape[0]  # one past the last vertex
+    md[0].faces = bad_faces.data_ptr()
+    assert lib.psdr_scene_validate(C.byref(desc), _stream()) == L.PSDR_ERR_INVALID_ARG
+    assert b"mesh 0 face" in lib.psdr_last_error()
+    out = C.c_void_p()
+    assert lib.psdr_scene_create(C.byref(desc), _stream(), C.byref(out)) == L.PSDR_ERR_INVALID_ARG
+    assert b"mesh 0 face" in lib.psdr_last_error()
+    bad_faces.view(-1)[17] = -1
+    assert lib.psdr_scene_validate(C.byref(desc), _stream()) == L.PSDR_ERR_INVALID_ARG
+    torch.cuda.synchronize()

@@ -489,7 +489,7 @@ class PathIntegrator:
                  secondary_edge_preprocess_rounds: int = 1, primary_edge_hypercube_resolution: int = 10000,
                  secondary_edge_hypercube_resolution: List[int] = [10000, 6, 6], estimator: str = "reference",
                  seed: int = 0, tile_paths: int = 0, gradient_terms: int = 0,
-                 spp_pixel_boundary: Optional[int] = None):
+                 spp_pixel_boundary: Optional[int] = None, trace_queue: int = 0):
         """Path-space differentiable integrator (torch_psdr.py:477-536; path_integrator.h:8-21).
 
         B200 extensions: estimator ("reference" reproduces renderD exactly; "unbiased"
@@ -499,7 +499,8 @@ class PathIntegrator:
         (bitmask: 1 interior, 2 primary edges, 4 direct edges, 8 pixel borders; 0 = those
         four; 16 adds the unbiased estimator's DiffuseBsdfMaterial BRDF-jump term, on request),
         spp_pixel_boundary (unbiased: samples per unit pixel-border segment; default
-        spp_primary_edge).
+        spp_primary_edge), trace_queue (rays each SM traverses concurrently, in units of
+        128; 0 = 8, the autotuner picks it).
         """
         assert n_pass > 0
         assert spp_interior > 0
@@ -534,6 +535,8 @@ class PathIntegrator:
         cfg.spp_pixel_boundary = spp_primary_edge if spp_pixel_boundary is None else spp_pixel_boundary
         assert cfg.spp_pixel_boundary >= 0
         cfg.seed = seed
+        assert 0 <= trace_queue <= 8
+        cfg.trace_queue = trace_queue
         self.cfg = cfg
         self._lib = L.load()
         self._ws = None
@@ -595,10 +598,12 @@ class PathIntegrator:
         cams = scene._camera_descs()
         L.check(self._lib.psdr_autotune(scene.handle, self._workspace(), cams, len(cams), C.byref(self.cfg),
                                         C.byref(leaf), C.byref(ms), _stream()), "psdr_autotune")
-        return {"tile_paths": int(self.cfg.tile_paths), "leaf_size": int(leaf.value), "forward_ms": float(ms.value)}
+        return {"tile_paths": int(self.cfg.tile_paths), "leaf_size": int(leaf.value),
+                "trace_queue": int(self.cfg.trace_queue), "forward_ms": float(ms.value)}
 
     def _apply_tuning(self, scene: Scene, entry: dict) -> None:
         self.cfg.tile_paths = int(entry["tile_paths"])
+        self.cfg.trace_queue = int(entry.get("trace_queue", 0))
         L.check(self._lib.psdr_scene_set_leaf_size(scene.handle, int(entry["leaf_size"]), _stream()),
                 "psdr_scene_set_leaf_size")
 

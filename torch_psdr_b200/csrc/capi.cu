@@ -79,6 +79,7 @@ void check_cfg(const psdr_config* c) {
   PSDR_CHECK(c->estimator == PSDR_EST_REFERENCE || c->estimator == PSDR_EST_UNBIASED, "bad estimator");
   PSDR_CHECK(c->tile_paths >= 0, "tile_paths must be >= 0");
   PSDR_CHECK(c->spp_pixel_boundary >= 0, "spp_pixel_boundary must be >= 0");
+  PSDR_CHECK(c->trace_queue >= 0 && c->trace_queue <= 8, "trace_queue must be in [0, 8]");
 }
 
 void check_cams(const psdr_camera_desc* cams, int n) {
@@ -159,6 +160,57 @@ using namespace psdr;
     return PSDR_ERR_CUDA;                                                \
   }                                                                      \
   return PSDR_OK;
+
+// Every face index of a mesh or area light in [0, num_vertices), every uv index in
+// [0, num_uvs): one min/max reduction per index buffer and one host read. Throws
+// PSDR_ERR_INVALID_ARG naming the first buffer out of range.
+static void check_index_ranges(const psdr_scene_desc* desc, void* stream) {
+  PSDR_CHECK(desc != nullptr, "null argument");
+  PSDR_CHECK(desc->num_meshes >= 0 && desc->num_lights >= 0, "negative counts");
+  PSDR_CHECK(desc->num_meshes == 0 || desc->meshes != nullptr, "null mesh array");
+  PSDR_CHECK(desc->num_lights == 0 || desc->lights != nullptr, "null light array");
+  // (index buffer, entries, bound, what) of every mesh's faces and uv indices and every
+  // area light's faces; environment lights have no caller index buffers
+  struct Job { const int* p; long long n; int bound; std::string what; };
+  std::vector<Job> jobs;
+  for (int i = 0; i < desc->num_meshes; ++i) {
+    const psdr_mesh_desc& m = desc->meshes[i];
+    PSDR_CHECK(m.num_faces >= 0 && m.num_vertices >= 0 && m.num_uvs >= 0, "negative counts");
+    PSDR_CHECK(m.num_faces == 0 || m.faces != nullptr, "null face buffer");
+    jobs.push_back({m.faces, 3LL * m.num_faces, m.num_vertices, "mesh " + std::to_string(i) + " face"});
+    if (m.uvs != nullptr && m.uv_indices != nullptr)
+      jobs.push_back({m.uv_indices, 3LL * m.num_faces, m.num_uvs, "mesh " + std::to_string(i) + " uv"});
+  }
+  for (int l = 0; l < desc->num_lights; ++l) {
+    const psdr_area_light_desc& L = desc->lights[l];
+    if (L.type != PSDR_LIGHT_AREA) continue;
+    PSDR_CHECK(L.num_faces >= 0 && L.num_vertices >= 0, "negative counts");
+    PSDR_CHECK(L.num_faces == 0 || L.faces != nullptr, "null face buffer");
+    jobs.push_back({L.faces, 3LL * L.num_faces, L.num_vertices, "light " + std::to_string(l) + " face"});
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int k = (int)jobs.size();
+  if (k == 0) return;
+  DBuf range;
+  range.alloc(sizeof(int) * 2 * k, st);
+  std::vector<int> h(2 * k);
+  for (int j = 0; j < k; ++j) { h[2 * j] = INT_MAX; h[2 * j + 1] = INT_MIN; }
+  PSDR_CUDA(cudaMemcpyAsync(range.p, h.data(), sizeof(int) * 2 * k, cudaMemcpyHostToDevice, st));
+  for (int j = 0; j < k; ++j) {
+    if (jobs[j].n == 0) continue;
+    const int blocks = (int)std::min<long long>((jobs[j].n + 255) / 256, 148LL * 8);
+    k_index_range<<<blocks, 256, 0, st>>>(jobs[j].p, jobs[j].n, range.as<int>() + 2 * j);
+  }
+  PSDR_CUDA(cudaGetLastError());
+  PSDR_CUDA(cudaMemcpyAsync(h.data(), range.p, sizeof(int) * 2 * k, cudaMemcpyDeviceToHost, st));
+  PSDR_CUDA(cudaStreamSynchronize(st));
+  for (int j = 0; j < k; ++j) {
+    if (jobs[j].n == 0) continue;
+    PSDR_CHECK(h[2 * j] >= 0 && h[2 * j + 1] < jobs[j].bound,
+               jobs[j].what + " indices must lie in [0, " + std::to_string(jobs[j].bound) + "): found [" +
+                   std::to_string(h[2 * j]) + ", " + std::to_string(h[2 * j + 1]) + "]");
+  }
+}
 
 extern "C" {
 
@@ -324,6 +376,8 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
       s->h_lights.push_back(L);
     }
     s->dev.ltri_base = nl > 0 ? s->obj_tri_off[nm] : 0;
+    // the build gathers vertices and uvs through the index buffers: check them first
+    check_index_ranges(desc, stream);
     psdr_scene_alloc(s);
     // fp64 gradient accumulators live with the scene
     cudaStream_t st = s->stream;
@@ -358,51 +412,7 @@ psdr_status psdr_scene_create(const psdr_scene_desc* desc, void* stream, psdr_sc
 
 psdr_status psdr_scene_validate(const psdr_scene_desc* desc, void* stream) {
   API_BEGIN
-  PSDR_CHECK(desc != nullptr, "null argument");
-  PSDR_CHECK(desc->num_meshes >= 0 && desc->num_lights >= 0, "negative counts");
-  PSDR_CHECK(desc->num_meshes == 0 || desc->meshes != nullptr, "null mesh array");
-  PSDR_CHECK(desc->num_lights == 0 || desc->lights != nullptr, "null light array");
-  // (index buffer, entries, bound, what) of every mesh's faces and uv indices and every
-  // area light's faces; environment lights have no caller index buffers
-  struct Job { const int* p; long long n; int bound; std::string what; };
-  std::vector<Job> jobs;
-  for (int i = 0; i < desc->num_meshes; ++i) {
-    const psdr_mesh_desc& m = desc->meshes[i];
-    PSDR_CHECK(m.num_faces >= 0 && m.num_vertices >= 0 && m.num_uvs >= 0, "negative counts");
-    PSDR_CHECK(m.num_faces == 0 || m.faces != nullptr, "null face buffer");
-    jobs.push_back({m.faces, 3LL * m.num_faces, m.num_vertices, "mesh " + std::to_string(i) + " face"});
-    if (m.uvs != nullptr && m.uv_indices != nullptr)
-      jobs.push_back({m.uv_indices, 3LL * m.num_faces, m.num_uvs, "mesh " + std::to_string(i) + " uv"});
-  }
-  for (int l = 0; l < desc->num_lights; ++l) {
-    const psdr_area_light_desc& L = desc->lights[l];
-    if (L.type != PSDR_LIGHT_AREA) continue;
-    PSDR_CHECK(L.num_faces >= 0 && L.num_vertices >= 0, "negative counts");
-    PSDR_CHECK(L.num_faces == 0 || L.faces != nullptr, "null face buffer");
-    jobs.push_back({L.faces, 3LL * L.num_faces, L.num_vertices, "light " + std::to_string(l) + " face"});
-  }
-  cudaStream_t st = (cudaStream_t)stream;
-  const int k = (int)jobs.size();
-  if (k == 0) return PSDR_OK;
-  DBuf range;
-  range.alloc(sizeof(int) * 2 * k, st);
-  std::vector<int> h(2 * k);
-  for (int j = 0; j < k; ++j) { h[2 * j] = INT_MAX; h[2 * j + 1] = INT_MIN; }
-  PSDR_CUDA(cudaMemcpyAsync(range.p, h.data(), sizeof(int) * 2 * k, cudaMemcpyHostToDevice, st));
-  for (int j = 0; j < k; ++j) {
-    if (jobs[j].n == 0) continue;
-    const int blocks = (int)std::min<long long>((jobs[j].n + 255) / 256, 148LL * 8);
-    k_index_range<<<blocks, 256, 0, st>>>(jobs[j].p, jobs[j].n, range.as<int>() + 2 * j);
-  }
-  PSDR_CUDA(cudaGetLastError());
-  PSDR_CUDA(cudaMemcpyAsync(h.data(), range.p, sizeof(int) * 2 * k, cudaMemcpyDeviceToHost, st));
-  PSDR_CUDA(cudaStreamSynchronize(st));
-  for (int j = 0; j < k; ++j) {
-    if (jobs[j].n == 0) continue;
-    PSDR_CHECK(h[2 * j] >= 0 && h[2 * j + 1] < jobs[j].bound,
-               jobs[j].what + " indices must lie in [0, " + std::to_string(jobs[j].bound) + "): found [" +
-                   std::to_string(h[2 * j]) + ", " + std::to_string(h[2 * j + 1]) + "]");
-  }
+  check_index_ranges(desc, stream);
   API_END
 }
 
@@ -553,14 +563,17 @@ psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_came
   cudaEvent_t e0 = ev0.e, e1 = ev1.e;
   const int leaves[3] = {1, 2, 4};
   const int tiles[4] = {1 << 18, 1 << 19, 1 << 20, 1 << 21};
+  const int queues[3] = {4, 6, 8};
   float best = INFINITY;
-  int bl = scene->leaf_size, bt = cfg->tile_paths;
+  int bl = scene->leaf_size, bt = cfg->tile_paths, bq = cfg->trace_queue;
   for (int leaf : leaves) {
     scene->leaf_size = leaf;
     scene_build_geometry(scene, st);
-    for (int tile : tiles) {
+    for (int trial = 0; trial < 12; ++trial) {
+      const int tile = tiles[trial % 4], queue = queues[trial / 4];
       psdr_config c = *cfg;
       c.tile_paths = tile;
+      c.trace_queue = queue;
       std::vector<DevView> v = views;
       render_forward_impl(dev_scene(scene), v, c, ws, st, nullptr);  // warm-up, sizes the workspace
       PSDR_CUDA(cudaEventRecord(e0, st));
@@ -570,13 +583,14 @@ psdr_status psdr_autotune(psdr_scene* scene, psdr_workspace* ws, const psdr_came
       float ms = 0.f;
       PSDR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       ms *= 0.5f;
-      if (ms < best) { best = ms; bl = leaf; bt = tile; }
+      if (ms < best) { best = ms; bl = leaf; bt = tile; bq = queue; }
     }
   }
   scene->leaf_size = bl;
   scene_build_geometry(scene, st);
   PSDR_CUDA(cudaStreamSynchronize(st));
   cfg->tile_paths = bt;
+  cfg->trace_queue = bq;
   if (best_leaf) *best_leaf = bl;
   if (best_ms) *best_ms = best;
   API_END

@@ -2493,7 +2493,7 @@ static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int 
       else k_shade<MODE_FWD, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
     }
     pf.begin_trace(st);
-    k_trace<<<num_sms() * 8, 128, 0, st>>>(w, scenes, views, d, pf.on ? pf.d_rays : nullptr);
+    k_trace<<<num_sms() * w.trace_bps, 128, 0, st>>>(w, scenes, views, d, pf.on ? pf.d_rays : nullptr);
     pf.end_trace(st);
     PSDR_LAUNCHED(3);
     if (w.bsdf) {
@@ -2602,6 +2602,7 @@ void set_wf(WF& w, const psdr_config& cfg, int nviews, int nB_override, int ligh
   // stream index): jobs of different seeds draw from disjoint stream ranges
   w.seed = cfg.seed * 2654435761ull;
   w.rec_stride = 1 + w.D * w.R + 2 * w.D;  // primary hit, hits per depth, (C, beta) per depth
+  w.trace_bps = cfg.trace_queue > 0 ? cfg.trace_queue : 8;
 }
 
 // Forward: the interior estimate of every view into V.image (and per-sample radiance

@@ -49,6 +49,7 @@ struct WF {
   int rec_stride;
   int bsdf;      // host side: launch the extended kernel instances (DiffuseBsdfMaterial, environment light)
   int ortho;     // host side: an orthographic view is in the job (camera kernel instance)
+  int trace_bps; // host side: blocks of 128 rays per SM of the closest-hit kernel (queue depth)
 };
 
 struct Tile {
