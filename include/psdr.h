@@ -128,9 +128,11 @@ typedef struct {
   int32_t tile_paths;
   int32_t leaf_size;
   int32_t terms;  /* gradient terms of psdr_render_bwd: bit 0 interior, bit 1 primary
-                     edges, bit 2 direct edges, bit 3 pixel borders (UNBIASED only);
-                     0 = those four. Bit 4: BRDF jumps of DiffuseBsdfMaterial
-                     (UNBIASED only, on request: not part of 0) */
+                     edges, bit 2 direct edges, bit 3 pixel borders (UNBIASED only),
+                     bit 5 interpenetration creases (UNBIASED only, perspective views:
+                     the curves where two meshes cut into each other); 0 = all of these.
+                     Bit 4: BRDF jumps of DiffuseBsdfMaterial (UNBIASED only, on
+                     request: not part of 0) */
   int32_t spp_pixel_boundary; /* UNBIASED: samples per unit pixel-border segment */
   uint64_t seed;
   int32_t trace_queue; /* ABI 5: rays each SM traverses concurrently in the wavefront

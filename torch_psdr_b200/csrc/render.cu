@@ -1775,6 +1775,331 @@ __global__ void k_lens_out(const GradAcc* __restrict__ acc, LensChain ch, float*
   }
 }
 
+// ------------------------------------------------------------------ interpenetration creases
+// Unbiased estimator: where the surfaces of two different meshes cut into each other (a
+// noisy icosphere sunk into the ground), the visible surface switches from one mesh to the
+// other along their intersection curve. That curve is not a mesh edge, so neither the
+// silhouette nor the shadow-boundary samples see it; it moves when either mesh moves. Its
+// term (primary visibility): with surface 1 seen on one side of the projected curve and
+// surface 2 on the other, n the raster normal from 1 to 2, the image changes by
+//   Int_curve g [L1 (v_c - v_1) - L2 (v_c - v_2)] . n dl
+// (raster velocities: v_c of the curve, v_k of surface k's material point at it). With
+// J = d(raster)/d(world), w = J^T n, c = n1.n2 and the curve's world velocity taken in the
+// plane of the two normals (it stays on both surfaces), the adjoint of surface k's material
+// point is K [(G1 - G2) A_k n_k -+ G_k w] (minus for 1), A_1 = (w.n1 - c w.n2) / (1 - c^2),
+// A_2 = (w.n2 - c w.n1) / (1 - c^2), G_k = g . L_k, K = raster length per sample.
+constexpr int kCreaseCap = 16384;          // intersection segments kept per scene
+constexpr int kCreaseSamplesPerSpp = 16384;  // crease samples per primary-edge spp
+constexpr unsigned long long kCreaseStream = 0xC0000000ull;  // sampler streams of the crease samples
+
+struct CreaseBuf {
+  float4* a;   // segment start xyz, length
+  float4* b;   // segment end xyz, -
+  int2* tris;  // the two triangles (different meshes)
+  int* count;  // segments found (may exceed kCreaseCap: the rest are dropped)
+};
+
+// The segment where triangles a and b cross (false when they do not, or are coplanar).
+// Double precision; a vertex exactly on the other plane counts as on its positive side.
+PSDR_D bool tri_tri_segment(const double3* A, const double3* B, double3& s0, double3& s1) {
+  auto sub = [](double3 p, double3 q) { return make_double3(p.x - q.x, p.y - q.y, p.z - q.z); };
+  auto dotd = [](double3 p, double3 q) { return p.x * q.x + p.y * q.y + p.z * q.z; };
+  auto crs = [](double3 p, double3 q) {
+    return make_double3(p.y * q.z - p.z * q.y, p.z * q.x - p.x * q.z, p.x * q.y - p.y * q.x);
+  };
+  // the two points where triangle T's edges cross the plane (n, d); false if none
+  auto cut = [&](const double3* T, double3 n, double d, double3& p, double3& q) {
+    double s[3];
+    for (int k = 0; k < 3; ++k) s[k] = dotd(n, T[k]) + d;
+    const bool pos0 = s[0] >= 0.0, pos1 = s[1] >= 0.0, pos2 = s[2] >= 0.0;
+    if (pos0 == pos1 && pos1 == pos2) return false;
+    // the lone vertex on its side
+    const int k = (pos0 != pos1 && pos0 != pos2) ? 0 : (pos1 != pos0 && pos1 != pos2) ? 1 : 2;
+    const int i = (k + 1) % 3, j = (k + 2) % 3;
+    const double ti = s[k] / (s[k] - s[i]), tj = s[k] / (s[k] - s[j]);
+    p = make_double3(T[k].x + (T[i].x - T[k].x) * ti, T[k].y + (T[i].y - T[k].y) * ti, T[k].z + (T[i].z - T[k].z) * ti);
+    q = make_double3(T[k].x + (T[j].x - T[k].x) * tj, T[k].y + (T[j].y - T[k].y) * tj, T[k].z + (T[j].z - T[k].z) * tj);
+    return true;
+  };
+  const double3 na = crs(sub(A[1], A[0]), sub(A[2], A[0])), nb = crs(sub(B[1], B[0]), sub(B[2], B[0]));
+  const double3 D = crs(na, nb);
+  const double dd = dotd(D, D);
+  if (!(dd > 1e-30 * dotd(na, na) * dotd(nb, nb))) return false;
+  double3 pa, qa, pb, qb;
+  if (!cut(A, nb, -dotd(nb, B[0]), pa, qa) || !cut(B, na, -dotd(na, A[0]), pb, qb)) return false;
+  double ta0 = dotd(pa, D), ta1 = dotd(qa, D), tb0 = dotd(pb, D), tb1 = dotd(qb, D);
+  if (ta0 > ta1) { const double t = ta0; ta0 = ta1; ta1 = t; const double3 x = pa; pa = qa; qa = x; }
+  if (tb0 > tb1) { const double t = tb0; tb0 = tb1; tb1 = t; const double3 x = pb; pb = qb; qb = x; }
+  const double lo = fmax(ta0, tb0), hi = fmin(ta1, tb1);
+  if (!(lo < hi)) return false;
+  s0 = ta0 >= tb0 ? pa : pb;
+  s1 = ta1 <= tb1 ? qa : qb;
+  return true;
+}
+
+// One thread per triangle of a mesh: the LBVH is walked with the triangle's box, and every
+// triangle of a later mesh (lights excluded) that it crosses adds one segment.
+__global__ void __launch_bounds__(128) k_crease_pairs(const DevScene* __restrict__ scenes, int si, CreaseBuf cb) {
+  const DevScene& sc = scenes[si];
+  const int nmesh = sc.nobj - sc.nlight;
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < sc.ntri; t += stride) {
+    const int4 tv = __ldg(sc.tri_v + t);
+    if (tv.w >= nmesh || sc.root == 0x7fffffff) continue;
+    const float4* R = sc.tri + 6 * (size_t)t;
+    const float3 p0 = xyz(__ldg(R)), p1 = xyz(__ldg(R + 1)), p2 = xyz(__ldg(R + 2));
+    const float3 lo = f3(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)), fminf(p0.z, fminf(p1.z, p2.z)));
+    const float3 hi = f3(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)), fmaxf(p0.z, fmaxf(p1.z, p2.z)));
+    const double3 A[3] = {make_double3(p0.x, p0.y, p0.z), make_double3(p1.x, p1.y, p1.z), make_double3(p2.x, p2.y, p2.z)};
+    int stack[64];
+    int sp = 0;
+    int node = sc.root;
+    while (true) {
+      if (node >= 0) {
+        const float4* nd = sc.nodes + 7 * (size_t)node;
+        const float4 lx = __ldg(nd), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
+        const float4 lz = __ldg(nd + 4), hz = __ldg(nd + 5);
+        const int4 e = __ldg(reinterpret_cast<const int4*>(nd + 6));
+        const float clx[4] = {lx.x, lx.y, lx.z, lx.w}, chx[4] = {hx.x, hx.y, hx.z, hx.w};
+        const float cly[4] = {ly.x, ly.y, ly.z, ly.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w};
+        const float clz[4] = {lz.x, lz.y, lz.z, lz.w}, chz[4] = {hz.x, hz.y, hz.z, hz.w};
+        const int ch[4] = {e.x, e.y, e.z, e.w};
+        for (int c = 0; c < 4; ++c) {
+          if (ch[c] == 0x7fffffff) continue;
+          if (clx[c] > hi.x || chx[c] < lo.x || cly[c] > hi.y || chy[c] < lo.y || clz[c] > hi.z || chz[c] < lo.z)
+            continue;
+          if (sp < 64) stack[sp++] = ch[c];
+          else atomicOr(sc.err, 1);
+        }
+      } else {
+        const int code = ~node;
+        const int first = code >> 3, cnt = (code & 7) + 1;
+        for (int k = 0; k < cnt; ++k) {
+          const float4* lt = sc.leaf + 3 * (size_t)(first + k);
+          const float4 q0 = __ldg(lt), q1 = __ldg(lt + 1), q2 = __ldg(lt + 2);
+          const int u = __float_as_int(q0.w);
+          const int ou = __ldg(sc.tri_v + u).w;
+          if (ou <= tv.w || ou >= nmesh) continue;
+          const double3 B[3] = {make_double3(q0.x, q0.y, q0.z), make_double3(q1.x, q1.y, q1.z),
+                                make_double3(q2.x, q2.y, q2.z)};
+          double3 s0, s1;
+          if (!tri_tri_segment(A, B, s0, s1)) continue;
+          const double len = sqrt((s1.x - s0.x) * (s1.x - s0.x) + (s1.y - s0.y) * (s1.y - s0.y) +
+                                  (s1.z - s0.z) * (s1.z - s0.z));
+          if (!(len > 0.0)) continue;
+          const int slot = atomicAdd(cb.count, 1);
+          if (slot >= kCreaseCap) continue;
+          cb.a[slot] = make_float4((float)s0.x, (float)s0.y, (float)s0.z, (float)len);
+          cb.b[slot] = make_float4((float)s1.x, (float)s1.y, (float)s1.z, 0.f);
+          cb.tris[slot] = make_int2(t, u);
+        }
+      }
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  }
+}
+
+// Segment lengths (0 past the segments found) as the masses of the length CDF.
+__global__ void k_crease_mass(CreaseBuf cb, double* __restrict__ w) {
+  const int n = min(*cb.count, kCreaseCap);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kCreaseCap; i += gridDim.x * blockDim.x)
+    w[i] = i < n ? (double)cb.a[i].w : 0.0;
+}
+
+// World-space gradients of the raster coordinates (J's rows) at camera-space point pc.
+PSDR_D void raster_grad(const DevView& V, float3 pc, float3& gx, float3& gy) {
+  const float* m = V.c2r;
+  const float* r = V.w2c;
+  const float wden = m[12] * pc.x + m[13] * pc.y + m[14] * pc.z + m[15];
+  float3 g[2];
+  for (int c = 0; c < 2; ++c) {
+    const float u = (m[4 * c] * pc.x + m[4 * c + 1] * pc.y + m[4 * c + 2] * pc.z + m[4 * c + 3]) / wden;
+    const float3 gpc = f3(m[4 * c] - u * m[12], m[4 * c + 1] - u * m[13], m[4 * c + 2] - u * m[14]) / wden;
+    g[c] = f3(r[0] * gpc.x + r[4] * gpc.y + r[8] * gpc.z, r[1] * gpc.x + r[5] * gpc.y + r[9] * gpc.z,
+              r[2] * gpc.x + r[6] * gpc.y + r[10] * gpc.z);
+  }
+  gx = g[0];
+  gy = g[1];
+}
+
+// Crease point of sample i (stratified by length over all segments) and its projection.
+struct CreasePt {
+  float3 x, tang;
+  float2 u;     // raster position
+  float2 n;     // unit raster normal of the projected curve
+  float rlen;   // raster length per unit world length along the curve
+  float wgt;    // world length per sample (total length / N)
+  int seg;
+  bool ok;
+};
+
+PSDR_D CreasePt crease_point(const DevView& V, CreaseBuf cb, const double* mw, const double* mpre, long long i,
+                             long long N, float xi) {
+  CreasePt c;
+  c.ok = false;
+  if (!(mpre[kCreaseCap - 1] > 0.0)) return c;
+  float t;
+  double pmf;
+  c.seg = (int)border_locate(mw, mpre, kCreaseCap, i, N, xi, t, pmf);
+  if (!(pmf > 0.0)) return c;
+  const float4 a = cb.a[c.seg], b = cb.b[c.seg];
+  const float3 s0 = xyz(a), s1 = xyz(b);
+  c.x = s0 + (s1 - s0) * t;
+  c.tang = (s1 - s0) * (1.f / a.w);
+  c.wgt = (float)(mw[c.seg] / (pmf * (double)N));
+  float3 pc, pr;
+  xform_pos(V.w2c, c.x, pc);
+  xform_pos(V.c2r, pc, pr);
+  if (!(pc.z < 0.f && pr.x > 0.f && pr.x < (float)V.W && pr.y > 0.f && pr.y < (float)V.H)) return c;
+  c.u = make_float2(pr.x, pr.y);
+  float3 gx, gy;
+  raster_grad(V, pc, gx, gy);
+  const float mx = dot(gx, c.tang), my = dot(gy, c.tang);
+  c.rlen = sqrtf(mx * mx + my * my);
+  if (!(c.rlen > 0.f)) return c;
+  c.n = make_float2(-my / c.rlen, mx / c.rlen);
+  c.ok = true;
+  return c;
+}
+
+// Offset rays on both sides of the projected curve; both must reach the two meshes next to
+// the crease point (else something hides it). Paths from both hits give L1 and L2 (slots
+// 2s: the -n side, surface 1; 2s + 1: the +n side, surface 2).
+constexpr float kCreaseOffset = 0.01f;  // pixels
+__global__ void __launch_bounds__(256) k_crease_init(WF w, const DevScene* __restrict__ scenes,
+                                                     const DevView* __restrict__ views, int v, EdgeBuf eb,
+                                                     CreaseBuf cb, const double* __restrict__ mw,
+                                                     const double* __restrict__ mpre, long long begin, int n,
+                                                     long long N) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool alive = false;
+    HitRec hs[2];
+    hs[0].tri = hs[1].tri = -1;
+    const DevView& V = views[v];
+    if (s < n && !V.ortho) {
+      const long long i = begin + s;
+      const DevScene& sc = scenes[V.scene];
+      Rng rng = make_rng(kCreaseStream + (unsigned long long)i + w.seed);
+      const CreasePt c = crease_point(V, cb, mw, mpre, i, N, rng.next_float());
+      bool ok = c.ok;
+      int flag = 0;
+      if (ok) {
+        const int2 tp = cb.tris[c.seg];
+        const int oa = __ldg(sc.tri_v + tp.x).w, ob = __ldg(sc.tri_v + tp.y).w;
+        const float tol = 1e-3f * norm(c.x - V.pos) + 1e-4f;
+        int objs[2];
+        for (int side = 0; side < 2; ++side) {
+          const float sg = side ? kCreaseOffset : -kCreaseOffset;
+          float3 pcam;
+          xform_pos(V.r2c, f3(c.u.x + sg * c.n.x, c.u.y + sg * c.n.y, 1.0f), pcam);
+          const float3 d = normalize(xform_dir(V.c2w, pcam));
+          hs[side] = trace_closest(sc, V.pos, d, kTmin, INFINITY);
+          objs[side] = -1;
+          if (hs[side].tri >= 0) {
+            const Surf x = make_surf(sc, hs[side].tri, hs[side].b1, hs[side].b2, V.pos);
+            if (norm(x.p - c.x) < tol) objs[side] = x.obj;
+          }
+        }
+        ok = objs[0] >= 0 && objs[1] >= 0 && objs[0] != objs[1] && (objs[0] == oa || objs[0] == ob) &&
+             (objs[1] == oa || objs[1] == ob);
+        flag = ok ? (objs[0] == oa ? 1 : 2) : 0;  // 1: surface 1 is the segment's first triangle
+      }
+      const int px = ok ? min(V.W - 1, (int)floorf(c.u.x)) : 0, py = ok ? min(V.H - 1, (int)floorf(c.u.y)) : 0;
+      eb.a[s] = make_float4(__int_as_float(c.seg), c.wgt * c.rlen, c.n.x, c.n.y);
+      eb.n[s] = make_float4(c.x.x, c.x.y, c.x.z, __int_as_float(py * V.W + px));
+      eb.hb[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(flag));
+      for (int side = 0; side < 2; ++side) {
+        const int slot = 2 * s + side;
+        const Rng r = make_rng(kCreaseStream + 0x10000000ull + 2 * (unsigned long long)i + side + w.seed);
+        w.rs[slot] = r.state;
+        w.ri[slot] = r.inc;
+        w.view[slot] = v;
+        w.pix[slot] = -1;
+        w.T[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+        w.L[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+        w.cur[slot] = hit4(hs[side]);
+        w.org[slot] = make_float4(V.pos.x, V.pos.y, V.pos.z, 0.f);
+      }
+      alive = ok;
+    }
+    for (int side = 0; side < 2; ++side) {
+      const int k = warp_append(&w.cnt[0], alive);
+      if (alive) w.q0[k] = 2 * s + side;
+    }
+  }
+}
+
+// Barycentric weights of point x in triangle tri (of its vertices v0, v1, v2).
+PSDR_D float3 bary_of(const DevScene& sc, int tri, float3 x) {
+  const float4* R = sc.tri + 6 * (size_t)tri;
+  const float3 p0 = xyz(__ldg(R)), p1 = xyz(__ldg(R + 1)), p2 = xyz(__ldg(R + 2));
+  const float3 e1 = p1 - p0, e2 = p2 - p0, q = x - p0;
+  const float d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2), q1 = dot(q, e1), q2 = dot(q, e2);
+  const float den = d11 * d22 - d12 * d12;
+  const float b1 = (d22 * q1 - d12 * q2) / den, b2 = (d11 * q2 - d12 * q1) / den;
+  return f3(1.f - b1 - b2, b1, b2);
+}
+
+__global__ void __launch_bounds__(256) k_crease_final(WF w, const DevScene* __restrict__ scenes,
+                                                      const DevView* __restrict__ views, int v, EdgeBuf eb,
+                                                      CreaseBuf cb, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  float3 go = f3(0.f, 0.f, 0.f);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    if (s >= n || !V.dimage) continue;
+    const int flag = __float_as_int(eb.hb[s].w);
+    if (flag == 0) continue;
+    const float4 a = eb.a[s], xn = eb.n[s];
+    const float* gp = V.dimage + 3 * (size_t)__float_as_int(xn.w);
+    const float3 L1 = xyz(w.L[2 * s]), L2 = xyz(w.L[2 * s + 1]);
+    const float G1 = gp[0] * L1.x + gp[1] * L1.y + gp[2] * L1.z, G2 = gp[0] * L2.x + gp[1] * L2.y + gp[2] * L2.z;
+    if (!isfinite(G1) || !isfinite(G2) || (G1 == 0.f && G2 == 0.f)) continue;
+    const int2 tp = cb.tris[__float_as_int(a.x)];
+    const int t1 = flag == 1 ? tp.x : tp.y, t2 = flag == 1 ? tp.y : tp.x;
+    const float3 x = xyz(xn);
+    const float3 n1 = normalize(xyz(__ldg(sc.tri + 6 * (size_t)t1 + 3)));
+    const float3 n2 = normalize(xyz(__ldg(sc.tri + 6 * (size_t)t2 + 3)));
+    float3 pc, gx, gy;
+    xform_pos(V.w2c, x, pc);
+    raster_grad(V, pc, gx, gy);
+    const float3 wv = gx * a.z + gy * a.w;  // J^T n
+    const float c = dot(n1, n2), sn2 = 1.f - c * c;
+    if (!(sn2 > 1e-6f)) continue;
+    const float w1 = dot(wv, n1), w2 = dot(wv, n2);
+    const float A1 = (w1 - c * w2) / sn2, A2 = (w2 - c * w1) / sn2;
+    const float K = a.y;
+    const float3 a1 = (n1 * ((G1 - G2) * A1) - wv * G1) * K;
+    const float3 a2 = (n2 * ((G1 - G2) * A2) + wv * G2) * K;
+    if (!finite3(a1) || !finite3(a2)) continue;
+    if (sc.grad_verts) {
+      const float3 b1 = bary_of(sc, t1, x), b2 = bary_of(sc, t2, x);
+      const int4 v1 = __ldg(sc.tri_v + t1), v2 = __ldg(sc.tri_v + t2);
+      vert_add(sc, v1.x, a1 * b1.x);
+      vert_add(sc, v1.y, a1 * b1.y);
+      vert_add(sc, v1.z, a1 * b1.z);
+      vert_add(sc, v2.x, a2 * b2.x);
+      vert_add(sc, v2.y, a2 * b2.y);
+      vert_add(sc, v2.z, a2 * b2.z);
+    }
+    go -= a1 + a2;  // moving the camera by d is moving both surfaces by -d
+  }
+  if (V.grad_pos) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      go.x += __shfl_xor_sync(0xffffffffu, go.x, o);
+      go.y += __shfl_xor_sync(0xffffffffu, go.y, o);
+      go.z += __shfl_xor_sync(0xffffffffu, go.z, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (go.x != 0.f || go.y != 0.f || go.z != 0.f)) atomic_add3(V.grad_pos, go);
+  }
+}
+
 // ------------------------------------------------------------------ BSDF jumps
 // Unbiased estimator, DiffuseBsdfMaterial with roughness > 0 (diffuse_bsdf.cc:56-88).
 // With N.L >= 0 and N.V >= 0 the rough-diffuse value jumps by color b (max(N.L, N.V) +
@@ -2679,6 +3004,30 @@ static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v,
   PSDR_CUDA(cudaGetLastError());
 }
 
+// Interpenetration-crease samples [begin, begin + n) of the N of view v: two paths per
+// sample (slots 2s, 2s + 1), so n is at most half the tile.
+static void crease_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
+                         const CreaseBuf& cb, const double* mw, const double* mpre, long long begin, int n,
+                         long long N, cudaStream_t st) {
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  k_crease_init<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, cb, mw, mpre, begin, n, N);
+  PSDR_LAUNCHED(1);
+  depth_loop(w, scenes, vd, MODE_FWD, st);
+  k_crease_final<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, cb, n);
+  PSDR_LAUNCHED(1);
+  PSDR_CUDA(cudaGetLastError());
+}
+
+static CreaseBuf crease_buf(psdr_workspace* ws) {
+  unsigned char* p = ws->crease.as<unsigned char>();
+  CreaseBuf cb;
+  cb.a = reinterpret_cast<float4*>(p);
+  cb.b = reinterpret_cast<float4*>(p + 16 * (size_t)kCreaseCap);
+  cb.tris = reinterpret_cast<int2*>(p + 32 * (size_t)kCreaseCap);
+  cb.count = reinterpret_cast<int*>(p + 40 * (size_t)kCreaseCap);
+  return cb;
+}
+
 // BSDF-jump samples [begin, begin + n) of view v at depth k (1 <= k <= D): the arc
 // paths run D - k bounces (none at k = D, where only a light seen along the arc counts).
 static void jump_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb, long long begin,
@@ -2704,9 +3053,10 @@ long long border_segments(const DevView& V) {
 
 void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector<DevView>& views, cudaStream_t st) {
   if (cfg.estimator != PSDR_EST_UNBIASED) return;
-  long long s = 0;
+  long long s = kCreaseCap;
   for (const DevView& v : views) s = std::max(s, border_segments(v));
   ws->ensure_mass(s, st);
+  ws->crease.alloc(40 * (size_t)kCreaseCap + 256, st);
 }
 
 static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, bool floor, cudaStream_t st) {
@@ -2757,7 +3107,7 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
                      int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
   const DevView* vd = ws->views.as<DevView>();
   const bool unb = cfg.estimator == PSDR_EST_UNBIASED;
-  const int terms = cfg.terms ? cfg.terms : (unb ? 15 : 7);
+  const int terms = cfg.terms ? cfg.terms : (unb ? 47 : 7);
   bool lens = false;  // a view wants the camera-lens gradient
   for (const DevView& V : views) lens = lens || V.grad_lens != nullptr;
   // ---- interior
@@ -2857,6 +3207,22 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       for (long long b0 = 0; b0 < N; b0 += cap)
         border_phase(wi, scenes_dev, vd, v, eb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), S, b0,
                      (int)std::min<long long>(cap, N - b0), N, V.grad_lens != nullptr, st);
+    }
+    // interpenetration creases (unbiased estimator, perspective views): the segments where
+    // two meshes cross, a length CDF over them, then the samples
+    if (unb && (terms & 32) && V.dimage && !V.ortho) {
+      const CreaseBuf cb = crease_buf(ws);
+      PSDR_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int), st));
+      k_crease_pairs<<<num_sms() * 4, 128, 0, st>>>(scenes_dev, V.scene, cb);
+      k_crease_mass<<<kCreaseCap / 256, 256, 0, st>>>(cb, ws->mass_d.as<double>());
+      PSDR_LAUNCHED(2);
+      inclusive_scan_double(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), kCreaseCap,
+                            ws->scan_tmp.as<double>(), st);
+      const long long N = (long long)cfg.spp_primary_edge * kCreaseSamplesPerSpp;
+      const int chunk = cap / 2;
+      for (long long b0 = 0; b0 < N; b0 += chunk)
+        crease_phase(wi, scenes_dev, vd, v, eb, cb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), b0,
+                     (int)std::min<long long>(chunk, N - b0), N, st);
     }
     // BSDF jumps (unbiased estimator, DiffuseBsdfMaterial scenes; on request only)
     if (unb && (terms & 16) && gi.bsdf && V.dimage) {

@@ -79,6 +79,7 @@ struct psdr_workspace {
   psdr::DBuf rs, ri, view, pix, T, L, cur, org, q0, q1, qs, cnt, ro, rd, ra, hit, rec;
   psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
   psdr::DBuf campos_acc, lens_acc;
+  psdr::DBuf crease;  // interpenetration segments (unbiased estimator): kCreaseCap records + count
   long long mass_cap = 0;
   // a DiffuseBsdfMaterial mesh or an environment light is in the scenes of the current job
   // (each entry point sets it; the extended kernel instances also handle the plain
