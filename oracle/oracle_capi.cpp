@@ -87,7 +87,7 @@ inline V3<S> interior_sample(const Ctx<S, AD>& c, uint64_t i, int& pix, bool& va
   using R = typename Traits<S>::R;
   const int W = c.cam.W;
   const int spp = c.cfg.spp_interior;
-  Pcg32 rng = make_sampler(i);
+  Pcg32 rng = make_sampler(i + c.cfg.seed * 2654435761ull);
   R jx = rng.next_float(), jy = rng.next_float();
   pix = spp > 1 ? int(i / (uint64_t)spp) : int(i);
   int x = pix % W, y = pix / W;
@@ -509,7 +509,7 @@ inline void pixel_border_sample(const Ctx<S, AD>& c, const Border& B, uint64_t i
   using R = typename Traits<S>::R;
   if constexpr (AD) {
     constexpr int KD = sizeof(S) / sizeof(double) - 1;
-    Pcg32 rng = make_sampler(i);
+    Pcg32 rng = make_sampler(i + c.cfg.seed * 2654435761ull);
     const float xi = rng.next_float();
     float t;
     double pmf;
@@ -582,7 +582,7 @@ inline void bsdf_jump_sample(const Ctx<S, AD>& c, uint64_t i, const double* dLdI
     constexpr int KD = sizeof(S) / sizeof(double) - 1;
     const int W = c.cam.W, spp = c.cfg.spp_interior, D = c.cfg.max_bounce;
     const int nL = c.cfg.mis_light_samples, nB = c.cfg.mis_bsdf_samples;
-    Pcg32 rng = make_sampler(i);
+    Pcg32 rng = make_sampler(i + c.cfg.seed * 2654435761ull);
     R jx = rng.next_float(), jy = rng.next_float();
     const int pix = spp > 1 ? int(i / (uint64_t)spp) : int(i);
     V3<R> fp(jx + R(pix % W), jy + R(pix / W), R(1));
@@ -617,7 +617,7 @@ inline void bsdf_jump_sample(const Ctx<S, AD>& c, uint64_t i, const double* dLdI
         if (nx.valid) {
           if (nx.is_light) Li = light_emit(c.scv, nx);
           else if (k < D) {
-            Pcg32 rli = make_sampler(i * kJumpStreams + (uint64_t)k);
+            Pcg32 rli = make_sampler(i * kJumpStreams + (uint64_t)k + c.cfg.seed * 2654435761ull);
             Li = trace2light<R, false>(c.scv, rli, nx, true, nL, nB, D - k, false);
           }
         }
@@ -790,6 +790,198 @@ inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
 
 using namespace orc;
 
+// Interpenetration creases (unbiased estimator; test restatement of the GPU term): the
+// curves where triangles of two different meshes cross. Along the projected curve the
+// visible surface switches from surface 1 (the -n side) to surface 2, and the image
+// changes by Int g [L1 (v_c - v_1) - L2 (v_c - v_2)] . n dl in raster units, v_c the
+// curve's raster velocity (the curve stays on both surfaces: its world velocity in the
+// plane of the two normals n1, n2 satisfies n_k . dx_c = n_k . dx_k) and v_k the velocity
+// of surface k's material point at the crease point. The derivative is carried by
+//   (G1 - G2) (A1 n1 . (X1 - o) + A2 n2 . (X2 - o)) - G1 w . (X1 - o) + G2 w . (X2 - o),
+// with w = J^T n (J the raster Jacobian), c = n1 . n2, A1 = (w.n1 - c w.n2) / (1 - c^2),
+// A2 = (w.n2 - c w.n1) / (1 - c^2), G_k = g . L_k, and X_k, o the differentiated material
+// points and camera origin. Segments are ordered by their triangle pair and sampled by
+// length, N = spp_primary_edge x 16384 stratified samples.
+constexpr uint64_t kCreaseStream = 0xC0000000ull;
+constexpr uint64_t kCreaseSamplesPerSpp = 16384;
+
+struct Crease {
+  std::vector<V3<float>> a, b;
+  std::vector<float> len;
+  std::vector<int> ta, tb;
+  std::vector<double> w, pre;
+  // Segment where triangles A and B cross (double arithmetic, vertices on a plane count as
+  // on its positive side).
+  static bool segment(const V3<double>* A, const V3<double>* B, V3<double>& s0, V3<double>& s1) {
+    auto cut = [](const V3<double>* T, const V3<double>& n, double d, V3<double>& p, V3<double>& q) {
+      double sd[3];
+      for (int k = 0; k < 3; ++k) sd[k] = dot(n, T[k]) + d;
+      const bool p0 = sd[0] >= 0, p1 = sd[1] >= 0, p2 = sd[2] >= 0;
+      if (p0 == p1 && p1 == p2) return false;
+      const int k = (p0 != p1 && p0 != p2) ? 0 : (p1 != p0 && p1 != p2) ? 1 : 2;
+      const int i = (k + 1) % 3, j = (k + 2) % 3;
+      p = T[k] + (T[i] - T[k]) * (sd[k] / (sd[k] - sd[i]));
+      q = T[k] + (T[j] - T[k]) * (sd[k] / (sd[k] - sd[j]));
+      return true;
+    };
+    const V3<double> na = cross(A[1] - A[0], A[2] - A[0]), nb = cross(B[1] - B[0], B[2] - B[0]);
+    const V3<double> D = cross(na, nb);
+    if (!(dot(D, D) > 1e-30 * dot(na, na) * dot(nb, nb))) return false;
+    V3<double> pa, qa, pb, qb;
+    if (!cut(A, nb, -dot(nb, B[0]), pa, qa) || !cut(B, na, -dot(na, A[0]), pb, qb)) return false;
+    double ta0 = dot(pa, D), ta1 = dot(qa, D), tb0 = dot(pb, D), tb1 = dot(qb, D);
+    if (ta0 > ta1) { std::swap(ta0, ta1); std::swap(pa, qa); }
+    if (tb0 > tb1) { std::swap(tb0, tb1); std::swap(pb, qb); }
+    if (!(std::max(ta0, tb0) < std::min(ta1, tb1))) return false;
+    s0 = ta0 >= tb0 ? pa : pb;
+    s1 = ta1 <= tb1 ? qa : qb;
+    return true;
+  }
+  void build(const Scene<float>& sf) {
+    const int nt = (int)sf.tris.size();
+    auto box = [&](int t, V3<float>& lo, V3<float>& hi) {
+      const Tri<float>& T = sf.tris[t];
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(T.p0[k], std::min(T.p1[k], T.p2[k]));
+        hi[k] = std::max(T.p0[k], std::max(T.p1[k], T.p2[k]));
+      }
+    };
+    auto dv = [](const V3<float>& p) { return V3<double>(p.x, p.y, p.z); };
+    const int nmesh = sf.n_obj - (int)sf.light_kind.size();  // objects are meshes, then light meshes
+    for (int t = 0; t < nt; ++t) {
+      const int ot = sf.tris[t].obj;
+      if (ot >= nmesh) continue;
+      V3<float> lo, hi;
+      box(t, lo, hi);
+      for (int u = 0; u < nt; ++u) {
+        const int ou = sf.tris[u].obj;
+        if (ou <= ot || ou >= nmesh) continue;
+        V3<float> l2, h2;
+        box(u, l2, h2);
+        if (l2.x > hi.x || h2.x < lo.x || l2.y > hi.y || h2.y < lo.y || l2.z > hi.z || h2.z < lo.z) continue;
+        const V3<double> A[3] = {dv(sf.tris[t].p0), dv(sf.tris[t].p1), dv(sf.tris[t].p2)};
+        const V3<double> B[3] = {dv(sf.tris[u].p0), dv(sf.tris[u].p1), dv(sf.tris[u].p2)};
+        V3<double> s0, s1;
+        if (!segment(A, B, s0, s1)) continue;
+        const double L = norm(s1 - s0);
+        if (!(L > 0)) continue;
+        a.push_back(V3<float>(float(s0.x), float(s0.y), float(s0.z)));
+        b.push_back(V3<float>(float(s1.x), float(s1.y), float(s1.z)));
+        len.push_back(float(L));
+        ta.push_back(t);
+        tb.push_back(u);
+      }
+    }
+    double acc = 0;
+    for (float l : len) { w.push_back(double(l)); acc += double(l); pre.push_back(acc); }
+  }
+  long long locate(long long i, long long N, float xi, float& t, double& pmf) const {
+    const double tot = pre.back();
+    const double tt = (double(i) + double(xi)) / double(N) * tot;
+    long long q = (long long)(std::upper_bound(pre.begin(), pre.end(), tt) - pre.begin());
+    if (q >= (long long)pre.size()) q = (long long)pre.size() - 1;
+    const double base = q > 0 ? pre[q - 1] : 0.0;
+    double r = (tt - base) / w[q];
+    t = std::min(float(r < 0 ? 0.0 : r), 0.99999994f);
+    pmf = w[q] / tot;
+    return q;
+  }
+};
+
+// Barycentric weights (of p1, p2) of point x in triangle T.
+inline void bary_in(const Tri<float>& T, const V3<float>& x, double& b1, double& b2) {
+  const V3<double> p0(T.p0.x, T.p0.y, T.p0.z), e1 = V3<double>(T.p1.x, T.p1.y, T.p1.z) - p0,
+      e2 = V3<double>(T.p2.x, T.p2.y, T.p2.z) - p0, q = V3<double>(x.x, x.y, x.z) - p0;
+  const double d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2), q1 = dot(q, e1), q2 = dot(q, e2);
+  const double den = d11 * d22 - d12 * d12;
+  b1 = (d22 * q1 - d12 * q2) / den;
+  b2 = (d11 * q2 - d12 * q1) / den;
+}
+
+template <class S, bool AD>
+inline void crease_sample(const Ctx<S, AD>& c, const Crease& K, uint64_t i, uint64_t N, const double* dLdI,
+                          double* dphi) {
+  if constexpr (AD) {
+    constexpr int KD = sizeof(S) / sizeof(double) - 1;
+    const uint64_t so = c.cfg.seed * 2654435761ull;
+    const Scene<float>& sf = *c.scf;
+    const Camera<float>& cam = c.camf;
+    Pcg32 rng = make_sampler(kCreaseStream + i + so);
+    const float xi = rng.next_float();
+    float t;
+    double pmf;
+    const long long q = K.locate((long long)i, (long long)N, xi, t, pmf);
+    if (!(pmf > 0)) return;
+    const V3<float> s0 = K.a[q], s1 = K.b[q];
+    const V3<float> x = s0 + (s1 - s0) * t;
+    const V3<float> tang = (s1 - s0) * (1.f / K.len[q]);
+    const double wgt = K.w[q] / (pmf * double(N));
+    const V3<float> pc = Camera<float>::xpos(cam.w2c, x), pr = Camera<float>::xpos(cam.c2r, pc);
+    if (!(pc.z < 0 && pr.x > 0 && pr.x < cam.W && pr.y > 0 && pr.y < cam.H)) return;
+    // raster Jacobian rows at x (gradients of u_x, u_y w.r.t. the world point)
+    V3<float> g[2];
+    {
+      const float wden = cam.c2r[3][0] * pc.x + cam.c2r[3][1] * pc.y + cam.c2r[3][2] * pc.z + cam.c2r[3][3];
+      for (int r = 0; r < 2; ++r) {
+        const float u = (cam.c2r[r][0] * pc.x + cam.c2r[r][1] * pc.y + cam.c2r[r][2] * pc.z + cam.c2r[r][3]) / wden;
+        const V3<float> gp((cam.c2r[r][0] - u * cam.c2r[3][0]) / wden, (cam.c2r[r][1] - u * cam.c2r[3][1]) / wden,
+                           (cam.c2r[r][2] - u * cam.c2r[3][2]) / wden);
+        for (int k = 0; k < 3; ++k)
+          g[r][k] = cam.w2c[0][k] * gp.x + cam.w2c[1][k] * gp.y + cam.w2c[2][k] * gp.z;
+      }
+    }
+    const float mx = dot(g[0], tang), my = dot(g[1], tang);
+    const float rlen = std::sqrt(mx * mx + my * my);
+    if (!(rlen > 0)) return;
+    const float nx = -my / rlen, ny = mx / rlen;
+    const int oa = sf.tris[K.ta[q]].obj, ob = sf.tris[K.tb[q]].obj;
+    const float tol = 1e-3f * norm(x - c.posf) + 1e-4f;
+    Its<float> hs[2];
+    int objs[2];
+    for (int side = 0; side < 2; ++side) {
+      const float sg = side ? 0.01f : -0.01f;
+      const V3<float> pcam = Camera<float>::xpos(cam.r2c, V3<float>(pr.x + sg * nx, pr.y + sg * ny, 1.f));
+      const V3<float> d = normalize(Camera<float>::xdir(cam.c2w, pcam));
+      hs[side] = scene_hit<float, false>(sf, c.posf, d, true);
+      objs[side] = hs[side].valid && norm(hs[side].p - x) < tol ? hs[side].obj : -1;
+    }
+    if (!(objs[0] >= 0 && objs[1] >= 0 && objs[0] != objs[1] && (objs[0] == oa || objs[0] == ob) &&
+          (objs[1] == oa || objs[1] == ob)))
+      return;
+    V3<float> Ls[2];
+    for (int side = 0; side < 2; ++side) {
+      Pcg32 rs = make_sampler(kCreaseStream + 0x10000000ull + 2 * i + (uint64_t)side + so);
+      Ls[side] = trace2light<float, false>(sf, rs, hs[side], true, c.cfg.mis_light_samples, c.cfg.mis_bsdf_samples,
+                                           c.cfg.max_bounce, c.cfg.enable_light_visable != 0);
+    }
+    const int px = std::min(cam.W - 1, (int)std::floor(pr.x)), py = std::min(cam.H - 1, (int)std::floor(pr.y));
+    const double* gp = dLdI + 3 * ((size_t)py * cam.W + px);
+    double G[2];
+    for (int side = 0; side < 2; ++side)
+      G[side] = gp[0] * double(Ls[side].x) + gp[1] * double(Ls[side].y) + gp[2] * double(Ls[side].z);
+    if (!std::isfinite(G[0]) || !std::isfinite(G[1])) return;
+    const int t1 = objs[0] == oa ? K.ta[q] : K.tb[q], t2 = objs[0] == oa ? K.tb[q] : K.ta[q];
+    const V3<double> n1 = normalize(V3<double>(sf.tris[t1].n.x, sf.tris[t1].n.y, sf.tris[t1].n.z));
+    const V3<double> n2 = normalize(V3<double>(sf.tris[t2].n.x, sf.tris[t2].n.y, sf.tris[t2].n.z));
+    const V3<double> wv = V3<double>(g[0].x, g[0].y, g[0].z) * double(nx) + V3<double>(g[1].x, g[1].y, g[1].z) * double(ny);
+    const double cc = dot(n1, n2), sn2 = 1 - cc * cc;
+    if (!(sn2 > 1e-6)) return;
+    const double A1 = (dot(wv, n1) - cc * dot(wv, n2)) / sn2, A2 = (dot(wv, n2) - cc * dot(wv, n1)) / sn2;
+    double b1, b2, c1, c2;
+    bary_in(sf.tris[t1], x, b1, b2);
+    bary_in(sf.tris[t2], x, c1, c2);
+    const Tri<S>& T1 = c.sc.tris[t1];
+    const Tri<S>& T2 = c.sc.tris[t2];
+    const V3<S> X1 = T1.p0 + (T1.p1 - T1.p0) * S(b1) + (T1.p2 - T1.p0) * S(b2) - c.cam_pos;
+    const V3<S> X2 = T2.p0 + (T2.p1 - T2.p0) * S(c1) + (T2.p2 - T2.p0) * S(c2) - c.cam_pos;
+    auto dotc = [](const V3<double>& a, const V3<S>& b) { return b.x * S(a.x) + b.y * S(a.y) + b.z * S(a.z); };
+    const S f = (dotc(n1, X1) * S(A1) + dotc(n2, X2) * S(A2)) * S(G[0] - G[1]) - dotc(wv, X1) * S(G[0]) +
+                dotc(wv, X2) * S(G[1]);
+    const double k = wgt * double(rlen);
+    for (int qd = 0; qd < KD; ++qd) dphi[qd] += k * f.d[qd];
+  }
+}
+
 // Film::add (camera.h:75-87): per pixel sum of the samples, divided by spp.
 template <class S, bool AD>
 static void render_camera(const Ctx<S, AD>& c, int which, double* img, const double* dLdI, double* dphi,
@@ -841,7 +1033,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
     std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < (int64_t)N; ++i) {
-      Pcg32 rng = make_sampler((uint64_t)i);
+      Pcg32 rng = make_sampler((uint64_t)i + c.cfg.seed * 2654435761ull);
       float s1 = rng.next_float();
       const double hp = unb ? hc.sample_unb(&s1, rng) : double(hc.sample_reuse(&s1));
       int rx, ry;
@@ -865,7 +1057,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
     std::vector<double> phi_s(KD ? N * KD : 0, 0.0);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < (int64_t)N; ++i) {
-      Pcg32 rng = make_sampler((uint64_t)i);
+      Pcg32 rng = make_sampler((uint64_t)i + c.cfg.seed * 2654435761ull);
       R s3[3];
       for (int k = 0; k < 3; ++k) s3[k] = rng.next_float();
       const double hp = unb ? hc.sample_unb(s3, rng) : double(hc.sample_reuse(s3));
@@ -910,6 +1102,20 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
       }
     }
   }
+  // ---- interpenetration creases (unbiased estimator only, perspective cameras)
+  if ((which & 32) && unb && !c.cam.ortho) {
+    if constexpr (KD > 0) {
+      Crease K;
+      K.build(*c.scf);
+      if (!K.pre.empty() && K.pre.back() > 0) {
+        const uint64_t N = (uint64_t)c.cfg.spp_primary_edge * kCreaseSamplesPerSpp;
+        std::vector<double> phi_s(N * KD, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t i = 0; i < (int64_t)N; ++i) crease_sample<S, AD>(c, K, (uint64_t)i, N, dLdI, &phi_s[i * KD]);
+        for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];
+      }
+    }
+  }
   // ---- BSDF jumps of DiffuseBsdfMaterial (unbiased estimator only)
   if ((which & 16) && unb &&
       std::find(c.sc.obj_mat.begin(), c.sc.obj_mat.end(), 1) != c.sc.obj_mat.end()) {
@@ -942,7 +1148,7 @@ static int render_impl(const OrcMesh* m, int nm, const OrcLight* l, int nl, cons
   else { scv_own = mk_scene<R>(m, nm, l, nl, none); scv = &scv_own; }
   Scene<float> scf_own;
   const Scene<float>* scf = nullptr;
-  if (which & 2) {
+  if (which & (2 | 32)) {
     if constexpr (std::is_same<S, float>::value) scf = &sc;
     else { scf_own = mk_scene<float>(m, nm, l, nl, Seeds<float>{}); scf = &scf_own; }
   }

@@ -45,7 +45,7 @@ class OrcConfig(C.Structure):
                 ("spp_primary_edge", C.c_int), ("spp_secondary_edge", C.c_int), ("max_bounce", C.c_int),
                 ("mis_light_samples", C.c_int), ("mis_bsdf_samples", C.c_int), ("pe_rounds", C.c_int),
                 ("se_rounds", C.c_int), ("pe_res", C.c_int), ("se_res", C.c_int * 3), ("mode", C.c_int),
-                ("spp_pixel_boundary", C.c_int)]
+                ("spp_pixel_boundary", C.c_int), ("seed", C.c_uint64)]
 
 
 def lib():
@@ -133,11 +133,11 @@ class Marshal:
 def make_config(n_pass=1, spp_interior=1, enable_light_visable=False, spp_primary_edge=1, spp_secondary_edge=1,
                 max_bounce=3, mis_light_samples=1, mis_bsdf_samples=1, primary_edge_preprocess_rounds=1,
                 secondary_edge_preprocess_rounds=1, primary_edge_hypercube_resolution=10000,
-                secondary_edge_hypercube_resolution=(10000, 6, 6), mode=0, spp_pixel_boundary=0, **_):
+                secondary_edge_hypercube_resolution=(10000, 6, 6), mode=0, spp_pixel_boundary=0, seed=0, **_):
     return OrcConfig(n_pass, spp_interior, int(enable_light_visable), spp_primary_edge, spp_secondary_edge,
                      max_bounce, mis_light_samples, mis_bsdf_samples, primary_edge_preprocess_rounds,
                      secondary_edge_preprocess_rounds, primary_edge_hypercube_resolution,
-                     (C.c_int * 3)(*secondary_edge_hypercube_resolution), mode, spp_pixel_boundary)
+                     (C.c_int * 3)(*secondary_edge_hypercube_resolution), mode, spp_pixel_boundary, int(seed))
 
 
 def set_threads(n: int):

@@ -293,6 +293,7 @@ struct OrcConfig {
   int pe_rounds, se_rounds, pe_res, se_res[3];
   int mode;  // 0: reference formulas, 1: unbiased estimator
   int spp_pixel_boundary;  // pixel-border samples per border segment (unbiased estimator)
+  uint64_t seed;  // stream offset seed * 2654435761 of every non-preprocess stream (the GPU's seed)
 };
 }
 

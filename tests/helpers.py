@@ -140,6 +140,18 @@ def gradient_case(name, h, w):
         return synth.SceneSpec([occ, wall_mesh(0)], [front_light()], [cam]), 0
     if name == "wall":
         return synth.SceneSpec([wall_mesh(15)], [front_light()], [cam]), 0
+    if name == "sunk":
+        # a smooth textured ball sunk 0.3 into a textured ground, seen from above: the curve
+        # where the two meshes cross is in view (interpenetration-crease term)
+        sph = ball(level=3, textured=True, noise=0.0, center=(0.0, -0.7, 0.0))
+        gV, gF = synth.quad((0.0, 0.0), 10.0, -1.0, facing_down=False)
+        uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+        ground = synth.MeshSpec(gV, gF, uv, gF.copy(), synth.uniform_texture(15, 15, 7))
+        lV, lF = synth.quad((0.0, 0.0), 1.0, 3.0, facing_down=True)
+        light = synth.LightSpec(lV, lF, np.array([20.0, 20.0, 20.0], np.float32))
+        top = synth.CameraSpec(np.array([0.3, 2.0, 3.0], np.float32), np.array([0.0, -0.8, 0.0], np.float32),
+                               np.array([0, 1, 0], np.float32), 0.8, h, w)
+        return synth.SceneSpec([sph, ground], [light], [top]), 0
     raise ValueError(name)
 
 

@@ -1793,9 +1793,12 @@ constexpr int kCreaseSamplesPerSpp = 16384;  // crease samples per primary-edge 
 constexpr unsigned long long kCreaseStream = 0xC0000000ull;  // sampler streams of the crease samples
 
 struct CreaseBuf {
-  float4* a;   // segment start xyz, length
+  float4* a;   // segment start xyz, length (ordered by the triangle pair)
   float4* b;   // segment end xyz, -
   int2* tris;  // the two triangles (different meshes)
+  float4* ra;  // the same, in the order the extraction found them
+  float4* rb;
+  int2* rtris;
   int* count;  // segments found (may exceed kCreaseCap: the rest are dropped)
 };
 
@@ -1889,14 +1892,34 @@ __global__ void __launch_bounds__(128) k_crease_pairs(const DevScene* __restrict
           if (!(len > 0.0)) continue;
           const int slot = atomicAdd(cb.count, 1);
           if (slot >= kCreaseCap) continue;
-          cb.a[slot] = make_float4((float)s0.x, (float)s0.y, (float)s0.z, (float)len);
-          cb.b[slot] = make_float4((float)s1.x, (float)s1.y, (float)s1.z, 0.f);
-          cb.tris[slot] = make_int2(t, u);
+          cb.ra[slot] = make_float4((float)s0.x, (float)s0.y, (float)s0.z, (float)len);
+          cb.rb[slot] = make_float4((float)s1.x, (float)s1.y, (float)s1.z, 0.f);
+          cb.rtris[slot] = make_int2(t, u);
         }
       }
       if (sp == 0) break;
       node = stack[--sp];
     }
+  }
+}
+
+// The extraction appends in whatever order the threads reach the counter; each segment's
+// rank by its (triangle, triangle) pair puts them in one fixed order, so the samples (and
+// the gradients) do not depend on scheduling.
+__global__ void k_crease_order(CreaseBuf cb) {
+  const int n = min(*cb.count, kCreaseCap);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int2 ti = cb.rtris[i];
+    const unsigned long long ki = ((unsigned long long)(unsigned)ti.x << 32) | (unsigned)ti.y;
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const int2 tj = cb.rtris[j];
+      const unsigned long long kj = ((unsigned long long)(unsigned)tj.x << 32) | (unsigned)tj.y;
+      rank += kj < ki;
+    }
+    cb.a[rank] = cb.ra[i];
+    cb.b[rank] = cb.rb[i];
+    cb.tris[rank] = ti;
   }
 }
 
@@ -3024,7 +3047,10 @@ static CreaseBuf crease_buf(psdr_workspace* ws) {
   cb.a = reinterpret_cast<float4*>(p);
   cb.b = reinterpret_cast<float4*>(p + 16 * (size_t)kCreaseCap);
   cb.tris = reinterpret_cast<int2*>(p + 32 * (size_t)kCreaseCap);
-  cb.count = reinterpret_cast<int*>(p + 40 * (size_t)kCreaseCap);
+  cb.ra = reinterpret_cast<float4*>(p + 40 * (size_t)kCreaseCap);
+  cb.rb = reinterpret_cast<float4*>(p + 56 * (size_t)kCreaseCap);
+  cb.rtris = reinterpret_cast<int2*>(p + 72 * (size_t)kCreaseCap);
+  cb.count = reinterpret_cast<int*>(p + 80 * (size_t)kCreaseCap);
   return cb;
 }
 
@@ -3056,7 +3082,7 @@ void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector
   long long s = kCreaseCap;
   for (const DevView& v : views) s = std::max(s, border_segments(v));
   ws->ensure_mass(s, st);
-  ws->crease.alloc(40 * (size_t)kCreaseCap + 256, st);
+  ws->crease.alloc(80 * (size_t)kCreaseCap + 256, st);
 }
 
 static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, bool floor, cudaStream_t st) {
@@ -3214,8 +3240,9 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       const CreaseBuf cb = crease_buf(ws);
       PSDR_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int), st));
       k_crease_pairs<<<num_sms() * 4, 128, 0, st>>>(scenes_dev, V.scene, cb);
+      k_crease_order<<<kCreaseCap / 128, 128, 0, st>>>(cb);
       k_crease_mass<<<kCreaseCap / 256, 256, 0, st>>>(cb, ws->mass_d.as<double>());
-      PSDR_LAUNCHED(2);
+      PSDR_LAUNCHED(3);
       inclusive_scan_double(ws->mass_d.as<double>(), ws->mass_pre.as<double>(), kCreaseCap,
                             ws->scan_tmp.as<double>(), st);
       const long long N = (long long)cfg.spp_primary_edge * kCreaseSamplesPerSpp;
