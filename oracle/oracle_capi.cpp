@@ -935,11 +935,12 @@ inline void crease_sample(const Ctx<S, AD>& c, const Crease& K, uint64_t i, uint
     if (!(rlen > 0)) return;
     const float nx = -my / rlen, ny = mx / rlen;
     const int oa = sf.tris[K.ta[q]].obj, ob = sf.tris[K.tb[q]].obj;
-    const float tol = 1e-3f * norm(x - c.posf) + 1e-4f;
+    const float off = 5.f * 1e-3f;  // 5 ray epsilons (tmin) in world units, scaled to pixels below
+    const float tol = 10.f * off;
     Its<float> hs[2];
     int objs[2];
     for (int side = 0; side < 2; ++side) {
-      const float sg = side ? 0.01f : -0.01f;
+      const float sg = (side ? off : -off) * rlen;
       const V3<float> pcam = Camera<float>::xpos(cam.r2c, V3<float>(pr.x + sg * nx, pr.y + sg * ny, 1.f));
       const V3<float> d = normalize(Camera<float>::xdir(cam.c2w, pcam));
       hs[side] = scene_hit<float, false>(sf, c.posf, d, true);

@@ -147,7 +147,8 @@ def gradient_case(name, h, w):
         gV, gF = synth.quad((0.0, 0.0), 10.0, -1.0, facing_down=False)
         uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
         ground = synth.MeshSpec(gV, gF, uv, gF.copy(), synth.uniform_texture(15, 15, 7))
-        lV, lF = synth.quad((0.0, 0.0), 1.0, 3.0, facing_down=True)
+        # the light in front of the ball, so that both sides of the front crease are lit
+        lV, lF = synth.quad((0.0, 2.5), 1.0, 3.0, facing_down=True)
         light = synth.LightSpec(lV, lF, np.array([20.0, 20.0, 20.0], np.float32))
         top = synth.CameraSpec(np.array([0.3, 2.0, 3.0], np.float32), np.array([0.0, -0.8, 0.0], np.float32),
                                np.array([0, 1, 0], np.float32), 0.8, h, w)

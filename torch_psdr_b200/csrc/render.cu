@@ -1988,8 +1988,10 @@ PSDR_D CreasePt crease_point(const DevView& V, CreaseBuf cb, const double* mw, c
 
 // Offset rays on both sides of the projected curve; both must reach the two meshes next to
 // the crease point (else something hides it). Paths from both hits give L1 and L2 (slots
-// 2s: the -n side, surface 1; 2s + 1: the +n side, surface 2).
-constexpr float kCreaseOffset = 0.01f;  // pixels
+// 2s: the -n side, surface 1; 2s + 1: the +n side, surface 2). The offset is 5 ray epsilons
+// (tmin) in world units: closer to the crease, rays leaving one surface skip the other
+// within tmin and the rendered radiance there is not the image's limit at the crease.
+constexpr float kCreaseOffset = 5.f * kTmin;  // world units
 __global__ void __launch_bounds__(256) k_crease_init(WF w, const DevScene* __restrict__ scenes,
                                                      const DevView* __restrict__ views, int v, EdgeBuf eb,
                                                      CreaseBuf cb, const double* __restrict__ mw,
@@ -2012,10 +2014,10 @@ __global__ void __launch_bounds__(256) k_crease_init(WF w, const DevScene* __res
       if (ok) {
         const int2 tp = cb.tris[c.seg];
         const int oa = __ldg(sc.tri_v + tp.x).w, ob = __ldg(sc.tri_v + tp.y).w;
-        const float tol = 1e-3f * norm(c.x - V.pos) + 1e-4f;
+        const float tol = 10.f * kCreaseOffset;
         int objs[2];
         for (int side = 0; side < 2; ++side) {
-          const float sg = side ? kCreaseOffset : -kCreaseOffset;
+          const float sg = (side ? kCreaseOffset : -kCreaseOffset) * c.rlen;  // pixels
           float3 pcam;
           xform_pos(V.r2c, f3(c.u.x + sg * c.n.x, c.u.y + sg * c.n.y, 1.0f), pcam);
           const float3 d = normalize(xform_dir(V.c2w, pcam));
