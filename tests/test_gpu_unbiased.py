@@ -159,3 +159,23 @@ def test_crease_term_matches_oracle(cuda):
     # the offset rays pass 0.01 pixel from the crease and start paths on either surface
     # next to it; float (GPU) and double (oracle) resolve a few of them differently
     assert err.max() < 1e-2
+
+
+def test_indirect_shadow_term_matches_oracle(cuda):
+    """The indirect shadow-boundary term (bit 64) against the oracle's restatement: the same
+    edge / source-point / receiver samples, guiding cells and source paths."""
+    spec = synth.sphere_scene(level=3, tex_hw=16, noise_sigma=0.02, noise_seed=2, height=24, width=24)
+    rng = np.random.default_rng(3)
+    gseeds, oseeds = _seeds_for(spec, ("verts",), rng)
+    kw = dict(BASE, spp_secondary_edge=16)
+    got, dLdI = _gpu_dir_derivs(spec, 64, gseeds, dict(kw, estimator="unbiased", spp_pixel_boundary=4),
+                                {"verts", "light_verts"})
+    ocfg = dict(kw, mode=1, spp_pixel_boundary=4,
+                secondary_edge_hypercube_resolution=tuple(kw["secondary_edge_hypercube_resolution"]))
+    ref = orc.grad_dir(spec, [dLdI], which=64, **oseeds, **ocfg)
+    err = np.abs(got - ref) / (np.abs(ref).max() + 1e-30)
+    print(f"indirect shadow boundaries: gpu {got[:4]} oracle {ref[:4]} max rel {err.max():.2e}")
+    assert np.abs(ref).max() > 0
+    # like the direct term, its rays start on silhouette edges (float on the GPU, double in
+    # the oracle)
+    assert err.max() < 1e-2

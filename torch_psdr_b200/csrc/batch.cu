@@ -134,6 +134,7 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
       if (b->backward) PSDR_CHECK(d_images[i] != nullptr, "null image gradient");
     }
     assign_offsets(b->views);
+    set_scene_ntri(b->views, scenes);
     b->cap = choose_cap(*cfg, b->views, true);
     const int Rmax = cfg->mis_light_samples + std::max(cfg->mis_bsdf_samples, 1) + 1;
     b->ws.ensure(b->cap, Rmax, cfg->max_bounce, n_cams, b->backward ? 1 : 0, st);

@@ -659,6 +659,10 @@ psdr_status psdr_render_bwd(psdr_scene* scene, psdr_workspace* ws, const psdr_ca
     views[i].grad_pos = ws->campos_acc.as<GradAcc>() + 3 * i;
     if (grads->camera_lens && grads->camera_lens[i] && unb) views[i].grad_lens = ws->lens_acc.as<GradAcc>() + kLensAcc * i;
   }
+  {
+    const psdr_scene* sl[1] = {scene};
+    set_scene_ntri(views, sl);
+  }
   render_backward_impl(dev_scene(scene), views, *cfg, ws, grad_info(scene), st);
   const int nm = (int)scene->meshes.size();
   for (int o = 0; o < scene->nobj; ++o) {

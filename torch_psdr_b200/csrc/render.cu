@@ -2544,6 +2544,233 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
   }
 }
 
+// ------------------------------------------------------------------ indirect shadow boundaries
+// Unbiased estimator: shadow boundaries of light that other surfaces reflect. The geometry
+// is the shadow-boundary term's with the light point replaced by a point y on any mesh
+// surface (area-sampled: pdf 1 / total mesh area): an edge point x_b that is a silhouette
+// seen from y, unoccluded toward y, and the receiver x_d beyond it, seen by the camera. The
+// radiance leaving y toward x_b is a path traced from y with max_bounce - 1 bounces (y is
+// the second vertex of the camera path through x_d); the boundary moves over the receiver
+// at d_eff = dx_b - dx_d / lam - dy (1 - 1/lam) as for the light. Receivers that reach the
+// camera only through further bounces are left out (their source paths would be one
+// bounce shorter per chain vertex).
+constexpr unsigned long long kIndirectStream = 0xE0000000ull;  // streams of the source paths
+
+struct SurfCdf {
+  const double* w;    // area of each mesh triangle (0 for light triangles)
+  const double* pre;  // inclusive prefix sums
+  int ntri;
+};
+
+// A point on the mesh surfaces by area: triangle by the prefix sums (rx rescaled for reuse),
+// then the light sampler's barycentric mapping.
+PSDR_D bool sample_surface(const DevScene& sc, const SurfCdf& cdf, float rx, float ry, LightSample& out) {
+  const double tot = cdf.pre[cdf.ntri - 1];
+  if (!(tot > 0.0)) return false;
+  const double t = (double)rx * tot;
+  int lo = 0, hi = cdf.ntri - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cdf.pre[mid] > t) hi = mid;
+    else lo = mid + 1;
+  }
+  if (!(cdf.w[lo] > 0.0)) return false;
+  const double base = lo > 0 ? cdf.pre[lo - 1] : 0.0;
+  const float r = fminf(fmaxf((float)((t - base) / cdf.w[lo]), 0.f), 0.99999994f);
+  const float4* R = sc.tri + 6 * (size_t)lo;
+  const float3 p0 = xyz(__ldg(R)), p1 = xyz(__ldg(R + 1)), p2 = xyz(__ldg(R + 2));
+  const float sq = ry > 0.f ? sqrtf(ry) : 0.f;
+  out.su = r * sq;
+  out.sv = 1.0f - sq;
+  out.y = p0 + (p1 - p0) * out.su + (p2 - p0) * out.sv;
+  out.pdf = (float)(1.0 / tot);
+  out.tri = lo;
+  out.light = -1;
+  return true;
+}
+
+__global__ void k_surf_mass(const DevScene* __restrict__ scenes, int si, double* __restrict__ w) {
+  const DevScene& sc = scenes[si];
+  const int nmesh = sc.nobj - sc.nlight;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < sc.ntri; t += gridDim.x * blockDim.x)
+    w[t] = __ldg(sc.tri_v + t).w < nmesh ? (double)__ldg(sc.tri + 6 * (size_t)t).w : 0.0;
+}
+
+// PRE: guiding mass per hypercube cell (|k0 J_cam| |f_r(x_d)| |w x e|; the source radiance
+// is not known yet). Otherwise: one sample per thread, side buffers for k_indirect_final and
+// a path from y (slot s) whose radiance toward x_b the depth loop computes.
+template <bool PRE>
+__global__ void __launch_bounds__(128) k_indirect(WF w, const DevScene* __restrict__ scenes,
+                                                  const DevView* __restrict__ views, int v, EdgeBuf eb, SurfCdf cdf,
+                                                  long long begin, int n, HCube hc, int round, float* mass) {
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n32; s += stride) {
+    bool alive = false;
+    if (s < n) {
+      const long long i = begin + s;
+      Rng rng;
+      float s3[3], hpdf = 1.f;
+      bool ok = true;
+      if (PRE) {
+        if (round == 0) rng = make_rng(kIndirectStream + (unsigned long long)i);
+        else { rng.state = w.rs[s]; rng.inc = w.ri[s]; }
+        const int r12 = hc.res[1] * hc.res[2];
+        const int c0 = (int)(i / r12);
+        const int rem = (int)(i - (long long)c0 * r12);
+        const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
+        const float d0 = rng.next_float(), d1 = rng.next_float(), d2 = rng.next_float();
+        s3[0] = ((float)c0 + d0) * hc.unit[0];
+        s3[1] = ((float)c1 + d1) * hc.unit[1];
+        s3[2] = ((float)c2 + d2) * hc.unit[2];
+        w.rs[s] = rng.state;
+        w.ri[s] = rng.inc;
+      } else {
+        rng = make_rng(kIndirectStream + (unsigned long long)i + w.seed);
+        s3[0] = rng.next_float(); s3[1] = rng.next_float(); s3[2] = rng.next_float();
+        double pm;
+        const int cell = hc_cell_unb(hc, s3[2], pm);
+        hpdf = (float)pm;
+        ok = pm > 0.0;
+        s3[2] = rng.next_float();
+        const int r12 = hc.res[1] * hc.res[2];
+        const int c0 = cell / r12, rem = cell - c0 * r12;
+        const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
+        s3[0] = (s3[0] + (float)c0) * hc.unit[0];
+        s3[1] = (s3[1] + (float)c1) * hc.unit[1];
+        s3[2] = (s3[2] + (float)c2) * hc.unit[2];
+      }
+      const int ne = *sc.n_edges;
+      float sx = s3[0], pe;
+      const int e = ok ? discrete_sample(sc.edge_pmf, sc.edge_cmf, ne, sx, pe) : 0;
+      LightSample ys;
+      ok = ok && sample_surface(sc, cdf, s3[1], s3[2], ys);
+      float3 xb = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f), nsv = f3(0.f, 0.f, 0.f);
+      float pdf_e = 0.f;
+      HitRec hd;
+      hd.tri = -1;
+      if (ok) {
+        const float4 E0 = __ldg(sc.edge + 4 * (size_t)e), E1 = __ldg(sc.edge + 4 * (size_t)e + 1),
+                     E2 = __ldg(sc.edge + 4 * (size_t)e + 2), E3 = __ldg(sc.edge + 4 * (size_t)e + 3);
+        const float3 p0 = xyz(E0), p1 = xyz(E1);
+        const float3 out = f3(E1.w, E2.x, E2.y), nl = f3(E2.z, E2.w, E3.x), nr = f3(E3.y, E3.z, E3.w);
+        xb = p0 + (p1 - p0) * sx;
+        pdf_e = pe / E0.w;
+        dir = normalize(xb - ys.y);
+        ok = dot(nl, dir) * dot(nr, dir) < 0.f && norm(nl - nr) > kEps;
+        if (ok) {
+          // x_b must see y: the closest hit toward y is y itself
+          const float dist = norm(xb - ys.y);
+          const HitRec hs = trace_closest(sc, xb, -dir, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
+          const Surf s0 = make_surf(sc, hs.tri, hs.b1, hs.b2, xb);
+          ok = s0.valid && !s0.is_light && sqnorm(s0.p - ys.y) < kEps;
+        }
+        if (ok) {
+          hd = trace_closest(sc, xb, dir, kTmin, INFINITY);
+          const Surf d0 = make_surf(sc, hd.tri, hd.b1, hd.b2, xb);
+          ok = d0.valid && !d0.is_light;
+          if (ok) {
+            float3 ev = normalize(p1 - p0);
+            if (dot(cross(dir, ev), out) < 0.f) ev = -ev;
+            nsv = cross(dir, ev);
+            // the receiver seen by the camera (perspective views)
+            const float3 rel = d0.p - V.pos;
+            const float dist = norm(rel);
+            const float3 cd = rel / dist;
+            int qx = 0, qy = 0;
+            ok = !V.ortho && dot(d0.n, cd) < 0.f && project(V, d0.p, qx, qy);
+            if (ok) {
+              const HitRec hc2 = trace_closest(sc, V.pos, cd, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
+              const Surf iv = make_surf(sc, hc2.tri, hc2.b1, hc2.b2, V.pos);
+              ok = iv.valid && !iv.is_light && sqnorm(iv.p - d0.p) < kEps;
+            }
+            if (ok) {
+              const float3 look = view_look(V);
+              const float z = dot(rel, look);
+              const float Jc = view_fxfy(V) * fabsf(dot(d0.n, rel)) / (z * z * z);
+              const float dby = norm(xb - ys.y);
+              const float4 yn = __ldg(sc.tri + 6 * (size_t)ys.tri + 3);
+              const float cos_y = fabsf(dot(normalize(xyz(yn)), dir));
+              const float k0 = -cos_y / (dby * dby) / (pdf_e * ys.pdf * (float)V.H * (float)V.W) * Jc;
+              const float lam = norm(d0.p - ys.y) / dby;
+              if (PRE) {
+                const float3 fr = surf_bsdf(sc, d0, -cd);
+                const float m = fabsf(k0) * norm(fr) * norm(nsv);
+                if (isfinite(m)) mass[i] = mass[i] + m;
+                ok = false;  // no path in the preprocess
+              } else {
+                eb.a[s] = make_float4(__int_as_float(e), sx, hpdf, __int_as_float(qy * V.W + qx));
+                eb.n[s] = make_float4(__int_as_float(ys.tri), ys.su, ys.sv, k0);
+                eb.hb[s] = make_float4(__int_as_float(hd.tri), hd.b1, hd.b2, lam);
+                eb.La[s] = make_float4(nsv.x, nsv.y, nsv.z, 0.f);
+              }
+            }
+          }
+        }
+      }
+      if (!PRE) {
+        eb.La[s].w = __int_as_float(ok ? 1 : 0);
+        const Rng r = make_rng(kIndirectStream + 0x10000000ull + (unsigned long long)i + w.seed);
+        w.rs[s] = r.state;
+        w.ri[s] = r.inc;
+        w.view[s] = v;
+        w.pix[s] = -1;
+        w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
+        w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        w.cur[s] = make_float4(__int_as_float(ok ? ys.tri : -1), ys.su, ys.sv, 0.f);
+        w.org[s] = make_float4(xb.x, xb.y, xb.z, 0.f);
+        alive = ok;
+      }
+    }
+    if (!PRE) {
+      const int k = warp_append(&w.cnt[0], alive);
+      if (alive) w.q0[k] = s;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_indirect_final(WF w, const DevScene* __restrict__ scenes,
+                                                        const DevView* __restrict__ views, int v, EdgeBuf eb, int n,
+                                                        float cells, int spp) {
+  const DevView& V = views[v];
+  const DevScene& sc = scenes[V.scene];
+  const int stride = gridDim.x * blockDim.x;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
+    if (!V.dimage || !sc.grad_verts) continue;
+    const float4 nv = eb.La[s];
+    if (__float_as_int(nv.w) != 1) continue;
+    const float4 a = eb.a[s], yn = eb.n[s], hd = eb.hb[s];
+    const float3 Lo = xyz(w.L[s]);
+    const int dtri = __float_as_int(hd.x);
+    const float4 E0 = __ldg(sc.edge + 4 * (size_t)__float_as_int(a.x)), E1 = __ldg(sc.edge + 4 * (size_t)__float_as_int(a.x) + 1);
+    const float3 xb = xyz(E0) + (xyz(E1) - xyz(E0)) * a.y;
+    // the receiver lit from the edge side, reflecting toward the camera
+    const Surf d0 = make_surf(sc, dtri, hd.y, hd.z, xb);
+    const float3 fr = surf_bsdf(sc, d0, normalize(V.pos - d0.p));
+    const float* gp = V.dimage + 3 * (size_t)__float_as_int(a.w);
+    const float wsum = (gp[0] * fr.x * Lo.x + gp[1] * fr.y * Lo.y + gp[2] * fr.z * Lo.z) * yn.w;
+    const float3 ag = xyz(nv) * (wsum / (a.z * cells * (float)spp));
+    if (!finite3(ag) || wsum == 0.f) continue;
+    const int e = __float_as_int(a.x);
+    const float sx = a.y, lam = hd.w;
+    const int2 evv = __ldg(sc.edge_v + e);
+    vert_add(sc, evv.x, ag * (1.f - sx));
+    vert_add(sc, evv.y, ag * sx);
+    const int4 td = __ldg(sc.tri_v + dtri);
+    const float3 ad = ag * (-1.f / lam);
+    vert_add(sc, td.x, ad * (1.f - hd.y - hd.z));
+    vert_add(sc, td.y, ad * hd.y);
+    vert_add(sc, td.z, ad * hd.z);
+    const int4 ty = __ldg(sc.tri_v + __float_as_int(yn.x));
+    const float3 ay = ag * (1.f / lam - 1.f);
+    vert_add(sc, ty.x, ay * (1.f - yn.y - yn.z));
+    vert_add(sc, ty.y, ay * yn.y);
+    vert_add(sc, ty.z, ay * yn.z);
+  }
+}
+
 // ------------------------------------------------------------------ small utilities
 __global__ void k_mass_cdf(const float* __restrict__ mass, int n, double* __restrict__ w) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2654,6 +2881,7 @@ void make_view(const psdr_camera_desc& c, int spp, DevView& v) {
   v.dimage = nullptr;
   v.grad_pos = nullptr;
   v.grad_lens = nullptr;
+  v.scene_ntri = 0;
 }
 
 // Forward-mode derivative of the raster-to-direction map M = C diag(2 t / W, -2 t / H, -1),
@@ -3029,6 +3257,21 @@ static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v,
   PSDR_CUDA(cudaGetLastError());
 }
 
+// Indirect shadow-boundary samples [begin, begin + n) of view v: one source path each.
+static void indirect_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
+                           const SurfCdf& cdf, long long begin, int n, const HCube& hc, int spp, cudaStream_t st) {
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  k_indirect<false><<<grid_for(n, 128, 16), 128, 0, st>>>(w, scenes, vd, v, eb, cdf, begin, n, hc, 0, nullptr);
+  PSDR_LAUNCHED(1);
+  WF wy = w;
+  wy.D = w.D - 1;  // the source y is the second vertex of the camera path
+  wy.light_vis = 0;
+  depth_loop(wy, scenes, vd, MODE_FWD, st);
+  k_indirect_final<<<grid_for(n, 128, 16), 128, 0, st>>>(w, scenes, vd, v, eb, n, (float)hc.ncells, spp);
+  PSDR_LAUNCHED(1);
+  PSDR_CUDA(cudaGetLastError());
+}
+
 // Interpenetration-crease samples [begin, begin + n) of the N of view v: two paths per
 // sample (slots 2s, 2s + 1), so n is at most half the tile.
 static void crease_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
@@ -3081,10 +3324,19 @@ long long border_segments(const DevView& V) {
 
 void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector<DevView>& views, cudaStream_t st) {
   if (cfg.estimator != PSDR_EST_UNBIASED) return;
-  long long s = kCreaseCap;
-  for (const DevView& v : views) s = std::max(s, border_segments(v));
-  ws->ensure_mass(s, st);
+  long long s = kCreaseCap, nt = 1;
+  for (const DevView& v : views) {
+    s = std::max(s, border_segments(v));
+    nt = std::max<long long>(nt, v.scene_ntri);
+  }
+  ws->ensure_mass(std::max(s, nt), st);
   ws->crease.alloc(80 * (size_t)kCreaseCap + 256, st);
+  ws->surf_w.alloc(8 * (size_t)nt, st);
+  ws->surf_pre.alloc(8 * (size_t)nt, st);
+}
+
+void set_scene_ntri(std::vector<DevView>& views, const psdr_scene* const* scenes) {
+  for (DevView& v : views) v.scene_ntri = scenes[v.scene]->ntri;
 }
 
 static HCube build_hcube(psdr_workspace* ws, int ncells, const int* res, int N, bool floor, cudaStream_t st) {
@@ -3135,7 +3387,7 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
                      int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
   const DevView* vd = ws->views.as<DevView>();
   const bool unb = cfg.estimator == PSDR_EST_UNBIASED;
-  const int terms = cfg.terms ? cfg.terms : (unb ? 47 : 7);
+  const int terms = cfg.terms ? cfg.terms : (unb ? 111 : 7);
   bool lens = false;  // a view wants the camera-lens gradient
   for (const DevView& V : views) lens = lens || V.grad_lens != nullptr;
   // ---- interior
@@ -3235,6 +3487,30 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       for (long long b0 = 0; b0 < N; b0 += cap)
         border_phase(wi, scenes_dev, vd, v, eb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), S, b0,
                      (int)std::min<long long>(cap, N - b0), N, V.grad_lens != nullptr, st);
+    }
+    // indirect shadow boundaries (unbiased estimator, perspective views, max_bounce >= 2):
+    // the mesh-surface area CDF, the guiding preprocess, then the samples
+    if (unb && (terms & 64) && V.dimage && !V.ortho && cfg.max_bounce >= 2 && V.scene_ntri > 0) {
+      const SurfCdf cdf{ws->surf_w.as<double>(), ws->surf_pre.as<double>(), V.scene_ntri};
+      k_surf_mass<<<num_sms() * 4, 256, 0, st>>>(scenes_dev, V.scene, ws->surf_w.as<double>());
+      PSDR_LAUNCHED(1);
+      inclusive_scan_double(ws->surf_w.as<double>(), ws->surf_pre.as<double>(), V.scene_ntri,
+                            ws->scan_tmp.as<double>(), st);
+      const int* r3 = cfg.secondary_edge_hypercube_resolution;
+      const int cells = r3[0] * r3[1] * r3[2];
+      PSDR_CUDA(cudaMemsetAsync(ws->mass.p, 0, sizeof(float) * cells, st));
+      HCube pre{};
+      for (int k = 0; k < 3; ++k) { pre.res[k] = r3[k]; pre.unit[k] = 1.0f / (float)r3[k]; }
+      for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r) {
+        k_indirect<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, eb, cdf, 0, cells, pre, r,
+                                                                   ws->mass.as<float>());
+        PSDR_LAUNCHED(1);
+      }
+      const HCube hc = build_hcube(ws, cells, r3, 3, true, st);
+      const long long N = (long long)V.H * V.W * cfg.spp_secondary_edge;
+      for (long long b0 = 0; b0 < N; b0 += cap)
+        indirect_phase(wi, scenes_dev, vd, v, eb, cdf, b0, (int)std::min<long long>(cap, N - b0), hc,
+                       cfg.spp_secondary_edge, st);
     }
     // interpenetration creases (unbiased estimator, perspective views): the segments where
     // two meshes cross, a length CDF over them, then the samples

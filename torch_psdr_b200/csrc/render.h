@@ -23,6 +23,7 @@ struct DevView {
   const float* dimage;   // (H,W,3) or null
   GradAcc* grad_pos;     // 3 accumulators or null
   GradAcc* grad_lens;    // 12 accumulators or null: the camera-lens sums (k_lens_interior, k_lens_border)
+  int scene_ntri;        // host side (backward): triangles of the view's scene
 };
 
 // Path states and ray queues of one tile (structure of arrays, capacity `cap`).
@@ -80,6 +81,7 @@ struct psdr_workspace {
   psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
   psdr::DBuf campos_acc, lens_acc;
   psdr::DBuf crease;  // interpenetration segments (unbiased estimator): kCreaseCap records + count
+  psdr::DBuf surf_w, surf_pre;  // mesh-surface area CDF of the indirect shadow-boundary term
   long long mass_cap = 0;
   // a DiffuseBsdfMaterial mesh or an environment light is in the scenes of the current job
   // (each entry point sets it; the extended kernel instances also handle the plain
@@ -148,4 +150,6 @@ constexpr int kLensAcc = 12;  // accumulators per view: S0, Sx, Sy, B (3x3)
 void lens_out(const GradAcc* acc, const LensChain& ch, float* out, int accumulate, cudaStream_t st);
 long long border_segments(const DevView& V);
 void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector<DevView>& views, cudaStream_t st);
+// Views of a backward job: their scene triangle counts (DevView::scene_ntri), before ensure_border.
+void set_scene_ntri(std::vector<DevView>& views, const psdr_scene* const* scenes);
 }  // namespace psdr
