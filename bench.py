@@ -190,14 +190,16 @@ def smooth_weights(torch, dev):
                         for c in range(3)], -1).float().contiguous()
 
 
-def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=4096, replicas=4):
+def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=4096, replicas=4, ad_replicas=16):
     """Translation gradient of Phi = sum(w * image) for a smooth weight image w, from the
     estimator at the benchmark's sample counts, against central differences of Phi from
-    fd_spp-spp renders (same sample streams at +-h). Both sides are averaged over
-    `replicas` independent sample streams (seeds 1..replicas), whose spread gives the
-    standard error of each mean. The benchmark's own L2 loss is not used here: its image
-    gradient is dominated by texel-scale residuals, which makes its finite differences
-    ill-conditioned (they move by tens of percent with h and spp)."""
+    fd_spp-spp renders (same sample streams at +-h). The estimator is averaged over
+    `ad_replicas` independent sample streams (seeds 1..ad_replicas; one step's gradient
+    costs a benchmark step), the finite differences over `replicas`; the spreads give the
+    standard error of each mean and the spread of a single step's gradient. The
+    benchmark's own L2 loss is not used here: its image gradient is dominated by
+    texel-scale residuals, which makes its finite differences ill-conditioned (they move by
+    tens of percent with h and spp)."""
     from torch_psdr_b200 import _lib as L
     w = smooth_weights(torch, dev)
     wd = w.double()
@@ -205,11 +207,12 @@ def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=409
                                               "spp_pixel_boundary", "max_bounce")}
     est = "unbiased" if integ.cfg.estimator == L.EST_UNBIASED else "reference"
     ads, fds = [], []
-    for r in range(1, replicas + 1):
+    for r in range(1, ad_replicas + 1):
         ad_integ = dr.PathIntegrator(estimator=est, seed=r, **kw)
         t = torch.zeros(3, device=dev, requires_grad=True)
         ad_integ.renderD(build_scene(base + t, tex))[0].backward(w)
         ads.append(t.grad.double().cpu().numpy())
+    for r in range(1, replicas + 1):
         fd_integ = dr.PathIntegrator(**dict(CFG, spp_interior=fd_spp, seed=r))
         fd = []
         with torch.no_grad():
@@ -223,12 +226,15 @@ def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=409
     ads, fds = np.array(ads), np.array(fds)
     ad, fd = ads.mean(0), fds.mean(0)
     se = lambda a: a.std(0, ddof=1) / np.sqrt(len(a)) if len(a) > 1 else np.zeros(3)
+    single = np.array([np.linalg.norm(a - fd) / np.linalg.norm(fd) for a in ads])
     return {"rel_l2_vs_fd": float(np.linalg.norm(ad - fd) / np.linalg.norm(fd)), "ad": ad.tolist(), "fd": fd.tolist(),
             "ad_stderr": se(ads).tolist(), "fd_stderr": se(fds).tolist(),
             "rel_l2_fd_stderr": float(np.linalg.norm(se(fds)) / np.linalg.norm(fd)),
+            "rel_l2_ad_stderr": float(np.linalg.norm(se(ads)) / np.linalg.norm(fd)),
+            "single_step_rel_l2_median": float(np.median(single)), "ad_replicas": ad_replicas,
             "functional": "sum(w * image), w = sin(2.6 pi x/W + c) cos(1.4 pi y/H) + 0.3 per channel c",
             "parameter": "translation of the icosphere", "estimator": est,
-            "fd_step": h, "fd_spp": fd_spp, "replicas": replicas, "seeds": list(range(1, replicas + 1))}
+            "fd_step": h, "fd_spp": fd_spp, "replicas": replicas, "seeds": list(range(1, max(replicas, ad_replicas) + 1))}
 
 
 # ---------------------------------------------------------------- replicas

@@ -130,7 +130,9 @@ typedef struct {
   int32_t terms;  /* gradient terms of psdr_render_bwd: bit 0 interior, bit 1 primary
                      edges, bit 2 direct edges, bit 3 pixel borders (UNBIASED only),
                      bit 5 interpenetration creases (UNBIASED only, perspective views:
-                     the curves where two meshes cut into each other); 0 = all of these.
+                     the curves where two meshes cut into each other), bit 6 indirect
+                     shadow boundaries (UNBIASED only, perspective views, max_bounce >= 2:
+                     occlusion of light reflected by other surfaces); 0 = all of these.
                      Bit 4: BRDF jumps of DiffuseBsdfMaterial (UNBIASED only, on
                      request: not part of 0) */
   int32_t spp_pixel_boundary; /* UNBIASED: samples per unit pixel-border segment */

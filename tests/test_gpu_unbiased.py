@@ -119,7 +119,8 @@ def test_unbiased_camera_translation_is_scene_translation(cuda, terms):
     np.testing.assert_allclose(cam, -tot, rtol=0, atol=2e-3 * scale)
 
 
-def test_interpenetration_crease_vs_fd(cuda):
+@pytest.mark.parametrize("depth", [1, 2])
+def test_interpenetration_crease_vs_fd(cuda, depth):
     """A ball sunk into the ground, seen from above: the visible surface switches from ball
     to ground along the curve where the meshes cross. With the crease term (bit 32, in the
     default mask) the translation gradient matches central differences; without it the
@@ -127,8 +128,8 @@ def test_interpenetration_crease_vs_fd(cuda):
     size = 96
     spec, mesh = gradient_case("sunk", size, size)
     g = smooth_weights(size, size)
-    kw = dict(spp_interior=256, spp_primary_edge=64, spp_secondary_edge=4096, spp_pixel_boundary=64, max_bounce=2,
-              secondary_edge_hypercube_resolution=[20000, 6, 6], secondary_edge_preprocess_rounds=4,
+    kw = dict(spp_interior=256, spp_primary_edge=64, spp_secondary_edge=4096, spp_pixel_boundary=64,
+              max_bounce=depth, secondary_edge_hypercube_resolution=[20000, 6, 6], secondary_edge_preprocess_rounds=4,
               estimator="unbiased")
     ad = _gpu_translation_grad(spec, mesh, dr.PathIntegrator(**kw), g)
     crease = _gpu_translation_grad(spec, mesh, dr.PathIntegrator(gradient_terms=32, **kw), g)
