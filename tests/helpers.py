@@ -153,6 +153,23 @@ def gradient_case(name, h, w):
         top = synth.CameraSpec(np.array([0.3, 2.0, 3.0], np.float32), np.array([0.0, -0.8, 0.0], np.float32),
                                np.array([0, 1, 0], np.float32), 0.8, h, w)
         return synth.SceneSpec([sph, ground], [light], [top]), 0
+    if name == "creased":
+        # a textured wall tilted 45 degrees, cut by a textured ground along a straight
+        # crease (texel edges kept off the crease), the light in front (interpenetration
+        # crease term; the planar case, where the crease velocity is exact)
+        x0 = 0.3
+        WV = np.array([[x0 - 1.0, -2, -3], [x0 - 1.0, -2, 3], [x0 + 2.0, 1, 3], [x0 + 2.0, 1, -3]], np.float32)
+        WF = np.array([[0, 1, 2], [0, 2, 3]], np.int32)
+        uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+        wall = synth.MeshSpec(WV, WF, uv * np.float32(0.93) + np.float32(0.031), WF.copy(),
+                              synth.uniform_texture(9, 9, 3))
+        gV, gF = synth.quad((0.0, 0.0), 10.0, -1.0, facing_down=False)
+        ground = synth.MeshSpec(gV, gF, uv, gF.copy(), synth.uniform_texture(15, 15, 7))
+        lV, lF = synth.quad((-1.0, 0.0), 1.0, 3.0, facing_down=True)
+        light = synth.LightSpec(lV, lF, np.array([20.0, 20.0, 20.0], np.float32))
+        side = synth.CameraSpec(np.array([-1.5, 1.0, 2.5], np.float32), np.array([0.3, -1.0, 0.0], np.float32),
+                                np.array([0, 1, 0], np.float32), 0.9, h, w)
+        return synth.SceneSpec([wall, ground], [light], [side]), 0
     raise ValueError(name)
 
 

@@ -121,12 +121,12 @@ def test_unbiased_camera_translation_is_scene_translation(cuda, terms):
 
 @pytest.mark.parametrize("depth", [1, 2])
 def test_interpenetration_crease_vs_fd(cuda, depth):
-    """A ball sunk into the ground, seen from above: the visible surface switches from ball
-    to ground along the curve where the meshes cross. With the crease term (bit 32, in the
-    default mask) the translation gradient matches central differences; without it the
-    gap is the crease's share."""
+    """A tilted wall cut by the ground: the visible surface switches from wall to ground
+    along the line where the meshes cross. With the crease term (bit 32, in the default
+    mask) the wall's translation gradient matches central differences; without it the gap
+    is the crease's share."""
     size = 96
-    spec, mesh = gradient_case("sunk", size, size)
+    spec, mesh = gradient_case("creased", size, size)
     g = smooth_weights(size, size)
     kw = dict(spp_interior=256, spp_primary_edge=64, spp_secondary_edge=4096, spp_pixel_boundary=64,
               max_bounce=depth, secondary_edge_hypercube_resolution=[20000, 6, 6], secondary_edge_preprocess_rounds=4,
@@ -135,7 +135,7 @@ def test_interpenetration_crease_vs_fd(cuda, depth):
     crease = _gpu_translation_grad(spec, mesh, dr.PathIntegrator(gradient_terms=32, **kw), g)
     fd = fd_translation(_gpu_render(dr.PathIntegrator(**dict(kw, spp_interior=4096))), spec, mesh, g, 1e-2)
     e, e_without = rel_l2(ad, fd), rel_l2(ad - crease, fd)
-    print(f"sunk ball: AD {ad} (crease share {crease}) FD {fd}: rel L2 {e:.3f}, without the crease term {e_without:.3f}")
+    print(f"creased wall: AD {ad} (crease share {crease}) FD {fd}: rel L2 {e:.3f}, without the crease term {e_without:.3f}")
     assert np.abs(crease).max() > 0
     assert e < 0.05
 
