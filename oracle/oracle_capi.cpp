@@ -444,46 +444,14 @@ inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32
 }
 
 // Indirect shadow-boundary term (test restatement of the GPU term): the shadow-boundary
-// geometry of eval_direct_unb with the light point replaced by a point y on any mesh
-// surface, area-sampled over the mesh triangles (light triangles excluded, pdf 1 / total
-// area; the triangle from the prefix sums with the uniform rescaled for reuse, then the
-// light sampler's barycentric mapping). The radiance leaving y toward x_b comes from a
-// path of max_bounce - 1 bounces from y (stream kIndirectStream + 2^28 + i); the receiver
-// connects to the camera directly (perspective views only).
+// geometry of eval_direct_unb with the light point replaced by the first mesh surface y seen
+// from the edge point x_b in a direction w drawn uniformly inside the edge's silhouette lune
+// (the directions for which exactly one of the two faces at the edge faces w: two opposite
+// wedges of angle alpha between the face normals, solid angle 4 alpha; coordinates (u2, u3):
+// the wedge and the position across it from u2, cos(theta) = 1 - 2 u3 along the edge). The
+// radiance leaving y toward x_b comes from a path of max_bounce - 1 bounces from y (stream
+// kIndirectStream + 2^28 + i); the receiver connects to the camera directly (perspective).
 constexpr uint64_t kIndirectStream = 0xE0000000ull;
-
-struct SurfCdfO {
-  std::vector<double> w, pre;
-  void build(const Scene<float>& sf) {
-    const int nmesh = sf.n_obj - (int)sf.light_kind.size();
-    double acc = 0;
-    for (const Tri<float>& t : sf.tris) {
-      const double a = t.obj < nmesh ? double(t.area) : 0.0;
-      w.push_back(a);
-      acc += a;
-      pre.push_back(acc);
-    }
-  }
-  bool sample(const Scene<float>& sf, float rx, float ry, int& tri, float& su, float& sv, V3<float>& y,
-              double& pdf) const {
-    const double tot = pre.back();
-    if (!(tot > 0)) return false;
-    const double t = double(rx) * tot;
-    int lo = int(std::upper_bound(pre.begin(), pre.end(), t) - pre.begin());
-    if (lo >= (int)pre.size()) lo = (int)pre.size() - 1;
-    if (!(w[lo] > 0)) return false;
-    const double base = lo > 0 ? pre[lo - 1] : 0.0;
-    const float r = std::min(std::max(float((t - base) / w[lo]), 0.f), 0.99999994f);
-    const Tri<float>& T = sf.tris[lo];
-    const float sq = ry > 0 ? std::sqrt(ry) : 0.f;
-    su = r * sq;
-    sv = 1.0f - sq;
-    y = T.p0 + (T.p1 - T.p0) * su + (T.p2 - T.p0) * sv;
-    pdf = double(float(1.0 / tot));
-    tri = lo;
-    return true;
-  }
-};
 
 // Intersection record of the point with barycentrics (b1, b2) on triangle tri, reached from o
 // (the construction of scene_hit for a given hit).
@@ -515,48 +483,51 @@ inline Its<S> its_at(const Scene<S>& sc, int tri, double b1, double b2, const V3
 }
 
 // Returns the derivative carrier d_eff . (w x e); out gets the camera connection of the
-// receiver (weight without the source radiance) and the source's triangle and barycentrics.
+// receiver (weight without the source radiance) and the source hit.
 struct IndirectOut {
   bool ok = false;
   int pix = 0;
   V3<double> w;  // k0 J_cam f_r(x_d) (the source radiance multiplies it)
   double nsn = 0;
   int ytri = -1;
-  float su = 0, sv = 0;
+  double yb1 = 0, yb2 = 0;
   V3<float> xb;
 };
 template <class S, bool AD>
-inline S eval_indirect_unb(const Ctx<S, AD>& c, const SurfCdfO& cdf, typename Traits<S>::R s3[3], IndirectOut& out) {
+inline S eval_indirect_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], IndirectOut& out) {
   using R = typename Traits<S>::R;
   const Scene<S>& sc = c.sc;
-  const Scene<float>& sf = *c.scf;
   out.ok = false;
   S dn = S(0);
   R s = s3[0], pe;
   int ei = sc.edge_cdf.sample_reuse(s, pe);
   const Edge<S>& E = sc.edges[ei];
-  int yt;
-  float su, sv;
-  V3<float> yf;
-  double pdf_y;
-  if (!cdf.sample(sf, float(s3[1]), float(s3[2]), yt, su, sv, yf, pdf_y)) return dn;
   V3<S> xb = E.p0 + (E.p1 - E.p0) * S(s);
-  const Tri<S>& ty = sc.tris[yt];
-  V3<S> yl = ty.p0 + (ty.p1 - ty.p0) * S(R(su)) + (ty.p2 - ty.p0) * S(R(sv));
   double pdf_e = double(pe) / val(E.len);
-  V3<S> dir = normalize(xb - yl);
-  bool valid = val(dot(E.nl, dir)) * val(dot(E.nr, dir)) < 0 && val(norm(E.nl - E.nr)) > 1e-5;
-  Its<S> is0 = scene_hit<S, AD>(sc, xb, -dir, valid);
-  valid = valid && is0.valid && !is0.is_light && val(sqnorm(is0.p - yl)) < double(R(1e-5));
+  // the lune direction toward the source
+  const V3<double> evd = normalize(val3(E.p1) - val3(E.p0)), nl = val3(E.nl), nr = val3(E.nr);
+  const V3<double> bb = cross(evd, nl);
+  const double ar = std::atan2(dot(nr, bb), dot(nr, nl)), alpha = std::fabs(ar);
+  const bool second = double(s3[1]) >= 0.5;
+  const double t = second ? 2 * double(s3[1]) - 1 : 2 * double(s3[1]);
+  const double psi = (second ? -0.5 * M_PI : 0.5 * M_PI) + t * ar;
+  const double ct = 1 - 2 * double(s3[2]), st = std::sqrt(std::max(0.0, 1 - ct * ct));
+  const V3<double> wyd = evd * ct + (nl * std::cos(psi) + bb * std::sin(psi)) * st;
+  const V3<S> wy(S(wyd.x), S(wyd.y), S(wyd.z));
+  const V3<S> dir = -wy;
+  bool valid = alpha > 1e-5 && val(dot(E.nl, dir)) * val(dot(E.nr, dir)) < 0 && !c.cam.ortho;
+  Its<S> is0 = scene_hit<S, AD>(sc, xb, wy, valid);
+  valid = valid && is0.valid && !is0.is_light;
   Its<S> id0 = scene_hit<S, AD>(sc, xb, dir, valid);
-  valid = valid && id0.valid && !id0.is_light && !c.cam.ortho;
+  valid = valid && id0.valid && !id0.is_light;
   if (!valid) return dn;
+  const V3<S> yl = is0.p;
   V3<double> xbv = val3(xb), yv = val3(yl), xdv = val3(id0.p);
-  V3<double> w = normalize(xbv - yv);
-  V3<double> ev = normalize(val3(E.p1) - val3(E.p0));
+  V3<double> w = val3(dir);
+  V3<double> ev = evd;
   if (dot(cross(w, ev), val3(E.out)) < 0) ev = -ev;
   V3<double> ns = cross(w, ev);
-  double dby = norm(xbv - yv), lam = norm(xdv - yv) / dby;
+  double lam = norm(xdv - yv) / norm(xbv - yv);
   // the receiver seen by the camera
   const V3<S> to_cam = normalize(c.cam_pos - id0.p);
   if (val(dot(id0.n, to_cam)) <= 0) return dn;
@@ -570,19 +541,16 @@ inline S eval_indirect_unb(const Ctx<S, AD>& c, const SurfCdfO& cdf, typename Tr
     V3<S> deff = (xb - detach(xb)) - (id0.p - detach(id0.p)) * S(1.0 / lam) - (yl - detach(yl)) * S(1.0 - 1.0 / lam);
     dn = dot(deff, V3<S>(S(ns.x), S(ns.y), S(ns.z)));
   }
-  const double cos_y = std::fabs(dot(normalize(val3(ty.n)), w));
-  const double k0 = -cos_y / (dby * dby) / (pdf_e * pdf_y * c.cam.H * c.cam.W);
+  const double k0 = -4 * alpha / (pdf_e * c.cam.H * c.cam.W);
   const double Jc = raster_fxfy(c.cam) * val(cam_jacobian(c.cam, val3(id0.p), val3(id0.n), val3(c.cam_pos)));
-  // the receiver as reached from the edge side, reflecting toward the camera
-  Its<S> idb = its_at(sc, id0.tri, id0.b1, id0.b2, xb);
-  const V3<double> fr = val3(bsdf_eval(sc, idb, to_cam));
+  const V3<double> fr = val3(bsdf_eval(sc, id0, to_cam));
   out.ok = true;
   out.pix = ry * c.cam.W + rx;
   out.w = fr * (k0 * Jc);
   out.nsn = norm(ns);
-  out.ytri = yt;
-  out.su = su;
-  out.sv = sv;
+  out.ytri = is0.tri;
+  out.yb1 = is0.b1;
+  out.yb2 = is0.b2;
   out.xb = V3<float>(float(xbv.x), float(xbv.y), float(xbv.z));
   return dn;
 }
@@ -933,7 +901,7 @@ inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
 // Guiding preprocess of the indirect shadow-boundary term: per cell the magnitude of its
 // sample's camera weight without the source radiance (|k0 J_cam| |f_r| |w x e|).
 template <class R>
-inline HyperCube<R> preprocess_indirect(const Ctx<R, false>& c, const SurfCdfO& cdf) {
+inline HyperCube<R> preprocess_indirect(const Ctx<R, false>& c) {
   HyperCube<R> hc;
   hc.init(3, c.cfg.se_res);
   std::vector<double> rst(hc.cells, 0.0);
@@ -949,7 +917,7 @@ inline HyperCube<R> preprocess_indirect(const Ctx<R, false>& c, const SurfCdfO& 
       for (int k = 0; k < 3; ++k) s3[k] = rngs[i].next_float();
       for (int k = 0; k < 3; ++k) s3[k] = (R(cc[k]) + s3[k]) * hc.unit[k];
       IndirectOut o;
-      eval_indirect_unb<R, false>(c, cdf, s3, o);
+      eval_indirect_unb<R, false>(c, s3, o);
       if (o.ok) add[i] = double(float(std::fabs(norm(o.w)) * o.nsn));
     }
     for (int i = 0; i < hc.cells; ++i) rst[i] = double(R(R(rst[i]) + R(add[i])));
@@ -1280,9 +1248,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
   // ---- indirect shadow boundaries (unbiased estimator only, perspective cameras, D >= 2)
   if ((which & 64) && unb && !c.cam.ortho && c.cfg.max_bounce >= 2) {
     if constexpr (KD > 0) {
-      SurfCdfO cdf;
-      cdf.build(*c.scf);
-      HyperCube<R> hc = preprocess_indirect<R>(*cv, cdf);
+      HyperCube<R> hc = preprocess_indirect<R>(*cv);
       const int spp = c.cfg.spp_secondary_edge;
       const uint64_t N = (uint64_t)npix * spp;
       const uint64_t so = c.cfg.seed * 2654435761ull;
@@ -1294,11 +1260,11 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
         for (int k = 0; k < 3; ++k) s3[k] = rng.next_float();
         const double hp = hc.sample_unb(s3, rng);
         IndirectOut o;
-        const S dn = eval_indirect_unb<S, AD>(c, cdf, s3, o);
+        const S dn = eval_indirect_unb<S, AD>(c, s3, o);
         if (!o.ok) continue;
         // the radiance leaving y toward x_b: a path of max_bounce - 1 bounces from y
         Pcg32 ry = make_sampler(kIndirectStream + 0x10000000ull + (uint64_t)i + so);
-        Its<float> iy = its_at(*c.scf, o.ytri, double(o.su), double(o.sv), o.xb);
+        Its<float> iy = its_at(*c.scf, o.ytri, o.yb1, o.yb2, o.xb);
         V3<float> Lo = trace2light<float, false>(*c.scf, ry, iy, true, c.cfg.mis_light_samples,
                                                  c.cfg.mis_bsdf_samples, c.cfg.max_bounce - 1, false);
         double wg = 0;

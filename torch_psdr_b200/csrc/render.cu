@@ -2546,54 +2546,34 @@ __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict
 
 // ------------------------------------------------------------------ indirect shadow boundaries
 // Unbiased estimator: shadow boundaries of light that other surfaces reflect. The geometry
-// is the shadow-boundary term's with the light point replaced by a point y on any mesh
-// surface (area-sampled: pdf 1 / total mesh area): an edge point x_b that is a silhouette
-// seen from y, unoccluded toward y, and the receiver x_d beyond it, seen by the camera. The
+// is the shadow-boundary term's with the light point replaced by the first surface y seen
+// from the edge point x_b in a direction w sampled inside the edge's silhouette lune: the
+// directions w = cos(t) e + sin(t) m(psi) for which exactly one of the two faces at the edge
+// faces w, two opposite wedges of angle alpha (the angle between the face normals) around
+// the edge, solid angle 4 alpha, sampled uniformly (pdf 1 / (4 alpha)). Measured this way
+// the geometric factor cos_y / |x_b - y|^2 of the area form cancels, so sample weights stay
+// bounded. y must be a mesh surface (light sources are the shadow-boundary term's); the
+// receiver x_d is the first hit from x_b away from y and must be seen by the camera. The
 // radiance leaving y toward x_b is a path traced from y with max_bounce - 1 bounces (y is
-// the second vertex of the camera path through x_d); the boundary moves over the receiver
-// at d_eff = dx_b - dx_d / lam - dy (1 - 1/lam) as for the light. Receivers that reach the
-// camera only through further bounces are left out (their source paths would be one
-// bounce shorter per chain vertex).
+// the second vertex of the camera path through x_d); the boundary moves over the receiver at
+// d_eff = dx_b - dx_d / lam - dy (1 - 1/lam) as for the light. Receivers that reach the
+// camera only through further bounces are left out (their source paths would be one bounce
+// shorter per chain vertex).
 constexpr unsigned long long kIndirectStream = 0xE0000000ull;  // streams of the source paths
 
-struct SurfCdf {
-  const double* w;    // area of each mesh triangle (0 for light triangles)
-  const double* pre;  // inclusive prefix sums
-  int ntri;
-};
-
-// A point on the mesh surfaces by area: triangle by the prefix sums (rx rescaled for reuse),
-// then the light sampler's barycentric mapping.
-PSDR_D bool sample_surface(const DevScene& sc, const SurfCdf& cdf, float rx, float ry, LightSample& out) {
-  const double tot = cdf.pre[cdf.ntri - 1];
-  if (!(tot > 0.0)) return false;
-  const double t = (double)rx * tot;
-  int lo = 0, hi = cdf.ntri - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (cdf.pre[mid] > t) hi = mid;
-    else lo = mid + 1;
-  }
-  if (!(cdf.w[lo] > 0.0)) return false;
-  const double base = lo > 0 ? cdf.pre[lo - 1] : 0.0;
-  const float r = fminf(fmaxf((float)((t - base) / cdf.w[lo]), 0.f), 0.99999994f);
-  const float4* R = sc.tri + 6 * (size_t)lo;
-  const float3 p0 = xyz(__ldg(R)), p1 = xyz(__ldg(R + 1)), p2 = xyz(__ldg(R + 2));
-  const float sq = ry > 0.f ? sqrtf(ry) : 0.f;
-  out.su = r * sq;
-  out.sv = 1.0f - sq;
-  out.y = p0 + (p1 - p0) * out.su + (p2 - p0) * out.sv;
-  out.pdf = (float)(1.0 / tot);
-  out.tri = lo;
-  out.light = -1;
-  return true;
-}
-
-__global__ void k_surf_mass(const DevScene* __restrict__ scenes, int si, double* __restrict__ w) {
-  const DevScene& sc = scenes[si];
-  const int nmesh = sc.nobj - sc.nlight;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < sc.ntri; t += gridDim.x * blockDim.x)
-    w[t] = __ldg(sc.tri_v + t).w < nmesh ? (double)__ldg(sc.tri + 6 * (size_t)t).w : 0.0;
+// Direction of lune coordinates (u2, u3) in [0, 1)^2 at an edge with unit direction ev and
+// unit face normals nl, nr (both perpendicular to ev); alpha gets the wedge angle.
+PSDR_D float3 lune_dir(float3 ev, float3 nl, float3 nr, float u2, float u3, float& alpha) {
+  const float3 b = cross(ev, nl);
+  const float ar = atan2f(dot(nr, b), dot(nr, nl));  // nr's angle from nl around ev
+  alpha = fabsf(ar);
+  const bool second = u2 >= 0.5f;
+  const float t = second ? 2.f * u2 - 1.f : 2.f * u2;
+  const float psi = (second ? -0.5f * kPi : 0.5f * kPi) + t * ar;
+  const float ct = 1.f - 2.f * u3, st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+  float sp, cp;
+  sincosf(psi, &sp, &cp);
+  return ev * ct + (nl * cp + b * sp) * st;
 }
 
 // PRE: guiding mass per hypercube cell (|k0 J_cam| |f_r(x_d)| |w x e|; the source radiance
@@ -2601,7 +2581,7 @@ __global__ void k_surf_mass(const DevScene* __restrict__ scenes, int si, double*
 // a path from y (slot s) whose radiance toward x_b the depth loop computes.
 template <bool PRE>
 __global__ void __launch_bounds__(128) k_indirect(WF w, const DevScene* __restrict__ scenes,
-                                                  const DevView* __restrict__ views, int v, EdgeBuf eb, SurfCdf cdf,
+                                                  const DevView* __restrict__ views, int v, EdgeBuf eb,
                                                   long long begin, int n, HCube hc, int round, float* mass) {
   const DevView& V = views[v];
   const DevScene& sc = scenes[V.scene];
@@ -2645,66 +2625,61 @@ __global__ void __launch_bounds__(128) k_indirect(WF w, const DevScene* __restri
       const int ne = *sc.n_edges;
       float sx = s3[0], pe;
       const int e = ok ? discrete_sample(sc.edge_pmf, sc.edge_cmf, ne, sx, pe) : 0;
-      LightSample ys;
-      ok = ok && sample_surface(sc, cdf, s3[1], s3[2], ys);
-      float3 xb = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 1.f), nsv = f3(0.f, 0.f, 0.f);
-      float pdf_e = 0.f;
-      HitRec hd;
-      hd.tri = -1;
+      float3 xb = f3(0.f, 0.f, 0.f), nsv = f3(0.f, 0.f, 0.f);
+      HitRec hy, hd;
+      hy.tri = hd.tri = -1;
+      hy.b1 = hy.b2 = 0.f;
       if (ok) {
         const float4 E0 = __ldg(sc.edge + 4 * (size_t)e), E1 = __ldg(sc.edge + 4 * (size_t)e + 1),
                      E2 = __ldg(sc.edge + 4 * (size_t)e + 2), E3 = __ldg(sc.edge + 4 * (size_t)e + 3);
         const float3 p0 = xyz(E0), p1 = xyz(E1);
         const float3 out = f3(E1.w, E2.x, E2.y), nl = f3(E2.z, E2.w, E3.x), nr = f3(E3.y, E3.z, E3.w);
         xb = p0 + (p1 - p0) * sx;
-        pdf_e = pe / E0.w;
-        dir = normalize(xb - ys.y);
-        ok = dot(nl, dir) * dot(nr, dir) < 0.f && norm(nl - nr) > kEps;
+        const float pdf_e = pe / E0.w;
+        float3 ev = normalize(p1 - p0);
+        float alpha;
+        const float3 wy = lune_dir(ev, nl, nr, s3[1], s3[2], alpha);  // toward the source
+        const float3 dir = -wy;                                       // from the source through x_b
+        ok = alpha > kEps && dot(nl, dir) * dot(nr, dir) < 0.f;
         if (ok) {
-          // x_b must see y: the closest hit toward y is y itself
-          const float dist = norm(xb - ys.y);
-          const HitRec hs = trace_closest(sc, xb, -dir, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
-          const Surf s0 = make_surf(sc, hs.tri, hs.b1, hs.b2, xb);
-          ok = s0.valid && !s0.is_light && sqnorm(s0.p - ys.y) < kEps;
-        }
-        if (ok) {
-          hd = trace_closest(sc, xb, dir, kTmin, INFINITY);
-          const Surf d0 = make_surf(sc, hd.tri, hd.b1, hd.b2, xb);
-          ok = d0.valid && !d0.is_light;
+          hy = trace_closest(sc, xb, wy, kTmin, INFINITY);
+          const Surf s0 = make_surf(sc, hy.tri, hy.b1, hy.b2, xb);
+          ok = s0.valid && !s0.is_light;
           if (ok) {
-            float3 ev = normalize(p1 - p0);
-            if (dot(cross(dir, ev), out) < 0.f) ev = -ev;
-            nsv = cross(dir, ev);
-            // the receiver seen by the camera (perspective views)
-            const float3 rel = d0.p - V.pos;
-            const float dist = norm(rel);
-            const float3 cd = rel / dist;
-            int qx = 0, qy = 0;
-            ok = !V.ortho && dot(d0.n, cd) < 0.f && project(V, d0.p, qx, qy);
+            hd = trace_closest(sc, xb, dir, kTmin, INFINITY);
+            const Surf d0 = make_surf(sc, hd.tri, hd.b1, hd.b2, xb);
+            ok = d0.valid && !d0.is_light;
             if (ok) {
-              const HitRec hc2 = trace_closest(sc, V.pos, cd, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
-              const Surf iv = make_surf(sc, hc2.tri, hc2.b1, hc2.b2, V.pos);
-              ok = iv.valid && !iv.is_light && sqnorm(iv.p - d0.p) < kEps;
-            }
-            if (ok) {
-              const float3 look = view_look(V);
-              const float z = dot(rel, look);
-              const float Jc = view_fxfy(V) * fabsf(dot(d0.n, rel)) / (z * z * z);
-              const float dby = norm(xb - ys.y);
-              const float4 yn = __ldg(sc.tri + 6 * (size_t)ys.tri + 3);
-              const float cos_y = fabsf(dot(normalize(xyz(yn)), dir));
-              const float k0 = -cos_y / (dby * dby) / (pdf_e * ys.pdf * (float)V.H * (float)V.W) * Jc;
-              const float lam = norm(d0.p - ys.y) / dby;
-              if (PRE) {
-                const float3 fr = surf_bsdf(sc, d0, -cd);
-                const float m = fabsf(k0) * norm(fr) * norm(nsv);
-                if (isfinite(m)) mass[i] = mass[i] + m;
-                ok = false;  // no path in the preprocess
-              } else {
-                eb.a[s] = make_float4(__int_as_float(e), sx, hpdf, __int_as_float(qy * V.W + qx));
-                eb.n[s] = make_float4(__int_as_float(ys.tri), ys.su, ys.sv, k0);
-                eb.hb[s] = make_float4(__int_as_float(hd.tri), hd.b1, hd.b2, lam);
-                eb.La[s] = make_float4(nsv.x, nsv.y, nsv.z, 0.f);
+              if (dot(cross(dir, ev), out) < 0.f) ev = -ev;
+              nsv = cross(dir, ev);
+              // the receiver seen by the camera (perspective views)
+              const float3 rel = d0.p - V.pos;
+              const float dist = norm(rel);
+              const float3 cd = rel / dist;
+              int qx = 0, qy = 0;
+              ok = !V.ortho && dot(d0.n, cd) < 0.f && project(V, d0.p, qx, qy);
+              if (ok) {
+                const HitRec hc2 = trace_closest(sc, V.pos, cd, kTmin, dist * 1.0001f + 4e-3f, dist - 4e-3f);
+                const Surf iv = make_surf(sc, hc2.tri, hc2.b1, hc2.b2, V.pos);
+                ok = iv.valid && !iv.is_light && sqnorm(iv.p - d0.p) < kEps;
+              }
+              if (ok) {
+                const float3 look = view_look(V);
+                const float z = dot(rel, look);
+                const float Jc = view_fxfy(V) * fabsf(dot(d0.n, rel)) / (z * z * z);
+                const float k0 = -4.f * alpha / (pdf_e * (float)V.H * (float)V.W) * Jc;
+                const float lam = norm(d0.p - s0.p) / norm(xb - s0.p);
+                if (PRE) {
+                  const float3 fr = surf_bsdf(sc, d0, -cd);
+                  const float m = fabsf(k0) * norm(fr) * norm(nsv);
+                  if (isfinite(m)) mass[i] = mass[i] + m;
+                  ok = false;  // no path in the preprocess
+                } else {
+                  eb.a[s] = make_float4(__int_as_float(e), sx, hpdf, __int_as_float(qy * V.W + qx));
+                  eb.n[s] = make_float4(__int_as_float(hy.tri), hy.b1, hy.b2, k0);
+                  eb.hb[s] = make_float4(__int_as_float(hd.tri), hd.b1, hd.b2, lam);
+                  eb.La[s] = make_float4(nsv.x, nsv.y, nsv.z, 0.f);
+                }
               }
             }
           }
@@ -2719,7 +2694,7 @@ __global__ void __launch_bounds__(128) k_indirect(WF w, const DevScene* __restri
         w.pix[s] = -1;
         w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
         w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-        w.cur[s] = make_float4(__int_as_float(ok ? ys.tri : -1), ys.su, ys.sv, 0.f);
+        w.cur[s] = make_float4(__int_as_float(ok ? hy.tri : -1), hy.b1, hy.b2, 0.f);
         w.org[s] = make_float4(xb.x, xb.y, xb.z, 0.f);
         alive = ok;
       }
@@ -3259,9 +3234,9 @@ static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v,
 
 // Indirect shadow-boundary samples [begin, begin + n) of view v: one source path each.
 static void indirect_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
-                           const SurfCdf& cdf, long long begin, int n, const HCube& hc, int spp, cudaStream_t st) {
+                           long long begin, int n, const HCube& hc, int spp, cudaStream_t st) {
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
-  k_indirect<false><<<grid_for(n, 128, 16), 128, 0, st>>>(w, scenes, vd, v, eb, cdf, begin, n, hc, 0, nullptr);
+  k_indirect<false><<<grid_for(n, 128, 16), 128, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, 0, nullptr);
   PSDR_LAUNCHED(1);
   WF wy = w;
   wy.D = w.D - 1;  // the source y is the second vertex of the camera path
@@ -3331,8 +3306,6 @@ void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector
   }
   ws->ensure_mass(std::max(s, nt), st);
   ws->crease.alloc(80 * (size_t)kCreaseCap + 256, st);
-  ws->surf_w.alloc(8 * (size_t)nt, st);
-  ws->surf_pre.alloc(8 * (size_t)nt, st);
 }
 
 void set_scene_ntri(std::vector<DevView>& views, const psdr_scene* const* scenes) {
@@ -3489,27 +3462,22 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
                      (int)std::min<long long>(cap, N - b0), N, V.grad_lens != nullptr, st);
     }
     // indirect shadow boundaries (unbiased estimator, perspective views, max_bounce >= 2):
-    // the mesh-surface area CDF, the guiding preprocess, then the samples
-    if (unb && (terms & 64) && V.dimage && !V.ortho && cfg.max_bounce >= 2 && V.scene_ntri > 0) {
-      const SurfCdf cdf{ws->surf_w.as<double>(), ws->surf_pre.as<double>(), V.scene_ntri};
-      k_surf_mass<<<num_sms() * 4, 256, 0, st>>>(scenes_dev, V.scene, ws->surf_w.as<double>());
-      PSDR_LAUNCHED(1);
-      inclusive_scan_double(ws->surf_w.as<double>(), ws->surf_pre.as<double>(), V.scene_ntri,
-                            ws->scan_tmp.as<double>(), st);
+    // the guiding preprocess, then the samples
+    if (unb && (terms & 64) && V.dimage && !V.ortho && cfg.max_bounce >= 2) {
       const int* r3 = cfg.secondary_edge_hypercube_resolution;
       const int cells = r3[0] * r3[1] * r3[2];
       PSDR_CUDA(cudaMemsetAsync(ws->mass.p, 0, sizeof(float) * cells, st));
       HCube pre{};
       for (int k = 0; k < 3; ++k) { pre.res[k] = r3[k]; pre.unit[k] = 1.0f / (float)r3[k]; }
       for (int r = 0; r < cfg.secondary_edge_preprocess_rounds; ++r) {
-        k_indirect<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, eb, cdf, 0, cells, pre, r,
+        k_indirect<true><<<grid_for(cells, 128, 16), 128, 0, st>>>(w, scenes_dev, vd, v, eb, 0, cells, pre, r,
                                                                    ws->mass.as<float>());
         PSDR_LAUNCHED(1);
       }
       const HCube hc = build_hcube(ws, cells, r3, 3, true, st);
       const long long N = (long long)V.H * V.W * cfg.spp_secondary_edge;
       for (long long b0 = 0; b0 < N; b0 += cap)
-        indirect_phase(wi, scenes_dev, vd, v, eb, cdf, b0, (int)std::min<long long>(cap, N - b0), hc,
+        indirect_phase(wi, scenes_dev, vd, v, eb, b0, (int)std::min<long long>(cap, N - b0), hc,
                        cfg.spp_secondary_edge, st);
     }
     // interpenetration creases (unbiased estimator, perspective views): the segments where

@@ -81,7 +81,6 @@ struct psdr_workspace {
   psdr::DBuf views, eb_a, eb_n, eb_hb, eb_La, eb_rng, mass, mass_d, mass_pre, hc_pmf, hc_cmf, scan_tmp, ncells;
   psdr::DBuf campos_acc, lens_acc;
   psdr::DBuf crease;  // interpenetration segments (unbiased estimator): kCreaseCap records + count
-  psdr::DBuf surf_w, surf_pre;  // mesh-surface area CDF of the indirect shadow-boundary term
   long long mass_cap = 0;
   // a DiffuseBsdfMaterial mesh or an environment light is in the scenes of the current job
   // (each entry point sets it; the extended kernel instances also handle the plain
