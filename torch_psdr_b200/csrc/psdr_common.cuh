@@ -399,7 +399,9 @@ PSDR_D void trace_begin(TraceState& s, float3 o, float3 d, float tmin, float tma
 }
 
 // One node or leaf visit; returns true when the query is finished (s.h holds the hit).
-PSDR_D bool trace_step(const DevScene& sc, TraceState& s, int* stack) {
+// Stk stores the traversal stack: push(i, node), pop(i).
+template <class Stk>
+PSDR_D bool trace_step(const DevScene& sc, TraceState& s, Stk& stack) {
   if (s.node >= 0) {
     const float4* nd = sc.nodes + 7 * (size_t)s.node;
     const float4 lx = __ldg(nd), hx = __ldg(nd + 1), ly = __ldg(nd + 2), hy = __ldg(nd + 3);
@@ -428,14 +430,14 @@ PSDR_D bool trace_step(const DevScene& sc, TraceState& s, int* stack) {
     cswap(k1, c1, k2, c2);
     if (k0 == INFINITY) {
       if (s.sp == 0) return true;
-      s.node = stack[--s.sp];
+      s.node = stack.pop(--s.sp);
       return false;
     }
     s.node = c0;
     if (s.sp + 3 <= kStack) {
-      if (k3 != INFINITY) stack[s.sp++] = c3;
-      if (k2 != INFINITY) stack[s.sp++] = c2;
-      if (k1 != INFINITY) stack[s.sp++] = c1;
+      if (k3 != INFINITY) stack.push(s.sp++, c3);
+      if (k2 != INFINITY) stack.push(s.sp++, c2);
+      if (k1 != INFINITY) stack.push(s.sp++, c1);
     } else {
       atomicOr(sc.err, 1);
     }
@@ -458,9 +460,10 @@ PSDR_D bool trace_step(const DevScene& sc, TraceState& s, int* stack) {
     }
   }
   if (s.sp == 0) return true;
-  s.node = stack[--s.sp];
+  s.node = stack.pop(--s.sp);
   return false;
 }
+
 
 // ------------------------------------------------------------------ surface points
 // scene.cc:106-161 Scene::hit: the point is re-formed from the triangle and the

@@ -260,7 +260,19 @@ __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict_
   const long long total = (long long)nk * Rd;
   if (ray_count && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ray_count, (unsigned long long)total);
   int* fetch = w.cnt + 2 * w.D + 2;
-  int stack[kStack];
+  // traversal stack: the first kShort entries of each lane in shared memory (one column per
+  // lane, so a warp's pushes and pops hit 32 banks), the deeper ones in local memory
+  constexpr int kShort = 16;
+  __shared__ int sst[kShort][128];
+  struct Stk {
+    int (*sh)[128];
+    int lane;
+    int deep[kStack - kShort];
+    __device__ __forceinline__ void push(int i, int v) { if (i < kShort) sh[i][lane] = v; else deep[i - kShort] = v; }
+    __device__ __forceinline__ int pop(int i) const { return i < kShort ? sh[i][lane] : deep[i - kShort]; }
+  } stack;
+  stack.sh = sst;
+  stack.lane = threadIdx.x;
   TraceState s;
   const DevScene* sc = nullptr;
   size_t slot = 0;
