@@ -452,6 +452,11 @@ inline S eval_direct_unb(const Ctx<S, AD>& c, typename Traits<S>::R s3[3], Pcg32
 // radiance leaving y toward x_b comes from a path of max_bounce - 1 bounces from y (stream
 // kIndirectStream + 2^28 + i); the receiver connects to the camera directly (perspective).
 constexpr uint64_t kIndirectStream = 0xE0000000ull;
+// a quarter of the shadow-boundary samples and of the guiding cells along the edge axis
+constexpr int kIndirectSampleDiv = 4, kIndirectCellDiv = 4;
+// the unbiased estimator's light-source shadow-boundary guide: four preprocess rounds per
+// requested round (the reference estimator keeps one)
+constexpr int kDirectGuideRounds = 4;
 
 // Intersection record of the point with barycentrics (b1, b2) on triangle tri, reached from o
 // (the construction of scene_hit for a given hit).
@@ -861,7 +866,8 @@ inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
   std::vector<double> rst(hc.cells, 0.0);
   std::vector<Pcg32> rngs(hc.cells);
   for (int i = 0; i < hc.cells; ++i) rngs[i] = make_sampler(i);
-  for (int round = 0; round < c.cfg.se_rounds; ++round) {
+  const int rounds = c.cfg.se_rounds * (c.cfg.mode == 1 ? kDirectGuideRounds : 1);
+  for (int round = 0; round < rounds; ++round) {
     std::vector<double> add(hc.cells, 0.0);
 #pragma omp parallel for schedule(dynamic, 256)
     for (int i = 0; i < hc.cells; ++i) {
@@ -903,7 +909,8 @@ inline HyperCube<R> preprocess_direct(const Ctx<R, false>& c) {
 template <class R>
 inline HyperCube<R> preprocess_indirect(const Ctx<R, false>& c) {
   HyperCube<R> hc;
-  hc.init(3, c.cfg.se_res);
+  const int res[3] = {std::max(1, c.cfg.se_res[0] / kIndirectCellDiv), c.cfg.se_res[1], c.cfg.se_res[2]};
+  hc.init(3, res);
   std::vector<double> rst(hc.cells, 0.0);
   std::vector<Pcg32> rngs(hc.cells);
   for (int i = 0; i < hc.cells; ++i) rngs[i] = make_sampler(kIndirectStream + (uint64_t)i);
@@ -1249,8 +1256,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
   if ((which & 64) && unb && !c.cam.ortho && c.cfg.max_bounce >= 2) {
     if constexpr (KD > 0) {
       HyperCube<R> hc = preprocess_indirect<R>(*cv);
-      const int spp = c.cfg.spp_secondary_edge;
-      const uint64_t N = (uint64_t)npix * spp;
+      const uint64_t N = std::max<uint64_t>(1, (uint64_t)npix * c.cfg.spp_secondary_edge / kIndirectSampleDiv);
       const uint64_t so = c.cfg.seed * 2654435761ull;
       std::vector<double> phi_s(N * KD, 0.0);
 #pragma omp parallel for schedule(dynamic, 64)
@@ -1270,7 +1276,7 @@ static void render_camera(const Ctx<S, AD>& c, int which, double* img, const dou
         double wg = 0;
         for (int k = 0; k < 3; ++k) wg += dLdI[3 * o.pix + k] * o.w[k] * double(Lo[k]);
         if (!std::isfinite(wg)) continue;
-        const double dens = hp * double(hc.cells) * spp;
+        const double dens = hp * double(hc.cells) * (double(N) / double(npix));
         for (int j = 0; j < KD; ++j) phi_s[i * KD + j] += wg * dn.d[j] / dens;
       }
       for (uint64_t i = 0; i < N; ++i) for (int j = 0; j < KD; ++j) dphi[j] += phi_s[i * KD + j];

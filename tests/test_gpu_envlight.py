@@ -149,6 +149,13 @@ def test_env_gradient_terms_match_oracle(cuda, kind, estimator, terms, kinds):
         # computation is compared without guiding (the guided path is compared in the
         # DiffuseMaterial, DiffuseBsdfMaterial and orthographic suites).
         kw.update(primary_edge_hypercube_resolution=1)
+    if terms == 4 and unb:
+        # The unbiased shadow-boundary guide takes four preprocess samples per cell; one of
+        # them resolving visibility differently in float (GPU) and double (oracle) changes
+        # that cell's mass and so shifts every later cell boundary of the guide, and the two
+        # sides then draw different samples. The per-sample computation is compared without
+        # guiding here (the guided path is compared in the DiffuseMaterial suite).
+        kw.update(secondary_edge_hypercube_resolution=[1, 1, 1])
     gseeds, oseeds = _env_seeds(spec, kinds, np.random.default_rng(3))
     params = set()
     for k in kinds:

@@ -58,6 +58,11 @@ def test_unbiased_translation_matches_fd_under_environment_light(kind):
     cfg = dict(CFG, spp_interior=spp, spp_primary_edge=spp, spp_secondary_edge=spp, spp_pixel_boundary=spp,
                secondary_edge_hypercube_resolution=(2000, 6, 6))
     g = smooth_weights(48, 48)
-    ad = orc.grad_dir(spec, [g], which=15, seed_verts=translation_seeds(spec, mesh), **cfg)[:3]
-    fd = fd_translation(lambda s: orc.render(s, precision=1, **cfg)[0], spec, mesh, g, 1e-2)
+    # the shadow-boundary term's samples are heavy-tailed here (one run moves its share by
+    # tens of percent, about 3 % of the whole gradient), so the gradient is the mean of eight
+    # independent runs and the finite differences the mean of two
+    ad = np.mean([orc.grad_dir(spec, [g], which=15, seed_verts=translation_seeds(spec, mesh), seed=s, **cfg)[:3]
+                  for s in range(8)], axis=0)
+    fd = np.mean([fd_translation(lambda sp: orc.render(sp, precision=1, seed=s, **cfg)[0], spec, mesh, g, 1e-2)
+                  for s in range(2)], axis=0)
     assert rel_l2(ad, fd) < 0.06, (ad, fd)
