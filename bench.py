@@ -237,6 +237,48 @@ def grad_check(torch, dr, integ, build_scene, base, tex, dev, h=1e-3, fd_spp=409
             "fd_step": h, "fd_spp": fd_spp, "replicas": replicas, "seeds": list(range(1, max(replicas, ad_replicas) + 1))}
 
 
+# ---------------------------------------------------------------- per-phase breakdown
+TERMS = ((1, "interior"), (2, "silhouettes"), (4, "shadow_boundaries"), (8, "pixel_borders"),
+         (64, "indirect_shadow_boundaries"), (32, "creases"))
+
+
+def phase_breakdown(torch, dr, integ_kw, run_step, flush, reps=3):
+    """Device milliseconds of the plain step's phases, each timed alone with CUDA events
+    (median of `reps` after one warm-up, L2 flushed before each): `forward` = scene
+    construction + renderD forward + loss with the backward skipped; each gradient term =
+    a plain step whose backward is restricted to that term (gradient_terms), minus
+    `forward`. run_step(integ, backward) runs one plain step."""
+    stream = torch.cuda.current_stream()
+
+    def med(fn):
+        ts = []
+        for r in range(reps + 1):
+            flush.fill_(float(r))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            if r:
+                ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    base = dr.PathIntegrator(**integ_kw)
+    fwd = med(lambda: run_step(base, False))
+    out = {"forward": fwd}
+    total = fwd
+    est = integ_kw.get("estimator", "reference")
+    for bit, name in TERMS:
+        if est != "unbiased" and bit not in (1, 2, 4):
+            continue
+        integ = dr.PathIntegrator(**dict(integ_kw, gradient_terms=bit))
+        t = max(0.0, med(lambda: run_step(integ, True)) - fwd)
+        out[name] = t
+        total += t
+    out["sum"] = total
+    return out
+
+
 # ---------------------------------------------------------------- replicas
 def max_over_ranks(value, dist, device):
     """The largest of the ranks' values (device times are taken as the max over ranks);
@@ -288,7 +330,8 @@ def run_b200(args):
     gV, gF, gT = tens(ground.vertices), tens(ground.faces, torch.int32), tens(ground.texture)
     lV, lF, lE = tens(light.vertices), tens(light.faces, torch.int32), tens(light.emit)
     cam = dr.PerspectiveCamera(tens(c.look_from), tens(c.look_at), tens(c.up), tens([c.vfov]), H, W)
-    integ = dr.PathIntegrator(estimator=args.estimator, **CFG)
+    integ = dr.PathIntegrator(estimator=args.estimator, batch_lanes=args.batch_lanes,
+                              batch_records=args.batch_records, **CFG)
 
     leaf = {"size": 1}
 
@@ -378,7 +421,13 @@ def run_b200(args):
     other = step_plain if args.mode == "batched" else step_batched
     total_ms, (launches, trace_launches, rays), trace_ms_v, clk = timed(step, True)
     value = job_rate(world, samples, args.steps, total_ms)
-    other_ms, _, _, _ = timed(other, False)
+    other_ms, other_prof, other_trace_ms, _ = timed(other, False)
+    # the trace kernel's launch durations for the roofline come from the plain step, whose
+    # launches run one at a time (the batched graph overlaps kernels of concurrent lanes)
+    if args.mode == "plain":
+        plain_ms, (_, plain_tl, plain_rays), plain_trace_ms = total_ms, (launches, trace_launches, rays), trace_ms_v
+    else:
+        plain_ms, (_, plain_tl, plain_rays), plain_trace_ms = other_ms, other_prof, other_trace_ms
     other_value = job_rate(world, samples, args.steps, other_ms)
 
     # ---------------- end-to-end through the public API with host buffers
@@ -415,8 +464,8 @@ def run_b200(args):
     d2h = h_grad.numel() * 4 + 4
 
     peak, peak_kind = peaks()
-    trace_avg_ms = trace_ms_v / max(1, trace_launches)
-    achieved = (rays / max(1, trace_launches)) * TRACE_BYTES_PER_RAY / (trace_avg_ms / 1e3) / 1e9
+    trace_avg_ms = plain_trace_ms / max(1, plain_tl)
+    achieved = (plain_rays / max(1, plain_tl)) * TRACE_BYTES_PER_RAY / (trace_avg_ms / 1e3) / 1e9
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded icosphere scene)",
@@ -432,12 +481,26 @@ def run_b200(args):
             "roofline": {"bound": "hbm", "kernel": "k_trace (LBVH closest hit)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": None,
-                         "bytes_per_unit": f"{TRACE_BYTES_PER_RAY} B/ray", "rays_per_launch": rays / max(1, trace_launches),
-                         "trace_share_of_step": trace_ms_v / max(total_ms, 1e-9),
+                         "bytes_per_unit": f"{TRACE_BYTES_PER_RAY} B/ray",
+                         "rays_per_launch": plain_rays / max(1, plain_tl), "avg_launch_ms": trace_avg_ms,
+                         "timed_in": "plain step (launches one at a time)",
+                         "trace_share_of_step": plain_trace_ms / max(plain_ms, 1e-9),
                          "step_algorithmic_gbs": samples * STEP_BYTES_PER_SAMPLE / (total_ms / args.steps / 1e3) / 1e9},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "clocks": clk,
             "rays_per_s": rays / (total_ms / 1e3)}
+    if rank == 0 and world == 1 and not args.no_phases:
+        integ_kw = dict(CFG, estimator=args.estimator, tile_paths=int(integ.cfg.tile_paths),
+                        trace_queue=int(integ.cfg.trace_queue))
+
+        def run_phase_step(pi, backward):
+            tt = torch.zeros(3, device=dev, requires_grad=backward)
+            img = pi.renderD(build_scene(base + tt, tex))[0]
+            loss = ((img - target) ** 2).sum()
+            if backward:
+                loss.backward()
+
+        line["config"]["phases_ms"] = phase_breakdown(torch, dr, integ_kw, run_phase_step, flush)
     if rank == 0 and world == 1 and not args.no_grad_check:
         try:
             line["grad_check"] = grad_check(torch, dr, integ, build_scene, base, tex, dev)
@@ -469,7 +532,7 @@ def run_multiview(args):
     torch.cuda.set_device(dev)
     cams = synth.orbit_cameras(64, 4.0, seed=3, size_lo=128, size_hi=512)
     cfg = dict(spp_interior=16, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=4, estimator=args.estimator)
-    integ = dr.PathIntegrator(**cfg)
+    integ = dr.PathIntegrator(batch_lanes=args.batch_lanes, batch_records=args.batch_records, **cfg)
 
     def tens(a, dt=torch.float32, rg=False):
         return torch.tensor(np.asarray(a), dtype=dt, device=dev, requires_grad=rg)
@@ -532,6 +595,17 @@ def run_multiview(args):
 
     b_ms, clk = timed(step_batched, True)
     p_ms, _ = timed(step_plain, False)
+    phases = None
+    if not args.no_phases:
+        def run_phase_step(pi, backward):
+            for d, tg in zip(scenes_data, targets):
+                for cam, t in zip(d["cams"], tg):
+                    img = pi.renderD(scene_of(d, [cam]))[0]
+                    loss = ((img - t) ** 2).sum()
+                    if backward:
+                        loss.backward()
+
+        phases = phase_breakdown(torch, dr, cfg, run_phase_step, flush, reps=1)
     value = paths * args.steps / (b_ms / 1e3)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": b_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -540,7 +614,7 @@ def run_multiview(args):
                        "mode": "batched (one work list, forward and backward graphs)",
                        "other_mode": {"mode": "plain (per view: new Scene, renderD, backward)",
                                       "value": paths * args.steps / (p_ms / 1e3), "ms_per_step": p_ms / args.steps},
-                       "batched_over_plain": p_ms / b_ms,
+                       "batched_over_plain": p_ms / b_ms, "phases_ms": phases,
                        "l2": "flushed between steps (256 MiB write outside the timed events)"},
             "clocks": clk}
     print(json.dumps(line), flush=True)
@@ -564,7 +638,7 @@ def run_large(args):
     torch.cuda.set_device(dev)
     spec = synth.large_scene()
     cfg = dict(spp_interior=64, spp_primary_edge=4, spp_secondary_edge=4, max_bounce=5, estimator=args.estimator)
-    integ = dr.PathIntegrator(**cfg)
+    integ = dr.PathIntegrator(batch_lanes=args.batch_lanes, batch_records=args.batch_records, **cfg)
 
     def tens(a, dt=torch.float32, rg=False):
         return torch.tensor(np.asarray(a), dtype=dt, device=dev, requires_grad=rg)
@@ -632,6 +706,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad-check", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-phases", action="store_true", help="skip the per-phase breakdown of the plain step")
+    ap.add_argument("--batch-lanes", type=int, default=0, help="PathIntegrator batch_lanes (0 = library default)")
+    ap.add_argument("--batch-records", type=int, default=0, choices=[-1, 0, 1],
+                    help="PathIntegrator batch_records (0 = keep when they fit a quarter of free memory)")
     ap.add_argument("--estimator", default="unbiased", choices=["unbiased", "reference"])
     ap.add_argument("--workload", default="geometry", choices=["geometry", "multiview", "large"],
                     help="geometry: the 512^2 fwd+bwd workload (default); multiview: 64 views over 3 scenes; "

@@ -140,6 +140,19 @@ typedef struct {
   int32_t trace_queue; /* ABI 5: rays each SM traverses concurrently in the wavefront
                           closest-hit kernel, in units of 128 (the traversal queue depth;
                           1..8, 0 = 8); psdr_autotune picks it. Results do not depend on it. */
+  int32_t batch_lanes; /* ABI 6: psdr_batch_* only: concurrent streams ("lanes"), each with
+                          its own wavefront workspace, over which a batch spreads the
+                          independent parts of its job -- the forward's tiles, and in the
+                          backward the interior tiles and every boundary term of every view
+                          (1..8, 0 = 4; psdr_render_* run them one after another). Gradients
+                          are bitwise the same for every value. */
+  int32_t batch_records; /* ABI 6: psdr_batch_* only: the forward keeps the replay records of
+                            every interior path (16 B x (1 + D x R + 2 D) + 8 B per path, D =
+                            max_bounce, R = light + BSDF samples + 1) and the backward runs the
+                            adjoint from them instead of re-tracing the paths. 0 = when they
+                            fit in a quarter of the device memory free at psdr_batch_create,
+                            1 = always, -1 = never (re-trace, memory O(tile)). Gradients are
+                            bitwise the same either way. */
 } psdr_config;
 
 /* Gradient outputs of psdr_render_bwd (caller-owned device buffers, fp32).

@@ -37,7 +37,7 @@ def test_header_symbols_exported(lib):
 
 def test_version_and_errors(lib):
     assert b"sm_100a" in lib.psdr_version()
-    assert lib.psdr_abi_version() == 5
+    assert lib.psdr_abi_version() == 6
     out = C.c_void_p()
     st = lib.psdr_scene_create(None, None, C.byref(out))
     assert st == L.PSDR_ERR_INVALID_ARG

@@ -121,3 +121,45 @@ def test_batch_extended_features_match_plain(cuda):
             got = T[k].grad
             err = (got - g).abs().max().item() / (g.abs().max().item() + 1e-30)
             assert err < 1e-5, (k, err)
+
+
+@pytest.mark.parametrize("estimator", ["unbiased", "reference"])
+def test_batch_lanes_give_bitwise_equal_results(cuda, estimator):
+    """The batch's concurrent lanes (forward tiles, backward interior tiles and per-view
+    boundary terms on forked streams with their own workspaces) and its kept replay
+    records (the backward's adjoint reads the forward's records instead of re-tracing)
+    change neither the images nor any gradient: the integer gradient sums do not depend on
+    the order of additions, and the kept records are the ones a replay writes."""
+    specs = make_specs()
+    kinds = {"verts", "tex", "emit", "cam", "light_verts"}
+    rng = np.random.default_rng(1)
+    results, gs = [], None
+    # small tiles: several interior tiles for the lanes to share
+    kw = dict(KW, tile_paths=4096)
+    for lanes, records in ((1, -1), (3, -1), (8, 0), (1, 1), (4, 1)):
+        integ = dr.PathIntegrator(estimator=estimator, batch_lanes=lanes, batch_records=records, **kw)
+        scenes, Ts = zip(*[to_torch_scene(s, requires_grad=kinds) for s in specs])
+        batch = dr.BatchRender(integ, list(scenes))
+        for rep in range(2):  # capture, then replay
+            for T in Ts:
+                for v in T.values():
+                    if v is not None:
+                        v.grad = None
+            imgs = batch.renderD()
+            if gs is None:
+                gs = [torch.tensor(rng.normal(size=tuple(i.shape)), dtype=torch.float32, device="cuda")
+                      for i in imgs]
+            torch.autograd.backward(imgs, gs)
+            torch.cuda.synchronize()
+        results.append(([i.detach().clone() for i in imgs],
+                        [{k: v.grad.clone() for k, v in T.items() if v is not None and v.grad is not None}
+                         for T in Ts]))
+    imgs0, grads0 = results[0]
+    assert sum(len(g) for g in grads0) >= 10
+    for imgs, grads in results[1:]:
+        for a, b in zip(imgs, imgs0):
+            assert torch.equal(a, b)
+        for g, g0 in zip(grads, grads0):
+            assert g.keys() == g0.keys()
+            for k in g0:
+                assert torch.equal(g[k], g0[k]), k

@@ -61,7 +61,8 @@ class Config(C.Structure):
                 ("primary_edge_hypercube_resolution", C.c_int32),
                 ("secondary_edge_hypercube_resolution", C.c_int32 * 3), ("estimator", C.c_int32),
                 ("tile_paths", C.c_int32), ("leaf_size", C.c_int32), ("terms", C.c_int32),
-                ("spp_pixel_boundary", C.c_int32), ("seed", C.c_uint64), ("trace_queue", C.c_int32)]
+                ("spp_pixel_boundary", C.c_int32), ("seed", C.c_uint64), ("trace_queue", C.c_int32),
+                ("batch_lanes", C.c_int32), ("batch_records", C.c_int32)]
 
 
 class GradTargets(C.Structure):

@@ -489,7 +489,8 @@ class PathIntegrator:
                  secondary_edge_preprocess_rounds: int = 1, primary_edge_hypercube_resolution: int = 10000,
                  secondary_edge_hypercube_resolution: List[int] = [10000, 6, 6], estimator: str = "reference",
                  seed: int = 0, tile_paths: int = 0, gradient_terms: int = 0,
-                 spp_pixel_boundary: Optional[int] = None, trace_queue: int = 0):
+                 spp_pixel_boundary: Optional[int] = None, trace_queue: int = 0, batch_lanes: int = 0,
+                 batch_records: int = 0):
         """Path-space differentiable integrator (torch_psdr.py:477-536; path_integrator.h:8-21).
 
         B200 extensions: estimator ("reference" reproduces renderD exactly; "unbiased"
@@ -501,7 +502,13 @@ class PathIntegrator:
         unbiased estimator's DiffuseBsdfMaterial BRDF-jump term, on request),
         spp_pixel_boundary (unbiased: samples per unit pixel-border segment; default
         spp_primary_edge), trace_queue (rays each SM traverses concurrently, in units of
-        128; 0 = 8, the autotuner picks it).
+        128; 0 = 8, the autotuner picks it), batch_lanes (BatchRender only: concurrent
+        streams, each with its own workspace, over which a batch spreads its forward tiles
+        and its backward's interior tiles and per-view boundary terms; 1..8, 0 = 4; the
+        gradients do not depend on it), batch_records (BatchRender only: the forward keeps
+        every interior path's replay record and the backward runs the adjoint from them
+        instead of re-tracing; 0 = when they fit in a quarter of the free device memory,
+        1 = always, -1 = never; the gradients do not depend on it).
         """
         assert n_pass > 0
         assert spp_interior > 0
@@ -538,6 +545,10 @@ class PathIntegrator:
         cfg.seed = seed
         assert 0 <= trace_queue <= 8
         cfg.trace_queue = trace_queue
+        assert 0 <= batch_lanes <= 8
+        cfg.batch_lanes = batch_lanes
+        assert batch_records in (-1, 0, 1)
+        cfg.batch_records = batch_records
         self.cfg = cfg
         self._lib = L.load()
         self._ws = None

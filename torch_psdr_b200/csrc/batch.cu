@@ -4,7 +4,12 @@
 // scene_optix.cc:240-277); here all views share the wavefront tiles (small views
 // are packed together), and the whole forward (optionally preceded by the scenes'
 // geometry rebuild) and the whole backward are each recorded once into a graph and
-// replayed with a single launch.
+// replayed with a single launch. Inside each graph the independent parts of the job run
+// on concurrent lanes (forked streams, one wavefront workspace each): the forward's
+// tiles, and the backward's interior tiles and every boundary term of every view, spread
+// by their ray counts. Each part is a chain of short dependent kernels (a wavefront depth
+// loop, guide preprocessing, prefix sums); running several chains at once fills the SMs
+// that one chain leaves idle between and at the tails of its launches.
 #include <algorithm>
 #include <memory>
 #include <string>
@@ -31,12 +36,24 @@ struct psdr_batch {
   std::vector<int> gacc;
   std::vector<std::unique_ptr<psdr::DBuf>> vmasks;  // per-scene vertex-gradient masks of this batch's targets
   std::vector<std::unique_ptr<psdr::DBuf>> objs;    // per-scene object tables (texture accumulators asked for)
+  // concurrent lanes: lane 0 is the caller's stream with `ws`, lane k >= 1 has its own
+  // stream and workspace; fork/join events of the graph captures
+  int nlanes = 1;
+  // replay records of every interior path, written by the forward (cfg.batch_records)
+  bool kept = false;
+  psdr::DBuf keep_rec, keep_view, keep_pix;
+  psdr::KeptRecords keep;
+  std::vector<std::unique_ptr<psdr_workspace>> lane_ws;
+  std::vector<cudaStream_t> lane_st;
+  std::vector<cudaEvent_t> lane_ev;
   cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
   long long fwd_launches = 0, bwd_launches = 0;
   std::vector<psdr::Profiler::EvPair> fwd_ev, bwd_ev;  // trace timing events recorded in the graphs
   ~psdr_batch() {
     if (fwd_exec) cudaGraphExecDestroy(fwd_exec);
     if (bwd_exec) cudaGraphExecDestroy(bwd_exec);
+    for (cudaStream_t s : lane_st) cudaStreamDestroy(s);
+    for (cudaEvent_t e : lane_ev) cudaEventDestroy(e);
     auto& reps = psdr::profiler().replays;
     for (size_t i = reps.size(); i-- > 0;)
       if (reps[i].first == &fwd_ev || reps[i].first == &bwd_ev) reps.erase(reps.begin() + i);
@@ -75,6 +92,23 @@ cudaGraphExec_t capture(cudaStream_t st, F body, long long& launches, std::vecto
   launches = pf.launches - l0;
   pf.launches = l0;
   return exec;
+}
+
+// Runs body(k, stream_k, workspace_k) for every lane k of the batch: lanes k >= 1 are
+// forked from st and joined back into it (inside a capture this forms parallel branches
+// of the graph).
+template <class F>
+void over_lanes(psdr_batch* b, cudaStream_t st, F body) {
+  const int K = b->nlanes;
+  if (K > 1) {
+    PSDR_CUDA(cudaEventRecord(b->lane_ev[0], st));
+    for (int k = 1; k < K; ++k) PSDR_CUDA(cudaStreamWaitEvent(b->lane_st[k - 1], b->lane_ev[0], 0));
+  }
+  for (int k = 0; k < K; ++k) body(k, k == 0 ? st : b->lane_st[k - 1], k == 0 ? &b->ws : b->lane_ws[k - 1].get());
+  for (int k = 1; k < K; ++k) {
+    PSDR_CUDA(cudaEventRecord(b->lane_ev[k], b->lane_st[k - 1]));
+    PSDR_CUDA(cudaStreamWaitEvent(st, b->lane_ev[k], 0));
+  }
 }
 
 }  // namespace
@@ -137,9 +171,50 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     set_scene_ntri(b->views, scenes);
     b->cap = choose_cap(*cfg, b->views, true);
     const int Rmax = cfg->mis_light_samples + std::max(cfg->mis_bsdf_samples, 1) + 1;
-    b->ws.ensure(b->cap, Rmax, cfg->max_bounce, n_cams, b->backward ? 1 : 0, st);
+    if (b->backward && cfg->batch_records >= 0) {
+      long long paths = 0;
+      for (const DevView& v : b->views) paths += (long long)v.H * v.W * v.spp;
+      const int R = cfg->mis_light_samples + cfg->mis_bsdf_samples + 1;
+      const size_t stride = 1 + (size_t)cfg->max_bounce * R + 2 * (size_t)cfg->max_bounce;
+      const size_t bytes = (size_t)paths * (16 * stride + 8);
+      size_t free_b = 0, total_b = 0;
+      PSDR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      b->kept = cfg->batch_records == 1 || bytes <= free_b / 4;
+      if (b->kept) {
+        b->keep_rec.alloc(16 * stride * (size_t)paths, st);
+        b->keep_view.alloc(4 * (size_t)paths, st);
+        b->keep_pix.alloc(4 * (size_t)paths, st);
+        b->keep.rec = b->keep_rec.as<float4>();
+        b->keep.view = b->keep_view.as<int>();
+        b->keep.pix = b->keep_pix.as<int>();
+      }
+    }
+    const int rec_needed = b->backward && !b->kept ? 1 : 0;
+    b->ws.ensure(b->cap, Rmax, cfg->max_bounce, n_cams, rec_needed, st);
     if (b->backward) ensure_border(&b->ws, *cfg, b->views, st);
     upload_views(&b->ws, b->views, st);
+    // lanes: no more than the job has independent parts
+    {
+      SceneGradInfo any;
+      any.bsdf = 1;
+      const size_t parts = std::max(plan_tiles(b->views, b->cap).size(),
+                                    b->backward ? backward_units(b->views, *cfg, b->cap, any).size() : (size_t)1);
+      b->nlanes = (int)std::min<size_t>(cfg->batch_lanes > 0 ? cfg->batch_lanes : 4, parts);
+    }
+    for (int k = 1; k < b->nlanes; ++k) {
+      b->lane_ws.emplace_back(new psdr_workspace());
+      psdr_workspace* lw = b->lane_ws.back().get();
+      lw->ensure(b->cap, Rmax, cfg->max_bounce, 1, rec_needed, st);
+      if (b->backward) ensure_border(lw, *cfg, b->views, st);
+      cudaStream_t ls = nullptr;
+      PSDR_CUDA(cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking));
+      b->lane_st.push_back(ls);
+    }
+    for (int k = 0; k < b->nlanes; ++k) {
+      cudaEvent_t e = nullptr;
+      PSDR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      b->lane_ev.push_back(e);
+    }
     std::vector<DevScene> ds(n_scenes);
     for (int i = 0; i < n_scenes; ++i) ds[i] = scenes[i]->dev;
     if (b->backward) {
@@ -177,6 +252,7 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     b->ws.bsdf = 0;
     for (int i = 0; i < n_scenes; ++i)
       if (scenes[i]->has_bsdf || scenes[i]->env_light >= 0) b->gi.bsdf = b->ws.bsdf = 1;
+    for (auto& lw : b->lane_ws) lw->bsdf = b->ws.bsdf;
     if (b->backward) {
       b->gv.resize(n_scenes);
       b->gt.resize(n_scenes);
@@ -231,7 +307,13 @@ PSDR_API psdr_status psdr_batch_forward(psdr_batch* b, void* stream) {
       b->fwd_exec = capture(st, [&] {
         if (b->rebuild)
           for (psdr_scene* s : b->scenes) scene_build_geometry(s, st);
-        forward_launch(b->scenes_dev.as<DevScene>(), b->views, b->cfg, b->cap, &b->ws, st, nullptr);
+        const DevView* vd = b->ws.views.as<DevView>();
+        const auto plan = schedule_tiles(plan_tiles(b->views, b->cap), b->nlanes);
+        over_lanes(b, st, [&](int k, cudaStream_t ls, psdr_workspace* lw) {
+          for (const Tile& t : plan[k])
+            forward_tile(b->scenes_dev.as<DevScene>(), b->views, vd, t, b->cfg, lw, ls, nullptr,
+                         b->kept ? &b->keep : nullptr);
+        });
       }, b->fwd_launches, &b->fwd_ev);
     }
     PSDR_CUDA(cudaGraphLaunch(b->fwd_exec, st));
@@ -261,7 +343,13 @@ PSDR_API psdr_status psdr_batch_backward(psdr_batch* b, void* stream) {
         }
         PSDR_CUDA(cudaMemsetAsync(b->campos.p, 0, sizeof(GradAcc) * 3 * b->views.size(), st));
         PSDR_CUDA(cudaMemsetAsync(b->lens.p, 0, sizeof(GradAcc) * kLensAcc * b->views.size(), st));
-        backward_launch(b->scenes_dev.as<DevScene>(), b->views, b->cfg, b->cap, &b->ws, b->gi, st);
+        const DevView* vd = b->ws.views.as<DevView>();
+        const auto plan = schedule_units(backward_units(b->views, b->cfg, b->cap, b->gi), b->nlanes);
+        over_lanes(b, st, [&](int k, cudaStream_t ls, psdr_workspace* lw) {
+          for (const BwdUnit& u : plan[k])
+            backward_unit(b->scenes_dev.as<DevScene>(), b->views, vd, u, b->cfg, b->cap, lw, b->gi, ls,
+                          b->kept ? &b->keep : nullptr);
+        });
         for (size_t i = 0; i < b->scenes.size(); ++i) {
           psdr_scene* s = b->scenes[i];
           const int nm = (int)s->meshes.size();

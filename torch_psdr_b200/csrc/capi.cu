@@ -80,6 +80,8 @@ void check_cfg(const psdr_config* c) {
   PSDR_CHECK(c->tile_paths >= 0, "tile_paths must be >= 0");
   PSDR_CHECK(c->spp_pixel_boundary >= 0, "spp_pixel_boundary must be >= 0");
   PSDR_CHECK(c->trace_queue >= 0 && c->trace_queue <= 8, "trace_queue must be in [0, 8]");
+  PSDR_CHECK(c->batch_lanes >= 0 && c->batch_lanes <= 8, "batch_lanes must be in [0, 8]");
+  PSDR_CHECK(c->batch_records >= -1 && c->batch_records <= 1, "batch_records must be -1, 0 or 1");
 }
 
 void check_cams(const psdr_camera_desc* cams, int n) {
@@ -216,7 +218,7 @@ extern "C" {
 
 const char* psdr_last_error(void) { return psdr::g_err.c_str(); }
 const char* psdr_version(void) { return "torch_psdr_b200 0.1.0 (sm_100a)"; }
-int32_t psdr_abi_version(void) { return 5; }
+int32_t psdr_abi_version(void) { return 6; }
 
 // emitter.cc:103-119: the environment lights' bounding-box mesh. Vertex v has x = max if
 // bit 2, y = max if bit 1, z = max if bit 0; the faces and the cube-map uvs (a 4 x 3 cross)

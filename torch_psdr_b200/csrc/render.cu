@@ -116,7 +116,7 @@ PSDR_D void vert_add(const DevScene& sc, int v, float3 a) {
 // The replay instance is held to 4 blocks per SM (64 registers): its record writes
 // otherwise take it to 76 registers and 3 blocks.
 template <int MODE, bool ORTHO>
-__global__ void __launch_bounds__(256, MODE == MODE_REPLAY ? 4 : 1) k_camera(WF w, const DevScene* __restrict__ scenes,
+__global__ void __launch_bounds__(256, MODE != MODE_FWD ? 4 : 1) k_camera(WF w, const DevScene* __restrict__ scenes,
                                                 const DevView* __restrict__ views, Tile tile) {
   const int stride = gridDim.x * blockDim.x;
   const int n32 = (tile.n + 31) & ~31;
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(256, MODE == MODE_REPLAY ? 4 : 1) k_camera(WF 
       w.T[s] = make_float4(1.f, 1.f, 1.f, 0.f);
       w.L[s] = make_float4(0.f, 0.f, 0.f, 0.f);
       w.cur[s] = hit4(h);
-      if (MODE == MODE_REPLAY) {
+      if (MODE != MODE_FWD) {
         float4* rec = w.rec + (size_t)s * w.rec_stride;
         rec[0] = hit4(h);
         float4* cb = rec + 1 + (size_t)w.D * w.R;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
       const float4 c = w.cur[s];
       x = make_surf(*sc, __float_as_int(c.x), c.y, c.z, xyz(w.org[s]));
       if (x.is_light) {
-        if (MODE == MODE_FWD && w.light_vis && d == 0) {
+        if (MODE != MODE_REPLAY && w.light_vis && d == 0) {
           const DevLight& Lt = sc->lights[x.light];
           float4 L = w.L[s];
           const float4 T = w.T[s];
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
           cont = true;
         }
       }
-      if (MODE == MODE_REPLAY) {
+      if (MODE != MODE_FWD) {
         float4* rec = w.rec + (size_t)s * w.rec_stride;
         float4* rh = rec + 1 + (size_t)d * w.R;
         const int Rd = last ? w.R - 1 : w.R;
@@ -417,7 +417,8 @@ __global__ void __launch_bounds__(256) k_accum(WF w, const DevScene* __restrict_
         float4* cb = rec + 1 + (size_t)w.D * w.R + 2 * d;
         cb[0] = make_float4(C.x, C.y, C.z, 0.f);
         cb[1] = make_float4(beta.x, beta.y, beta.z, 0.f);
-      } else {
+      }
+      if (MODE != MODE_REPLAY) {
         const float3 T = xyz(w.T[s]);
         const float3 L = xyz(w.L[s]) + mul(T, C);
         const float3 Tn = mul(T, beta);
@@ -1804,6 +1805,10 @@ constexpr int kCreaseCap = 16384;          // intersection segments kept per sce
 constexpr int kCreaseSamplesPerSpp = 16384;  // crease samples per primary-edge spp
 constexpr unsigned long long kCreaseStream = 0xC0000000ull;  // sampler streams of the crease samples
 
+// Meshes whose boxes the crease extraction keeps (a triangle of a mesh beyond this many
+// walks the tree without the box test).
+constexpr int kCreaseBoxObjs = 4096;
+
 struct CreaseBuf {
   float4* a;   // segment start xyz, length (ordered by the triangle pair)
   float4* b;   // segment end xyz, -
@@ -1812,7 +1817,85 @@ struct CreaseBuf {
   float4* rb;
   int2* rtris;
   int* count;  // segments found (may exceed kCreaseCap: the rest are dropped)
+  int* obox;   // per mesh: its box (min xyz, max xyz as order-preserving ints), kCreaseBoxObjs
+  int* later;  // per mesh m: the box of meshes m+1 .. (the ones its triangles are tested against)
 };
+
+// Order-preserving int image of a float (for atomicMin / atomicMax on boxes).
+PSDR_D int f2ord(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+PSDR_D float ord2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__global__ void k_crease_box_init(const DevScene* __restrict__ scenes, int si, CreaseBuf cb) {
+  const int n = min(scenes[si].nobj, kCreaseBoxObjs);
+  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x)
+    for (int k = 0; k < 3; ++k) {
+      cb.obox[6 * o + k] = 0x7fffffff;
+      cb.obox[6 * o + 3 + k] = (int)0x80000000;
+    }
+}
+
+// Box of every mesh (lights excluded): one thread per triangle, reduced over the warp when
+// its triangles belong to one mesh (meshes are contiguous ranges of triangles).
+__global__ void k_crease_boxes(const DevScene* __restrict__ scenes, int si, CreaseBuf cb) {
+  const DevScene& sc = scenes[si];
+  const int nmesh = min(sc.nobj - sc.nlight, kCreaseBoxObjs);
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (sc.ntri + 31) & ~31;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n32; t += stride) {
+    int o = -1;
+    int v[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000, (int)0x80000000, (int)0x80000000};
+    if (t < sc.ntri) {
+      o = __ldg(sc.tri_v + t).w;
+      if (o < nmesh) {
+        const float4* R = sc.tri + 6 * (size_t)t;
+        const float3 p0 = xyz(__ldg(R)), p1 = xyz(__ldg(R + 1)), p2 = xyz(__ldg(R + 2));
+        v[0] = f2ord(fminf(p0.x, fminf(p1.x, p2.x)));
+        v[1] = f2ord(fminf(p0.y, fminf(p1.y, p2.y)));
+        v[2] = f2ord(fminf(p0.z, fminf(p1.z, p2.z)));
+        v[3] = f2ord(fmaxf(p0.x, fmaxf(p1.x, p2.x)));
+        v[4] = f2ord(fmaxf(p0.y, fmaxf(p1.y, p2.y)));
+        v[5] = f2ord(fmaxf(p0.z, fmaxf(p1.z, p2.z)));
+      } else {
+        o = -1;
+      }
+    }
+    const int o0 = __shfl_sync(0xffffffffu, o, 0);
+    if (__all_sync(0xffffffffu, o == o0)) {
+      if (o0 < 0) continue;
+      for (int k = 0; k < 3; ++k) {
+        const int mn = __reduce_min_sync(0xffffffffu, v[k]);
+        const int mx = __reduce_max_sync(0xffffffffu, v[3 + k]);
+        if ((threadIdx.x & 31) == 0) {
+          atomicMin(cb.obox + 6 * o0 + k, mn);
+          atomicMax(cb.obox + 6 * o0 + 3 + k, mx);
+        }
+      }
+    } else if (o >= 0) {
+      for (int k = 0; k < 3; ++k) {
+        atomicMin(cb.obox + 6 * o + k, v[k]);
+        atomicMax(cb.obox + 6 * o + 3 + k, v[3 + k]);
+      }
+    }
+  }
+}
+
+// later[m] = union of the boxes of meshes m+1 .. nmesh-1 (empty for the last).
+__global__ void k_crease_later(const DevScene* __restrict__ scenes, int si, CreaseBuf cb) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const DevScene& sc = scenes[si];
+  const int nmesh = min(sc.nobj - sc.nlight, kCreaseBoxObjs);
+  int u[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000, (int)0x80000000, (int)0x80000000};
+  for (int m = nmesh - 1; m >= 0; --m) {
+    for (int k = 0; k < 6; ++k) cb.later[6 * m + k] = u[k];
+    for (int k = 0; k < 3; ++k) {
+      u[k] = min(u[k], cb.obox[6 * m + k]);
+      u[3 + k] = max(u[3 + k], cb.obox[6 * m + 3 + k]);
+    }
+  }
+}
 
 // The segment where triangles a and b cross (false when they do not, or are coplanar).
 // Double precision; a vertex exactly on the other plane counts as on its positive side.
@@ -1865,6 +1948,13 @@ __global__ void __launch_bounds__(128) k_crease_pairs(const DevScene* __restrict
     const float3 p0 = xyz(__ldg(R)), p1 = xyz(__ldg(R + 1)), p2 = xyz(__ldg(R + 2));
     const float3 lo = f3(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)), fminf(p0.z, fminf(p1.z, p2.z)));
     const float3 hi = f3(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)), fmaxf(p0.z, fmaxf(p1.z, p2.z)));
+    if (tv.w < kCreaseBoxObjs) {
+      // a triangle clear of every later mesh's box crosses none of its triangles
+      const int* L = cb.later + 6 * tv.w;
+      if (__ldg(L) == 0x7fffffff || ord2f(__ldg(L)) > hi.x || ord2f(__ldg(L + 3)) < lo.x || ord2f(__ldg(L + 1)) > hi.y ||
+          ord2f(__ldg(L + 4)) < lo.y || ord2f(__ldg(L + 2)) > hi.z || ord2f(__ldg(L + 5)) < lo.z)
+        continue;
+    }
     const double3 A[3] = {make_double3(p0.x, p0.y, p0.z), make_double3(p1.x, p1.y, p1.z), make_double3(p2.x, p2.y, p2.z)};
     int stack[64];
     int sp = 0;
@@ -3056,44 +3146,44 @@ static void launch_direct(const WF& w, int grid, cudaStream_t st, const DevScene
   else k_direct<PRE, UNB, false><<<grid, 128, 0, st>>>(w, scenes, vd, v, n, hc, round, mass, spp);
 }
 
-static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int mode, cudaStream_t st) {
+template <int MODE>
+static void depth_loop_t(WF& w, const DevScene* scenes, const DevView* views, cudaStream_t st) {
   const int cap = w.cap;
   Profiler& pf = profiler();
   for (int d = 0; d < w.D; ++d) {
     const int gs = grid_for(cap, 256, 8);
-    if (w.bsdf) {
-      if (mode == MODE_REPLAY) k_shade<MODE_REPLAY, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
-      else k_shade<MODE_FWD, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
-    } else {
-      if (mode == MODE_REPLAY) k_shade<MODE_REPLAY, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
-      else k_shade<MODE_FWD, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
-    }
+    if (w.bsdf) k_shade<MODE, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
+    else k_shade<MODE, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
     pf.begin_trace(st);
     k_trace<<<num_sms() * w.trace_bps, 128, 0, st>>>(w, scenes, views, d, pf.on ? pf.d_rays : nullptr);
     pf.end_trace(st);
     PSDR_LAUNCHED(3);
-    if (w.bsdf) {
-      if (mode == MODE_REPLAY) k_accum<MODE_REPLAY, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
-      else k_accum<MODE_FWD, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
-    } else {
-      if (mode == MODE_REPLAY) k_accum<MODE_REPLAY, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
-      else k_accum<MODE_FWD, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
-    }
+    if (w.bsdf) k_accum<MODE, true><<<gs, 256, 0, st>>>(w, scenes, views, d);
+    else k_accum<MODE, false><<<gs, 256, 0, st>>>(w, scenes, views, d);
   }
   PSDR_CUDA(cudaGetLastError());
+}
+
+static void depth_loop(WF& w, const DevScene* scenes, const DevView* views, int mode, cudaStream_t st) {
+  if (mode == MODE_REPLAY) depth_loop_t<MODE_REPLAY>(w, scenes, views, st);
+  else if (mode == MODE_KEEP) depth_loop_t<MODE_KEEP>(w, scenes, views, st);
+  else depth_loop_t<MODE_FWD>(w, scenes, views, st);
+}
+
+template <int MODE>
+static void launch_camera(const WF& w, const DevScene* scenes, const DevView* views, const Tile& tile, int g,
+                          cudaStream_t st) {
+  if (w.ortho) k_camera<MODE, true><<<g, 256, 0, st>>>(w, scenes, views, tile);
+  else k_camera<MODE, false><<<g, 256, 0, st>>>(w, scenes, views, tile);
 }
 
 static void run_tile(WF& w, const DevScene* scenes, const DevView* views, const Tile& tile, int mode,
                      cudaStream_t st) {
   PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
   const int g = grid_for(tile.n, 256, 8);
-  if (w.ortho) {
-    if (mode == MODE_REPLAY) k_camera<MODE_REPLAY, true><<<g, 256, 0, st>>>(w, scenes, views, tile);
-    else k_camera<MODE_FWD, true><<<g, 256, 0, st>>>(w, scenes, views, tile);
-  } else {
-    if (mode == MODE_REPLAY) k_camera<MODE_REPLAY, false><<<g, 256, 0, st>>>(w, scenes, views, tile);
-    else k_camera<MODE_FWD, false><<<g, 256, 0, st>>>(w, scenes, views, tile);
-  }
+  if (mode == MODE_REPLAY) launch_camera<MODE_REPLAY>(w, scenes, views, tile, g, st);
+  else if (mode == MODE_KEEP) launch_camera<MODE_KEEP>(w, scenes, views, tile, g, st);
+  else launch_camera<MODE_FWD>(w, scenes, views, tile, g, st);
   PSDR_LAUNCHED(1);
   depth_loop(w, scenes, views, mode, st);
 }
@@ -3181,24 +3271,33 @@ void set_wf(WF& w, const psdr_config& cfg, int nviews, int nB_override, int ligh
   w.trace_bps = cfg.trace_queue > 0 ? cfg.trace_queue : 8;
 }
 
+void forward_tile(const DevScene* scenes_dev, const std::vector<DevView>& views, const DevView* vd, const Tile& t,
+                  const psdr_config& cfg, psdr_workspace* ws, cudaStream_t st, float* samples_out,
+                  const KeptRecords* keep) {
+  WF w = ws->wf;
+  w.cap = ws->cap;
+  set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
+  w.bsdf = ws->bsdf;
+  w.ortho = any_ortho(views);
+  if (keep) {
+    w.rec = keep->rec + (size_t)t.begin * w.rec_stride;
+    w.view = keep->view + t.begin;
+    w.pix = keep->pix + t.begin;
+  }
+  run_tile(w, scenes_dev, vd, t, keep ? MODE_KEEP : MODE_FWD, st);
+  k_film<<<grid_for(t.npix, 256, 8), 256, 0, st>>>(w, vd, t, std::max(1, cfg.n_pass), samples_out);
+  PSDR_LAUNCHED(1);
+  PSDR_CUDA(cudaGetLastError());
+}
+
 // Forward: the interior estimate of every view into V.image (and per-sample radiance
 // of view 0 into samples_out when given).
 // Device work of a forward job whose views are already in ws->views (tiles of `cap`
 // paths). Makes no allocation and no host copy, so it can be recorded into a graph.
 void forward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg, int cap,
                     psdr_workspace* ws, cudaStream_t st, float* samples_out) {
-  WF w = ws->wf;
-  w.cap = ws->cap;
-  set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
-  w.bsdf = ws->bsdf;
-  w.ortho = any_ortho(views);
   const DevView* vd = ws->views.as<DevView>();
-  for (const Tile& t : plan_tiles(views, cap)) {
-    run_tile(w, scenes_dev, vd, t, MODE_FWD, st);
-    k_film<<<grid_for(t.npix, 256, 8), 256, 0, st>>>(w, vd, t, std::max(1, cfg.n_pass), samples_out);
-    PSDR_LAUNCHED(1);
-  }
-  PSDR_CUDA(cudaGetLastError());
+  for (const Tile& t : plan_tiles(views, cap)) forward_tile(scenes_dev, views, vd, t, cfg, ws, st, samples_out);
 }
 
 void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
@@ -3294,6 +3393,8 @@ static CreaseBuf crease_buf(psdr_workspace* ws) {
   cb.rb = reinterpret_cast<float4*>(p + 56 * (size_t)kCreaseCap);
   cb.rtris = reinterpret_cast<int2*>(p + 72 * (size_t)kCreaseCap);
   cb.count = reinterpret_cast<int*>(p + 80 * (size_t)kCreaseCap);
+  cb.obox = reinterpret_cast<int*>(p + 80 * (size_t)kCreaseCap + 256);
+  cb.later = cb.obox + 6 * kCreaseBoxObjs;
   return cb;
 }
 
@@ -3328,7 +3429,7 @@ void ensure_border(psdr_workspace* ws, const psdr_config& cfg, const std::vector
     nt = std::max<long long>(nt, v.scene_ntri);
   }
   ws->ensure_mass(std::max(s, nt), st);
-  ws->crease.alloc(80 * (size_t)kCreaseCap + 256, st);
+  ws->crease.alloc(80 * (size_t)kCreaseCap + 256 + 2 * 24 * (size_t)kCreaseBoxObjs, st);
 }
 
 void set_scene_ntri(std::vector<DevView>& views, const psdr_scene* const* scenes) {
@@ -3378,41 +3479,129 @@ void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& view
   backward_launch(scenes_dev, views, cfg, cap, ws, gi, st);
 }
 
-// Device work of a backward job (views already uploaded); no allocation, no host copy.
-void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg,
-                     int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
-  const DevView* vd = ws->views.as<DevView>();
+static int job_terms(const psdr_config& cfg) {
+  return cfg.terms ? cfg.terms : (cfg.estimator == PSDR_EST_UNBIASED ? 111 : 7);
+}
+
+// The units of a backward job, in the serial order: every interior tile, then per view
+// its boundary terms (primary edges, direct edges, pixel borders, indirect shadow
+// boundaries, creases, BRDF jumps). Costs count traced rays.
+std::vector<BwdUnit> backward_units(const std::vector<DevView>& views, const psdr_config& cfg, int cap,
+                                    const SceneGradInfo& gi) {
+  std::vector<BwdUnit> u;
   const bool unb = cfg.estimator == PSDR_EST_UNBIASED;
-  const int terms = cfg.terms ? cfg.terms : (unb ? 111 : 7);
+  const int terms = job_terms(cfg);
+  const double D = cfg.max_bounce;
+  const double R = cfg.mis_light_samples + cfg.mis_bsdf_samples + 1;
+  const double R1 = cfg.mis_light_samples + 2;  // boundary paths of the reference estimator: one BSDF sample
+  if (terms & 1)
+    for (const Tile& t : plan_tiles(views, cap)) u.push_back(BwdUnit{1, -1, t, 2.0 * t.n * (1 + D * R)});
+  for (int v = 0; v < (int)views.size(); ++v) {
+    const DevView& V = views[v];
+    const double px = (double)V.H * V.W;
+    if (terms & 2) {
+      const double pre = (double)cfg.primary_edge_hypercube_resolution * cfg.primary_edge_preprocess_rounds *
+                         2.0 * (1 + D * R1);
+      const double n = px * cfg.spp_primary_edge * (unb ? 2 + D * R : 2.0 * (1 + D * R1));
+      u.push_back(BwdUnit{2, v, Tile{}, pre + n});
+    }
+    if (terms & 4) {
+      const int* r3 = cfg.secondary_edge_hypercube_resolution;
+      const double per = unb ? 3.0 + 2.0 * (D - 1) : 3.0;
+      const double pre = (double)r3[0] * r3[1] * r3[2] * cfg.secondary_edge_preprocess_rounds *
+                         (unb ? kDirectGuideRounds : 1) * per;
+      u.push_back(BwdUnit{4, v, Tile{}, pre + px * cfg.spp_secondary_edge * per});
+    }
+    if (unb && (terms & 8) && cfg.spp_pixel_boundary > 0 && V.dimage)
+      u.push_back(BwdUnit{8, v, Tile{}, (double)border_segments(V) * cfg.spp_pixel_boundary * (1 + D * R)});
+    if (unb && (terms & 64) && V.dimage && !V.ortho && cfg.max_bounce >= 2) {
+      const int* rs = cfg.secondary_edge_hypercube_resolution;
+      const double cells = (double)std::max(1, rs[0] / kIndirectCellDiv) * rs[1] * rs[2];
+      const double n = std::max(1.0, px * cfg.spp_secondary_edge / kIndirectSampleDiv);
+      u.push_back(BwdUnit{64, v, Tile{}, (cells * cfg.secondary_edge_preprocess_rounds + n) * 3.0 +
+                                             n * (D - 1) * R});
+    }
+    if (unb && (terms & 32) && V.dimage && !V.ortho)
+      u.push_back(BwdUnit{32, v, Tile{}, 8.0 * V.scene_ntri +
+                                             (double)cfg.spp_primary_edge * kCreaseSamplesPerSpp * 2.0 * (1 + D * R)});
+    if (unb && (terms & 16) && gi.bsdf && V.dimage) {
+      double c = 0.0;
+      for (int k = 1; k <= cfg.max_bounce; ++k) c += k + 1 + (D - k) * R;
+      u.push_back(BwdUnit{16, v, Tile{}, px * V.spp * c});
+    }
+  }
+  return u;
+}
+
+std::vector<std::vector<BwdUnit>> schedule_units(const std::vector<BwdUnit>& units, int lanes) {
+  lanes = std::max(1, lanes);
+  std::vector<int> order(units.size());
+  for (size_t i = 0; i < units.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return units[a].cost > units[b].cost; });
+  std::vector<double> load(lanes, 0.0);
+  std::vector<int> lane_of(units.size(), 0);
+  for (int i : order) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lane_of[i] = k;
+    load[k] += units[i].cost;
+  }
+  std::vector<std::vector<BwdUnit>> out(lanes);
+  for (size_t i = 0; i < units.size(); ++i) out[lane_of[i]].push_back(units[i]);
+  return out;
+}
+
+std::vector<std::vector<Tile>> schedule_tiles(const std::vector<Tile>& tiles, int lanes) {
+  std::vector<BwdUnit> u;
+  for (const Tile& t : tiles) u.push_back(BwdUnit{1, -1, t, (double)t.n});
+  std::vector<std::vector<Tile>> out;
+  for (const auto& l : schedule_units(u, lanes)) {
+    out.emplace_back();
+    for (const BwdUnit& x : l) out.back().push_back(x.tile);
+  }
+  return out;
+}
+
+// Device work of one backward unit on workspace ws (views at vd); no allocation, no
+// host copy.
+void backward_unit(const DevScene* scenes_dev, const std::vector<DevView>& views, const DevView* vd,
+                   const BwdUnit& u, const psdr_config& cfg, int cap, psdr_workspace* ws, const SceneGradInfo& gi,
+                   cudaStream_t st, const KeptRecords* keep) {
+  const bool unb = cfg.estimator == PSDR_EST_UNBIASED;
   bool lens = false;  // a view wants the camera-lens gradient
   for (const DevView& V : views) lens = lens || V.grad_lens != nullptr;
-  // ---- interior
-  if (terms & 1) {
+  // ---- interior tile
+  if (u.term == 1) {
     WF w = ws->wf;
     w.cap = ws->cap;
     set_wf(w, cfg, (int)views.size(), -1, cfg.enable_light_visable);
     w.bsdf = ws->bsdf;
     w.ortho = any_ortho(views);
-    for (const Tile& t : plan_tiles(views, cap)) {
+    const Tile& t = u.tile;
+    if (keep) {
+      w.rec = keep->rec + (size_t)t.begin * w.rec_stride;
+      w.view = keep->view + t.begin;
+      w.pix = keep->pix + t.begin;
+    } else {
       run_tile(w, scenes_dev, vd, t, MODE_REPLAY, st);
-      const int g = grid_for(t.n, 128, 16);
-      if (gi.bsdf) {
-        if (unb) k_adjoint<true, true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
-        else k_adjoint<false, true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
-      } else {
-        if (unb) k_adjoint<true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
-        else k_adjoint<false><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
-      }
+    }
+    const int g = grid_for(t.n, 128, 16);
+    if (gi.bsdf) {
+      if (unb) k_adjoint<true, true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+      else k_adjoint<false, true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+    } else {
+      if (unb) k_adjoint<true><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+      else k_adjoint<false><<<g, 128, 0, st>>>(w, scenes_dev, vd, t, gi.hot_lv0, gi.hot_nlv, gi.emit_hot);
+    }
+    PSDR_LAUNCHED(1);
+    if (lens) {
+      if (gi.bsdf) k_lens_interior<true><<<grid_for(t.n, 256, 8), 256, 0, st>>>(w, scenes_dev, vd, t);
+      else k_lens_interior<false><<<grid_for(t.n, 256, 8), 256, 0, st>>>(w, scenes_dev, vd, t);
       PSDR_LAUNCHED(1);
-      if (lens) {
-        if (gi.bsdf) k_lens_interior<true><<<grid_for(t.n, 256, 8), 256, 0, st>>>(w, scenes_dev, vd, t);
-        else k_lens_interior<false><<<grid_for(t.n, 256, 8), 256, 0, st>>>(w, scenes_dev, vd, t);
-        PSDR_LAUNCHED(1);
-      }
     }
     PSDR_CUDA(cudaGetLastError());
+    return;
   }
-  // ---- boundary terms per view
+  // ---- boundary terms of view v
   WF w = ws->wf;
   w.cap = ws->cap;
   set_wf(w, cfg, (int)views.size(), 1, 0);
@@ -3425,10 +3614,10 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
   wi.bsdf = ws->bsdf;
   wi.ortho = any_ortho(views);
   EdgeBuf eb{ws->eb_a.as<float4>(), ws->eb_n.as<float4>(), ws->eb_hb.as<float4>(), ws->eb_La.as<float4>(), nullptr};
-  for (int v = 0; v < (int)views.size(); ++v) {
-    const DevView& V = views[v];
-    // primary edges: preprocess over the hypercube cells, then the edge samples
-    if (terms & 2) {
+  const int v = u.view;
+  const DevView& V = views[v];
+  switch (u.term) {
+    case 2: {  // primary edges: preprocess over the hypercube cells, then the edge samples
       const int cells = cfg.primary_edge_hypercube_resolution;
       PSDR_CUDA(cudaMemsetAsync(ws->mass.p, 0, sizeof(float) * cells, st));
       HCube none{};
@@ -3443,9 +3632,9 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
         if (unb) edge_phase_unb(wi, scenes_dev, vd, v, eb, b, nb, hc, cfg.spp_primary_edge, st);
         else edge_phase(w, scenes_dev, vd, v, eb, b, nb, hc, 0, false, nullptr, cfg.spp_primary_edge, st);
       }
+      break;
     }
-    // direct edges
-    if (terms & 4) {
+    case 4: {  // direct edges
       const int* r3 = cfg.secondary_edge_hypercube_resolution;
       const int cells = r3[0] * r3[1] * r3[2];
       PSDR_CUDA(cudaMemsetAsync(ws->mass.p, 0, sizeof(float) * cells, st));
@@ -3470,9 +3659,9 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
         launch_direct<false, false>(w, grid_for(N, 128, 16), st, scenes_dev, vd, v, N, hc, 0, nullptr,
                                     cfg.spp_secondary_edge);
       PSDR_CUDA(cudaGetLastError());
+      break;
     }
-    // pixel borders (unbiased estimator): segment masses, their prefix sums, samples
-    if (unb && (terms & 8) && cfg.spp_pixel_boundary > 0 && V.dimage) {
+    case 8: {  // pixel borders (unbiased estimator): segment masses, their prefix sums, samples
       const long long S = border_segments(V);
       const long long N = S * cfg.spp_pixel_boundary;
       const int b = (int)((S + 255) / 256);
@@ -3484,10 +3673,9 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       for (long long b0 = 0; b0 < N; b0 += cap)
         border_phase(wi, scenes_dev, vd, v, eb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), S, b0,
                      (int)std::min<long long>(cap, N - b0), N, V.grad_lens != nullptr, st);
+      break;
     }
-    // indirect shadow boundaries (unbiased estimator, perspective views, max_bounce >= 2):
-    // the guiding preprocess, then the samples
-    if (unb && (terms & 64) && V.dimage && !V.ortho && cfg.max_bounce >= 2) {
+    case 64: {  // indirect shadow boundaries: the guiding preprocess, then the samples
       const int* rs = cfg.secondary_edge_hypercube_resolution;
       const int r3[3] = {std::max(1, rs[0] / kIndirectCellDiv), rs[1], rs[2]};
       const int cells = r3[0] * r3[1] * r3[2];
@@ -3503,12 +3691,15 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       const long long N = std::max(1LL, (long long)V.H * V.W * cfg.spp_secondary_edge / kIndirectSampleDiv);
       for (long long b0 = 0; b0 < N; b0 += cap)
         indirect_phase(wi, scenes_dev, vd, v, eb, b0, (int)std::min<long long>(cap, N - b0), hc, N, st);
+      break;
     }
-    // interpenetration creases (unbiased estimator, perspective views): the segments where
-    // two meshes cross, a length CDF over them, then the samples
-    if (unb && (terms & 32) && V.dimage && !V.ortho) {
+    case 32: {  // creases: the segments where two meshes cross, a length CDF over them, samples
       const CreaseBuf cb = crease_buf(ws);
       PSDR_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int), st));
+      k_crease_box_init<<<kCreaseBoxObjs / 256, 256, 0, st>>>(scenes_dev, V.scene, cb);
+      k_crease_boxes<<<grid_for(V.scene_ntri, 256, 8), 256, 0, st>>>(scenes_dev, V.scene, cb);
+      k_crease_later<<<1, 32, 0, st>>>(scenes_dev, V.scene, cb);
+      PSDR_LAUNCHED(3);
       k_crease_pairs<<<num_sms() * 4, 128, 0, st>>>(scenes_dev, V.scene, cb);
       k_crease_order<<<kCreaseCap / 128, 128, 0, st>>>(cb);
       k_crease_mass<<<kCreaseCap / 256, 256, 0, st>>>(cb, ws->mass_d.as<double>());
@@ -3520,15 +3711,27 @@ void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& vie
       for (long long b0 = 0; b0 < N; b0 += chunk)
         crease_phase(wi, scenes_dev, vd, v, eb, cb, ws->mass_d.as<double>(), ws->mass_pre.as<double>(), b0,
                      (int)std::min<long long>(chunk, N - b0), N, st);
+      break;
     }
-    // BSDF jumps (unbiased estimator, DiffuseBsdfMaterial scenes; on request only)
-    if (unb && (terms & 16) && gi.bsdf && V.dimage) {
+    case 16: {  // BSDF jumps (DiffuseBsdfMaterial scenes)
       const long long N = (long long)V.H * V.W * V.spp;
       for (int k = 1; k <= cfg.max_bounce; ++k)
         for (long long b0 = 0; b0 < N; b0 += cap)
           jump_phase(wi, scenes_dev, vd, v, eb, b0, (int)std::min<long long>(cap, N - b0), k, st);
+      break;
     }
+    default:
+      throw Error{PSDR_ERR_INVALID_ARG, "unknown backward unit"};
   }
+}
+
+// Device work of a backward job (views already uploaded); no allocation, no host copy.
+// The units run one after another on st with one workspace.
+void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg,
+                     int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st) {
+  const DevView* vd = ws->views.as<DevView>();
+  for (const BwdUnit& u : backward_units(views, cfg, cap, gi))
+    backward_unit(scenes_dev, views, vd, u, cfg, cap, ws, gi, st);
 }
 
 void grad_out(const GradAcc* acc, float* out, long long n, int accumulate, cudaStream_t st) {

@@ -69,7 +69,19 @@ struct EdgeBuf {
   unsigned long long* rng_keep;  // preprocess: sampler state across rounds
 };
 
-enum Mode { MODE_FWD = 0, MODE_REPLAY = 1 };
+// MODE_FWD accumulates the image; MODE_REPLAY re-traces a tile's paths for the backward
+// and writes their replay records; MODE_KEEP does both in one pass (the batch's forward
+// when it keeps the records of every tile for its backward).
+enum Mode { MODE_FWD = 0, MODE_REPLAY = 1, MODE_KEEP = 2 };
+
+// Replay records of every interior path of a job kept from its forward (psdr_batch): path
+// s of the job's sample space has its record at rec + s * rec_stride and its view and
+// pixel at view[s], pix[s].
+struct KeptRecords {
+  float4* rec = nullptr;
+  int* view = nullptr;
+  int* pix = nullptr;
+};
 
 struct psdr_ws_impl;
 
@@ -130,6 +142,33 @@ void forward_launch(const DevScene* scenes_dev, const std::vector<DevView>& view
                     psdr_workspace* ws, cudaStream_t st, float* samples_out);
 void backward_launch(const DevScene* scenes_dev, const std::vector<DevView>& views, const psdr_config& cfg,
                      int cap, psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
+// One forward tile (camera paths, depth loop, film) on workspace ws; views at vd.
+// With `keep`, the tile's replay records, views and pixels go to its place in `keep`.
+void forward_tile(const DevScene* scenes_dev, const std::vector<DevView>& views, const DevView* vd, const Tile& t,
+                  const psdr_config& cfg, psdr_workspace* ws, cudaStream_t st, float* samples_out,
+                  const KeptRecords* keep = nullptr);
+// The backward of a job as independent units: the interior replay + adjoint of each
+// wavefront tile (term 1) and each boundary term (bits 2..64 of psdr_config.terms) of
+// each view. A unit writes only its own workspace and the integer gradient accumulators,
+// whose sums do not depend on the order of the additions, so units may run in any order,
+// or concurrently on separate workspaces, with bitwise the same gradients.
+struct BwdUnit {
+  int term;      // 1 interior tile, else the boundary term's bit
+  int view;      // boundary terms: the view
+  Tile tile;     // interior: the tile
+  double cost;   // relative device work (rays traced), for scheduling
+};
+std::vector<BwdUnit> backward_units(const std::vector<DevView>& views, const psdr_config& cfg, int cap,
+                                    const SceneGradInfo& gi);
+// With `keep` (records kept by the forward), an interior unit runs only the adjoint.
+void backward_unit(const DevScene* scenes_dev, const std::vector<DevView>& views, const DevView* vd,
+                   const BwdUnit& u, const psdr_config& cfg, int cap, psdr_workspace* ws, const SceneGradInfo& gi,
+                   cudaStream_t st, const KeptRecords* keep = nullptr);
+// Units split over `lanes` lists by longest-processing-time-first scheduling on `cost`
+// (each list keeps the units' original order).
+std::vector<std::vector<BwdUnit>> schedule_units(const std::vector<BwdUnit>& units, int lanes);
+// Forward tiles split over `lanes` lists the same way (cost = paths).
+std::vector<std::vector<Tile>> schedule_tiles(const std::vector<Tile>& tiles, int lanes);
 SceneGradInfo grad_info(const psdr_scene* s);
 void check_config(const psdr_config* c);
 void check_cameras(const psdr_camera_desc* cams, int n);
