@@ -331,7 +331,7 @@ def run_b200(args):
     lV, lF, lE = tens(light.vertices), tens(light.faces, torch.int32), tens(light.emit)
     cam = dr.PerspectiveCamera(tens(c.look_from), tens(c.look_at), tens(c.up), tens([c.vfov]), H, W)
     integ = dr.PathIntegrator(estimator=args.estimator, batch_lanes=args.batch_lanes,
-                              batch_records=args.batch_records, **CFG)
+                              batch_records=args.batch_records, tile_paths=args.tile_paths, **CFG)
 
     leaf = {"size": 1}
 
@@ -605,7 +605,7 @@ def run_multiview(args):
                     if backward:
                         loss.backward()
 
-        phases = phase_breakdown(torch, dr, cfg, run_phase_step, flush, reps=1)
+        phases = phase_breakdown(torch, dr, cfg, run_phase_step, flush, reps=3)
     value = paths * args.steps / (b_ms / 1e3)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": b_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -707,6 +707,8 @@ def main():
     ap.add_argument("--no-grad-check", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-phases", action="store_true", help="skip the per-phase breakdown of the plain step")
+    ap.add_argument("--tile-paths", type=int, default=0,
+                    help="wavefront tile (paths; 0 = library default, or the autotuner's pick)")
     ap.add_argument("--batch-lanes", type=int, default=0, help="PathIntegrator batch_lanes (0 = library default)")
     ap.add_argument("--batch-records", type=int, default=0, choices=[-1, 0, 1],
                     help="PathIntegrator batch_records (0 = keep when they fit a quarter of free memory)")

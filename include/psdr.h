@@ -132,9 +132,9 @@ typedef struct {
                      bit 5 interpenetration creases (UNBIASED only, perspective views:
                      the curves where two meshes cut into each other), bit 6 indirect
                      shadow boundaries (UNBIASED only, perspective views, max_bounce >= 2:
-                     occlusion of light reflected by other surfaces); 0 = all of these.
-                     Bit 4: BRDF jumps of DiffuseBsdfMaterial (UNBIASED only, on
-                     request: not part of 0) */
+                     occlusion of light reflected by other surfaces), bit 4 BRDF jumps
+                     of DiffuseBsdfMaterial (UNBIASED only); 0 = all of these that
+                     apply (bit 4 when the job holds a DiffuseBsdfMaterial mesh) */
   int32_t spp_pixel_boundary; /* UNBIASED: samples per unit pixel-border segment */
   uint64_t seed;
   int32_t trace_queue; /* ABI 5: rays each SM traverses concurrently in the wavefront

@@ -119,7 +119,7 @@ BSDF_GRAD_CASES = [
     ("unbiased", 2, ("verts",)),
     ("unbiased", 4, ("verts",)),
     ("unbiased", 8, ("verts",)),
-    # the BRDF-jump term (on request: gradient_terms bit 16)
+    # the BRDF-jump term (gradient_terms bit 16; in the unbiased default for these scenes)
     ("unbiased", 16, ("verts",)),
     ("unbiased", 16, ("normal", "cam")),
 ]
@@ -156,3 +156,23 @@ def test_bsdf_gradient_terms_match_oracle(cuda, estimator, terms, kinds):
     # bounce chains: small differences in a few samples move it more than the others
     # the BRDF-jump arc rays start on the surface, like the shadow-boundary rays
     assert err.max() < (1e-2 if terms in (4, 16) else 2e-3)
+
+
+def test_unbiased_default_terms_include_brdf_jumps(cuda):
+    """With a DiffuseBsdfMaterial mesh in the scene, the unbiased estimator's default
+    gradient terms (gradient_terms=0) are the six terms plus the BRDF jumps (bit 16)."""
+    spec = bsdf_spec()
+    kw = _cfg(spp_interior=4, spp_primary_edge=2, spp_secondary_edge=2, primary_edge_hypercube_resolution=500,
+              secondary_edge_hypercube_resolution=[500, 3, 3], spp_pixel_boundary=2)
+    dLdI = None
+    grads = {}
+    for terms in (0, 111 | 16, 111):
+        scene, T = to_torch_scene(spec, requires_grad={"verts"})
+        img = dr.PathIntegrator(gradient_terms=terms, estimator="unbiased", **kw).renderD(scene)[0]
+        if dLdI is None:
+            dLdI = torch.tensor(np.random.default_rng(7).normal(size=tuple(img.shape)), dtype=torch.float32,
+                                device="cuda")
+        img.backward(dLdI)
+        grads[terms] = T["verts0"].grad.clone()
+    assert torch.equal(grads[0], grads[111 | 16])
+    assert not torch.equal(grads[0], grads[111])

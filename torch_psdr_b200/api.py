@@ -497,9 +497,10 @@ class PathIntegrator:
         is the derivative of the rendered image: material-form interior term plus
         pixel-border, silhouette and shadow-boundary terms), seed (0 = the reference's
         sample streams), tile_paths (wavefront tile, 0 = automatic), gradient_terms
-        (bitmask: 1 interior, 2 primary edges, 4 direct edges, 8 pixel borders, 32
-        interpenetration creases, 64 indirect shadow boundaries; 0 = those six; 16 adds the
-        unbiased estimator's DiffuseBsdfMaterial BRDF-jump term, on request),
+        (bitmask: 1 interior, 2 primary edges, 4 direct edges, 8 pixel borders, 16
+        DiffuseBsdfMaterial BRDF jumps, 32 interpenetration creases, 64 indirect shadow
+        boundaries; 0 = all that apply: bits 8-64 with the unbiased estimator only, bit 16
+        when a DiffuseBsdfMaterial mesh is in the scene),
         spp_pixel_boundary (unbiased: samples per unit pixel-border segment; default
         spp_primary_edge), trace_queue (rays each SM traverses concurrently, in units of
         128; 0 = 8, the autotuner picks it), batch_lanes (BatchRender only: concurrent

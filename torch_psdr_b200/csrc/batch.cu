@@ -196,7 +196,7 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     // lanes: no more than the job has independent parts
     {
       SceneGradInfo any;
-      any.bsdf = 1;
+      any.bsdf = any.jump = 1;
       const size_t parts = std::max(plan_tiles(b->views, b->cap).size(),
                                     b->backward ? backward_units(b->views, *cfg, b->cap, any).size() : (size_t)1);
       b->nlanes = (int)std::min<size_t>(cfg->batch_lanes > 0 ? cfg->batch_lanes : 4, parts);
@@ -250,8 +250,10 @@ PSDR_API psdr_status psdr_batch_create(psdr_scene* const* scenes, int32_t n_scen
     PSDR_CUDA(cudaMemcpyAsync(b->scenes_dev.p, ds.data(), sizeof(DevScene) * n_scenes, cudaMemcpyHostToDevice, st));
     if (n_scenes == 1) b->gi = grad_info(scenes[0]);
     b->ws.bsdf = 0;
-    for (int i = 0; i < n_scenes; ++i)
+    for (int i = 0; i < n_scenes; ++i) {
       if (scenes[i]->has_bsdf || scenes[i]->env_light >= 0) b->gi.bsdf = b->ws.bsdf = 1;
+      if (scenes[i]->has_bsdf) b->gi.jump = 1;
+    }
     for (auto& lw : b->lane_ws) lw->bsdf = b->ws.bsdf;
     if (b->backward) {
       b->gv.resize(n_scenes);

@@ -100,6 +100,7 @@ DevScene* dev_scene(psdr_scene* s) { return s->d_dev.as<DevScene>(); }
 SceneGradInfo grad_info(const psdr_scene* s) {
   SceneGradInfo gi;
   gi.bsdf = s->has_bsdf || s->env_light >= 0 ? 1 : 0;
+  gi.jump = s->has_bsdf ? 1 : 0;
   const int nm = (int)s->meshes.size();
   if (s->nlight == 1) {
     gi.emit_hot = 1;

@@ -3146,6 +3146,12 @@ static void launch_direct(const WF& w, int grid, cudaStream_t st, const DevScene
   else k_direct<PRE, UNB, false><<<grid, 128, 0, st>>>(w, scenes, vd, v, n, hc, round, mass, spp);
 }
 
+// Zeroes the queue counters of a wavefront before a new set of paths enters its depth
+// loop (k_shade resets the ray fetch counter of k_trace itself).
+static void clear_counts(const WF& w, cudaStream_t st) {
+  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+}
+
 template <int MODE>
 static void depth_loop_t(WF& w, const DevScene* scenes, const DevView* views, cudaStream_t st) {
   const int cap = w.cap;
@@ -3179,7 +3185,7 @@ static void launch_camera(const WF& w, const DevScene* scenes, const DevView* vi
 
 static void run_tile(WF& w, const DevScene* scenes, const DevView* views, const Tile& tile, int mode,
                      cudaStream_t st) {
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  clear_counts(w, st);
   const int g = grid_for(tile.n, 256, 8);
   if (mode == MODE_REPLAY) launch_camera<MODE_REPLAY>(w, scenes, views, tile, g, st);
   else if (mode == MODE_KEEP) launch_camera<MODE_KEEP>(w, scenes, views, tile, g, st);
@@ -3312,12 +3318,12 @@ void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views
 
 static void edge_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb, long long begin,
                        int n, const HCube& hc, int round, bool pre, float* mass, int spp, cudaStream_t st) {
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  clear_counts(w, st);
   if (pre) k_edge_init<true><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round, 0);
   else k_edge_init<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, round, 0);
   PSDR_LAUNCHED(1);
   depth_loop(w, scenes, vd, MODE_FWD, st);
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  clear_counts(w, st);
   k_edge_mid<<<grid_for(n, 256, 8), 256, 0, st>>>(w, vd, v, eb, n);
   PSDR_LAUNCHED(1);
   depth_loop(w, scenes, vd, MODE_FWD, st);
@@ -3330,7 +3336,7 @@ static void edge_phase(WF w, const DevScene* scenes, const DevView* vd, int v, c
 // Unbiased silhouette samples: one path per sample (the background side).
 static void edge_phase_unb(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
                            long long begin, int n, const HCube& hc, int spp, cudaStream_t st) {
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  clear_counts(w, st);
   k_edge_init<false><<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, 0, 1);
   PSDR_LAUNCHED(2);
   depth_loop(w, scenes, vd, MODE_FWD, st);
@@ -3342,7 +3348,7 @@ static void edge_phase_unb(WF w, const DevScene* scenes, const DevView* vd, int 
 static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
                          const double* mw, const double* mpre, long long S, long long begin, int n, long long N,
                          bool lens, cudaStream_t st) {
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  clear_counts(w, st);
   k_border_init<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, mw, mpre, S, begin, n, N);
   PSDR_LAUNCHED(2);
   depth_loop(w, scenes, vd, MODE_FWD, st);
@@ -3357,7 +3363,7 @@ static void border_phase(WF w, const DevScene* scenes, const DevView* vd, int v,
 // Indirect shadow-boundary samples [begin, begin + n) of view v: one source path each.
 static void indirect_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
                            long long begin, int n, const HCube& hc, long long N, cudaStream_t st) {
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  clear_counts(w, st);
   k_indirect<false><<<grid_for(n, 128, 16), 128, 0, st>>>(w, scenes, vd, v, eb, begin, n, hc, 0, nullptr);
   PSDR_LAUNCHED(1);
   WF wy = w;
@@ -3374,7 +3380,7 @@ static void indirect_phase(WF w, const DevScene* scenes, const DevView* vd, int 
 static void crease_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb,
                          const CreaseBuf& cb, const double* mw, const double* mpre, long long begin, int n,
                          long long N, cudaStream_t st) {
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (w.D + 1), st));
+  clear_counts(w, st);
   k_crease_init<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, cb, mw, mpre, begin, n, N);
   PSDR_LAUNCHED(1);
   depth_loop(w, scenes, vd, MODE_FWD, st);
@@ -3403,7 +3409,7 @@ static CreaseBuf crease_buf(psdr_workspace* ws) {
 static void jump_phase(WF w, const DevScene* scenes, const DevView* vd, int v, const EdgeBuf& eb, long long begin,
                        int n, int k, cudaStream_t st) {
   const int D = w.D;
-  PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int) * 2 * (D + 1), st));
+  clear_counts(w, st);
   k_jump_init<<<grid_for(n, 256, 8), 256, 0, st>>>(w, scenes, vd, v, eb, begin, n, k, D);
   PSDR_LAUNCHED(1);
   if (k < D) {
@@ -3479,8 +3485,13 @@ void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& view
   backward_launch(scenes_dev, views, cfg, cap, ws, gi, st);
 }
 
-static int job_terms(const psdr_config& cfg) {
-  return cfg.terms ? cfg.terms : (cfg.estimator == PSDR_EST_UNBIASED ? 111 : 7);
+// The terms of a backward job: cfg.terms, or by default interior + primary + direct edges
+// (reference estimator), and for the unbiased estimator also the pixel borders, creases,
+// indirect shadow boundaries and, when a DiffuseBsdfMaterial mesh is in the job, its BRDF
+// jumps.
+static int job_terms(const psdr_config& cfg, const SceneGradInfo& gi) {
+  if (cfg.terms) return cfg.terms;
+  return cfg.estimator == PSDR_EST_UNBIASED ? (111 | (gi.jump ? 16 : 0)) : 7;
 }
 
 // The units of a backward job, in the serial order: every interior tile, then per view
@@ -3490,7 +3501,7 @@ std::vector<BwdUnit> backward_units(const std::vector<DevView>& views, const psd
                                     const SceneGradInfo& gi) {
   std::vector<BwdUnit> u;
   const bool unb = cfg.estimator == PSDR_EST_UNBIASED;
-  const int terms = job_terms(cfg);
+  const int terms = job_terms(cfg, gi);
   const double D = cfg.max_bounce;
   const double R = cfg.mis_light_samples + cfg.mis_bsdf_samples + 1;
   const double R1 = cfg.mis_light_samples + 2;  // boundary paths of the reference estimator: one BSDF sample

@@ -131,6 +131,7 @@ void render_forward_impl(const DevScene* scenes_dev, std::vector<DevView>& views
 struct SceneGradInfo {
   int hot_lv0 = 0, hot_nlv = 0, emit_hot = 0;
   int bsdf = 0;  // a DiffuseBsdfMaterial mesh or an environment light (extended adjoint kernel)
+  int jump = 0;  // a DiffuseBsdfMaterial mesh: the unbiased default terms include its BRDF jumps
 };
 void render_backward_impl(const DevScene* scenes_dev, std::vector<DevView>& views, const psdr_config& cfg,
                           psdr_workspace* ws, const SceneGradInfo& gi, cudaStream_t st);
