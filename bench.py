@@ -52,6 +52,13 @@ WORKLOAD = ("geometry gradient: level-5 icosphere 20,480 tris (+ground, light = 
             "+ 4 spp primary edges + 4 spp secondary edges (+ 4 per pixel-border segment, unbiased estimator), "
             "depth 3, L2 loss, fwd+bwd incl. scene rebuild")
 TRACE_BYTES_PER_RAY = 40  # ray read 24 B + hit write 16 B (per-ray share of the trace kernel)
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of k_trace, mean over the 38 launches of
+# one plain step of this workload (2^21-path tiles; ncu flushes the caches before every
+# launch, so the BVH is read from DRAM each time), from one capture of
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum -k regex:k_trace -s 12 -c 38
+#   python bench.py --mode plain --tile-paths 2097152 --no-autotune --steps 1 --warmup 1 ...
+TRACE_DRAM_BYTES_PER_LAUNCH = 72.39e6
+TRACE_L2_THROUGHPUT_PCT = (11.9, 14.9)  # ncu lts__throughput, % of peak, 256^2 case
 STEP_BYTES_PER_SAMPLE = 2628  # fwd+bwd algorithmic bytes per path sample at depth 3
 
 
@@ -480,7 +487,10 @@ def run_b200(args):
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "kernel": "k_trace (LBVH closest hit)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind, "traffic": TRACE_DRAM_BYTES_PER_LAUNCH,
+                         "traffic_source": "ncu DRAM bytes per k_trace launch, mean over the 38 launches of "
+                                           "one plain step at 2^21-path tiles (caches flushed per launch)",
+                         "l2_throughput_pct_of_peak_ncu": list(TRACE_L2_THROUGHPUT_PCT),
                          "bytes_per_unit": f"{TRACE_BYTES_PER_RAY} B/ray",
                          "rays_per_launch": plain_rays / max(1, plain_tl), "avg_launch_ms": trace_avg_ms,
                          "timed_in": "plain step (launches one at a time)",
