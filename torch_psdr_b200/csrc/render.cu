@@ -99,7 +99,10 @@ PSDR_D int find_view_pix(const DevView* __restrict__ views, int nv, long long g)
 
 PSDR_D float4 hit4(const HitRec& h) { return make_float4(__int_as_float(h.tri), h.b1, h.b2, h.t); }
 
-PSDR_D void atomic_add3(GradAcc* p, float3 v) {
+// Out of line: the adjoint kernels scatter vertex and texel gradients from many call
+// sites, and one copy of the three fixed-point conversions keeps their loops smaller in
+// the instruction cache.
+static __device__ __noinline__ void atomic_add3(GradAcc* p, float3 v) {
   acc_add(p, v.x);
   acc_add(p + 1, v.y);
   acc_add(p + 2, v.z);
