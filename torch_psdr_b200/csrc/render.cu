@@ -544,8 +544,8 @@ PSDR_D void add_vertex(const DevScene& sc, HotAcc& hot, int v, float3 a) {
 // Adjoint of Scene::hit's surface attributes (point, flipped normal and tangent,
 // area) w.r.t. the triangle vertices (mesh.cc:27-67; area via |cross|/2, the same
 // function as Heron's formula).
-PSDR_D void surf_vertex_adj(const DevScene& sc, int tri, float b1, float b2, bool front, const SurfAdj& a,
-                            float3& g0, float3& g1, float3& g2) {
+static __device__ __noinline__ void surf_vertex_adj(const DevScene& sc, int tri, float b1, float b2, bool front,
+                                                    const SurfAdj& a, float3& g0, float3& g1, float3& g2) {
   const float4* r = sc.tri + 6 * (size_t)tri;
   const float4 q0 = __ldg(r), q1 = __ldg(r + 1), q2 = __ldg(r + 2), q3 = __ldg(r + 3), q5 = __ldg(r + 5);
   const float3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2);
@@ -2423,62 +2423,120 @@ __global__ void __launch_bounds__(256) k_jump_final(WF w, const DevScene* __rest
 // albedos of the diffuse bounces between x_d and the camera-visible vertex.
 // BSDF: the DiffuseBsdfMaterial instance (direction-dependent f at the receiver and
 // along the bounce chain); the other instance is the DiffuseMaterial one.
+// The draws of shadow-boundary sample i: hypercube cell and position (PRE: the cell's
+// sampler stream, persisted across rounds in w.rs / w.ri from round 1 on), edge point x_b,
+// light point y; returns the silhouette test (the edge's faces see y on opposite sides).
+// PRE leaves the sampler state after the draws in `rng`; the caller persists it.
+struct DirDraw {
+  Rng rng;
+  float hpdf, sx, pdf_e;
+  int e;
+  float3 p0, p1, out, nl, nr, xb, dir;
+  LightSample ls;
+};
+
+template <bool PRE, bool UNB>
+PSDR_D bool direct_draw(const WF& w, const DevScene& sc, const HCube& hc, int round, long long i, DirDraw& o) {
+  float s3[3];
+  o.hpdf = 1.f;
+  if (PRE) {
+    if (round == 0) o.rng = make_rng((unsigned long long)i);
+    else { o.rng.state = w.rs[i]; o.rng.inc = w.ri[i]; }
+    const int r12 = hc.res[1] * hc.res[2];
+    const int c0 = (int)(i / r12);
+    const int rem = (int)(i - (long long)c0 * r12);
+    const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
+    const float d0 = o.rng.next_float(), d1 = o.rng.next_float(), d2 = o.rng.next_float();
+    s3[0] = ((float)c0 + d0) * hc.unit[0];
+    s3[1] = ((float)c1 + d1) * hc.unit[1];
+    s3[2] = ((float)c2 + d2) * hc.unit[2];
+  } else {
+    o.rng = make_rng((unsigned long long)i + w.seed);
+    s3[0] = o.rng.next_float(); s3[1] = o.rng.next_float(); s3[2] = o.rng.next_float();
+    int cell;
+    if (UNB) {
+      double pm;
+      cell = hc_cell_unb(hc, s3[2], pm);
+      o.hpdf = (float)pm;
+      s3[2] = o.rng.next_float();
+    } else {
+      cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s3[2], o.hpdf);
+    }
+    if (!(o.hpdf > 0.f)) return false;
+    const int r12 = hc.res[1] * hc.res[2];
+    const int c0 = cell / r12, rem = cell - c0 * r12;
+    const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
+    s3[0] = (s3[0] + (float)c0) * hc.unit[0];
+    s3[1] = (s3[1] + (float)c1) * hc.unit[1];
+    s3[2] = (s3[2] + (float)c2) * hc.unit[2];
+  }
+  const int ne = *sc.n_edges;
+  float pe;
+  o.sx = s3[0];
+  o.e = discrete_sample(sc.edge_pmf, sc.edge_cmf, ne, o.sx, pe);
+  const float4 E0 = __ldg(sc.edge + 4 * (size_t)o.e), E1 = __ldg(sc.edge + 4 * (size_t)o.e + 1),
+               E2 = __ldg(sc.edge + 4 * (size_t)o.e + 2), E3 = __ldg(sc.edge + 4 * (size_t)o.e + 3);
+  o.p0 = xyz(E0);
+  o.p1 = xyz(E1);
+  o.out = f3(E1.w, E2.x, E2.y);
+  o.nl = f3(E2.z, E2.w, E3.x);
+  o.nr = f3(E3.y, E3.z, E3.w);
+  o.xb = o.p0 + (o.p1 - o.p0) * o.sx;
+  o.pdf_e = pe / E0.w;
+  o.ls = sample_light(sc, s3[1], s3[2]);
+  o.dir = normalize(o.xb - o.ls.y);
+  return dot(o.nl, o.dir) * dot(o.nr, o.dir) < 0.f && norm(o.nl - o.nr) > kEps;
+}
+
+// First stage of the shadow-boundary samples [begin, begin + n): the draws and the
+// silhouette test only; the samples that pass are queued (w.q0, count in w.cnt[0]) for
+// k_direct, whose warps then start with every lane on a sample that traces (most samples
+// fail the test, and a lane that fails would idle while its warp traces). PRE persists the
+// sampler state of the cells that fail; k_direct does it for the others.
+template <bool PRE, bool UNB>
+__global__ void __launch_bounds__(256) k_direct_pick(WF w, const DevScene* __restrict__ scenes,
+                                                     const DevView* __restrict__ views, int v, long long begin,
+                                                     int n, HCube hc, int round) {
+  const DevScene& sc = scenes[views[v].scene];
+  const int stride = gridDim.x * blockDim.x;
+  const int n32 = (n + 31) & ~31;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n32; k += stride) {
+    bool ok = false;
+    if (k < n) {
+      const long long i = begin + k;
+      DirDraw o;
+      ok = direct_draw<PRE, UNB>(w, sc, hc, round, i, o);
+      if (PRE && !ok) {
+        w.rs[i] = o.rng.state;
+        w.ri[i] = o.rng.inc;
+      }
+    }
+    const int q = warp_append(&w.cnt[0], ok);
+    if (ok) w.q0[q] = k;
+  }
+}
+
 template <bool PRE, bool UNB, bool BSDF>
 __global__ void __launch_bounds__(128) k_direct(WF w, const DevScene* __restrict__ scenes,
-                                                const DevView* __restrict__ views, int v, long long n, HCube hc,
+                                                const DevView* __restrict__ views, int v, long long begin, HCube hc,
                                                 int round, float* mass, int spp) {
   const DevView& V = views[v];
   const DevScene& sc = scenes[V.scene];
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
-    Rng rng;
-    float s3[3], hpdf = 1.f;
+  const int nq = w.cnt[0];
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+    const long long i = begin + w.q0[q];
+    DirDraw o;
+    if (!direct_draw<PRE, UNB>(w, sc, hc, round, i, o)) continue;
+    Rng& rng = o.rng;
     if (PRE) {
-      if (round == 0) rng = make_rng((unsigned long long)i);
-      else { rng.state = w.rs[i]; rng.inc = w.ri[i]; }
-      const int r12 = hc.res[1] * hc.res[2];
-      const int c0 = (int)(i / r12);
-      const int rem = (int)(i - (long long)c0 * r12);
-      const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
-      const float d0 = rng.next_float(), d1 = rng.next_float(), d2 = rng.next_float();
-      s3[0] = ((float)c0 + d0) * hc.unit[0];
-      s3[1] = ((float)c1 + d1) * hc.unit[1];
-      s3[2] = ((float)c2 + d2) * hc.unit[2];
       w.rs[i] = rng.state;
       w.ri[i] = rng.inc;
-    } else {
-      rng = make_rng((unsigned long long)i + w.seed);
-      s3[0] = rng.next_float(); s3[1] = rng.next_float(); s3[2] = rng.next_float();
-      int cell;
-      if (UNB) {
-        double pm;
-        cell = hc_cell_unb(hc, s3[2], pm);
-        hpdf = (float)pm;
-        s3[2] = rng.next_float();
-      } else {
-        cell = discrete_sample(hc.pmf, hc.cmf, hc.ncells, s3[2], hpdf);
-      }
-      if (!(hpdf > 0.f)) continue;
-      const int r12 = hc.res[1] * hc.res[2];
-      const int c0 = cell / r12, rem = cell - c0 * r12;
-      const int c1 = rem / hc.res[2], c2 = rem - c1 * hc.res[2];
-      s3[0] = (s3[0] + (float)c0) * hc.unit[0];
-      s3[1] = (s3[1] + (float)c1) * hc.unit[1];
-      s3[2] = (s3[2] + (float)c2) * hc.unit[2];
     }
-    const int ne = *sc.n_edges;
-    float sx = s3[0], pe;
-    const int e = discrete_sample(sc.edge_pmf, sc.edge_cmf, ne, sx, pe);
-    const float4 E0 = __ldg(sc.edge + 4 * (size_t)e), E1 = __ldg(sc.edge + 4 * (size_t)e + 1),
-                 E2 = __ldg(sc.edge + 4 * (size_t)e + 2), E3 = __ldg(sc.edge + 4 * (size_t)e + 3);
-    const float3 p0 = xyz(E0), p1 = xyz(E1);
-    const float3 out = f3(E1.w, E2.x, E2.y), nl = f3(E2.z, E2.w, E3.x), nr = f3(E3.y, E3.z, E3.w);
-    const float3 xb = p0 + (p1 - p0) * sx;
-    const float pdf_e = pe / E0.w;
-    const LightSample ls = sample_light(sc, s3[1], s3[2]);
-    const float3 dir = normalize(xb - ls.y);
-    bool valid = dot(nl, dir) * dot(nr, dir) < 0.f && norm(nl - nr) > kEps;
-    if (!valid) continue;
+    const float hpdf = o.hpdf, sx = o.sx, pdf_e = o.pdf_e;
+    const int e = o.e;
+    const float3 p0 = o.p0, p1 = o.p1, out = o.out, xb = o.xb, dir = o.dir;
+    const LightSample& ls = o.ls;
     // edge -> light: the same occlusion shortcut as the NEE rays (valid needs the
     // closest hit to be the light within sqrt(1e-5) of y)
     const float dist_l = norm(xb - ls.y);
@@ -3141,12 +3199,22 @@ static int any_ortho(const std::vector<DevView>& views) {
   return 0;
 }
 
-// k_direct instance for the job's materials (w.bsdf).
+// Shadow-boundary samples [0, n) in chunks of the tile capacity: the pick stage queues the
+// samples that pass the silhouette test, then the k_direct instance for the job's
+// materials (w.bsdf) traces them.
 template <bool PRE, bool UNB>
-static void launch_direct(const WF& w, int grid, cudaStream_t st, const DevScene* scenes, const DevView* vd, int v,
+static void launch_direct(const WF& w, cudaStream_t st, const DevScene* scenes, const DevView* vd, int v,
                           long long n, const HCube& hc, int round, float* mass, int spp) {
-  if (w.bsdf) k_direct<PRE, UNB, true><<<grid, 128, 0, st>>>(w, scenes, vd, v, n, hc, round, mass, spp);
-  else k_direct<PRE, UNB, false><<<grid, 128, 0, st>>>(w, scenes, vd, v, n, hc, round, mass, spp);
+  for (long long b = 0; b < n; b += w.cap) {
+    const int nb = (int)std::min<long long>(w.cap, n - b);
+    PSDR_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int), st));
+    k_direct_pick<PRE, UNB><<<grid_for(nb, 256, 8), 256, 0, st>>>(w, scenes, vd, v, b, nb, hc, round);
+    const int g = grid_for(nb, 128, 16);
+    if (w.bsdf) k_direct<PRE, UNB, true><<<g, 128, 0, st>>>(w, scenes, vd, v, b, hc, round, mass, spp);
+    else k_direct<PRE, UNB, false><<<g, 128, 0, st>>>(w, scenes, vd, v, b, hc, round, mass, spp);
+    PSDR_LAUNCHED(2);
+  }
+  PSDR_CUDA(cudaGetLastError());
 }
 
 // Zeroes the queue counters of a wavefront before a new set of paths enters its depth
@@ -3655,23 +3723,15 @@ void backward_unit(const DevScene* scenes_dev, const std::vector<DevView>& views
       HCube pre{};
       for (int k = 0; k < 3; ++k) { pre.res[k] = r3[k]; pre.unit[k] = 1.0f / (float)r3[k]; }
       const int rounds = cfg.secondary_edge_preprocess_rounds * (unb ? kDirectGuideRounds : 1);
-      PSDR_LAUNCHED(rounds + 1);
+      PSDR_LAUNCHED(1);
       for (int r = 0; r < rounds; ++r) {
-        if (unb)
-          launch_direct<true, true>(w, grid_for(cells, 128, 16), st, scenes_dev, vd, v, cells, pre, r,
-                                    ws->mass.as<float>(), 1);
-        else
-          launch_direct<true, false>(w, grid_for(cells, 128, 16), st, scenes_dev, vd, v, cells, pre, r,
-                                     ws->mass.as<float>(), 1);
+        if (unb) launch_direct<true, true>(w, st, scenes_dev, vd, v, cells, pre, r, ws->mass.as<float>(), 1);
+        else launch_direct<true, false>(w, st, scenes_dev, vd, v, cells, pre, r, ws->mass.as<float>(), 1);
       }
       const HCube hc = build_hcube(ws, cells, r3, 3, unb, st);
       const long long N = (long long)V.H * V.W * cfg.spp_secondary_edge;
-      if (unb)
-        launch_direct<false, true>(w, grid_for(N, 128, 16), st, scenes_dev, vd, v, N, hc, 0, nullptr,
-                                   cfg.spp_secondary_edge);
-      else
-        launch_direct<false, false>(w, grid_for(N, 128, 16), st, scenes_dev, vd, v, N, hc, 0, nullptr,
-                                    cfg.spp_secondary_edge);
+      if (unb) launch_direct<false, true>(w, st, scenes_dev, vd, v, N, hc, 0, nullptr, cfg.spp_secondary_edge);
+      else launch_direct<false, false>(w, st, scenes_dev, vd, v, N, hc, 0, nullptr, cfg.spp_secondary_edge);
       PSDR_CUDA(cudaGetLastError());
       break;
     }
