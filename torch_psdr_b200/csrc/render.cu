@@ -1021,7 +1021,7 @@ PSDR_D void cam_jacobian_adj(const DevView& V, const Surf& x, float phi, SurfAdj
 // the previous vertex (or the camera origin), so a vertex's surface adjoint is scattered
 // one depth later.
 template <bool UNB, bool BSDF = false>
-__global__ void __launch_bounds__(128, BSDF ? 2 : 3) k_adjoint(WF w, const DevScene* __restrict__ scenes,
+__global__ void __launch_bounds__(128, BSDF ? 2 : 4) k_adjoint(WF w, const DevScene* __restrict__ scenes,
                                                  const DevView* __restrict__ views, Tile tile, int hot_lv0,
                                                  int hot_nlv, int emit_hot) {
   const int stride = gridDim.x * blockDim.x;
