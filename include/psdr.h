@@ -227,7 +227,9 @@ PSDR_API psdr_status psdr_scene_edges(psdr_scene* scene, int32_t* v01, float* ge
 
 /* Closest hit for n rays (device, 8 floats per ray: ox oy oz tmin dx dy dz tmax).
  * Outputs the global triangle id (-1 on miss), OptiX-convention barycentrics
- * (weights of p1, p2) and t. brute_force != 0 tests every triangle (the KAT path).
+ * (weights of p1, p2) and t. brute_force 1 tests every triangle (the KAT path); 2 runs
+ * the resumable traversal of the wavefront closest-hit kernel instead of the one-shot
+ * traversal of 0 (both must return brute force's hits). 
  * Replaces SceneOptix::hit (scene_optix.cc:240-277) + device_programs.cu:13-47. */
 PSDR_API psdr_status psdr_intersect(psdr_scene* scene, const float* rays, int64_t n, int32_t* tri, float* bary,
                            float* t, int32_t brute_force, void* stream);

@@ -20,12 +20,13 @@ def test_leaf_sizes_match_brute_force(cuda, leaf):
     scene, _ = to_torch_scene(spec)
     L.check(L.load().psdr_scene_set_leaf_size(scene.handle, leaf, _stream()), "leaf")
     rays = _random_rays(spec, 20000, 13)
-    t_bvh, b_bvh, tt_bvh = gpu_intersect(scene, rays, False)
-    t_bf, b_bf, tt_bf = gpu_intersect(scene, rays, True)
+    t_bf, b_bf, tt_bf = gpu_intersect(scene, rays, 1)
     assert (t_bf >= 0).mean() > 0.3
-    np.testing.assert_array_equal(t_bvh, t_bf)
-    np.testing.assert_array_equal(b_bvh, b_bf)
-    np.testing.assert_array_equal(tt_bvh, tt_bf)
+    for mode in (0, 2):  # one-shot traversal, the wavefront kernel's resumable traversal
+        t_bvh, b_bvh, tt_bvh = gpu_intersect(scene, rays, mode)
+        np.testing.assert_array_equal(t_bvh, t_bf)
+        np.testing.assert_array_equal(b_bvh, b_bf)
+        np.testing.assert_array_equal(tt_bvh, tt_bf)
 
 
 def test_tiny_scene_with_large_leaves(cuda):
@@ -37,10 +38,11 @@ def test_tiny_scene_with_large_leaves(cuda):
     scene, _ = to_torch_scene(spec)
     L.check(L.load().psdr_scene_set_leaf_size(scene.handle, 8, _stream()), "leaf")
     rays = _random_rays(spec, 4000, 17)
-    a = gpu_intersect(scene, rays, False)
-    b = gpu_intersect(scene, rays, True)
-    for x, y in zip(a, b):
-        np.testing.assert_array_equal(x, y)
+    b = gpu_intersect(scene, rays, 1)
+    for mode in (0, 2):
+        a = gpu_intersect(scene, rays, mode)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
 
 
 def test_autotune_keeps_images(cuda):

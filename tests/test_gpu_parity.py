@@ -51,13 +51,17 @@ def test_intersect_kat_bit_exact(cuda, level, noise):
     spec = synth.sphere_scene(level=level, noise_sigma=noise, height=8, width=8)
     scene, _ = to_torch_scene(spec)
     rays = _random_rays(spec, 20000, 11)
-    t_bvh, b_bvh, tt_bvh = gpu_intersect(scene, rays, False)
-    t_bf, b_bf, tt_bf = gpu_intersect(scene, rays, True)
+    t_bvh, b_bvh, tt_bvh = gpu_intersect(scene, rays, 0)
+    t_bf, b_bf, tt_bf = gpu_intersect(scene, rays, 1)
+    t_wf, b_wf, tt_wf = gpu_intersect(scene, rays, 2)  # the wavefront kernel's traversal
     t_or, b_or, tt_or = orc.intersect(spec, rays, use_bvh=False)
     assert (t_bf >= 0).mean() > 0.3
     np.testing.assert_array_equal(t_bvh, t_bf)
     np.testing.assert_array_equal(b_bvh, b_bf)
     np.testing.assert_array_equal(tt_bvh, tt_bf)
+    np.testing.assert_array_equal(t_wf, t_bf)
+    np.testing.assert_array_equal(b_wf, b_bf)
+    np.testing.assert_array_equal(tt_wf, tt_bf)
     np.testing.assert_array_equal(t_bf, t_or)
     np.testing.assert_array_equal(b_bf, b_or)
     np.testing.assert_array_equal(tt_bf, tt_or)
@@ -70,10 +74,11 @@ def test_intersect_single_triangle_and_misses(cuda):
                            [synth.default_camera(4, 4)])
     scene, _ = to_torch_scene(spec)
     rays = np.array([[0.2, 0.2, 1, 0, 0, -1], [2, 2, 1, 0, 0, -1], [0.2, 0.2, -1, 0, 0, -1]], np.float32)
-    t, b, tt = gpu_intersect(scene, rays, False)
-    assert list(t) == [0, -1, -1]
-    np.testing.assert_allclose(b[0], [0.2, 0.2], atol=1e-6)
-    np.testing.assert_allclose(tt[0], 1.0, atol=1e-6)
+    for mode in (0, 2):
+        t, b, tt = gpu_intersect(scene, rays, mode)
+        assert list(t) == [0, -1, -1]
+        np.testing.assert_allclose(b[0], [0.2, 0.2], atol=1e-6)
+        np.testing.assert_allclose(tt[0], 1.0, atol=1e-6)
 
 
 def test_edges_match_oracle(cuda):

@@ -25,8 +25,21 @@ __global__ void k_intersect(DevScene sc, const float* __restrict__ rays, long lo
     const float3 o = f3(r[0], r[1], r[2]), d = f3(r[4], r[5], r[6]);
     const float tmin = r[3], tmax = r[7];
     HitRec h;
-    if (!brute) {
+    if (brute == 0) {
       h = trace_closest(sc, o, d, tmin, tmax);
+    } else if (brute == 2) {
+      // the resumable traversal of the wavefront closest-hit kernel (trace_step)
+      struct Stk {
+        int a[kStack];
+        __device__ void push(int i, int v) { a[i] = v; }
+        __device__ int pop(int i) const { return a[i]; }
+      } stk;
+      TraceState s;
+      trace_begin(s, o, d, tmin, tmax, -INFINITY, sc.root);
+      if (sc.ntri > 0)
+        while (!trace_step(sc, s, stk)) {
+        }
+      h = s.h;
     } else {
       h.tri = -1; h.t = tmax; h.b1 = h.b2 = 0.f;
       const RayPre rp = ray_pre(o, d);
