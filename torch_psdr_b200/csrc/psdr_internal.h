@@ -85,6 +85,7 @@ struct psdr_scene {
   // tree topology of the last full build, kept for psdr_scene_refit: binary child links,
   // leaf triangle order, 4-wide node flags and indices (the build's scratch is reused)
   psdr::DBuf bvh_child, bvh_order, bvh_f4;
+  psdr::DBuf bvh_slots;  // per 4-wide node (by binary node id): its four children, -1 for none
   // build scratch
   psdr::DBuf keys, vals, aux_i, aux_i2, aux_d, aux_d2, aabb, parent, range, flags, cbox;
   psdr::SortTmp sort_tmp;

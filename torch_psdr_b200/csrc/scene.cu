@@ -328,26 +328,119 @@ __global__ void k_bottom_up(int n, const uint32_t* __restrict__ order, const flo
   }
 }
 
-// ---- 4-wide BVH: every internal node at even depth of the binary tree becomes a
-// 4-wide node whose children are its grandchildren (or its children where those are
-// leaves), i.e. a pairwise collapse of two binary levels.
-__global__ void k_depth_flags(int n, const int* __restrict__ parent, const int2* __restrict__ range, int leaf_size,
-                              int* __restrict__ flag) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n - 1) return;
-  int d = 0;
-  bool inside = false;
-  for (int a = i; a != 0; ++d) {
-    a = parent[a];
-    const int2 r = range[a];
-    if (r.y - r.x + 1 <= leaf_size) inside = true;
-  }
-  const int2 r = range[i];
-  const bool leafy = r.y - r.x + 1 <= leaf_size;
-  flag[i] = (!inside && !leafy && (d & 1) == 0) ? 1 : 0;
+// ---- 4-wide BVH: greedy collapse of the binary tree. Starting from the root, a 4-wide
+// node takes the two children of its binary node and keeps replacing the internal child
+// with the largest surface area by that child's two children until it holds four (or
+// only leaves are left); every internal child left in it becomes a 4-wide node of the
+// next level. A binary node whose range holds at most leaf_size triangles is a leaf.
+// One block walks the tree level by level; within a level the nodes take their indices
+// in queue order through a block-wide scan, so the layout is the same on every build.
+__device__ __forceinline__ float box_area(const float* b) {
+  const float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+  return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_layout4(int n, int leaf_size, const int2* __restrict__ child, const int2* __restrict__ range,
+__global__ void __launch_bounds__(1024) k_collapse4(int n, int leaf_size, const int2* __restrict__ child,
+                                                    const int2* __restrict__ range, const float* __restrict__ aabb,
+                                                    int* __restrict__ flag, int* __restrict__ idx4,
+                                                    int* __restrict__ slots4, int* __restrict__ qa,
+                                                    int* __restrict__ qb) {
+  __shared__ int warp_sum[32];
+  __shared__ int level_n, next_n, next_idx;
+  auto expandable = [&](int c) {
+    if (c >= n - 1) return false;
+    const int2 r = range[c];
+    return r.y - r.x + 1 > leaf_size;
+  };
+  if (threadIdx.x == 0) {
+    qa[0] = 0;
+    flag[0] = 1;
+    idx4[0] = 0;
+    level_n = 1;
+    next_idx = 1;
+  }
+  __syncthreads();
+  int* cur = qa;
+  int* nxt = qb;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  while (level_n > 0) {
+    const int m = level_n;
+    if (threadIdx.x == 0) next_n = 0;
+    __syncthreads();
+    for (int base = 0; base < m; base += blockDim.x) {
+      const int q = base + threadIdx.x;
+      int sl[4] = {-1, -1, -1, -1};
+      int cnt = 0;
+      if (q < m) {
+        const int i = cur[q];
+        const int2 ch = child[i];
+        sl[0] = ch.x;
+        sl[1] = ch.y;
+        int ns = 2;
+        while (ns < 4) {
+          int best = -1;
+          float ba = -1.f;
+          for (int k = 0; k < ns; ++k)
+            if (expandable(sl[k])) {
+              const float a = box_area(aabb + 6 * (size_t)sl[k]);
+              if (a > ba) { ba = a; best = k; }
+            }
+          if (best < 0) break;
+          const int2 g = child[sl[best]];
+          sl[best] = g.x;
+          sl[ns++] = g.y;
+        }
+        for (int k = 0; k < 4; ++k) {
+          slots4[4 * (size_t)i + k] = sl[k];
+          if (sl[k] >= 0 && expandable(sl[k])) ++cnt;
+        }
+      }
+      // block-wide exclusive scan of cnt (queue order)
+      int x = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) warp_sum[wid] = x;
+      __syncthreads();
+      if (wid == 0) {
+        int w = lane < (int)(blockDim.x >> 5) ? warp_sum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, w, o);
+          if (lane >= o) w += y;
+        }
+        warp_sum[lane] = w;  // inclusive over warps
+      }
+      __syncthreads();
+      const int excl = x - cnt + (wid > 0 ? warp_sum[wid - 1] : 0);
+      const int total = warp_sum[(blockDim.x >> 5) - 1];
+      if (cnt > 0) {
+        int k2 = excl;
+        for (int k = 0; k < 4; ++k)
+          if (sl[k] >= 0 && expandable(sl[k])) {
+            const int c = sl[k];
+            flag[c] = 1;
+            idx4[c] = next_idx + k2;
+            nxt[next_n + k2] = c;
+            ++k2;
+          }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        next_idx += total;
+        next_n += total;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) level_n = next_n;
+    int* t = cur;
+    cur = nxt;
+    nxt = t;
+    __syncthreads();
+  }
+}
+
+__global__ void k_layout4(int n, int leaf_size, const int* __restrict__ slots4, const int2* __restrict__ range,
                           const float* __restrict__ aabb, const unsigned int* __restrict__ cbox,
                           const int* __restrict__ flag, const int* __restrict__ idx4, float4* __restrict__ nodes4) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -368,13 +461,9 @@ __global__ void k_layout4(int n, int leaf_size, const int2* __restrict__ child, 
   };
   int slot[4];
   int ns = 0;
-  const int2 ch = child[i];
-  for (int s = 0; s < 2; ++s) {
-    const int c = s == 0 ? ch.x : ch.y;
-    if (is_leaf(c)) { slot[ns++] = c; continue; }
-    const int2 g = child[c];
-    slot[ns++] = g.x;
-    slot[ns++] = g.y;
+  for (int k = 0; k < 4; ++k) {
+    const int c = slots4[4 * (size_t)i + k];
+    if (c >= 0) slot[ns++] = c;
   }
   float lo[3][4], hi[3][4];
   int enc[4];
@@ -517,16 +606,19 @@ void scene_build_geometry(psdr_scene* s, cudaStream_t st) {
     const int leaf = std::min(s->leaf_size, n - 1);
     int* f4 = s->aux_i2.as<int>();
     int* idx4 = s->aux_i2.as<int>() + n;
-    k_depth_flags<<<nblk(n - 1), 256, 0, st>>>(n, parent, range, leaf, f4);
-    exclusive_scan_int(f4, idx4, n - 1, s->flags.as<int>() + 2 * (size_t)n, st);
-    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, leaf, child, range, aabb, cbox, f4, idx4, s->nodes.as<float4>());
+    int* slots4 = s->bvh_slots.as<int>();
+    PSDR_CUDA(cudaMemsetAsync(f4, 0, sizeof(int) * (size_t)n, st));
+    // the Morton keys are no longer needed: their storage holds the two level queues
+    int* qa = reinterpret_cast<int*>(keys);
+    k_collapse4<<<1, 1024, 0, st>>>(n, leaf, child, range, aabb, f4, idx4, slots4, qa, qa + n);
+    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, leaf, slots4, range, aabb, cbox, f4, idx4, s->nodes.as<float4>());
     PSDR_CUDA(cudaMemcpyAsync(s->bvh_child.p, child, sizeof(int2) * (n - 1), cudaMemcpyDeviceToDevice, st));
     PSDR_CUDA(cudaMemcpyAsync(s->bvh_f4.p, f4, sizeof(int) * 2 * (size_t)n, cudaMemcpyDeviceToDevice, st));
   }
   k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, vals, s->tri.as<float4>(), s->leaf.as<float4>());
   PSDR_CUDA(cudaMemcpyAsync(s->bvh_order.p, vals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
   // records + lights + half-edge sort (2 x passes x 5) + edge build/CDF (8) + BVH (9 + morton sort)
-  count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 9 + 3 * 4);
+  count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 8 + 3 * 4);
   PSDR_CUDA(cudaGetLastError());
 }
 
@@ -550,8 +642,8 @@ void scene_refit_geometry(psdr_scene* s, cudaStream_t st) {
   if (n > 1) {
     const int leaf = std::min(s->leaf_size, n - 1);
     const int* f4 = s->bvh_f4.as<int>();
-    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, leaf, child, s->range.as<int2>(), aabb, cbox, f4, f4 + n,
-                                           s->nodes.as<float4>());
+    k_layout4<<<nblk(n - 1), 256, 0, st>>>(n, leaf, s->bvh_slots.as<int>(), s->range.as<int2>(), aabb, cbox, f4,
+                                           f4 + n, s->nodes.as<float4>());
   }
   k_leaf_tris<<<nblk(n), 256, 0, st>>>(n, order, s->tri.as<float4>(), s->leaf.as<float4>());
   count_launches(s->nobj + (s->nlight > 0) + 3 + 3 * ((32 + vbits + 7) / 8) + 8 + 6);
@@ -594,6 +686,7 @@ void psdr_scene_alloc(psdr_scene* s) {
   s->bvh_child.alloc(sizeof(int2) * n, st);
   s->bvh_order.alloc(sizeof(uint32_t) * n, st);
   s->bvh_f4.alloc(sizeof(int) * 2 * (size_t)n, st);
+  s->bvh_slots.alloc(sizeof(int) * 4 * (size_t)n, st);
   s->d_dev.alloc(sizeof(DevScene), st);
   PSDR_CUDA(cudaMemsetAsync(s->err.p, 0, sizeof(int), st));
   DevScene& d = s->dev;
