@@ -584,6 +584,21 @@ PSDR_D void scatter_surf(const DevScene& sc, HotAcc& hot, int tri, float b1, flo
   add_vertex(sc, hot, tv.z, g2);
 }
 
+// scatter_surf for a triangle that is not a light's: path vertices past the camera hit
+// (paths end at lights), whose vertices never fall in the light-vertex register range.
+// Out of line: the adjoint scatters from several depths' call sites.
+static __device__ __noinline__ void scatter_mesh(const DevScene& sc, int tri, float b1, float b2, bool front,
+                                                 SurfAdj a) {
+  if (!sc.grad_verts) return;
+  const int4 tv = __ldg(sc.tri_v + tri);
+  if (!vert_wanted(sc, tv.x) && !vert_wanted(sc, tv.y) && !vert_wanted(sc, tv.z)) return;
+  float3 g0, g1, g2;
+  surf_vertex_adj(sc, tri, b1, b2, front, a, g0, g1, g2);
+  vert_add(sc, tv.x, g0);
+  vert_add(sc, tv.y, g1);
+  vert_add(sc, tv.z, g2);
+}
+
 PSDR_D void scatter_tex(const DevTex& tx, int off, float3 a, bool /*unused*/) {
   if (!tx.grad) return;
   if (tx.ch == 1) acc_add(tx.grad + off, a.x + a.y + a.z);
@@ -1124,7 +1139,7 @@ __global__ void __launch_bounds__(128, BSDF ? 2 : 4) k_adjoint(WF w, const DevSc
                 if (d == 0) cam.add(&V, aorg);
                 else if (d == 1) ax0.p += aorg;
                 else axq.p += aorg;
-                if (triq >= 0) scatter_surf(sc, hot, triq, hq.y, hq.z, frontq, axq);
+                if (triq >= 0) scatter_mesh(sc, triq, hq.y, hq.z, frontq, axq);
                 triq = -1;
                 const int off = texel_offset(ob.color, xc.u, xc.v);
                 if (d == 0) {
@@ -1151,7 +1166,7 @@ __global__ void __launch_bounds__(128, BSDF ? 2 : 4) k_adjoint(WF w, const DevSc
                   toff0 = off;
                 } else {
                   if (ob.color.grad) scatter_tex(ob.color, off, atx, false);
-                  scatter_surf(sc, hot, tric, hc.y, hc.z, xc.front, ax);
+                  scatter_mesh(sc, tric, hc.y, hc.z, xc.front, ax);
                 }
                 if (!dv.has_next) break;
               }
@@ -1163,7 +1178,7 @@ __global__ void __launch_bounds__(128, BSDF ? 2 : 4) k_adjoint(WF w, const DevSc
               if (xc.is_light) break;  // the path ends on a light: nothing downstream
               ax = nextc;
             }
-            if (BSDF && triq >= 0) scatter_surf(sc, hot, triq, hq.y, hq.z, frontq, axq);
+            if (BSDF && triq >= 0) scatter_mesh(sc, triq, hq.y, hq.z, frontq, axq);
           }
         }
       }
