@@ -255,6 +255,9 @@ __global__ void __launch_bounds__(256) k_shade(WF w, const DevScene* __restrict_
 // warp differ in traversal length by an order of magnitude). The fetch counter is
 // w.cnt[2D+2], reset by k_shade.
 constexpr int kTraceSteps = 8;
+// Lights of at most this many triangles in all let k_trace answer MIS BSDF-sample rays
+// with a light test and a bounded occlusion query.
+constexpr int kMisLightTris = 16;
 __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict__ scenes,
                                                    const DevView* __restrict__ views, int d,
                                                    unsigned long long* __restrict__ ray_count) {
@@ -298,7 +301,38 @@ __global__ void __launch_bounds__(128) k_trace(WF w, const DevScene* __restrict_
           const float t_occ = r < w.nL ? (o.w - 4e-3f) / 1.0001f - 4e-3f : -INFINITY;
           trace_begin(s, xyz(o), xyz(dd), kTmin, o.w, t_occ, sc->root);
           live = sc->ntri > 0;
-          if (!live) w.hit[slot] = make_float4(__int_as_float(-1), 0.f, 0.f, o.w);
+          if (live && r >= w.nL && r < w.nL + w.nB && sc->nlight > 0) {
+            // MIS BSDF-sample ray: only a light hit contributes (the shade, accumulate and
+            // adjoint kernels skip any other hit). The closest light triangle along the ray
+            // (the traversal's test and tie rule) bounds an occlusion query: a nearer hit is
+            // reported as a miss, and with no light along the ray nothing is traversed.
+            int nlt = 0;
+            for (int l = 0; l < sc->nlight; ++l) nlt += sc->lights[l].ntri;
+            if (nlt <= kMisLightTris) {
+              float tl = o.w;
+              int best = -1;
+              for (int l = 0; l < sc->nlight; ++l) {
+                const DevLight& Lt = sc->lights[l];
+                for (int t = Lt.tri0; t < Lt.tri0 + Lt.ntri; ++t) {
+                  const float4* q = sc->tri + 6 * (size_t)t;
+                  float tt, b1, b2;
+                  if (tri_test(s.rp, xyz(__ldg(q)), xyz(__ldg(q + 1)), xyz(__ldg(q + 2)), kTmin, tl, tt, b1, b2) &&
+                      (tt < tl || best < 0 || t < best)) {
+                    tl = tt;
+                    best = t;
+                  }
+                }
+              }
+              if (best < 0) {
+                live = false;
+                w.hit[slot] = make_float4(__int_as_float(-1), 0.f, 0.f, o.w);
+              } else {
+                s.h.t = tl;
+                s.t_occ = tl;
+              }
+            }
+          }
+          if (!live && sc->ntri <= 0) w.hit[slot] = make_float4(__int_as_float(-1), 0.f, 0.f, o.w);
         } else {
           done = true;
         }
@@ -1258,7 +1292,7 @@ PSDR_D bool tri_has_edge(const DevScene& sc, int tri, int2 ev) {
 // (foreground); the path of the other side (background, possibly a miss) is traced,
 // and eb.hb keeps that background hit with flag 1 (background on the +eps side) or 2.
 template <bool PRE>
-__global__ void __launch_bounds__(256) k_edge_init(WF w, const DevScene* __restrict__ scenes,
+__global__ void __launch_bounds__(256, 3) k_edge_init(WF w, const DevScene* __restrict__ scenes,
                                                    const DevView* __restrict__ views, int v, EdgeBuf eb,
                                                    long long begin, int n, HCube hc, int round, int unb) {
   const int stride = gridDim.x * blockDim.x;
