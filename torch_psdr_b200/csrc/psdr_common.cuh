@@ -40,6 +40,7 @@ constexpr float kInvPi = 0.318309886183790671538f;
 constexpr float k2Pi = 6.28318530717958647692f;
 constexpr float kEps = 1e-5f;       // types.h:114 REAL_EPS
 constexpr float kTmin = 1e-3f;      // device_programs.cu:8 tmin of every trace
+constexpr int kEdgeNonManifold = -2;  // DevScene::edge_f of an edge with more than two faces
 
 // ------------------------------------------------------------------ PCG32 + TEA
 // One PCG32 stream per sample index (sampler.h:8-84), seeded through 4-round TEA.
@@ -166,6 +167,9 @@ struct DevScene {
   const int* n_edges;      // device scalar
   const float4* edge;      // 4 x float4: (p0,len) (p1,out.x) (out.yz,nl.xy) (nl.z,nr)
   const int2* edge_v;
+  // the edge's faces (global triangle ids; y = -1 for a boundary edge); kEdgeNonManifold in x
+  // for an edge of more than two faces
+  const int2* edge_f;
   const float* edge_pmf;
   const float* edge_cmf;
   int root;

@@ -80,7 +80,7 @@ struct psdr_scene {
   std::vector<psdr::DevLight> h_lights;
   // device storage
   psdr::DBuf verts, tri, tri_v, objs, lights_buf, light_pmf, light_cmf, ltri_pmf, ltri_cmf;
-  psdr::DBuf n_edges, edge, edge_v, edge_pmf, edge_cmf;
+  psdr::DBuf n_edges, edge, edge_v, edge_f, edge_pmf, edge_cmf;
   psdr::DBuf nodes, leaf, err;
   // tree topology of the last full build, kept for psdr_scene_refit: binary child links,
   // leaf triangle order, 4-wide node flags and indices (the build's scratch is reused)

@@ -567,9 +567,11 @@ PSDR_D void add_vertex(const DevScene& sc, HotAcc& hot, int v, float3 a) {
   if (!sc.grad_verts) return;
   const int rel = v - hot.lv0;
   if (hot.nlv > 0 && rel >= 0 && rel < hot.nlv) {
-#pragma unroll
-    for (int k = 0; k < kMaxLightVerts; ++k)
-      if (k == rel) { hot.g[3 * k] += a.x; hot.g[3 * k + 1] += a.y; hot.g[3 * k + 2] += a.z; }
+    // dynamic index: the accumulators live in local memory (L1), which keeps this code
+    // short at each of the adjoint's scatter sites
+    hot.g[3 * rel] += a.x;
+    hot.g[3 * rel + 1] += a.y;
+    hot.g[3 * rel + 2] += a.z;
     return;
   }
   vert_add(sc, v, a);
@@ -1346,8 +1348,48 @@ __global__ void __launch_bounds__(256, 3) k_edge_init(WF w, const DevScene* __re
       ha.tri = hb.tri = -1;
       ha.b1 = ha.b2 = hb.b1 = hb.b2 = 0.f;
       if (valid) {
-        ha = trace_closest(sc, eo, sub_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
-        hb = trace_closest(sc, eo, add_rn(rd, scale_rn(nrm, kEps)), kTmin, INFINITY);
+        const float3 da = sub_rn(rd, scale_rn(nrm, kEps)), db = add_rn(rd, scale_rn(nrm, kEps));
+        const int2 ef = (!PRE && unb) ? __ldg(sc.edge_f + e) : make_int2(kEdgeNonManifold, -1);
+        if (ef.x == kEdgeNonManifold) {
+          ha = trace_closest(sc, eo, da, kTmin, INFINITY);
+          hb = trace_closest(sc, eo, db, kTmin, INFINITY);
+        } else {
+          // Unbiased silhouette sample: valid only when exactly one offset ray's closest hit
+          // is a face of the edge. Test each ray against the edge's faces first (the
+          // traversal's test and tie rule): a ray that misses both cannot have one as its
+          // closest hit, and for a ray that hits one at t an occlusion query bounded at t
+          // decides. Only the other ray of a valid sample needs its full closest hit (its
+          // background); with both rays on the faces, both are traced in full as before.
+          auto face_hit = [&](float3 d, float& tf) {
+            const RayPre rp = ray_pre(eo, d);
+            int best = -1;
+            tf = INFINITY;
+            for (int k = 0; k < 2; ++k) {
+              const int f = k == 0 ? ef.x : ef.y;
+              if (f < 0) continue;
+              const float4* q = sc.tri + 6 * (size_t)f;
+              float tt, b1, b2;
+              if (tri_test(rp, xyz(__ldg(q)), xyz(__ldg(q + 1)), xyz(__ldg(q + 2)), kTmin, tf, tt, b1, b2) &&
+                  (tt < tf || best < 0 || f < best)) {
+                tf = tt;
+                best = f;
+              }
+            }
+            return best >= 0;
+          };
+          float tfa, tfb;
+          const bool fa = face_hit(da, tfa), fb = face_hit(db, tfb);
+          if (fa && fb) {
+            ha = trace_closest(sc, eo, da, kTmin, INFINITY);
+            hb = trace_closest(sc, eo, db, kTmin, INFINITY);
+          } else if (fa) {
+            ha = trace_closest(sc, eo, da, kTmin, tfa, tfa);
+            if (tri_has_edge(sc, ha.tri, __ldg(sc.edge_v + e))) hb = trace_closest(sc, eo, db, kTmin, INFINITY);
+          } else if (fb) {
+            hb = trace_closest(sc, eo, db, kTmin, tfb, tfb);
+            if (tri_has_edge(sc, hb.tri, __ldg(sc.edge_v + e))) ha = trace_closest(sc, eo, da, kTmin, INFINITY);
+          }
+        }
       }
       int flag;
       HitRec hcur = ha;

@@ -124,8 +124,8 @@ PSDR_D float3 ldv(const float* v, int i) { return f3(v[3 * i], v[3 * i + 1], v[3
 __global__ void k_edge_build(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals, int n,
                              const int* __restrict__ flags, const int* __restrict__ eidx,
                              const int4* __restrict__ tri_v, const float* __restrict__ verts,
-                             float4* __restrict__ edge, int2* __restrict__ edge_v, float* __restrict__ elen,
-                             int* __restrict__ n_edges) {
+                             float4* __restrict__ edge, int2* __restrict__ edge_v, int2* __restrict__ edge_f,
+                             float* __restrict__ elen, int* __restrict__ n_edges) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == n - 1) *n_edges = eidx[i] + flags[i];
   if (i >= n || !flags[i]) return;
@@ -154,6 +154,7 @@ __global__ void k_edge_build(const uint64_t* __restrict__ keys, const uint32_t* 
   edge[4 * e + 2] = make_float4(out.y, out.z, nl.x, nl.y);
   edge[4 * e + 3] = make_float4(nl.z, nr.x, nr.y, nr.z);
   edge_v[e] = make_int2(v0, v1);
+  edge_f[e] = j > i + 1 ? make_int2(kEdgeNonManifold, -1) : make_int2(fl, shared ? fr : -1);
   elen[e] = len;
 }
 
@@ -569,7 +570,8 @@ static int build_records_and_edges(psdr_scene* s, cudaStream_t st, int& vbits_ou
   exclusive_scan_int(flags, eidx, nh, s->flags.as<int>(), st);
   float* elen = reinterpret_cast<float*>(s->aux_d2.as<double>() + nh);  // scratch tail
   k_edge_build<<<nblk(nh), 256, 0, st>>>(keys, vals, nh, flags, eidx, s->tri_v.as<int4>(), s->verts.as<float>(),
-                                         s->edge.as<float4>(), s->edge_v.as<int2>(), elen, s->n_edges.as<int>());
+                                         s->edge.as<float4>(), s->edge_v.as<int2>(), s->edge_f.as<int2>(), elen,
+                                         s->n_edges.as<int>());
   k_to_double<<<nblk(nh), 256, 0, st>>>(elen, s->n_edges.as<int>(), nh, s->aux_d.as<double>());
   inclusive_scan_double(s->aux_d.as<double>(), s->aux_d2.as<double>(), nh,
                         reinterpret_cast<double*>(s->flags.as<int>()), st);
@@ -667,6 +669,7 @@ void psdr_scene_alloc(psdr_scene* s) {
   s->n_edges.alloc(sizeof(int), st);
   s->edge.alloc(sizeof(float4) * 4 * nh, st);
   s->edge_v.alloc(sizeof(int2) * nh, st);
+  s->edge_f.alloc(sizeof(int2) * nh, st);
   s->edge_pmf.alloc(sizeof(float) * nh, st);
   s->edge_cmf.alloc(sizeof(float) * nh, st);
   s->nodes.alloc(sizeof(float4) * 7 * n, st);
@@ -696,6 +699,7 @@ void psdr_scene_alloc(psdr_scene* s) {
   d.light_pmf = s->light_pmf.as<float>(); d.light_cmf = s->light_cmf.as<float>();
   d.ltri_pmf = s->ltri_pmf.as<float>(); d.ltri_cmf = s->ltri_cmf.as<float>();
   d.edge_cap = nh; d.n_edges = s->n_edges.as<int>(); d.edge = s->edge.as<float4>(); d.edge_v = s->edge_v.as<int2>();
+  d.edge_f = s->edge_f.as<int2>();
   d.edge_pmf = s->edge_pmf.as<float>(); d.edge_cmf = s->edge_cmf.as<float>();
   d.nodes = s->nodes.as<float4>(); d.leaf = s->leaf.as<float4>();
   d.root = s->ntri > 1 ? 0 : ~0;  // a single triangle makes the root a leaf
