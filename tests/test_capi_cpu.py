@@ -62,6 +62,27 @@ def test_render_rejects_bad_config(lib):
     assert lib.psdr_workspace_destroy(ws) == 0
 
 
+def test_batch_options_are_checked(lib):
+    """batch_lanes (0..8) and batch_records (-1, 0, 1) are range-checked by the C ABI and
+    the Python constructor, before any device work."""
+    ws = C.c_void_p()
+    assert lib.psdr_workspace_create(C.byref(ws)) == 0
+    cam = L.CameraDesc()
+    img = (C.c_void_p * 1)(None)
+    for field, bad in (("batch_lanes", 9), ("batch_lanes", -1), ("batch_records", 2), ("batch_records", -2)):
+        cfg = dr.PathIntegrator().cfg
+        setattr(cfg, field, bad)
+        st = lib.psdr_render_fwd(C.c_void_p(1), ws, C.byref(cam), 1, C.byref(cfg), img, None)
+        assert st == L.PSDR_ERR_INVALID_ARG and field.encode() in lib.psdr_last_error()
+    assert lib.psdr_workspace_destroy(ws) == 0
+    with pytest.raises(AssertionError):
+        dr.PathIntegrator(batch_lanes=9)
+    with pytest.raises(AssertionError):
+        dr.PathIntegrator(batch_records=2)
+    cfg = dr.PathIntegrator(batch_lanes=8, batch_records=-1).cfg
+    assert (cfg.batch_lanes, cfg.batch_records) == (8, -1)
+
+
 def test_api_asserts_mirror_reference():
     t3 = torch.zeros(3)
     with pytest.raises(AssertionError):
