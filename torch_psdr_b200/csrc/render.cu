@@ -2515,7 +2515,7 @@ __global__ void __launch_bounds__(256) k_jump_final(WF w, const DevScene* __rest
 // BSDF: the DiffuseBsdfMaterial instance (direction-dependent f at the receiver and
 // along the bounce chain); the other instance is the DiffuseMaterial one.
 // The draws of shadow-boundary sample i: hypercube cell and position (PRE: the cell's
-// sampler stream, persisted across rounds in w.rs / w.ri from round 1 on), edge point x_b,
+// sampler stream, persisted in w.rs / w.ri from the second preprocess round on), edge point x_b,
 // light point y; returns the silhouette test (the edge's faces see y on opposite sides).
 // PRE leaves the sampler state after the draws in `rng`; the caller persists it.
 struct DirDraw {
