@@ -1359,7 +1359,7 @@ __global__ void __launch_bounds__(256, 3) k_edge_init(WF w, const DevScene* __re
           // traversal's test and tie rule): a ray that misses both cannot have one as its
           // closest hit, and for a ray that hits one at t an occlusion query bounded at t
           // decides. Only the other ray of a valid sample needs its full closest hit (its
-          // background); with both rays on the faces, both are traced in full as before.
+          // background).
           auto face_hit = [&](float3 d, float& tf) {
             const RayPre rp = ray_pre(eo, d);
             int best = -1;
@@ -1380,8 +1380,14 @@ __global__ void __launch_bounds__(256, 3) k_edge_init(WF w, const DevScene* __re
           float tfa, tfb;
           const bool fa = face_hit(da, tfa), fb = face_hit(db, tfb);
           if (fa && fb) {
-            ha = trace_closest(sc, eo, da, kTmin, INFINITY);
-            hb = trace_closest(sc, eo, db, kTmin, INFINITY);
+            // both rays reach the faces: bounded queries decide each ray; only a ray whose
+            // face is hidden while the other's is seen needs its full closest hit
+            const int2 ev = __ldg(sc.edge_v + e);
+            ha = trace_closest(sc, eo, da, kTmin, tfa, tfa);
+            hb = trace_closest(sc, eo, db, kTmin, tfb, tfb);
+            const bool na = tri_has_edge(sc, ha.tri, ev), nb = tri_has_edge(sc, hb.tri, ev);
+            if (na && !nb) hb = trace_closest(sc, eo, db, kTmin, INFINITY);
+            else if (nb && !na) ha = trace_closest(sc, eo, da, kTmin, INFINITY);
           } else if (fa) {
             ha = trace_closest(sc, eo, da, kTmin, tfa, tfa);
             if (tri_has_edge(sc, ha.tri, __ldg(sc.edge_v + e))) hb = trace_closest(sc, eo, db, kTmin, INFINITY);
