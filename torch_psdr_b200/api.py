@@ -727,6 +727,14 @@ class BatchRender:
     meshes and lights whose vertices require grad when the batch is created (keep
     that when swapping buffers with `Mesh.set_vertices`). Extension: the reference has
     no batching.
+
+    Inside each graph the job's independent parts (the forward's tiles; the backward's
+    interior tiles and every boundary term of every view) run on the integrator's
+    `batch_lanes` concurrent streams, each with its own workspace, and with
+    `batch_records` the forward keeps every interior path's replay record so that the
+    backward runs the adjoint without re-tracing. Images and gradients are bitwise the
+    same as those of `PathIntegrator.renderD` on the same job; the memory cost is one
+    workspace per lane plus, with kept records, 16 B x (1 + D R + 2 D) + 8 B per path.
     """
 
     def __init__(self, integrator: PathIntegrator, scenes: List[Scene], differentiable: bool = True):
