@@ -732,9 +732,12 @@ class BatchRender:
     interior tiles and every boundary term of every view) run on the integrator's
     `batch_lanes` concurrent streams, each with its own workspace, and with
     `batch_records` the forward keeps every interior path's replay record so that the
-    backward runs the adjoint without re-tracing. Images and gradients are bitwise the
-    same as those of `PathIntegrator.renderD` on the same job; the memory cost is one
-    workspace per lane plus, with kept records, 16 B x (1 + D R + 2 D) + 8 B per path.
+    backward runs the adjoint without re-tracing. Neither changes a bit of the images or
+    gradients. Against `PathIntegrator.renderD` of each scene alone the images are equal
+    and the gradients agree to float rounding (the batch packs all scenes' paths into
+    shared tiles, which changes the per-thread sums of the light and camera gradients).
+    The memory cost is one workspace per lane plus, with kept records,
+    16 B x (1 + D R + 2 D) + 8 B per path (D = max_bounce, R = light + BSDF samples + 1).
     """
 
     def __init__(self, integrator: PathIntegrator, scenes: List[Scene], differentiable: bool = True):
